@@ -1,0 +1,205 @@
+"""Initial conditions and advector fields of the reference's test problems and
+of the synthetic benchmark workloads.
+
+Arrays are returned in the reference's accessor conventions:
+  advectee(e)  -> shape grid, index (i, j, k) = cell
+  advector(d)  -> view with lower bound (-1, 0, 0): shape grid for d = 0 and
+                  (n0 + 1, n1, n2) for d >= 1; view element (a, b, c) holds the
+                  value the reference computes at view index (a - 1, b, c)
+                  (libmpdata++/concurr/detail/sharedmem.hpp:431-456, 543-577)
+Expressions follow the reference's operand order so that FP64 inputs are
+bit-identical to what its Blitz++ expressions produce.
+"""
+import math
+
+import numpy as np
+
+from . import opts as o
+
+
+def _view_idx(shape):
+    """Index grids of an advector view: first axis starts at -1."""
+    g = list(np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij"))
+    g[0] = g[0] - 1.0
+    return g
+
+
+# --- tests/paper_2015_GMD/1_advscheme_opts/advscheme_opts.cpp:24-56 -----------
+def advscheme_opts(nx=601):
+    i = np.arange(nx)
+    box = (i <= 75) | (i >= 125)
+    psi0 = np.where(box, 2.0, 4.0)
+    psi1 = np.where(box, -1.0, 1.0)
+    return {"grid": (nx,), "bcs": ["cyclic"] * 2, "advectee": [psi0, psi1],
+            "advector": [np.full((nx,), -0.75)], "nt": 1200, "n_iters": 2}
+
+
+ADVSCHEME_CASES = {"abs": o.abs, "iga": o.iga, "iga_tot": o.iga | o.tot, "iga_fct": o.iga | o.fct,
+                   "iga_tot_fct": o.iga | o.tot | o.fct}
+
+
+# --- tests/paper_2015_GMD/0_basic_example/basic_example.cpp:10-50 -------------
+def basic_example(nx=101, dx=0.1):
+    i = np.arange(nx, dtype=np.float64)
+    psi = -.5 + 1 / ((dx * (i - (nx - 1) / 2.)) ** 2 + 1)
+    return {"grid": (nx,), "bcs": ["open"] * 2, "advectee": [psi], "advector": [np.full((nx,), .5)],
+            "nt": 100, "outfreq": 20, "opts": o.iga | o.fct, "n_iters": 2}
+
+
+# --- tests/paper_2015_GMD/3_rotating_cone_2d/rotating_cone_2d.cpp:32-138 ------
+def rotating_cone(nx=101, ny=101):
+    dt, dx, dy, omega, h, h0 = .1, 1., 1., .1, 4., 1.
+    r, x0, y0 = 15. * dx, 50 * dx, 75 * dy
+    xc, yc = .5 * (nx - 1) * dx, .5 * (ny - 1) * dy
+    i, j = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(ny, dtype=np.float64), indexing="ij")
+    tmp = (i * dx - x0) ** 2 + (j * dy - y0) ** 2
+    psi = h0 + np.where(tmp - r ** 2 <= 0, h - np.sqrt(tmp / (r / h) ** 2), 0.)
+    vi, vj = _view_idx((nx, ny))
+    gx = omega * (vj * dy - yc) * dt / dx
+    vi, vj = _view_idx((nx + 1, ny))
+    gy = -omega * (vi * dx - xc) * dt / dy
+    return {"grid": (nx, ny), "bcs": ["open"] * 4, "advectee": [psi], "advector": [gx, gy], "nt": 628 * 6,
+            "dt": dt}
+
+
+CONE_CASES = {"basic": (0, 2), "fct": (o.fct, 2), "iga_fct": (o.iga | o.fct, 2)}
+
+
+def cone_stats(psi_init, psi_final, nt, dt):
+    """rotating_cone_stats.hpp:52-67"""
+    err2 = (psi_init - psi_final) ** 2
+    rms = math.sqrt(err2.sum() / psi_init.shape[0] / psi_init.shape[1]) / nt / dt
+    return {"min(psi)": float(psi_final.min()), "max(psi)": float(psi_final.max()), "rms error": rms}
+
+
+# --- tests/paper_2015_GMD/4_revolving_sphere_3d/revolving_sphere_3d.cpp:29-100 -
+def revolving_sphere(nx=59):
+    dt = 0.018 * 2 * math.pi
+    L = 100.
+    dx = L / (nx - 1)
+    dy = dz = dx
+    h, r = 4., 15.
+    d = 25 / math.sqrt(3)
+    x0, y0, z0 = 50 - d, 50 + d, 50 + d
+    i, j, k = np.meshgrid(*[np.arange(nx, dtype=np.float64)] * 3, indexing="ij")
+    tmp = (i * dx - x0) ** 2 + (j * dx - y0) ** 2 + (k * dx - z0) ** 2
+    psi = np.where(tmp - r ** 2 <= 0, h, 0.)
+    omega, xc, yc, zc = 0.1, 50., 50., 50.
+    w = omega / math.sqrt(3)
+    vi, vj, vk = _view_idx((nx, nx, nx))
+    gx = w * (-(vj * dy - yc) + (vk * dz - zc)) * dt / dx
+    vi, vj, vk = _view_idx((nx + 1, nx, nx))
+    gy = w * ((vi * dx - xc) - (vk * dz - zc)) * dt / dy
+    gz = w * (-(vi * dx - xc) + (vj * dy - yc)) * dt / dz
+    return {"grid": (nx, nx, nx), "bcs": ["open"] * 6, "advectee": [psi], "advector": [gx, gy, gz],
+            "nt": 556, "dt": dt}
+
+
+SPHERE_CASES = {"upwind": (0, 1), "basic": (0, 2), "iga": (o.iga, 2), "fct": (o.fct, 2),
+                "iga_fct": (o.iga | o.fct, 2)}
+
+
+def sphere_stats(ic, fc, nt, dt):
+    """revolving_sphere_stats.hpp:46-64"""
+    n3 = float(ic.shape[0]) ** 3
+    dif = fc - ic
+    return {"max(solution)": float(fc.max()), "min(solution)": float(fc.min()),
+            "Linf": float(np.abs(dif).max()),
+            "L2": 1.0 / (nt * dt) * math.sqrt(1.0 / n3 * float((dif ** 2).sum())),
+            "L1": 1.0 / (nt * dt) * (1.0 / n3 * float(np.abs(dif).sum()))}
+
+
+# --- tests/unit/cone_bugs/test_issue.cpp: FP32 fct, exact background ----------
+def cone_bugs():
+    nx, ny = 15, 14
+    dx = dy = 1.
+    h, h0, r, x0, y0 = 4., 1., 12. * dx, 1., 0.
+    i, j = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(ny, dtype=np.float64), indexing="ij")
+    a = ((i * dx - x0) ** 2 + (j * dy - y0) ** 2).astype(np.float32).astype(np.float64)
+    psi = h0 + np.where(a - r ** 2 <= 0, h * (1 - a / r ** 2) ** 2, 0.)
+    return {"grid": (nx, ny), "bcs": ["cyclic"] * 4, "advectee": [psi.astype(np.float32).astype(np.float64)],
+            "advector": [np.full((nx, ny), .3), np.full((nx + 1, ny), .3)], "nt": 2, "opts": o.fct,
+            "n_iters": 2}
+
+
+# --- synthetic periodic workloads (duplicated-endpoint convention: x[n-1] == x[0]) ---
+
+def periodic_curl_2d(nx, ny, seed, n_modes=8, cmax=0.5, dtype=np.float64):
+    """Divergence-free 2D Courant field from a streamfunction of random Fourier
+    modes on the (nx-1) x (ny-1) periodic torus: GC_x = dPsi/dy, GC_y = -dPsi/dx
+    taken as differences of Psi at cell corners, so the discrete divergence of
+    the returned faces vanishes up to rounding.  Returns (gx, gy) in advector
+    view layout."""
+    rng = np.random.default_rng(seed)
+    Px, Py = nx - 1, ny - 1
+    # corner values Psi(I, J) at corner (I - 1/2, J - 1/2), periodic in (Px, Py)
+    I, J = np.meshgrid(np.arange(Px, dtype=np.float64), np.arange(Py, dtype=np.float64), indexing="ij")
+    psi = np.zeros((Px, Py))
+    for _ in range(n_modes):
+        kx, ky = rng.integers(1, 5, size=2)
+        amp = rng.normal()
+        ph = rng.uniform(0, 2 * math.pi)
+        psi += amp * np.cos(2 * math.pi * (kx * I / Px + ky * J / Py) + ph)
+    # face (i+1/2, j) between corners (i+1/2, j-1/2) and (i+1/2, j+1/2): GC_x = Psi(i+1, j+1) - Psi(i+1, j)
+    gxu = np.roll(np.roll(psi, -1, 0), -1, 1) - np.roll(psi, -1, 0)     # (Px, Py), index (i, j) -> face i+1/2
+    # face (i, j+1/2): GC_y = -(Psi(i+1, j+1) - Psi(i, j+1))
+    gyu = -(np.roll(np.roll(psi, -1, 0), -1, 1) - np.roll(psi, -1, 1))  # (Px, Py), index (i, j) -> face j+1/2
+    s = cmax / max(np.abs(gxu).max(), np.abs(gyu).max())
+    gxu *= s
+    gyu *= s
+    gxu = gxu.astype(dtype).astype(np.float64)
+    gyu = gyu.astype(dtype).astype(np.float64)
+    # x view: element (a, b) = face (a - 1 + 1/2, b) over a in [0, nx-1], b in [0, ny-1]
+    a = (np.arange(nx) - 1) % Px
+    b = np.arange(ny) % Py
+    gx = gxu[np.ix_(a, b)]
+    # y view: element (a, b) = GC_y at x = a - 1, face b - 1 + 1/2 (view index b <-> face b - 1/2)
+    a = (np.arange(nx + 1) - 1) % Px
+    b = (np.arange(ny) - 1) % Py
+    gy = gyu[np.ix_(a, b)]
+    return gx, gy
+
+
+def periodic_curl_3d(n, seed, n_modes=8, cmax=0.4, dtype=np.float32):
+    """Divergence-free 3D Courant field: discrete curl of a vector potential A
+    (3 components of random Fourier modes periodic on (n-1)^3, integer
+    wave-vectors in [1, 4]^3, N(0,1) amplitudes, U[0, 2pi) phases), computed in
+    FP64 on cell edges so that the face fluxes have zero discrete divergence.
+    Returns (gx, gy, gz) in advector view layout."""
+    rng = np.random.default_rng(seed)
+    P = n - 1
+    idx = np.arange(P, dtype=np.float64)
+    I, J, K = np.meshgrid(idx, idx, idx, indexing="ij")
+    A = []
+    for _c in range(3):
+        a = np.zeros((P, P, P))
+        for _ in range(n_modes):
+            kv = rng.integers(1, 5, size=3)
+            amp = rng.normal()
+            ph = rng.uniform(0, 2 * math.pi)
+            a += amp * np.cos(2 * math.pi * (kv[0] * I + kv[1] * J + kv[2] * K) / P + ph)
+        A.append(a)
+    Ax, Ay, Az = A
+    r = lambda x, ax: np.roll(x, -1, ax)
+    # Ax on x-edges (i+1/2, j-1/2, k-1/2) etc.; face flux = circulation around the face
+    fx = (r(Az, 1) - Az) - (r(Ay, 2) - Ay)        # face (i+1/2, j, k) stored at (i, j, k) after shift below
+    fy = (r(Ax, 2) - Ax) - (r(Az, 0) - Az)
+    fz = (r(Ay, 0) - Ay) - (r(Ax, 1) - Ax)
+    s = cmax / max(np.abs(fx).max(), np.abs(fy).max(), np.abs(fz).max())
+    fx, fy, fz = [(f * s).astype(dtype).astype(np.float64) for f in (fx, fy, fz)]
+    a0 = (np.arange(n) - 1) % P
+    a1 = (np.arange(n + 1) - 1) % P
+    b = np.arange(n) % P
+    bm = (np.arange(n) - 1) % P
+    gx = fx[np.ix_(a0, b, b)]
+    gy = fy[np.ix_(a1, bm, b)]
+    gz = fz[np.ix_(a1, b, bm)]
+    return gx, gy, gz
+
+
+def wrap_periodic(u):
+    """Apply the duplicated-endpoint convention to a field defined on the
+    (n-1)^d unique cells: returns the n^d array with x[n-1] = x[0] per axis."""
+    for ax in range(u.ndim):
+        u = np.concatenate([u, np.take(u, [0], axis=ax)], axis=ax)
+    return u

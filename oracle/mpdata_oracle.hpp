@@ -1,0 +1,619 @@
+// ORACLE -- test infrastructure only.
+//
+// A plain C++17 CPU restatement of libmpdata++'s MPDATA advection step
+// (donor-cell flux, antidiffusive corrective iterations, FCT limiter), of its
+// halo fills for cyclic/open boundaries and of its time loop.  It exists to
+// check the CUDA product path: only tests/, __graft_entry__.smoke() and the
+// cpu_baseline leg of bench.py load it, and only as the checker.  Nothing in
+// the shipped library calls it.
+//
+// Every function follows the reference's evaluation order (parenthesisation,
+// loop ranges, halo-fill order) so that an IEEE build (-O2 -ffp-contract=off)
+// reproduces the reference's FP64 arithmetic.  Arrays are NaN-filled at
+// allocation (as the reference's debug builds do, libmpdata++/blitz.hpp:107-112)
+// so that any read of a halo cell that the reference never fills shows up.
+//
+// Parity pinned against the reference's own golden data (tests/golden/*):
+// 1D advscheme_opts field dumps, 2D rotating-cone stats, 3D revolving-sphere
+// stats (see tests/test_oracle_golden.py).
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace mpdx_oracle {
+
+// option bits -- same values as libmpdata++/opts.hpp:34-49
+enum : unsigned {
+  o_fct = 1u << 0, o_abs = 1u << 1, o_tot = 1u << 2, o_pfc = 1u << 3,
+  o_npa = 1u << 4, o_iga = 1u << 5, o_nug = 1u << 6, o_dfl = 1u << 7,
+  o_khn = 1u << 8
+};
+enum { bc_cyclic = 0, bc_open = 1, bc_rigid = 2 };
+
+struct rng { int f, l; };
+// r^n (libmpdata++/formulae/arakawa_c.hpp:41-49)
+inline rng ext(rng r, int n) { return {r.f - n, r.l + n}; }
+// r^h: (r-h).first() .. (r+h).last()
+inline rng exh(rng r) { return {r.f - 1, r.l}; }
+
+template <class T>
+struct arr {
+  std::vector<T> v;
+  int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  long s0 = 1, s1 = 1;
+  void alloc(rng r0, rng r1, rng r2) {
+    lo[0] = r0.f; lo[1] = r1.f; lo[2] = r2.f;
+    hi[0] = r0.l; hi[1] = r1.l; hi[2] = r2.l;
+    s1 = r2.l - r2.f + 1;
+    s0 = s1 * (r1.l - r1.f + 1);
+    v.assign(size_t(s0) * size_t(r0.l - r0.f + 1), std::numeric_limits<T>::quiet_NaN());
+  }
+  inline T &operator()(int i, int j, int k) {
+    return v[size_t((i - lo[0]) * s0 + (j - lo[1]) * s1 + (k - lo[2]))];
+  }
+  inline const T &operator()(int i, int j, int k) const {
+    return v[size_t((i - lo[0]) * s0 + (j - lo[1]) * s1 + (k - lo[2]))];
+  }
+  bool has(int i, int j, int k) const {
+    return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+  }
+};
+template <class T> using vctr = std::array<arr<T>, 3>;
+
+// index permutation pi<d> (libmpdata++/formulae/idxperm.hpp:15-71): frame
+// coordinates (a along d, b along d+1, c along d+2) -> (i, j, k)
+template <int ND, int D> struct pi;
+template <> struct pi<1, 0> { static inline void m(int a, int, int, int &i, int &j, int &k) { i = a; j = 0; k = 0; } };
+template <> struct pi<2, 0> { static inline void m(int a, int b, int, int &i, int &j, int &k) { i = a; j = b; k = 0; } };
+template <> struct pi<2, 1> { static inline void m(int a, int b, int, int &i, int &j, int &k) { i = b; j = a; k = 0; } };
+template <> struct pi<3, 0> { static inline void m(int a, int b, int c, int &i, int &j, int &k) { i = a; j = b; k = c; } };
+template <> struct pi<3, 1> { static inline void m(int a, int b, int c, int &i, int &j, int &k) { i = c; j = a; k = b; } };
+template <> struct pi<3, 2> { static inline void m(int a, int b, int c, int &i, int &j, int &k) { i = b; j = c; k = a; } };
+
+template <int ND, int D, class T>
+inline T &P(arr<T> &A, int a, int b = 0, int c = 0) {
+  int i, j, k; pi<ND, D>::m(a, b, c, i, j, k); return A(i, j, k);
+}
+template <int ND, int D, class T>
+inline const T &P(const arr<T> &A, int a, int b = 0, int c = 0) {
+  int i, j, k; pi<ND, D>::m(a, b, c, i, j, k); return A(i, j, k);
+}
+
+// runtime-dimension variant used by halo fills
+inline void pim(int nd, int d, int a, int b, int c, int &i, int &j, int &k) {
+  if (nd == 1) { i = a; j = 0; k = 0; return; }
+  if (nd == 2) { if (d == 0) { i = a; j = b; } else { i = b; j = a; } k = 0; return; }
+  if (d == 0) { i = a; j = b; k = c; } else if (d == 1) { i = c; j = a; k = b; } else { i = b; j = c; k = a; }
+}
+template <class T> inline T &PR(arr<T> &A, int nd, int d, int a, int b, int c) {
+  int i, j, k; pim(nd, d, a, b, c, i, j, k); return A(i, j, k);
+}
+
+// pospart / negpart (libmpdata++/formulae/common.hpp:86-124); min/max follow
+// std::min/std::max as the scalar (ix_t=int) reference paths do
+template <class T> inline T pospart(unsigned o, T x) { return (o & o_npa) ? (x + std::abs(x)) / 2 : std::max(T(0), x); }
+template <class T> inline T negpart(unsigned o, T x) { return (o & o_npa) ? (x - std::abs(x)) / 2 : std::min(T(0), x); }
+
+// frac (formulae_mpdata_common.hpp:61-86) and fct_frac (:88-98)
+template <class T> inline T frac(unsigned o, T nom, T den) {
+  if (o & o_pfc) return den != 0 ? nom / den : T(0);
+  return nom / (den + std::numeric_limits<T>::min());
+}
+template <class T> inline T fct_frac(T nom, T den) { return nom / (den + std::numeric_limits<T>::epsilon()); }
+
+// donor-cell flux F (donorcell_formulae.hpp:25-34)
+template <class T> inline T Fdc(unsigned o, T psi_l, T psi_r, T C) {
+  return pospart(o, C) * psi_l + negpart(o, C) * psi_r;
+}
+
+template <class T>
+struct mpdata {
+  // configuration
+  int nd = 1, n[3] = {1, 1, 1}, H = 1, n_eqns = 1, n_iters = 2;
+  unsigned opts = o_iga | o_fct;
+  int bcs[3][2] = {{bc_cyclic, bc_cyclic}, {bc_cyclic, bc_cyclic}, {bc_cyclic, bc_cyclic}};
+  T max_abs_div_eps = std::numeric_limits<T>::epsilon();
+
+  // state
+  std::vector<std::array<arr<T>, 2>> psi;  // psi[e][tlev]
+  std::vector<int> tl;                     // per-eqn time level n[e] (mod 2)
+  vctr<T> GC, tmp0, tmp1, flux, GC_mono;
+  arr<T> psi_min, psi_max, beta_up, beta_dn;
+  long long timestep = 0;
+
+  rng ir[3];  // interior ranges
+  rng im[3];  // (i.first-1 .. i.last) -- mpdata_osc_*d.hpp ctor
+
+  static int mpdata_halo(unsigned o) { return (o & (o_tot | o_dfl)) ? 2 : 1; }  // formulae_mpdata_common.hpp:50-59
+
+  void setup(int nd_, const int *n_, int n_eqns_, unsigned opts_, int n_iters_, const int *bcs_) {
+    nd = nd_; n_eqns = n_eqns_; opts = opts_; n_iters = n_iters_;
+    if (n_iters < 1) throw std::runtime_error("n_iters must be positive");
+    for (int d = 0; d < 3; ++d) n[d] = d < nd ? n_[d] : 1;
+    for (int d = 0; d < nd; ++d) if (n[d] < 1) throw std::runtime_error("libmpdata++: bogus grid size");
+    for (int d = 0; d < nd; ++d) for (int s = 0; s < 2; ++s) bcs[d][s] = bcs_[2 * d + s];
+    H = mpdata_halo(opts);
+    if (opts & o_fct) H = std::max(H, 2);  // fct_min_halo (mpdata_fct_common.hpp:15)
+    for (int d = 0; d < 3; ++d) {
+      ir[d] = {0, n[d] - 1};
+      im[d] = d < nd ? rng{-1, n[d] - 1} : rng{0, 0};
+    }
+    psi.assign(n_eqns, {});
+    tl.assign(n_eqns, 0);
+    for (auto &p : psi) for (auto &a : p) alloc_sclr(a);
+    alloc_vctr(GC); alloc_vctr(tmp0); alloc_vctr(flux);
+    if (n_iters > 2) alloc_vctr(tmp1);  // n_tmp (mpdata_common.hpp:67-70)
+    if (opts & o_fct) {
+      alloc_sclr(psi_min); alloc_sclr(psi_max); alloc_sclr(beta_up); alloc_sclr(beta_dn);
+      alloc_vctr(GC_mono);
+    }
+  }
+
+  rng sr(int d) const { return d < nd ? ext(ir[d], H) : rng{0, 0}; }     // rng_sclr
+  // threads pay off only on large grids; loops are elementwise, so results do not depend on it
+  bool big() const { return long(n[0]) * n[1] * n[2] >= (1L << 17); }
+  void alloc_sclr(arr<T> &a) { a.alloc(sr(0), sr(1), sr(2)); }
+  void alloc_vctr(vctr<T> &v) {  // rng_vctr along its own axis: i^h^(halo-1)
+    for (int c = 0; c < nd; ++c) {
+      rng r[3] = {sr(0), sr(1), sr(2)};
+      r[c] = ext(exh(ir[c]), H - 1);
+      v[c].alloc(r[0], r[1], r[2]);
+    }
+  }
+
+  // ---- bcond ranges (bcond_common.hpp:225-275) ----
+  rng left_halo_sclr(int d) const { return {-H, -1}; }
+  rng rght_halo_sclr(int d) const { return {n[d], n[d] + H - 1}; }
+  rng left_intr_sclr(int d) const { return {1, H}; }
+  rng rght_intr_sclr(int d) const { return {n[d] - 1 - H, n[d] - 2}; }
+  rng left_halo_vctr(int d) const { return {-H, -1}; }
+  rng rght_halo_vctr(int d) const { return {n[d] - 1, n[d] + H - 2}; }
+  rng left_intr_vctr(int d) const { return {0, H - 1}; }
+  rng rght_intr_vctr(int d) const { return {n[d] - 1 - H, n[d] - 2}; }
+
+  // loops over the two transverse frame ranges (b along d+1, c along d+2)
+  template <class F> void each(rng rb, rng rc, F f) {
+    if (nd == 1) { f(0, 0); return; }
+    if (nd == 2) { for (int b = rb.f; b <= rb.l; ++b) f(b, 0); return; }
+    for (int b = rb.f; b <= rb.l; ++b) for (int c = rc.f; c <= rc.l; ++c) f(b, c);
+  }
+
+  // ---- halo fills: cyclic_{1,2,3}d.hpp, open_{1,2,3}d.hpp ----
+  void fill_sclr(int d, int side, arr<T> &A, rng rb, rng rc, bool deriv = false) {
+    const int kind = bcs[d][side];
+    each(rb, rc, [&](int b, int c) {
+      if (kind == bc_cyclic) {
+        if (side == 0) { rng h = left_halo_sclr(d), s = rght_intr_sclr(d);
+          for (int t = 0; t <= h.l - h.f; ++t) PR(A, nd, d, h.f + t, b, c) = PR(A, nd, d, s.f + t, b, c); }
+        else { rng h = rght_halo_sclr(d), s = left_intr_sclr(d);
+          for (int t = 0; t <= h.l - h.f; ++t) PR(A, nd, d, h.f + t, b, c) = PR(A, nd, d, s.f + t, b, c); }
+      } else if (kind == bc_open) {
+        rng h = side == 0 ? left_halo_sclr(d) : rght_halo_sclr(d);
+        int e = side == 0 ? 0 : n[d] - 1;
+        for (int i = h.f; i <= h.l; ++i) PR(A, nd, d, i, b, c) = deriv ? T(0) : PR(A, nd, d, e, b, c);
+      } else throw std::runtime_error("oracle: bcond kind not supported for scalars");
+    });
+  }
+  void fill_vctr_nrml(int d, int side, arr<T> &A, rng rb, rng rc) {
+    const int kind = bcs[d][side];
+    if (kind == bc_cyclic) { fill_sclr(d, side, A, rb, rc); return; }
+    if (kind == bc_open) {
+      rng h = side == 0 ? left_halo_sclr(d) : rght_halo_sclr(d);
+      each(rb, rc, [&](int b, int c) { for (int i = h.f; i <= h.l; ++i) PR(A, nd, d, i, b, c) = T(0); });
+      return;
+    }
+    throw std::runtime_error("oracle: bcond kind not supported for vectors");
+  }
+  void fill_vctr_alng(int d, int side, vctr<T> &AV, rng rb, rng rc, bool ad, bool cyclic_only = false) {
+    const int kind = bcs[d][side];
+    if (kind == bc_cyclic) {
+      each(rb, rc, [&](int b, int c) {
+        if (side == 0) { rng h = left_halo_vctr(d), s = rght_intr_vctr(d);
+          for (int t = 0; t <= h.l - h.f; ++t) PR(AV[d], nd, d, h.f + t, b, c) = PR(AV[d], nd, d, s.f + t, b, c); }
+        else { rng h = rght_halo_vctr(d), s = left_intr_vctr(d);
+          for (int t = 0; t <= h.l - h.f; ++t) PR(AV[d], nd, d, h.f + t, b, c) = PR(AV[d], nd, d, s.f + t, b, c); }
+      });
+      return;
+    }
+    if (cyclic_only) return;  // fill_halos_vctr_alng_cyclic is a no-op for non-cyclic bconds
+    if (kind != bc_open) throw std::runtime_error("oracle: bcond kind not supported for vectors");
+    if (nd == 1) {  // open_1d.hpp:36-40, 66-70
+      if (side == 0) { rng h = left_halo_vctr(0); T v = AV[0](left_intr_vctr(0).f, 0, 0);
+        for (int i = h.f; i <= h.l - (ad ? 1 : 0); ++i) AV[0](i, 0, 0) = v; }
+      else { rng h = rght_halo_vctr(0); T v = AV[0](rght_intr_vctr(0).f, 0, 0);
+        for (int i = h.f + (ad ? 1 : 0); i <= h.l; ++i) AV[0](i, 0, 0) = v; }
+      return;
+    }
+    const int e = side == 0 ? 0 : n[d] - 1;
+    const int d1 = (d + 1) % nd, d2 = (d + 2) % nd;
+    if (nd == 2) {  // open_2d.hpp:71-91 (left), 167-186 (right)
+      if (d == 0) { PR(AV[d1], nd, d, e, rb.f - 1, 0) = T(0); PR(AV[d1], nd, d, e, rb.l, 0) = T(0); }
+      rng h = side == 0 ? left_halo_vctr(d) : rght_halo_vctr(d);
+      int f = side == 0 ? h.f : h.f + (ad ? 1 : 0);
+      int l = side == 0 ? h.l - (ad ? 1 : 0) : h.l;
+      for (int ii = f; ii <= l; ++ii)
+        for (int b = rb.f; b <= rb.l; ++b) {
+          if (side == 0)
+            PR(AV[d], nd, d, ii, b, 0) = PR(AV[d], nd, d, e, b, 0) - (PR(AV[d1], nd, d, e, b - 1, 0) - PR(AV[d1], nd, d, e, b, 0));
+          else
+            PR(AV[d], nd, d, ii, b, 0) = PR(AV[d], nd, d, e - 1, b, 0) + (PR(AV[d1], nd, d, e, b - 1, 0) - PR(AV[d1], nd, d, e, b, 0));
+        }
+      return;
+    }
+    // nd == 3: open_3d.hpp:66-125 (left), 197-243 (right)
+    if (d == 0) {
+      for (int b = rb.f; b <= rb.l; ++b) { PR(AV[d2], nd, d, e, b, rc.f - 1) = T(0); PR(AV[d2], nd, d, e, b, rc.l) = T(0); }
+      for (int c = rc.f; c <= rc.l; ++c) { PR(AV[d1], nd, d, e, rb.f - 1, c) = T(0); PR(AV[d1], nd, d, e, rb.l, c) = T(0); }
+    } else if (d == 1) {
+      for (int c = rc.f; c <= rc.l; ++c) { PR(AV[d1], nd, d, e, rb.f - 1, c) = T(0); PR(AV[d1], nd, d, e, rb.l, c) = T(0); }
+    }
+    rng h = side == 0 ? left_halo_vctr(d) : rght_halo_vctr(d);
+    int f = side == 0 ? h.f : h.f + (ad ? 1 : 0);
+    int l = side == 0 ? h.l - (ad ? 1 : 0) : h.l;
+    for (int ii = f; ii <= l; ++ii)
+      for (int b = rb.f; b <= rb.l; ++b)
+        for (int c = rc.f; c <= rc.l; ++c) {
+          if (side == 0)
+            PR(AV[d], nd, d, ii, b, c) = PR(AV[d], nd, d, e, b, c)
+              - (PR(AV[d1], nd, d, e, b - 1, c) - PR(AV[d1], nd, d, e, b, c))
+              - (PR(AV[d2], nd, d, e, b, c - 1) - PR(AV[d2], nd, d, e, b, c));
+          else
+            PR(AV[d], nd, d, ii, b, c) = PR(AV[d], nd, d, e - 1, b, c)
+              + (PR(AV[d1], nd, d, e, b - 1, c) - PR(AV[d1], nd, d, e, b, c))
+              + (PR(AV[d2], nd, d, e, b, c - 1) - PR(AV[d2], nd, d, e, b, c));
+        }
+  }
+
+  // ---- exchange orchestration: solver_{1,2,3}d.hpp ----
+  void xchng_sclr(arr<T> &A, int ex, bool deriv = false) {
+    if (nd == 1) { for (int s = 0; s < 2; ++s) fill_sclr(0, s, A, {0, 0}, {0, 0}, deriv); return; }
+    if (nd == 2) {  // solver_2d.hpp:40-56
+      for (int s = 0; s < 2; ++s) fill_sclr(0, s, A, ext(ir[1], ex), {0, 0}, deriv);
+      for (int s = 0; s < 2; ++s) fill_sclr(1, s, A, ext(ir[0], ex), {0, 0}, deriv);
+      return;
+    }
+    // solver_3d.hpp:47-67
+    for (int s = 0; s < 2; ++s) fill_sclr(1, s, A, ext(ir[2], ex), ext(ir[0], ex), deriv);
+    for (int s = 0; s < 2; ++s) fill_sclr(0, s, A, ext(ir[1], ex), ext(ir[2], ex), deriv);
+    for (int s = 0; s < 2; ++s) fill_sclr(2, s, A, ext(ir[0], ex), ext(ir[1], ex), deriv);
+  }
+  void xchng(int e) { xchng_sclr(psi[e][tl[e]], H); }
+  void xchng_vctr_alng(vctr<T> &AV, bool ad = false, bool cyclic = false) {
+    if (nd == 1) { for (int s = 0; s < 2; ++s) fill_vctr_alng(0, s, AV, {0, 0}, {0, 0}, ad, cyclic); return; }
+    if (nd == 2) {  // solver_2d.hpp:63-88
+      for (int s = 0; s < 2; ++s) fill_vctr_alng(0, s, AV, ir[1], {0, 0}, ad, cyclic);
+      for (int s = 0; s < 2; ++s) fill_vctr_alng(1, s, AV, ir[0], {0, 0}, ad, cyclic);
+      return;
+    }
+    // solver_3d.hpp:73-103
+    for (int s = 0; s < 2; ++s) fill_vctr_alng(0, s, AV, ir[1], ir[2], ad, cyclic);
+    for (int s = 0; s < 2; ++s) fill_vctr_alng(1, s, AV, ir[2], ir[0], ad, cyclic);
+    for (int s = 0; s < 2; ++s) fill_vctr_alng(2, s, AV, ir[0], ir[1], ad, cyclic);
+  }
+  void xchng_vctr_nrml(vctr<T> &AV, int ex = 0) {
+    if (nd == 1) return;
+    if (nd == 2) {  // solver_2d.hpp:171-202
+      for (int s = 0; s < 2; ++s) fill_vctr_nrml(1, s, AV[0], exh(ext(ir[0], ex)), {0, 0});
+      for (int s = 0; s < 2; ++s) fill_vctr_nrml(0, s, AV[1], exh(ext(ir[1], ex)), {0, 0});
+      return;
+    }
+    // solver_3d.hpp:207-286
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(1, s, AV[0], ext(ext(ir[2], ex), 1), exh(ext(ir[0], ex)));
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(2, s, AV[0], exh(ext(ir[0], ex)), ext(ext(ir[1], ex), 1));
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(0, s, AV[1], exh(ext(ir[1], ex)), ext(ext(ir[2], ex), 1));
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(2, s, AV[1], ext(ext(ir[0], ex), 1), exh(ext(ir[1], ex)));
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(0, s, AV[2], ext(ext(ir[1], ex), 1), exh(ext(ir[2], ex)));
+    for (int s = 0; s < 2; ++s) fill_vctr_nrml(1, s, AV[2], exh(ext(ir[2], ex)), ext(ext(ir[0], ex), 1));
+  }
+
+  // ---- mpdata_common.hpp:40-60 ----
+  vctr<T> &GC_unco(int iter) { return iter == 1 ? GC : (iter % 2 ? tmp1 : tmp0); }
+  vctr<T> &GC_corr(int iter) { return iter % 2 ? tmp0 : tmp1; }
+  vctr<T> &GCit(int iter) {  // virtual GC(iter); fct override mpdata_fct_common.hpp:31-35
+    if (iter == 0) return GC;
+    if (opts & o_fct) return GC_mono;
+    return GC_corr(iter);
+  }
+  void cycle(int e) { tl[e] = (tl[e] + 1) % 2; }
+
+  // ---- psi-derivative helpers (formulae_mpdata_psi_{1,2,3}d.hpp) ----
+  // ndx_psi at (i+1/2): 1D :51-105, 2D :127-185, 3D :262-318
+  template <int ND, int D> T ndx(const arr<T> &p, int a, int b, int c) const {
+    const T p1 = P<ND, D>(p, a + 1, b, c), p0 = P<ND, D>(p, a, b, c);
+    if (opts & o_iga) {
+      if (ND == 3) return p1 - p0;
+      return T(2) * (p1 - p0) / T(2);
+    }
+    if (opts & o_abs) return T(2) * frac(opts, std::abs(p1) - std::abs(p0), std::abs(p1) + std::abs(p0));
+    return T(2) * frac(opts, p1 - p0, p1 + p0);
+  }
+  // ndy_psi at (i+1/2): 2D :188-240, 3D :321-392 (b is the +1 frame axis)
+  template <int ND, int D> T ndy(const arr<T> &p, int a, int b, int c) const {
+    T pa = P<ND, D>(p, a + 1, b + 1, c), pb = P<ND, D>(p, a, b + 1, c);
+    T pc = P<ND, D>(p, a + 1, b - 1, c), pd = P<ND, D>(p, a, b - 1, c);
+    if (opts & o_iga) return (pa + pb - pc - pd) / T(4);
+    if (opts & o_abs) { pa = std::abs(pa); pb = std::abs(pb); pc = std::abs(pc); pd = std::abs(pd); }
+    return frac(opts, pa + pb - pc - pd, pa + pb + pc + pd);
+  }
+  // ndz_psi at (i+1/2): 3D :395-466 (c is the +2 frame axis)
+  template <int ND, int D> T ndz(const arr<T> &p, int a, int b, int c) const {
+    T pa = P<ND, D>(p, a + 1, b, c + 1), pb = P<ND, D>(p, a, b, c + 1);
+    T pc = P<ND, D>(p, a + 1, b, c - 1), pd = P<ND, D>(p, a, b, c - 1);
+    if (opts & o_iga) return (pa + pb - pc - pd) / T(4);
+    if (opts & o_abs) { pa = std::abs(pa); pb = std::abs(pb); pc = std::abs(pc); pd = std::abs(pd); }
+    return frac(opts, pa + pb - pc - pd, pa + pb + pc + pd);
+  }
+  // 1D ndxx_psi (formulae_mpdata_psi_1d.hpp:110-161) and TOT (formulae_mpdata_hot_1d.hpp:19-52)
+  T ndxx1(const arr<T> &p, int i) const {
+    T a = p(i + 2, 0, 0), b = p(i + 1, 0, 0), c = p(i, 0, 0), d = p(i - 1, 0, 0);
+    if (opts & o_iga) return T(2) * (a - b - c + d) / T(4);
+    if (opts & o_abs) { a = std::abs(a); b = std::abs(b); c = std::abs(c); d = std::abs(d); }
+    return T(2) * frac(opts, a - b - c + d, a + b + c + d);
+  }
+  T tot1(const arr<T> &p, const arr<T> &G0, int i) const {
+    if (!(opts & o_tot)) return T(0);
+    const T C = G0(i, 0, 0);
+    const T coeff = (T(3) * C * std::abs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6);
+    return ndxx1(p, i) * coeff;
+  }
+
+  // ---- antidiffusive velocity ----
+  // 1D: formulae_mpdata_1d.hpp:186-210
+  void antidiff1(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
+    for (int i = im[0].f; i <= im[0].l; ++i) {
+      const T C = G[0](i, 0, 0);
+      T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<1, 0>(p, i, 0, 0);
+      r = r + tot1(p, G[0], i);
+      res(i, 0, 0) = r;
+    }
+  }
+  // 2D: formulae_mpdata_2d.hpp:242-278 with GC1_bar_xy (formulae_mpdata_gc_2d.hpp:76-90)
+  template <int D> void antidiff2(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
+    const arr<T> &Gd = G[D], &Gt = G[(D + 1) % 2];
+    const rng ra = im[D], rb = ir[(D + 1) % 2];
+    for (int a = ra.f; a <= ra.l; ++a)
+      for (int b = rb.f; b <= rb.l; ++b) {
+        const T C = P<2, D>(Gd, a, b);
+        const T gc1 = (P<2, D>(Gt, a + 1, b) + P<2, D>(Gt, a, b) + P<2, D>(Gt, a + 1, b - 1) + P<2, D>(Gt, a, b - 1)) / T(4);
+        P<2, D>(res, a, b) =
+            std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<2, D>(p, a, b, 0)
+            - C * gc1 / T(2) * ndy<2, D>(p, a, b, 0);
+      }
+  }
+  // 3D: formulae_mpdata_3d.hpp:254-295 with GC1_bar_xy / GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
+  template <int D> void antidiff3(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
+    const arr<T> &Gd = G[D], &G1 = G[(D + 1) % 3], &G2 = G[(D + 2) % 3];
+    const rng ra = im[D], rb = ir[(D + 1) % 3], rc = ir[(D + 2) % 3];
+#pragma omp parallel for schedule(static) if (big())
+    for (int a = ra.f; a <= ra.l; ++a)
+      for (int b = rb.f; b <= rb.l; ++b)
+        for (int c = rc.f; c <= rc.l; ++c) {
+          const T C = P<3, D>(Gd, a, b, c);
+          const T gc1 = (P<3, D>(G1, a + 1, b, c) + P<3, D>(G1, a, b, c) + P<3, D>(G1, a + 1, b - 1, c) + P<3, D>(G1, a, b - 1, c)) / T(4);
+          const T gc2 = (P<3, D>(G2, a + 1, b, c) + P<3, D>(G2, a, b, c) + P<3, D>(G2, a + 1, b, c - 1) + P<3, D>(G2, a, b, c - 1)) / T(4);
+          P<3, D>(res, a, b, c) =
+              std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<3, D>(p, a, b, c)
+              - C / T(2) * (gc1 * ndy<3, D>(p, a, b, c) + gc2 * ndz<3, D>(p, a, b, c)) / T(1);
+        }
+  }
+
+  // ---- donor-cell flux over faces ra (frame a) x rb x rc (make_flux, donorcell_formulae.hpp:36-79) ----
+  template <int ND, int D> void make_flux(arr<T> &F, const arr<T> &p, const arr<T> &C, rng ra, rng rb, rng rc) {
+#pragma omp parallel for schedule(static) if (big())
+    for (int a = ra.f; a <= ra.l; ++a)
+      for (int b = rb.f; b <= rb.l; ++b)
+        for (int c = rc.f; c <= rc.l; ++c)
+          P<ND, D>(F, a, b, c) = Fdc(opts, P<ND, D>(p, a, b, c), P<ND, D>(p, a + 1, b, c), P<ND, D>(C, a, b, c));
+  }
+  void fluxes(vctr<T> &F, const arr<T> &p, const vctr<T> &C, bool extended) {
+    // extended: ranges im^1 x j^1 x k^1 (fct_adjust_antidiff); else im x j x k
+    auto R = [&](int d) { return extended ? ext(ir[d], 1) : ir[d]; };
+    auto RM = [&](int d) { return extended ? ext(im[d], 1) : im[d]; };
+    if (nd == 1) make_flux<1, 0>(F[0], p, C[0], RM(0), {0, 0}, {0, 0});
+    else if (nd == 2) {
+      make_flux<2, 0>(F[0], p, C[0], RM(0), R(1), {0, 0});
+      make_flux<2, 1>(F[1], p, C[1], RM(1), R(0), {0, 0});
+    } else {
+      make_flux<3, 0>(F[0], p, C[0], RM(0), R(1), R(2));
+      make_flux<3, 1>(F[1], p, C[1], RM(1), R(2), R(0));
+      make_flux<3, 2>(F[2], p, C[2], RM(2), R(0), R(1));
+    }
+  }
+
+  // ---- donorcell_sum (donorcell_formulae.hpp:81-165), G = 1 ----
+  void donorcell_sum(arr<T> &pn, const arr<T> &po, const vctr<T> &f) {
+#pragma omp parallel for schedule(static) if (big())
+    for (int i = 0; i < n[0]; ++i)
+      for (int j = 0; j < n[1]; ++j)
+        for (int k = 0; k < n[2]; ++k) {
+          if (nd == 1)
+            pn(i, j, k) = po(i, j, k) + (-f[0](i, j, k) + f[0](i - 1, j, k)) / T(1);
+          else if (nd == 2)
+            pn(i, j, k) = po(i, j, k) + ((-f[0](i, j, k) + f[0](i - 1, j, k)) + (-f[1](i, j, k) + f[1](i, j - 1, k))) / T(1);
+          else
+            pn(i, j, k) = po(i, j, k) + ((-f[0](i, j, k) + f[0](i - 1, j, k)) + (-f[1](i, j, k) + f[1](i, j - 1, k))
+                                         + (-f[2](i, j, k) + f[2](i, j, k - 1))) / T(1);
+        }
+  }
+
+  // ---- FCT: fct_init (mpdata_fct_{1,2,3}d.hpp:31-55) ----
+  void fct_init(int e) {
+    const arr<T> &p = psi[e][tl[e]];
+    rng r0 = ext(ir[0], 1), r1 = nd > 1 ? ext(ir[1], 1) : rng{0, 0}, r2 = nd > 2 ? ext(ir[2], 1) : rng{0, 0};
+    for (int i = r0.f; i <= r0.l; ++i)
+      for (int j = r1.f; j <= r1.l; ++j)
+        for (int k = r2.f; k <= r2.l; ++k) {
+          T mn, mx;
+          if (nd == 1) {
+            mn = std::min(std::min(p(i - 1, 0, 0), p(i, 0, 0)), p(i + 1, 0, 0));
+            mx = std::max(std::max(p(i - 1, 0, 0), p(i, 0, 0)), p(i + 1, 0, 0));
+          } else if (nd == 2) {
+            mn = std::min(std::min(std::min(std::min(p(i, j + 1, 0), p(i - 1, j, 0)), p(i, j, 0)), p(i + 1, j, 0)), p(i, j - 1, 0));
+            mx = std::max(std::max(std::max(std::max(p(i, j + 1, 0), p(i - 1, j, 0)), p(i, j, 0)), p(i + 1, j, 0)), p(i, j - 1, 0));
+          } else {
+            mn = std::min(std::min(std::min(std::min(std::min(std::min(p(i, j, k), p(i + 1, j, k)), p(i - 1, j, k)), p(i, j + 1, k)), p(i, j - 1, k)), p(i, j, k + 1)), p(i, j, k - 1));
+            mx = std::max(std::max(std::max(std::max(std::max(std::max(p(i, j, k), p(i + 1, j, k)), p(i - 1, j, k)), p(i, j + 1, k)), p(i, j - 1, k)), p(i, j, k + 1)), p(i, j, k - 1));
+          }
+          psi_min(i, j, k) = mn;
+          psi_max(i, j, k) = mx;
+        }
+  }
+
+  // ---- beta_up / beta_dn (formulae_mpdata_fct_{1,2,3}d.hpp) over i^1 x j^1 x k^1 ----
+  void betas(const arr<T> &p, const vctr<T> &f) {
+    rng r0 = ext(ir[0], 1), r1 = nd > 1 ? ext(ir[1], 1) : rng{0, 0}, r2 = nd > 2 ? ext(ir[2], 1) : rng{0, 0};
+    const unsigned o = opts;
+#pragma omp parallel for schedule(static) if (big())
+    for (int i = r0.f; i <= r0.l; ++i)
+      for (int j = r1.f; j <= r1.l; ++j)
+        for (int k = r2.f; k <= r2.l; ++k) {
+          const T c = p(i, j, k);
+          T mx, mn, den_up, den_dn;
+          if (nd == 1) {
+            mx = std::max(psi_max(i, j, k), std::max(p(i - 1, j, k), std::max(c, p(i + 1, j, k))));
+            mn = std::min(psi_min(i, j, k), std::min(p(i - 1, j, k), std::min(c, p(i + 1, j, k))));
+            den_up = pospart(o, f[0](i - 1, j, k)) - negpart(o, f[0](i, j, k));
+            den_dn = pospart(o, f[0](i, j, k)) - negpart(o, f[0](i - 1, j, k));
+          } else if (nd == 2) {
+            // max(psi_max, psi(i,j+1), psi(i-1,j), psi(i,j), psi(i+1,j), psi(i,j-1)) as a right fold
+            mx = std::max(psi_max(i, j, k), std::max(p(i, j + 1, k), std::max(p(i - 1, j, k), std::max(c, std::max(p(i + 1, j, k), p(i, j - 1, k))))));
+            mn = std::min(psi_min(i, j, k), std::min(p(i, j + 1, k), std::min(p(i - 1, j, k), std::min(c, std::min(p(i + 1, j, k), p(i, j - 1, k))))));
+            den_up = (pospart(o, f[0](i - 1, j, k)) - negpart(o, f[0](i, j, k)))
+                   + (pospart(o, f[1](i, j - 1, k)) - negpart(o, f[1](i, j, k)));
+            den_dn = (pospart(o, f[0](i, j, k)) - negpart(o, f[0](i - 1, j, k)))
+                   + (pospart(o, f[1](i, j, k)) - negpart(o, f[1](i, j - 1, k)));
+          } else {
+            mx = std::max(psi_max(i, j, k), std::max(c, std::max(p(i + 1, j, k), std::max(p(i - 1, j, k),
+                   std::max(p(i, j + 1, k), std::max(p(i, j - 1, k), std::max(p(i, j, k + 1), p(i, j, k - 1))))))));
+            mn = std::min(psi_min(i, j, k), std::min(p(i, j + 1, k), std::min(p(i - 1, j, k), std::min(c,
+                   std::min(p(i + 1, j, k), std::min(p(i, j, k + 1), std::min(p(i, j, k - 1), p(i, j - 1, k))))))));
+            den_up = (pospart(o, f[0](i - 1, j, k)) - negpart(o, f[0](i, j, k)))
+                   + (pospart(o, f[1](i, j - 1, k)) - negpart(o, f[1](i, j, k)))
+                   + (pospart(o, f[2](i, j, k - 1)) - negpart(o, f[2](i, j, k)));
+            den_dn = (pospart(o, f[0](i, j, k)) - negpart(o, f[0](i - 1, j, k)))
+                   + (pospart(o, f[1](i, j, k)) - negpart(o, f[1](i, j - 1, k)))
+                   + (pospart(o, f[2](i, j, k)) - negpart(o, f[2](i, j, k - 1)));
+          }
+          beta_up(i, j, k) = fct_frac((mx - c) * T(1), den_up);
+          beta_dn(i, j, k) = fct_frac((c - mn) * T(1), den_dn);
+        }
+  }
+
+  // ---- GC_mono (formulae_mpdata_fct_{1,2,3}d.hpp) over im x j x k ----
+  template <int ND, int D> void gc_mono(arr<T> &out, const arr<T> &corr, const arr<T> &p) {
+    const rng ra = im[D];
+    const rng rb = ND > 1 ? ir[(D + 1) % ND] : rng{0, 0};
+    const rng rc = ND > 2 ? ir[(D + 2) % ND] : rng{0, 0};
+    const bool absv = (opts & o_abs) && !(opts & o_iga);
+#pragma omp parallel for schedule(static) if (big())
+    for (int a = ra.f; a <= ra.l; ++a)
+      for (int b = rb.f; b <= rb.l; ++b)
+        for (int c = rc.f; c <= rc.l; ++c) {
+          const T C = P<ND, D>(corr, a, b, c);
+          const T bd0 = P<ND, D>(beta_dn, a, b, c), bu1 = P<ND, D>(beta_up, a + 1, b, c);
+          const T bu0 = P<ND, D>(beta_up, a, b, c), bd1 = P<ND, D>(beta_dn, a + 1, b, c);
+          T lim;
+          if (!absv) lim = C > 0 ? std::min(T(1), std::min(bd0, bu1)) : std::min(T(1), std::min(bu0, bd1));
+          else if (C > 0) lim = P<ND, D>(p, a, b, c) > 0 ? std::min(T(1), std::min(bd0, bu1)) : std::min(T(1), std::min(bu0, bd1));
+          else lim = P<ND, D>(p, a + 1, b, c) > 0 ? std::min(T(1), std::min(bu0, bd1)) : std::min(T(1), std::min(bd0, bu1));
+          P<ND, D>(out, a, b, c) = C * lim;
+        }
+  }
+
+  // fct_adjust_antidiff (mpdata_fct_{1,2,3}d.hpp)
+  void fct_adjust_antidiff(int e, int iter) {
+    const arr<T> &p = psi[e][tl[e]];
+    vctr<T> &corr = GC_corr(iter);
+    xchng_vctr_alng(corr, true);
+    xchng_vctr_nrml(corr);
+    const vctr<T> *flx = &corr;
+    if (!(opts & o_iga)) { fluxes(flux, p, corr, true); flx = &flux; }
+    betas(p, *flx);
+    if (nd == 1) gc_mono<1, 0>(GC_mono[0], corr[0], p);
+    else if (nd == 2) { gc_mono<2, 0>(GC_mono[0], corr[0], p); gc_mono<2, 1>(GC_mono[1], corr[1], p); }
+    else { gc_mono<3, 0>(GC_mono[0], corr[0], p); gc_mono<3, 1>(GC_mono[1], corr[1], p); gc_mono<3, 2>(GC_mono[2], corr[2], p); }
+  }
+
+  // advop (mpdata_osc_{1,2,3}d.hpp)
+  void advop(int e) {
+    if (opts & o_fct) fct_init(e);
+    for (int iter = 0; iter < n_iters; ++iter) {
+      if (iter != 0) {
+        cycle(e);
+        xchng(e);
+        const arr<T> &p = psi[e][tl[e]];
+        vctr<T> &corr = GC_corr(iter), &unco = GC_unco(iter);
+        if (nd == 1) antidiff1(corr[0], p, unco);
+        else if (nd == 2) { antidiff2<0>(corr[0], p, unco); antidiff2<1>(corr[1], p, unco); }
+        else { antidiff3<0>(corr[0], p, unco); antidiff3<1>(corr[1], p, unco); antidiff3<2>(corr[2], p, unco); }
+        if (!(opts & o_fct) && iter != n_iters - 1) xchng_vctr_nrml(corr);
+        if (opts & o_fct) fct_adjust_antidiff(e, iter);
+      }
+      const arr<T> &p = psi[e][tl[e]];
+      const vctr<T> *flx = &flux;
+      if (!(opts & o_iga) || iter == 0) fluxes(flux, p, GCit(iter), false);
+      else flx = &GCit(iter);
+      donorcell_sum(psi[e][(tl[e] + 1) % 2], p, *flx);
+    }
+  }
+
+  T max_abs_vctr_div() {
+    T mx = 0;
+    for (int i = 0; i < n[0]; ++i)
+      for (int j = 0; j < n[1]; ++j)
+        for (int k = 0; k < n[2]; ++k) {
+          T v;
+          if (nd == 1) v = std::abs(GC[0](i, 0, 0) - GC[0](i - 1, 0, 0));
+          else if (nd == 2) v = std::abs((GC[0](i, j, 0) - GC[0](i - 1, j, 0)) + (GC[1](i, j, 0) - GC[1](i, j - 1, 0)));
+          else v = std::abs((GC[0](i, j, k) - GC[0](i - 1, j, k)) + (GC[1](i, j, k) - GC[1](i, j - 1, k)) + (GC[2](i, j, k) - GC[2](i, j, k - 1)));
+          mx = std::max(mx, v);
+        }
+    return mx;
+  }
+
+  // hook_ante_loop chain (solver_common.hpp:191-211, solver_2d.hpp:279-293, mpdata_osc_2d.hpp:40-67)
+  void ante_loop() {
+    xchng_vctr_alng(GC);
+    if (nd > 1 && !(opts & o_dfl)) {
+      if (max_abs_vctr_div() > max_abs_div_eps)
+        throw std::runtime_error("libmpdata++: initial advector field is divergent");
+    }
+    if (nd > 1) xchng_vctr_nrml(GC, H - 1);
+  }
+
+  // solver_common::solve (solver_common.hpp:270-358) with solve_loop_body (:127-136)
+  void advance(long long nt) {
+    nt += timestep;
+    if (timestep == 0) ante_loop();
+    while (timestep < nt) {
+      for (int e = 0; e < n_eqns; ++e) { xchng(e); advop(e); cycle(e); }
+      ++timestep;
+    }
+  }
+
+  // ---- accessors mirroring sharedmem::advectee()/advector() ----
+  // advectee(e): interior n0 x n1 x n2, C order
+  arr<T> &state(int e) { return psi[e][tl[e]]; }
+  // advector(d): view with lower bound (-1, 0, 0); view element (a, b, c) maps to
+  // GC[d](a-1, b-1*[d==1], c-1*[d==2]) (sharedmem.hpp:431-456, 543-577, 1D :356-372);
+  // extents: d=0 (n0, n1, n2); d>=1 (n0+1, n1, n2)
+  void advector_extent(int d, int ex[3]) const {
+    for (int q = 0; q < 3; ++q) ex[q] = n[q];
+    if (d > 0) ex[0] = n[0] + 1;
+  }
+  T &advector_at(int d, int a, int b, int c) {
+    int i = a - 1, j = b, k = c;
+    if (d == 1) j = b - 1;
+    if (d == 2) k = c - 1;
+    return GC[d](i, j, k);
+  }
+};
+
+}  // namespace mpdx_oracle

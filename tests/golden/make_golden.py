@@ -1,0 +1,132 @@
+"""Extract the reference's own golden data into small committed fixtures.
+
+Runs only where the libmpdata++ source tree is available (it reads the
+gzip'd refdata files of its test suite as text); the GPU host never runs it.
+Outputs, next to this script:
+
+  golden_stats.json   rotating-cone (2D) and revolving-sphere (3D) error stats,
+                      2D Boussinesq per-10-step stats (min/max theta, max |u|)
+  advscheme_opts.npz  1D field dumps of tests/paper_2015_GMD/1_advscheme_opts
+                      (601 cells, 5 option sets, t=0 and t=1200, 2 equations)
+  basic_example.npz   1D field dumps of tests/paper_2015_GMD/0_basic_example
+                      (101 cells, every 20 steps up to t=100)
+
+Usage:  python tests/golden/make_golden.py [path-to-libmpdataxx-checkout]
+"""
+import gzip
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def read_gz(path):
+    with gzip.open(path, "rt") as f:
+        return f.read()
+
+
+def parse_gnuplot_log(text):
+    """Split a gnuplot command stream into plots; each plot is a list of
+    inline datasets (lists of floats) terminated by 'e' lines."""
+    plots, cur, ds, name = [], None, None, None
+    for line in text.splitlines():
+        s = line.strip()
+        if s.startswith("set output"):
+            name = s.split("'")[1]
+        elif s.startswith("plot") or s.startswith("splot"):
+            cur = {"name": name, "data": []}
+            plots.append(cur)
+            ds = []
+        elif s == "e":
+            cur["data"].append(ds)
+            ds = []
+        elif cur is not None and s and re.match(r"^[-+0-9.eE ]+$", s):
+            ds.append([float(x) for x in s.split()])
+    return plots
+
+
+def stats_file(path):
+    out = {}
+    for line in read_gz(path).splitlines():
+        if "=" in line:
+            k, v = line.split("=", 1)
+            k = k.strip()
+            if k == "timestep":
+                ts = int(v)
+                out.setdefault("timesteps", []).append(ts)
+                continue
+            key = k if len(out.get("timesteps", [])) <= 1 else k
+            try:
+                val = float(v)
+            except ValueError:
+                continue
+            prefix = "t0" if len(out["timesteps"]) == 1 else "tN"
+            out[prefix + ":" + key] = val
+    return out
+
+
+def boussinesq_stats(path):
+    rows, cur = [], None
+    head = {}
+    for line in read_gz(path).splitlines():
+        if "=" not in line:
+            continue
+        k, v = [x.strip() for x in line.split("=", 1)]
+        if k == "timestep":
+            cur = {"timestep": int(v)}
+            rows.append(cur)
+        elif k.startswith("sum of initial perturbation squared"):
+            head["sum_init_pert_2"] = float(v)
+        elif k.startswith("sum of initial perturbation"):
+            head["sum_init_pert"] = float(v)
+        elif cur is not None:
+            try:
+                cur[k] = float(v)
+            except ValueError:
+                pass
+    rows = [r for r in rows if r["timestep"] > 0]
+    return {"header": head, "rows": rows}
+
+
+def main(ref):
+    gmd = os.path.join(ref, "tests", "paper_2015_GMD")
+    golden = {"source": "libmpdata++ tests/paper_2015_GMD refdata"}
+
+    cone = {}
+    for case in ["basic", "fct", "iters3_tot_fct", "iga_fct", "iga_tot_fct"]:
+        cone[case] = stats_file(os.path.join(gmd, "3_rotating_cone_2d", "refdata", f"stats_{case}_.txt.gz"))
+    golden["rotating_cone_2d"] = cone
+
+    sphere = {}
+    for case in ["upwind", "basic", "iga", "fct", "iga_fct"]:
+        sphere[case] = stats_file(os.path.join(gmd, "4_revolving_sphere_3d", "refdata", f"stats_{case}.txt.gz"))
+    golden["revolving_sphere_3d"] = sphere
+
+    golden["boussinesq_2d"] = boussinesq_stats(os.path.join(gmd, "8_boussinesq_2d", "refdata", "stats.txt.gz"))
+
+    with open(os.path.join(HERE, "golden_stats.json"), "w") as f:
+        json.dump(golden, f, indent=1, sort_keys=True)
+
+    plots = parse_gnuplot_log(read_gz(os.path.join(gmd, "1_advscheme_opts", "refdata", "log-orig.gz")))
+    arrs = {}
+    for p in plots:
+        tag = p["name"].replace("out_", "").replace(".svg", "")
+        data = np.array([[v[0] for v in ds] for ds in p["data"]], dtype=np.float64)
+        arrs[tag] = data  # 4 datasets x 601 values
+    np.savez_compressed(os.path.join(HERE, "advscheme_opts.npz"), **arrs)
+
+    plots = parse_gnuplot_log(read_gz(os.path.join(gmd, "0_basic_example", "refdata", "log-orig.gz")))
+    # 1D splot output repeats every value twice to emulate histeps
+    # (libmpdata++/output/gnuplot.hpp:167-175); keep one copy per cell
+    recs = [np.array([v[0] for v in ds])[::2] for p in plots for ds in p["data"]]
+    np.savez_compressed(os.path.join(HERE, "basic_example.npz"), records=np.array(recs),
+                        timesteps=np.arange(0, 101, 20))
+    print("wrote", sorted(os.listdir(HERE)))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

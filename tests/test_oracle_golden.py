@@ -1,0 +1,90 @@
+"""Pins the CPU oracle to the reference's own golden data (tests/golden/*,
+extracted from libmpdata++ tests/paper_2015_GMD/*/refdata by make_golden.py).
+The oracle is trusted as the parity checker for the CUDA path only because it
+reproduces these numbers."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from libmpdataxx_b200 import opts as o
+from libmpdataxx_b200 import setups
+from oracle import Oracle
+from runners import run_oracle
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def golden():
+    with open(os.path.join(GOLD, "golden_stats.json")) as f:
+        return json.load(f)
+
+
+# 1_advscheme_opts: 601-cell cyclic, C = -0.75, 1200 steps; values printed with 5 decimals
+@pytest.mark.parametrize("case", ["abs", "iga", "iga_tot", "iga_fct", "iga_tot_fct"])
+def test_advscheme_opts_1d(case):
+    ref = np.load(os.path.join(GOLD, "advscheme_opts.npz"))[case]
+    s = setups.advscheme_opts()
+    np.testing.assert_allclose(ref[0], s["advectee"][0], atol=6e-6)
+    np.testing.assert_allclose(ref[1], s["advectee"][1], atol=6e-6)
+    out = run_oracle(s, setups.ADVSCHEME_CASES[case])
+    np.testing.assert_allclose(out[0], ref[2], rtol=0, atol=6e-6)
+    np.testing.assert_allclose(out[1], ref[3], rtol=0, atol=6e-6)
+
+
+# 0_basic_example: 101-cell open, iga|fct (default opts), records every 20 steps
+def test_basic_example_1d():
+    ref = np.load(os.path.join(GOLD, "basic_example.npz"))
+    s = setups.basic_example()
+    orc = Oracle(s["grid"], s["opts"], n_iters=2, bcs=s["bcs"])
+    orc.set_advectee(s["advectee"][0])
+    orc.set_advector(s["advector"][0])
+    np.testing.assert_allclose(orc.advectee(), ref["records"][0], atol=6e-6)
+    for rec in ref["records"][1:]:
+        orc.advance(20)
+        np.testing.assert_allclose(orc.advectee(), rec, rtol=0, atol=6e-6)
+
+
+def _check_stats(got, want, keys, atol=6e-9):
+    for k in keys:
+        assert abs(got[k] - want["tN:" + k]) <= atol, (k, got[k], want["tN:" + k])
+
+
+# 3_rotating_cone_2d: 101^2 open, 3768 steps; stats with 8 decimals
+@pytest.mark.parametrize("case", list(setups.CONE_CASES))
+def test_rotating_cone_2d(case):
+    s = setups.rotating_cone()
+    opts, iters = setups.CONE_CASES[case]
+    out = run_oracle(s, opts, n_iters=iters)[0]
+    st = setups.cone_stats(s["advectee"][0], out, s["nt"], s["dt"])
+    _check_stats(st, golden()["rotating_cone_2d"][case], ["min(psi)", "max(psi)", "rms error"])
+
+
+# 4_revolving_sphere_3d: 59^3 open, 556 steps; stats with 8 decimals
+@pytest.mark.parametrize("case", list(setups.SPHERE_CASES))
+def test_revolving_sphere_3d(case):
+    s = setups.revolving_sphere()
+    opts, iters = setups.SPHERE_CASES[case]
+    out = run_oracle(s, opts, n_iters=iters)[0]
+    st = setups.sphere_stats(s["advectee"][0], out, s["nt"], s["dt"])
+    _check_stats(st, golden()["revolving_sphere_3d"][case], ["max(solution)", "min(solution)", "Linf", "L2", "L1"])
+
+
+# tests/unit/cone_bugs: FP32 fct never undershoots the background (exact)
+def test_cone_bugs_fp32_exact_min():
+    s = setups.cone_bugs()
+    out = run_oracle(s, s["opts"], n_iters=2, dtype=np.float32)[0]
+    assert out.min() - 1 == 0
+
+
+def test_divergent_advector_raises():
+    s = setups.cone_bugs()
+    s["advector"][0] = s["advector"][0] + np.linspace(0, 0.1, s["grid"][0])[:, None]
+    with pytest.raises(RuntimeError, match="initial advector field is divergent"):
+        run_oracle(s, o.fct)
+
+
+def test_bogus_grid_raises():
+    with pytest.raises(RuntimeError, match="bogus grid size"):
+        Oracle((0, 4), o.fct)
