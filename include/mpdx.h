@@ -1,0 +1,149 @@
+/*
+ * libmpdataxx_b200 -- C ABI of the B200 (sm_100a) MPDATA / pressure-solve backend.
+ *
+ * This is the boundary that a concurr::cuda backend (header-only C++, see
+ * libmpdataxx_b200/include/libmpdata++/concurr/cuda.hpp) or any FFI binds.
+ * Plain pointers and sizes only.  Each entry point names the reference
+ * interface it replaces (paths inside the libmpdata++ source tree).
+ *
+ * Fields live on the device for the life of the handle.  Host buffers are
+ * caller-owned and copied synchronously; element strides describe the host
+ * layout (so the reference's 3D storage order -- k fastest, then i, then j,
+ * libmpdata++/blitz.hpp:116-117 -- is accepted as is).
+ *
+ * Threading: a handle is used from one host thread at a time; its work is
+ * serialised on the handle's CUDA stream.
+ */
+#ifndef MPDX_H
+#define MPDX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; the C++ header maps each to the reference's exception text. */
+typedef enum {
+  MPDX_OK = 0,
+  MPDX_E_GRID = 1,        /* "libmpdata++: bogus grid size" (solver_common.hpp:246-248) */
+  MPDX_E_DIVERGENT = 2,   /* "libmpdata++: initial advector field is divergent" (solver_2d.hpp:290-291) */
+  MPDX_E_PRS_STUCK = 3,   /* "libmpdata++: stuck in pressure solver" (mpdata_rhs_vip_prs_common.hpp:121-125) */
+  MPDX_E_UNSUPPORTED = 4, /* option / boundary-condition combination not built on this backend */
+  MPDX_E_CUDA = 5,        /* CUDA runtime error (message in mpdx_last_error) */
+  MPDX_E_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+  MPDX_E_ARG = 7          /* invalid argument (null pointer, index out of range, ...) */
+} mpdx_status;
+
+/* boundary kinds (libmpdata++/bcond/detail/bcond_common.hpp bcond_e) */
+enum { MPDX_BC_CYCLIC = 0, MPDX_BC_OPEN = 1, MPDX_BC_RIGID = 2 };
+
+/* solver families (solvers::mpdata, solvers::boussinesq) */
+enum { MPDX_SOLVER_MPDATA = 0, MPDX_SOLVER_BOUSSINESQ = 1 };
+
+/* pressure schemes (solvers::prs_scheme_t, mpdata_rhs_vip_prs.hpp:17-30) */
+enum { MPDX_PRS_CR = 0, MPDX_PRS_GCRK = 1 };
+
+/* preconditioner inside GCR: identity (the reference's) or the learned one */
+enum { MPDX_PRECOND_IDENTITY = 0, MPDX_PRECOND_LEARNED = 1 };
+
+/* execution path: AUTO picks the fused kernels when the configuration allows
+ * (all-cyclic, supported opts, periodic seams consistent) else GENERAL, which
+ * runs one kernel per reference formula; both are CUDA. */
+enum { MPDX_PATH_AUTO = 0, MPDX_PATH_GENERAL = 1, MPDX_PATH_FUSED = 2 };
+
+/* field kinds for mpdx_set_field / mpdx_get_field */
+enum {
+  MPDX_FIELD_ADVECTEE = 0,   /* idx = equation; interior n0 x n1 x n2 */
+  MPDX_FIELD_ADVECTOR = 1,   /* idx = dimension; reference view extents (below) */
+  MPDX_FIELD_SCLR_ARRAY = 2, /* idx = MPDX_SCLR_* named scalar array */
+  MPDX_FIELD_PRESSURE = 3    /* Boussinesq: Phi, interior */
+};
+enum { MPDX_SCLR_THT_E = 0 };
+
+/* Run-time and compile-time parameters of one solver (ct_params_t + rt_params_t,
+ * libmpdata++/opts.hpp:81-100, solver_common.hpp:217-221, mpdata_common.hpp:74-78,
+ * mpdata_rhs_vip_prs_common.hpp:193-196, boussinesq_common.hpp:32-35). */
+typedef struct {
+  int solver;              /* MPDX_SOLVER_* */
+  int n_dims;              /* 1..3 */
+  int n_eqns;              /* advected equations */
+  int grid[3];             /* grid_size */
+  uint64_t opts;           /* opts bitmask, same bit values as libmpdata++/opts.hpp */
+  int n_iters;             /* MPDATA iterations (default 2) */
+  int dtype;               /* sizeof(real_t): 4 (float) or 8 (double) */
+  int bcs[6];              /* MPDX_BC_* for (x left, x right, y left, y right, z left, z right) */
+  double dt, di, dj, dk;   /* time step and grid spacings */
+  double max_abs_div_eps;  /* < 0 selects the reference default, machine epsilon of real_t */
+  int path;                /* MPDX_PATH_* */
+  /* Boussinesq / pressure solve */
+  int prs_scheme;          /* MPDX_PRS_CR or MPDX_PRS_GCRK */
+  int prs_k_iters;         /* k of GCR(k) for MPDX_PRS_GCRK (default 4) */
+  double prs_tol;          /* stop when max|err| <= prs_tol / dt */
+  double g, tht_ref;       /* gravity, reference potential temperature */
+  int ix_u, ix_v, ix_w, ix_tht;  /* equation indices (ct_params_t::ix); ix_v = -1 in 2D */
+  int precond;             /* MPDX_PRECOND_* */
+  int prs_fp64;            /* 1: pressure fields in FP64 even when real_t is float */
+} mpdx_config;
+
+typedef struct mpdx_solver *mpdx_handle;
+
+/* Per-step device-side statistics, read back on demand. */
+typedef struct {
+  int64_t timestep;
+  double time;
+  double mass;             /* FP64 compensated sum of advectee(0) over the interior */
+  double min, max;         /* of advectee(0) */
+  int64_t gcr_iters;       /* iterations of the last pressure solve (Boussinesq) */
+  int64_t gcr_iters_total; /* since creation */
+  double gcr_residual;     /* max|err| at the end of the last pressure solve */
+  int path;                /* path used by the last advance (MPDX_PATH_GENERAL/FUSED) */
+} mpdx_step_stats;
+
+/* Fill *cfg with the reference defaults (opts = iga|fct, n_iters = 2, ...). */
+void mpdx_config_default(mpdx_config *cfg);
+
+/* concurr::<backend><solver_t, bc...> run(p)  (concurr_common.hpp:176-187, any.hpp:15-74):
+ * allocates every device field of the solver. */
+mpdx_status mpdx_create(const mpdx_config *cfg, mpdx_handle *out);
+
+/* run.advectee(e) = ... / run.advector(d) = ... / run.sclr_array(name) = ...
+ * (concurr_common.hpp:387-433, sharedmem.hpp:411-456, 543-577).
+ * Advector views follow the reference: lower bound (-1, 0, 0); extents
+ * (n0, n1, n2) for d = 0 and (n0 + 1, n1, n2) for d >= 1.  Strides are in
+ * elements of real_t; NULL strides mean C order. */
+mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, const int64_t *strides);
+mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const int64_t *strides);
+
+/* Same with device pointers (C order), for callers that keep data on the GPU. */
+mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev);
+mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev);
+
+/* run.advance(nt)  (concurr_common.hpp:380-385 -> solver_common.hpp:270-358).
+ * Asynchronous with respect to the host except on the first call (the
+ * divergence check of hook_ante_loop reads one device scalar back). */
+mpdx_status mpdx_advance(mpdx_handle h, int64_t nt);
+
+/* Blocks until the handle's stream is idle. */
+mpdx_status mpdx_sync(mpdx_handle h);
+
+/* run.min()/max()/timestep plus FP64 mass and pressure-solver counters
+ * (sharedmem.hpp:115-246). */
+mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that order work with it. */
+void *mpdx_stream(mpdx_handle h);
+
+/* Message of the last failing call on this handle ("" if none). */
+const char *mpdx_last_error(mpdx_handle h);
+
+/* Message of the last failing mpdx_create in this thread. */
+const char *mpdx_create_error(void);
+
+void mpdx_destroy(mpdx_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPDX_H */

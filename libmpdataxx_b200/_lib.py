@@ -1,0 +1,97 @@
+"""ctypes binding of libmpdx.so (the C ABI declared in include/mpdx.h).
+
+The shared library is built in-tree by __graft_entry__.build() (or `make -C
+libmpdataxx_b200/csrc`).  There is no fallback: if the library is missing the
+import of this module's `lib()` raises, and on a machine without a CUDA device
+every solver call fails with the CUDA runtime's message.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(HERE, "libmpdx.so")
+
+MPDX_OK, MPDX_E_GRID, MPDX_E_DIVERGENT, MPDX_E_PRS_STUCK, MPDX_E_UNSUPPORTED, MPDX_E_CUDA, MPDX_E_TIMEOUT, MPDX_E_ARG = range(8)
+BC = {"cyclic": 0, "open": 1, "rigid": 2}
+SOLVER_MPDATA, SOLVER_BOUSSINESQ = 0, 1
+PRS_CR, PRS_GCRK = 0, 1
+PRECOND_IDENTITY, PRECOND_LEARNED = 0, 1
+PATH_AUTO, PATH_GENERAL, PATH_FUSED = 0, 1, 2
+FIELD_ADVECTEE, FIELD_ADVECTOR, FIELD_SCLR_ARRAY, FIELD_PRESSURE = 0, 1, 2, 3
+SCLR_THT_E = 0
+
+# every entry point declared in include/mpdx.h
+EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
+           "mpdx_get_field_device", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
+           "mpdx_create_error", "mpdx_destroy"]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("solver", ctypes.c_int), ("n_dims", ctypes.c_int), ("n_eqns", ctypes.c_int),
+                ("grid", ctypes.c_int * 3), ("opts", ctypes.c_uint64), ("n_iters", ctypes.c_int),
+                ("dtype", ctypes.c_int), ("bcs", ctypes.c_int * 6), ("dt", ctypes.c_double),
+                ("di", ctypes.c_double), ("dj", ctypes.c_double), ("dk", ctypes.c_double),
+                ("max_abs_div_eps", ctypes.c_double), ("path", ctypes.c_int), ("prs_scheme", ctypes.c_int),
+                ("prs_k_iters", ctypes.c_int), ("prs_tol", ctypes.c_double), ("g", ctypes.c_double),
+                ("tht_ref", ctypes.c_double), ("ix_u", ctypes.c_int), ("ix_v", ctypes.c_int),
+                ("ix_w", ctypes.c_int), ("ix_tht", ctypes.c_int), ("precond", ctypes.c_int),
+                ("prs_fp64", ctypes.c_int)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("timestep", ctypes.c_int64), ("time", ctypes.c_double), ("mass", ctypes.c_double),
+                ("min", ctypes.c_double), ("max", ctypes.c_double), ("gcr_iters", ctypes.c_int64),
+                ("gcr_iters_total", ctypes.c_int64), ("gcr_residual", ctypes.c_double), ("path", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SO_PATH):
+        raise ImportError(f"{SO_PATH} is not built; run __graft_entry__.build() (or make -C libmpdataxx_b200/csrc)")
+    L = ctypes.CDLL(SO_PATH)
+    vp, i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
+    L.mpdx_config_default.argtypes = [ctypes.POINTER(Config)]
+    L.mpdx_config_default.restype = None
+    L.mpdx_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    L.mpdx_create.restype = ctypes.c_int
+    L.mpdx_create_error.argtypes = []
+    L.mpdx_create_error.restype = ctypes.c_char_p
+    for f in ("mpdx_set_field", "mpdx_get_field"):
+        getattr(L, f).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, i64p]
+        getattr(L, f).restype = ctypes.c_int
+    for f in ("mpdx_set_field_device", "mpdx_get_field_device"):
+        getattr(L, f).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+        getattr(L, f).restype = ctypes.c_int
+    L.mpdx_advance.argtypes = [vp, ctypes.c_int64]
+    L.mpdx_advance.restype = ctypes.c_int
+    L.mpdx_sync.argtypes = [vp]
+    L.mpdx_sync.restype = ctypes.c_int
+    L.mpdx_stats.argtypes = [vp, ctypes.POINTER(StepStats)]
+    L.mpdx_stats.restype = ctypes.c_int
+    L.mpdx_stream.argtypes = [vp]
+    L.mpdx_stream.restype = vp
+    L.mpdx_last_error.argtypes = [vp]
+    L.mpdx_last_error.restype = ctypes.c_char_p
+    L.mpdx_destroy.argtypes = [vp]
+    L.mpdx_destroy.restype = None
+    _lib = L
+    return L
+
+
+# exception text per status, as the reference throws them
+MESSAGES = {
+    MPDX_E_GRID: "libmpdata++: bogus grid size",
+    MPDX_E_DIVERGENT: "libmpdata++: initial advector field is divergent",
+    MPDX_E_PRS_STUCK: "libmpdata++: stuck in pressure solver",
+}
+
+
+class MpdxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code

@@ -1,0 +1,14 @@
+"""Boundary-condition kinds (libmpdata++/bcond/detail/bcond_common.hpp bcond_e)."""
+
+
+class _bc:
+    def __init__(self, name):
+        self.name = name
+
+    def __repr__(self):
+        return f"bcond.{self.name}"
+
+
+cyclic = _bc("cyclic")
+open = _bc("open")
+rigid = _bc("rigid")

@@ -1,0 +1,170 @@
+"""concurr::cuda -- the run object of the reference's API on top of the CUDA library.
+
+Mirrors libmpdata++'s concurr::{serial,openmp,threads}<solver_t, bc...>
+(concurr/detail/concurr_common.hpp:122-454, concurr/any.hpp:15-74):
+
+    run = cuda(solvers.mpdata(ct_params), bcond.cyclic, bcond.cyclic, ..., p=rt)
+    run.advectee(e)[...] = ...      # writable host mirror of the device field
+    run.advector(d)[...] = ...      # view with lower bound (-1, 0, 0): element a <-> index a - 1
+    run.advance(nt)
+    run.advectee(e)                  # state after nt steps (downloaded on access)
+
+Host mirrors handed out by advectee()/advector()/sclr_array() are uploaded
+before the next advance() (the reference's views alias solver memory, so any
+write through them is seen by the next step); after advance() they are
+refreshed on the next access.  Fields otherwise stay on the device.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .solvers import boussinesq as _bq
+
+
+def _check(L, h, rc):
+    if rc != _lib.MPDX_OK:
+        msg = L.mpdx_last_error(h).decode() if h else L.mpdx_create_error().decode()
+        raise _lib.MpdxError(rc, _lib.MESSAGES.get(rc, msg) if rc in _lib.MESSAGES else msg)
+
+
+class cuda:
+    def __init__(self, solver, *bcs, p=None, path="auto"):
+        self.solver = solver
+        ct = solver.ct
+        self.nd = int(ct.n_dims)
+        if len(bcs) != 2 * self.nd:
+            raise TypeError(f"expected {2 * self.nd} boundary conditions, got {len(bcs)}")
+        if p is None:
+            raise TypeError("rt_params p is required")
+        self.p = p
+        self.real_t = np.dtype(ct.real_t)
+        self.n_eqns = int(ct.n_eqns)
+        self.grid = tuple(int(g) for g in p.grid_size)[: self.nd]
+        L = _lib.lib()
+        self.L = L
+        cfg = _lib.Config()
+        L.mpdx_config_default(ctypes.byref(cfg))
+        cfg.solver = _lib.SOLVER_BOUSSINESQ if isinstance(solver, _bq) else _lib.SOLVER_MPDATA
+        cfg.n_dims = self.nd
+        cfg.n_eqns = self.n_eqns
+        for d in range(3):
+            cfg.grid[d] = self.grid[d] if d < self.nd else 1
+        cfg.opts = int(ct.opts)
+        cfg.n_iters = int(getattr(p, "n_iters", 2))
+        cfg.dtype = self.real_t.itemsize
+        for q, b in enumerate(bcs):
+            cfg.bcs[q] = _lib.BC[b if isinstance(b, str) else b.name]
+        cfg.dt = float(getattr(p, "dt", 0.0))
+        cfg.di = float(getattr(p, "di", 1.0) or 1.0)
+        cfg.dj = float(getattr(p, "dj", 1.0) or 1.0)
+        cfg.dk = float(getattr(p, "dk", 1.0) or 1.0)
+        eps = getattr(p, "max_abs_div_eps", None)
+        cfg.max_abs_div_eps = -1.0 if eps is None else float(eps)
+        cfg.path = {"auto": _lib.PATH_AUTO, "general": _lib.PATH_GENERAL, "fused": _lib.PATH_FUSED}[path]
+        if isinstance(solver, _bq):
+            solver.fill_config(cfg, p)
+        h = ctypes.c_void_p()
+        rc = L.mpdx_create(ctypes.byref(cfg), ctypes.byref(h))
+        _check(L, None, rc)
+        self.h = h
+        self._mirrors = {}   # (kind, idx) -> ndarray
+        self._fresh = set()  # mirrors known to equal the device copy
+
+    # -- lifetime --------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mpdx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- views ------------------------------------------------------------
+    def _shape(self, kind, idx):
+        if kind == _lib.FIELD_ADVECTOR:
+            s = list(self.grid)
+            if idx > 0:
+                s[0] += 1
+            return tuple(s)
+        return self.grid
+
+    def _mirror(self, kind, idx):
+        key = (kind, idx)
+        a = self._mirrors.get(key)
+        if a is None:
+            a = np.empty(self._shape(kind, idx), dtype=self.real_t)
+            self._mirrors[key] = a
+        if key not in self._fresh:
+            _check(self.L, self.h, self.L.mpdx_get_field(self.h, kind, idx, a.ctypes.data, None))
+            self._fresh.add(key)
+        return a
+
+    def advectee(self, e=0):
+        return self._mirror(_lib.FIELD_ADVECTEE, e)
+
+    def advector(self, d=0):
+        return self._mirror(_lib.FIELD_ADVECTOR, d)
+
+    def sclr_array(self, name, n=0):
+        if name != "tht_e":
+            raise KeyError(name)
+        return self._mirror(_lib.FIELD_SCLR_ARRAY, _lib.SCLR_THT_E)
+
+    def advectee_global(self, e=0):
+        return self.advectee(e)
+
+    def _flush(self):
+        for (kind, idx), a in self._mirrors.items():
+            if (kind, idx) in self._fresh:
+                _check(self.L, self.h, self.L.mpdx_set_field(self.h, kind, idx, np.ascontiguousarray(a).ctypes.data, None))
+        # state fields change on the device; advectors and scalar arrays do not
+        self._fresh = {k for k in self._fresh if k[0] in (_lib.FIELD_ADVECTOR, _lib.FIELD_SCLR_ARRAY)}
+
+    # -- explicit transfers ---------------------------------------------------
+    def set_field(self, kind, idx, a):
+        a = np.ascontiguousarray(np.broadcast_to(a, self._shape(kind, idx)), dtype=self.real_t)
+        _check(self.L, self.h, self.L.mpdx_set_field(self.h, kind, idx, a.ctypes.data, None))
+        self._mirrors.pop((kind, idx), None)
+        self._fresh.discard((kind, idx))
+
+    def set_advectee(self, a, e=0):
+        self.set_field(_lib.FIELD_ADVECTEE, e, a)
+
+    def set_advector(self, a, d=0):
+        self.set_field(_lib.FIELD_ADVECTOR, d, a)
+
+    def set_field_device(self, kind, idx, ptr):
+        _check(self.L, self.h, self.L.mpdx_set_field_device(self.h, kind, idx, ctypes.c_void_p(ptr)))
+        self._mirrors.pop((kind, idx), None)
+        self._fresh.discard((kind, idx))
+
+    def get_field_device(self, kind, idx, ptr):
+        _check(self.L, self.h, self.L.mpdx_get_field_device(self.h, kind, idx, ctypes.c_void_p(ptr)))
+
+    # -- time stepping ----------------------------------------------------------
+    def advance(self, nt):
+        self._flush()
+        _check(self.L, self.h, self.L.mpdx_advance(self.h, int(nt)))
+
+    def sync(self):
+        _check(self.L, self.h, self.L.mpdx_sync(self.h))
+
+    @property
+    def stream(self):
+        return self.L.mpdx_stream(self.h)
+
+    def stats(self):
+        s = _lib.StepStats()
+        _check(self.L, self.h, self.L.mpdx_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.StepStats._fields_}
+
+    def min(self, e=0):
+        return float(self.advectee(e).min())
+
+    def max(self, e=0):
+        return float(self.advectee(e).max())
+
+    def time(self):
+        st = self.stats()
+        return st["timestep"] * float(getattr(self.p, "dt", 0.0))

@@ -1,0 +1,638 @@
+// Reference-structured MPDATA path: one kernel per libmpdata++ formula and one
+// small kernel per halo fill, launched in the order the reference's solvers call
+// them.  It covers every dimension, the cyclic and open boundary conditions
+// and the MPDATA options that the fused kernels do not, and it is the FP64
+// parity path (this file is compiled with --fmad=false so that FP64 results
+// follow the reference's rounding).
+//
+// Reference call structure mirrored here:
+//   advop            libmpdata++/solvers/detail/mpdata_osc_{1,2,3}d.hpp
+//   fct_init / fct_adjust_antidiff   mpdata_fct_{1,2,3}d.hpp
+//   halo exchanges   solvers/detail/solver_{1,2,3}d.hpp, bcond/{cyclic,open}_{1,2,3}d.hpp
+#include <cfloat>
+
+#include "general.cuh"
+
+namespace mpdx {
+
+// ---------------------------------------------------------------------------
+// frame permutation pi<d> (libmpdata++/formulae/idxperm.hpp:15-71):
+// frame (a along d, b along d+1, c along d+2)  <->  physical (i, j, k)
+template <int ND, int D> struct fr;
+template <> struct fr<1, 0> {
+  __device__ static void to(int a, int, int, int &i, int &j, int &k) { i = a; j = 0; k = 0; }
+  __device__ static void from(int i, int, int, int &a, int &b, int &c) { a = i; b = 0; c = 0; }
+};
+template <> struct fr<2, 0> {
+  __device__ static void to(int a, int b, int, int &i, int &j, int &k) { i = a; j = b; k = 0; }
+  __device__ static void from(int i, int j, int, int &a, int &b, int &c) { a = i; b = j; c = 0; }
+};
+template <> struct fr<2, 1> {
+  __device__ static void to(int a, int b, int, int &i, int &j, int &k) { i = b; j = a; k = 0; }
+  __device__ static void from(int i, int j, int, int &a, int &b, int &c) { a = j; b = i; c = 0; }
+};
+template <> struct fr<3, 0> {
+  __device__ static void to(int a, int b, int c, int &i, int &j, int &k) { i = a; j = b; k = c; }
+  __device__ static void from(int i, int j, int k, int &a, int &b, int &c) { a = i; b = j; c = k; }
+};
+template <> struct fr<3, 1> {
+  __device__ static void to(int a, int b, int c, int &i, int &j, int &k) { i = c; j = a; k = b; }
+  __device__ static void from(int i, int j, int k, int &a, int &b, int &c) { a = j; b = k; c = i; }
+};
+template <> struct fr<3, 2> {
+  __device__ static void to(int a, int b, int c, int &i, int &j, int &k) { i = b; j = c; k = a; }
+  __device__ static void from(int i, int j, int k, int &a, int &b, int &c) { a = k; b = i; c = j; }
+};
+
+template <int ND, int D, class T>
+__device__ __forceinline__ T &P(const dfield<T> &A, int a, int b = 0, int c = 0) {
+  int i, j, k;
+  fr<ND, D>::to(a, b, c, i, j, k);
+  return A(i, j, k);
+}
+
+__device__ __forceinline__ void pim(int nd, int d, int a, int b, int c, int &i, int &j, int &k) {
+  if (nd == 1) { i = a; j = 0; k = 0; return; }
+  if (nd == 2) { if (d == 0) { i = a; j = b; } else { i = b; j = a; } k = 0; return; }
+  if (d == 0) { i = a; j = b; k = c; } else if (d == 1) { i = c; j = a; k = b; } else { i = b; j = c; k = a; }
+}
+template <class T>
+__device__ __forceinline__ T &PR(const dfield<T> &A, int nd, int d, int a, int b, int c) {
+  int i, j, k;
+  pim(nd, d, a, b, c, i, j, k);
+  return A(i, j, k);
+}
+
+// pospart/negpart (formulae/common.hpp:86-124) follow std::max(0, x)/std::min(0, x)
+template <class T> __device__ __forceinline__ T pospart(unsigned o, T x) {
+  if (o & o_npa) return (x + fabs(x)) / T(2);
+  return T(0) < x ? x : T(0);
+}
+template <class T> __device__ __forceinline__ T negpart(unsigned o, T x) {
+  if (o & o_npa) return (x - fabs(x)) / T(2);
+  return x < T(0) ? x : T(0);
+}
+template <class T> __device__ __forceinline__ T dmax(T a, T b) { return a < b ? b : a; }  // std::max
+template <class T> __device__ __forceinline__ T dmin(T a, T b) { return b < a ? b : a; }  // std::min
+template <class T> struct lim;
+template <> struct lim<float> {
+  __device__ static float tiny() { return FLT_MIN; }
+  __device__ static float eps() { return FLT_EPSILON; }
+};
+template <> struct lim<double> {
+  __device__ static double tiny() { return DBL_MIN; }
+  __device__ static double eps() { return DBL_EPSILON; }
+};
+// frac (formulae_mpdata_common.hpp:61-86), fct_frac (:88-98)
+template <class T> __device__ __forceinline__ T frac(unsigned o, T nom, T den) {
+  if (o & o_pfc) return den != T(0) ? nom / den : T(0);
+  return nom / (den + lim<T>::tiny());
+}
+template <class T> __device__ __forceinline__ T fct_frac(T nom, T den) { return nom / (den + lim<T>::eps()); }
+
+// ---------------------------------------------------------------------------
+// generic launcher: one thread per point of a physical box, op(a, b, c) in frame
+template <int ND, int D, class Op>
+__global__ void k_box(Op op, int i0, int j0, int k0, int ni, int nj, int nk) {
+  const long long tot = (long long)ni * nj * nk;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int k = k0 + int(q % nk);
+    const long long r = q / nk;
+    const int j = j0 + int(r % nj);
+    const int i = i0 + int(r / nj);
+    int a, b, c;
+    fr<ND, D>::from(i, j, k, a, b, c);
+    op(a, b, c);
+  }
+}
+
+template <int ND, int D, class Op>
+void launch_frame(cudaStream_t s, Op op, rng ra, rng rb, rng rc) {
+  // frame ranges -> physical box
+  rng ph[3] = {{0, 0}, {0, 0}, {0, 0}};
+  ph[D] = ra;
+  if (ND >= 2) ph[(D + 1) % ND] = rb;
+  if (ND >= 3) ph[(D + 2) % ND] = rc;
+  const long long tot = (long long)ph[0].n() * ph[1].n() * ph[2].n();
+  if (tot <= 0) return;
+  const int bs = 256;
+  unsigned g = ceil_div(tot, bs);
+  if (g > 65535u * 8u) g = 65535u * 8u;
+  k_box<ND, D><<<g, bs, 0, s>>>(op, ph[0].f, ph[1].f, ph[2].f, ph[0].n(), ph[1].n(), ph[2].n());
+  MPDX_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// formulae
+
+// nondimensional psi derivatives at (a+1/2, b, c) (formulae_mpdata_psi_{1,2,3}d.hpp)
+template <int ND, int D, class T>
+__device__ __forceinline__ T ndx(unsigned o, const dfield<T> &p, int a, int b, int c) {
+  const T p1 = P<ND, D>(p, a + 1, b, c), p0 = P<ND, D>(p, a, b, c);
+  if (o & o_iga) {
+    if (ND == 3) return p1 - p0;
+    return T(2) * (p1 - p0) / T(2);
+  }
+  if (o & o_abs) return T(2) * frac(o, fabs(p1) - fabs(p0), fabs(p1) + fabs(p0));
+  return T(2) * frac(o, p1 - p0, p1 + p0);
+}
+template <class T>
+__device__ __forceinline__ T nd4(unsigned o, T pa, T pb, T pc, T pd) {
+  if (o & o_iga) return (pa + pb - pc - pd) / T(4);
+  if (o & o_abs) { pa = fabs(pa); pb = fabs(pb); pc = fabs(pc); pd = fabs(pd); }
+  return frac(o, pa + pb - pc - pd, pa + pb + pc + pd);
+}
+template <int ND, int D, class T>
+__device__ __forceinline__ T ndy(unsigned o, const dfield<T> &p, int a, int b, int c) {
+  return nd4(o, P<ND, D>(p, a + 1, b + 1, c), P<ND, D>(p, a, b + 1, c), P<ND, D>(p, a + 1, b - 1, c), P<ND, D>(p, a, b - 1, c));
+}
+template <int ND, int D, class T>
+__device__ __forceinline__ T ndz(unsigned o, const dfield<T> &p, int a, int b, int c) {
+  return nd4(o, P<ND, D>(p, a + 1, b, c + 1), P<ND, D>(p, a, b, c + 1), P<ND, D>(p, a + 1, b, c - 1), P<ND, D>(p, a, b, c - 1));
+}
+
+// antidiffusive velocity (formulae_mpdata_{1,2,3}d.hpp antidiff, standard form)
+template <int ND, int D, class T>
+struct op_antidiff {
+  dfield<T> res, psi, G0, G1, G2;  // G0 = GC[D], G1 = GC[D+1], G2 = GC[D+2]
+  unsigned o;
+  __device__ void operator()(int a, int b, int c) const {
+    const T C = P<ND, D>(G0, a, b, c);
+    T r = fabs(C) / T(2) * (T(1) - fabs(C) / T(1)) * ndx<ND, D>(o, psi, a, b, c);
+    if (ND == 1) {
+      if (o & o_tot) {  // TOT (formulae_mpdata_hot_1d.hpp:19-52)
+        const T pa = psi(a + 2, 0, 0), pb = psi(a + 1, 0, 0), pc = psi(a, 0, 0), pd = psi(a - 1, 0, 0);
+        T xx;
+        if (o & o_iga) xx = T(2) * (pa - pb - pc + pd) / T(4);
+        else if (o & o_abs) xx = T(2) * frac(o, fabs(pa) - fabs(pb) - fabs(pc) + fabs(pd), fabs(pa) + fabs(pb) + fabs(pc) + fabs(pd));
+        else xx = T(2) * frac(o, pa - pb - pc + pd, pa + pb + pc + pd);
+        const T coeff = (T(3) * C * fabs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6);
+        r = r + xx * coeff;
+      }
+    } else if (ND == 2) {
+      // GC1_bar_xy (formulae_mpdata_gc_2d.hpp:76-90)
+      const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
+      r = r - C * gc1 / T(2) * ndy<ND, D>(o, psi, a, b, c);
+    } else {
+      // GC1_bar_xy, GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
+      const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
+      const T gc2 = (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) + P<ND, D>(G2, a + 1, b, c - 1) + P<ND, D>(G2, a, b, c - 1)) / T(4);
+      r = r - C / T(2) * (gc1 * ndy<ND, D>(o, psi, a, b, c) + gc2 * ndz<ND, D>(o, psi, a, b, c)) / T(1);
+    }
+    P<ND, D>(res, a, b, c) = r;
+  }
+};
+
+// donor-cell flux (donorcell_formulae.hpp:25-79)
+template <int ND, int D, class T>
+struct op_flux {
+  dfield<T> F, psi, C;
+  unsigned o;
+  __device__ void operator()(int a, int b, int c) const {
+    const T g = P<ND, D>(C, a, b, c);
+    P<ND, D>(F, a, b, c) = pospart(o, g) * P<ND, D>(psi, a, b, c) + negpart(o, g) * P<ND, D>(psi, a + 1, b, c);
+  }
+};
+
+// donorcell_sum with G = 1 (donorcell_formulae.hpp:81-165)
+template <int ND, class T>
+struct op_donorcell {
+  dfield<T> pn, po, f0, f1, f2;
+  __device__ void operator()(int i, int j, int k) const {
+    if (ND == 1) pn(i, j, k) = po(i, j, k) + (-f0(i, j, k) + f0(i - 1, j, k)) / T(1);
+    else if (ND == 2)
+      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k))) / T(1);
+    else
+      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k)) + (-f2(i, j, k) + f2(i, j, k - 1))) / T(1);
+  }
+};
+
+// fct_init (mpdata_fct_{1,2,3}d.hpp:31-55)
+template <int ND, class T>
+struct op_fct_init {
+  dfield<T> mn, mx, p;
+  __device__ void operator()(int i, int j, int k) const {
+    T lo, hi;
+    if (ND == 1) {
+      lo = dmin(dmin(p(i - 1, j, k), p(i, j, k)), p(i + 1, j, k));
+      hi = dmax(dmax(p(i - 1, j, k), p(i, j, k)), p(i + 1, j, k));
+    } else if (ND == 2) {
+      lo = dmin(dmin(dmin(dmin(p(i, j + 1, k), p(i - 1, j, k)), p(i, j, k)), p(i + 1, j, k)), p(i, j - 1, k));
+      hi = dmax(dmax(dmax(dmax(p(i, j + 1, k), p(i - 1, j, k)), p(i, j, k)), p(i + 1, j, k)), p(i, j - 1, k));
+    } else {
+      lo = dmin(dmin(dmin(dmin(dmin(dmin(p(i, j, k), p(i + 1, j, k)), p(i - 1, j, k)), p(i, j + 1, k)), p(i, j - 1, k)), p(i, j, k + 1)), p(i, j, k - 1));
+      hi = dmax(dmax(dmax(dmax(dmax(dmax(p(i, j, k), p(i + 1, j, k)), p(i - 1, j, k)), p(i, j + 1, k)), p(i, j - 1, k)), p(i, j, k + 1)), p(i, j, k - 1));
+    }
+    mn(i, j, k) = lo;
+    mx(i, j, k) = hi;
+  }
+};
+
+// beta_up / beta_dn (formulae_mpdata_fct_{1,2,3}d.hpp)
+template <int ND, class T>
+struct op_betas {
+  dfield<T> bu, bd, p, pmax, pmin, f0, f1, f2;
+  unsigned o;
+  __device__ void operator()(int i, int j, int k) const {
+    const T c = p(i, j, k);
+    T mx, mn, du, dd;
+    if (ND == 1) {
+      mx = dmax(pmax(i, j, k), dmax(p(i - 1, j, k), dmax(c, p(i + 1, j, k))));
+      mn = dmin(pmin(i, j, k), dmin(p(i - 1, j, k), dmin(c, p(i + 1, j, k))));
+      du = pospart(o, f0(i - 1, j, k)) - negpart(o, f0(i, j, k));
+      dd = pospart(o, f0(i, j, k)) - negpart(o, f0(i - 1, j, k));
+    } else if (ND == 2) {
+      mx = dmax(pmax(i, j, k), dmax(p(i, j + 1, k), dmax(p(i - 1, j, k), dmax(c, dmax(p(i + 1, j, k), p(i, j - 1, k))))));
+      mn = dmin(pmin(i, j, k), dmin(p(i, j + 1, k), dmin(p(i - 1, j, k), dmin(c, dmin(p(i + 1, j, k), p(i, j - 1, k))))));
+      du = (pospart(o, f0(i - 1, j, k)) - negpart(o, f0(i, j, k))) + (pospart(o, f1(i, j - 1, k)) - negpart(o, f1(i, j, k)));
+      dd = (pospart(o, f0(i, j, k)) - negpart(o, f0(i - 1, j, k))) + (pospart(o, f1(i, j, k)) - negpart(o, f1(i, j - 1, k)));
+    } else {
+      mx = dmax(pmax(i, j, k), dmax(c, dmax(p(i + 1, j, k), dmax(p(i - 1, j, k), dmax(p(i, j + 1, k), dmax(p(i, j - 1, k), dmax(p(i, j, k + 1), p(i, j, k - 1))))))));
+      mn = dmin(pmin(i, j, k), dmin(p(i, j + 1, k), dmin(p(i - 1, j, k), dmin(c, dmin(p(i + 1, j, k), dmin(p(i, j, k + 1), dmin(p(i, j, k - 1), p(i, j - 1, k))))))));
+      du = (pospart(o, f0(i - 1, j, k)) - negpart(o, f0(i, j, k))) + (pospart(o, f1(i, j - 1, k)) - negpart(o, f1(i, j, k)))
+         + (pospart(o, f2(i, j, k - 1)) - negpart(o, f2(i, j, k)));
+      dd = (pospart(o, f0(i, j, k)) - negpart(o, f0(i - 1, j, k))) + (pospart(o, f1(i, j, k)) - negpart(o, f1(i, j - 1, k)))
+         + (pospart(o, f2(i, j, k)) - negpart(o, f2(i, j, k - 1)));
+    }
+    bu(i, j, k) = fct_frac((mx - c) * T(1), du);
+    bd(i, j, k) = fct_frac((c - mn) * T(1), dd);
+  }
+};
+
+// GC_mono (formulae_mpdata_fct_{1,2,3}d.hpp)
+template <int ND, int D, class T>
+struct op_gc_mono {
+  dfield<T> out, corr, p, bu, bd;
+  unsigned o;
+  __device__ void operator()(int a, int b, int c) const {
+    const T C = P<ND, D>(corr, a, b, c);
+    const T bd0 = P<ND, D>(bd, a, b, c), bu1 = P<ND, D>(bu, a + 1, b, c);
+    const T bu0 = P<ND, D>(bu, a, b, c), bd1 = P<ND, D>(bd, a + 1, b, c);
+    T l;
+    const bool absv = (o & o_abs) && !(o & o_iga);
+    if (!absv) l = C > T(0) ? dmin(T(1), dmin(bd0, bu1)) : dmin(T(1), dmin(bu0, bd1));
+    else if (C > T(0)) l = P<ND, D>(p, a, b, c) > T(0) ? dmin(T(1), dmin(bd0, bu1)) : dmin(T(1), dmin(bu0, bd1));
+    else l = P<ND, D>(p, a + 1, b, c) > T(0) ? dmin(T(1), dmin(bu0, bd1)) : dmin(T(1), dmin(bd0, bu1));
+    P<ND, D>(out, a, b, c) = C * l;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// halo fills (runtime dimension; frame ranges b x c)
+template <class T>
+__global__ void k_halo_copy(dfield<T> A, int nd, int d, int dst, int src, int cnt, int bf, int nb, int cf, int nc) {
+  const long long tot = (long long)cnt * nb * nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int c = cf + int(q % nc);
+    const long long r = q / nc;
+    const int b = bf + int(r % nb);
+    const int t = int(r / nb);
+    PR(A, nd, d, dst + t, b, c) = PR(A, nd, d, src + t, b, c);
+  }
+}
+// A(pi(f + t, b, c)) = edge >= -1000000 ? A(pi(edge, b, c)) : val
+template <class T>
+__global__ void k_halo_set(dfield<T> A, int nd, int d, int f, int cnt, int edge, bool use_edge, T val, int bf, int nb, int cf, int nc) {
+  const long long tot = (long long)cnt * nb * nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int c = cf + int(q % nc);
+    const long long r = q / nc;
+    const int b = bf + int(r % nb);
+    const int t = int(r / nb);
+    PR(A, nd, d, f + t, b, c) = use_edge ? PR(A, nd, d, edge, b, c) : val;
+  }
+}
+// open zero-divergence fill of the along-halo (open_2d.hpp:71-91, 167-186; open_3d.hpp:101-125, 227-243)
+template <class T>
+__global__ void k_zero_div(dfield<T> Ad, dfield<T> A1, dfield<T> A2, int nd, int d, int side, int e, int f, int cnt,
+                           int bf, int nb, int cf, int nc) {
+  const long long tot = (long long)cnt * nb * nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int c = cf + int(q % nc);
+    const long long r = q / nc;
+    const int b = bf + int(r % nb);
+    const int ii = f + int(r / nb);
+    T v;
+    if (side == 0) {
+      v = PR(Ad, nd, d, e, b, c) - (PR(A1, nd, d, e, b - 1, c) - PR(A1, nd, d, e, b, c));
+      if (nd == 3) v = v - (PR(A2, nd, d, e, b, c - 1) - PR(A2, nd, d, e, b, c));
+    } else {
+      v = PR(Ad, nd, d, e - 1, b, c) + (PR(A1, nd, d, e, b - 1, c) - PR(A1, nd, d, e, b, c));
+      if (nd == 3) v = v + (PR(A2, nd, d, e, b, c - 1) - PR(A2, nd, d, e, b, c));
+    }
+    PR(Ad, nd, d, ii, b, c) = v;
+  }
+}
+
+static unsigned grid_for(long long tot) {
+  unsigned g = ceil_div(tot, 256);
+  if (g > 65535u * 8u) g = 65535u * 8u;
+  return g < 1 ? 1 : g;
+}
+
+// ---------------------------------------------------------------------------
+// sequencer (host)
+
+template <class T>
+void general<T>::fill_sclr(int d, int side, field<T> &A, rng rb, rng rc, bool deriv) {
+  auto &S = *s;
+  const int kind = S.bcs[d][side];
+  const int nd = S.nd, H = S.H, n = S.n[d];
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  const long long tot = (long long)H * rb.n() * rc.n();
+  if (kind == MPDX_BC_CYCLIC) {
+    // left: [-H, -1] <- [n-1-H, n-2];  right: [n, n+H-1] <- [1, H]  (cyclic_{1,2,3}d.hpp)
+    const int dst = side == 0 ? -H : n, src = side == 0 ? n - 1 - H : 1;
+    k_halo_copy<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, dst, src, H, rb.f, rb.n(), rc.f, rc.n());
+  } else if (kind == MPDX_BC_OPEN) {
+    // zero-gradient (open_{1,2,3}d.hpp fill_halos_sclr)
+    const int f = side == 0 ? -H : n, e = side == 0 ? 0 : n - 1;
+    k_halo_set<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, f, H, e, !deriv, T(0), rb.f, rb.n(), rc.f, rc.n());
+  } else {
+    throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for scalars on this path");
+  }
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::fill_vctr_nrml(int d, int side, field<T> &A, rng rb, rng rc) {
+  auto &S = *s;
+  const int kind = S.bcs[d][side];
+  if (kind == MPDX_BC_CYCLIC) { fill_sclr(d, side, A, rb, rc); return; }
+  if (kind != MPDX_BC_OPEN) throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for vectors on this path");
+  const int nd = S.nd, H = S.H, n = S.n[d];
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  const int f = side == 0 ? -H : n;
+  const long long tot = (long long)H * rb.n() * rc.n();
+  k_halo_set<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, f, H, 0, false, T(0), rb.f, rb.n(), rc.f, rc.n());
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::fill_vctr_alng(int d, int side, field<T> *AV, rng rb, rng rc, bool ad, bool cyclic_only) {
+  auto &S = *s;
+  const int kind = S.bcs[d][side];
+  const int nd = S.nd, H = S.H, n = S.n[d];
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  if (kind == MPDX_BC_CYCLIC) {
+    // left: [-H, -1] <- [n-1-H, n-2];  right: [n-1, n+H-2] <- [0, H-1]
+    const int dst = side == 0 ? -H : n - 1, src = side == 0 ? n - 1 - H : 0;
+    const long long tot = (long long)H * rb.n() * rc.n();
+    k_halo_copy<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, nd, d, dst, src, H, rb.f, rb.n(), rc.f, rc.n());
+    MPDX_LAUNCH_CHECK();
+    return;
+  }
+  if (cyclic_only) return;
+  if (kind != MPDX_BC_OPEN) throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for vectors on this path");
+  if (nd == 1) {  // open_1d.hpp:36-40, 66-70
+    int f, cnt, src;
+    if (side == 0) { f = -H; cnt = H - (ad ? 1 : 0); src = 0; }
+    else { f = n - 1 + (ad ? 1 : 0); cnt = H - (ad ? 1 : 0); src = n - 1 - H; }
+    if (cnt > 0) {
+      k_halo_set<T><<<1, 32, 0, S.stream>>>(AV[0].v, 1, 0, f, cnt, src, true, T(0), 0, 1, 0, 1);
+      MPDX_LAUNCH_CHECK();
+    }
+    return;
+  }
+  const int e = side == 0 ? 0 : n - 1;
+  const int d1 = (d + 1) % nd, d2 = (d + 2) % nd;
+  // zero the perpendicular components on the domain edge lines (open_2d.hpp:77-82, open_3d.hpp:72-94)
+  if (nd == 2) {
+    if (d == 0) {
+      k_halo_set<T><<<1, 32, 0, S.stream>>>(AV[d1].v, nd, d, e, 1, 0, false, T(0), rb.f - 1, 1, 0, 1);
+      k_halo_set<T><<<1, 32, 0, S.stream>>>(AV[d1].v, nd, d, e, 1, 0, false, T(0), rb.l, 1, 0, 1);
+    }
+  } else {
+    if (d == 0) {
+      k_halo_set<T><<<grid_for(rb.n()), 256, 0, S.stream>>>(AV[d2].v, nd, d, e, 1, 0, false, T(0), rb.f, rb.n(), rc.f - 1, 1);
+      k_halo_set<T><<<grid_for(rb.n()), 256, 0, S.stream>>>(AV[d2].v, nd, d, e, 1, 0, false, T(0), rb.f, rb.n(), rc.l, 1);
+    }
+    if (d == 0 || d == 1) {
+      k_halo_set<T><<<grid_for(rc.n()), 256, 0, S.stream>>>(AV[d1].v, nd, d, e, 1, 0, false, T(0), rb.f - 1, 1, rc.f, rc.n());
+      k_halo_set<T><<<grid_for(rc.n()), 256, 0, S.stream>>>(AV[d1].v, nd, d, e, 1, 0, false, T(0), rb.l, 1, rc.f, rc.n());
+    }
+  }
+  MPDX_LAUNCH_CHECK();
+  int f, cnt;
+  if (side == 0) { f = -H; cnt = H - (ad ? 1 : 0); }
+  else { f = n - 1 + (ad ? 1 : 0); cnt = H - (ad ? 1 : 0); }
+  if (cnt <= 0) return;
+  const long long tot = (long long)cnt * rb.n() * rc.n();
+  k_zero_div<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, AV[d1].v, AV[nd == 3 ? d2 : d1].v, nd, d, side, e, f, cnt,
+                                                     rb.f, rb.n(), rc.f, rc.n());
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::xchng_sclr(field<T> &A, int ex, bool deriv) {
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) { for (int q = 0; q < 2; ++q) fill_sclr(0, q, A, {0, 0}, {0, 0}, deriv); return; }
+  if (S.nd == 2) {  // solver_2d.hpp:40-56
+    for (int q = 0; q < 2; ++q) fill_sclr(0, q, A, ext(ir[1], ex), {0, 0}, deriv);
+    for (int q = 0; q < 2; ++q) fill_sclr(1, q, A, ext(ir[0], ex), {0, 0}, deriv);
+    return;
+  }
+  // solver_3d.hpp:47-67
+  for (int q = 0; q < 2; ++q) fill_sclr(1, q, A, ext(ir[2], ex), ext(ir[0], ex), deriv);
+  for (int q = 0; q < 2; ++q) fill_sclr(0, q, A, ext(ir[1], ex), ext(ir[2], ex), deriv);
+  for (int q = 0; q < 2; ++q) fill_sclr(2, q, A, ext(ir[0], ex), ext(ir[1], ex), deriv);
+}
+
+template <class T>
+void general<T>::xchng_vctr_alng(field<T> *AV, bool ad, bool cyclic) {
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) { for (int q = 0; q < 2; ++q) fill_vctr_alng(0, q, AV, {0, 0}, {0, 0}, ad, cyclic); return; }
+  if (S.nd == 2) {  // solver_2d.hpp:63-88
+    for (int q = 0; q < 2; ++q) fill_vctr_alng(0, q, AV, ir[1], {0, 0}, ad, cyclic);
+    for (int q = 0; q < 2; ++q) fill_vctr_alng(1, q, AV, ir[0], {0, 0}, ad, cyclic);
+    return;
+  }
+  // solver_3d.hpp:73-103
+  for (int q = 0; q < 2; ++q) fill_vctr_alng(0, q, AV, ir[1], ir[2], ad, cyclic);
+  for (int q = 0; q < 2; ++q) fill_vctr_alng(1, q, AV, ir[2], ir[0], ad, cyclic);
+  for (int q = 0; q < 2; ++q) fill_vctr_alng(2, q, AV, ir[0], ir[1], ad, cyclic);
+}
+
+template <class T>
+void general<T>::xchng_vctr_nrml(field<T> *AV, int ex) {
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) return;
+  if (S.nd == 2) {  // solver_2d.hpp:171-202
+    for (int q = 0; q < 2; ++q) fill_vctr_nrml(1, q, AV[0], exh(ext(ir[0], ex)), {0, 0});
+    for (int q = 0; q < 2; ++q) fill_vctr_nrml(0, q, AV[1], exh(ext(ir[1], ex)), {0, 0});
+    return;
+  }
+  // solver_3d.hpp:207-286
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(1, q, AV[0], ext(ext(ir[2], ex), 1), exh(ext(ir[0], ex)));
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(2, q, AV[0], exh(ext(ir[0], ex)), ext(ext(ir[1], ex), 1));
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(0, q, AV[1], exh(ext(ir[1], ex)), ext(ext(ir[2], ex), 1));
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(2, q, AV[1], ext(ext(ir[0], ex), 1), exh(ext(ir[1], ex)));
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(0, q, AV[2], ext(ext(ir[1], ex), 1), exh(ext(ir[2], ex)));
+  for (int q = 0; q < 2; ++q) fill_vctr_nrml(1, q, AV[2], exh(ext(ir[2], ex)), ext(ext(ir[0], ex), 1));
+}
+
+template <class T>
+field<T> *general<T>::GC_unco(int iter) { return iter == 1 ? s->GC : (iter % 2 ? s->tmp1 : s->tmp0); }
+template <class T>
+field<T> *general<T>::GC_corr(int iter) { return iter % 2 ? s->tmp0 : s->tmp1; }
+template <class T>
+field<T> *general<T>::GCit(int iter) {
+  if (iter == 0) return s->GC;
+  if (s->opts & o_fct) return s->GC_mono;
+  return GC_corr(iter);
+}
+
+template <class T>
+template <int ND>
+void general<T>::antidiff_nd(field<T> *res, field<T> &psi, field<T> *G) {
+  auto &S = *s;
+  const unsigned o = S.opts;
+  const rng *ir = S.ir, *im = S.im;
+  if (ND == 1) {
+    launch_frame<1, 0>(S.stream, op_antidiff<1, 0, T>{res[0].v, psi.v, G[0].v, G[0].v, G[0].v, o}, im[0], {0, 0}, {0, 0});
+  } else if (ND == 2) {
+    launch_frame<2, 0>(S.stream, op_antidiff<2, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[1].v, o}, im[0], ir[1], {0, 0});
+    launch_frame<2, 1>(S.stream, op_antidiff<2, 1, T>{res[1].v, psi.v, G[1].v, G[0].v, G[0].v, o}, im[1], ir[0], {0, 0});
+  } else {
+    launch_frame<3, 0>(S.stream, op_antidiff<3, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[2].v, o}, im[0], ir[1], ir[2]);
+    launch_frame<3, 1>(S.stream, op_antidiff<3, 1, T>{res[1].v, psi.v, G[1].v, G[2].v, G[0].v, o}, im[1], ir[2], ir[0]);
+    launch_frame<3, 2>(S.stream, op_antidiff<3, 2, T>{res[2].v, psi.v, G[2].v, G[0].v, G[1].v, o}, im[2], ir[0], ir[1]);
+  }
+}
+
+template <class T>
+template <int ND>
+void general<T>::fluxes_nd(field<T> *F, field<T> &psi, field<T> *C, bool extended) {
+  auto &S = *s;
+  const unsigned o = S.opts;
+  auto R = [&](int d) { return extended ? ext(S.ir[d], 1) : S.ir[d]; };
+  auto RM = [&](int d) { return extended ? ext(S.im[d], 1) : S.im[d]; };
+  if (ND == 1) {
+    launch_frame<1, 0>(S.stream, op_flux<1, 0, T>{F[0].v, psi.v, C[0].v, o}, RM(0), {0, 0}, {0, 0});
+  } else if (ND == 2) {
+    launch_frame<2, 0>(S.stream, op_flux<2, 0, T>{F[0].v, psi.v, C[0].v, o}, RM(0), R(1), {0, 0});
+    launch_frame<2, 1>(S.stream, op_flux<2, 1, T>{F[1].v, psi.v, C[1].v, o}, RM(1), R(0), {0, 0});
+  } else {
+    launch_frame<3, 0>(S.stream, op_flux<3, 0, T>{F[0].v, psi.v, C[0].v, o}, RM(0), R(1), R(2));
+    launch_frame<3, 1>(S.stream, op_flux<3, 1, T>{F[1].v, psi.v, C[1].v, o}, RM(1), R(2), R(0));
+    launch_frame<3, 2>(S.stream, op_flux<3, 2, T>{F[2].v, psi.v, C[2].v, o}, RM(2), R(0), R(1));
+  }
+}
+
+template <class T>
+template <int ND>
+void general<T>::fct_adjust_nd(int e, int iter) {
+  auto &S = *s;
+  field<T> &p = S.psi[e][S.tl[e]];
+  field<T> *corr = GC_corr(iter);
+  xchng_vctr_alng(corr, true);
+  xchng_vctr_nrml(corr, 0);
+  field<T> *flx = corr;
+  if (!(S.opts & o_iga)) { fluxes_nd<ND>(S.flux, p, corr, true); flx = S.flux; }
+  rng r0 = ext(S.ir[0], 1), r1 = ND > 1 ? ext(S.ir[1], 1) : rng{0, 0}, r2 = ND > 2 ? ext(S.ir[2], 1) : rng{0, 0};
+  const dfield<T> z = flx[0].v;
+  launch_frame<ND, 0>(S.stream, op_betas<ND, T>{S.beta_up.v, S.beta_dn.v, p.v, S.psi_max.v, S.psi_min.v, flx[0].v,
+                                                ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z, S.opts},
+                      r0, r1, r2);
+  const rng *ir = S.ir, *im = S.im;
+  if (ND == 1) {
+    launch_frame<1, 0>(S.stream, op_gc_mono<1, 0, T>{S.GC_mono[0].v, corr[0].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[0], {0, 0}, {0, 0});
+  } else if (ND == 2) {
+    launch_frame<2, 0>(S.stream, op_gc_mono<2, 0, T>{S.GC_mono[0].v, corr[0].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[0], ir[1], {0, 0});
+    launch_frame<2, 1>(S.stream, op_gc_mono<2, 1, T>{S.GC_mono[1].v, corr[1].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[1], ir[0], {0, 0});
+  } else {
+    launch_frame<3, 0>(S.stream, op_gc_mono<3, 0, T>{S.GC_mono[0].v, corr[0].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[0], ir[1], ir[2]);
+    launch_frame<3, 1>(S.stream, op_gc_mono<3, 1, T>{S.GC_mono[1].v, corr[1].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[1], ir[2], ir[0]);
+    launch_frame<3, 2>(S.stream, op_gc_mono<3, 2, T>{S.GC_mono[2].v, corr[2].v, p.v, S.beta_up.v, S.beta_dn.v, S.opts}, im[2], ir[0], ir[1]);
+  }
+}
+
+template <class T>
+template <int ND>
+void general<T>::advop_nd(int e) {
+  auto &S = *s;
+  if (S.opts & o_fct) {  // fct_init over i^1 x j^1 x k^1
+    rng r0 = ext(S.ir[0], 1), r1 = ND > 1 ? ext(S.ir[1], 1) : rng{0, 0}, r2 = ND > 2 ? ext(S.ir[2], 1) : rng{0, 0};
+    launch_frame<ND, 0>(S.stream, op_fct_init<ND, T>{S.psi_min.v, S.psi_max.v, S.psi[e][S.tl[e]].v}, r0, r1, r2);
+  }
+  for (int iter = 0; iter < S.n_iters; ++iter) {
+    if (iter != 0) {
+      S.tl[e] ^= 1;  // cycle(e)
+      xchng_sclr(S.psi[e][S.tl[e]], S.H);
+      field<T> *corr = GC_corr(iter);
+      antidiff_nd<ND>(corr, S.psi[e][S.tl[e]], GC_unco(iter));
+      if (!(S.opts & o_fct) && iter != S.n_iters - 1) xchng_vctr_nrml(corr, 0);
+      if (S.opts & o_fct) fct_adjust_nd<ND>(e, iter);
+    }
+    field<T> &p = S.psi[e][S.tl[e]];
+    field<T> *flx = S.flux;
+    if (!(S.opts & o_iga) || iter == 0) fluxes_nd<ND>(S.flux, p, GCit(iter), false);
+    else flx = GCit(iter);
+    const dfield<T> z = flx[0].v;
+    launch_frame<ND, 0>(S.stream, op_donorcell<ND, T>{S.psi[e][S.tl[e] ^ 1].v, p.v, flx[0].v, ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z},
+                        S.ir[0], ND > 1 ? S.ir[1] : rng{0, 0}, ND > 2 ? S.ir[2] : rng{0, 0});
+  }
+}
+
+// divergence of the advector: max |div GC| over the interior (solver_{2,3}d.hpp max_abs_vctr_div)
+template <class T>
+__global__ void k_max_abs_div(int nd, int n0, int n1, int n2, dfield<T> g0, dfield<T> g1, dfield<T> g2, double *out) {
+  double m = 0;
+  const long long tot = (long long)n0 * n1 * n2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int k = int(q % n2);
+    const long long r = q / n2;
+    const int j = int(r % n1), i = int(r / n1);
+    T v;
+    if (nd == 1) v = fabs(g0(i, j, k) - g0(i - 1, j, k));
+    else if (nd == 2) v = fabs((g0(i, j, k) - g0(i - 1, j, k)) + (g1(i, j, k) - g1(i, j - 1, k)));
+    else v = fabs((g0(i, j, k) - g0(i - 1, j, k)) + (g1(i, j, k) - g1(i, j - 1, k)) + (g2(i, j, k) - g2(i, j, k - 1)));
+    m = fmax(m, double(v));
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long *>(out), (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+template <class T>
+void general<T>::ante_loop(double *dev_scratch) {
+  auto &S = *s;
+  xchng_vctr_alng(S.GC);
+  if (S.nd > 1 && !(S.opts & o_dfl)) {
+    MPDX_CUDA(cudaMemsetAsync(dev_scratch, 0, sizeof(double), S.stream));
+    const dfield<T> z = S.GC[0].v;
+    k_max_abs_div<T><<<grid_for(S.cells()), 256, 0, S.stream>>>(S.nd, S.n[0], S.n[1], S.n[2], S.GC[0].v,
+                                                                S.nd > 1 ? S.GC[1].v : z, S.nd > 2 ? S.GC[2].v : z, dev_scratch);
+    MPDX_LAUNCH_CHECK();
+    double m = 0;
+    MPDX_CUDA(cudaMemcpyAsync(&m, dev_scratch, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+    MPDX_CUDA(cudaStreamSynchronize(S.stream));
+    if (T(m) > S.max_abs_div_eps) throw error(MPDX_E_DIVERGENT, "libmpdata++: initial advector field is divergent");
+  }
+  if (S.nd > 1) xchng_vctr_nrml(S.GC, S.H - 1);
+}
+
+template <class T>
+void general<T>::step() {
+  auto &S = *s;
+  for (int e = 0; e < S.n_eqns; ++e) {
+    xchng_sclr(S.psi[e][S.tl[e]], S.H);  // solve_loop_body: xchng(e)
+    if (S.nd == 1) advop_nd<1>(e);
+    else if (S.nd == 2) advop_nd<2>(e);
+    else advop_nd<3>(e);
+    S.tl[e] ^= 1;  // cycle(e)
+  }
+}
+
+template struct general<float>;
+template struct general<double>;
+
+}  // namespace mpdx

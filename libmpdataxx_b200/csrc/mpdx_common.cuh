@@ -1,0 +1,100 @@
+// Shared definitions of the libmpdataxx_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/mpdx.h"
+
+namespace mpdx {
+
+// option bits (libmpdata++/opts.hpp:34-49)
+enum : unsigned {
+  o_fct = 1u << 0, o_abs = 1u << 1, o_tot = 1u << 2, o_pfc = 1u << 3,
+  o_npa = 1u << 4, o_iga = 1u << 5, o_nug = 1u << 6, o_dfl = 1u << 7,
+  o_khn = 1u << 8, o_div_2nd = 1u << 9, o_div_3rd = 1u << 10,
+  o_div_3rd_dt = 1u << 11, o_fot = 1u << 12
+};
+
+struct error : std::runtime_error {
+  mpdx_status code;
+  error(mpdx_status c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define MPDX_CUDA(call)                                                                     \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::mpdx::error(MPDX_E_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));   \
+  } while (0)
+
+#define MPDX_LAUNCH_CHECK() MPDX_CUDA(cudaGetLastError())
+
+struct rng {
+  int f, l;
+  int n() const { return l - f + 1; }
+};
+inline rng ext(rng r, int n) { return {r.f - n, r.l + n}; }  // r^n
+inline rng exh(rng r) { return {r.f - 1, r.l}; }             // r^h
+
+// Device view of a field stored with its halo: element (i, j, k) lives at
+// o[i*s0 + j*s1 + k*s2]; unused dimensions are pinned to index 0.
+template <class T>
+struct dfield {
+  T *o = nullptr;
+  long long s0 = 0, s1 = 0, s2 = 0;
+  __host__ __device__ __forceinline__ T &operator()(int i, int j, int k) const {
+    return o[i * s0 + j * s1 + k * s2];
+  }
+};
+
+// Owning device allocation of one field (scalar, or one vector component).
+// The fastest-varying dimension is padded so that index 0 of every row sits on
+// a 128-byte boundary; rows have a pitch that is a multiple of 128 bytes.
+template <class T>
+struct field {
+  void *base = nullptr;
+  size_t bytes = 0;
+  int nd = 0;
+  rng r[3] = {{0, 0}, {0, 0}, {0, 0}};
+  dfield<T> v;
+  field() = default;
+  field(const field &) = delete;
+  field &operator=(const field &) = delete;
+  field(field &&o) noexcept { *this = std::move(o); }
+  field &operator=(field &&o) noexcept {
+    std::swap(base, o.base); std::swap(bytes, o.bytes); nd = o.nd;
+    for (int q = 0; q < 3; ++q) r[q] = o.r[q];
+    v = o.v; return *this;
+  }
+  ~field() { if (base) cudaFree(base); }
+
+  void alloc(int nd_, const rng *rr) {
+    nd = nd_;
+    for (int q = 0; q < 3; ++q) r[q] = q < nd ? rr[q] : rng{0, 0};
+    const int align = int(128 / sizeof(T));
+    const int f = nd - 1;  // fastest dimension
+    const int front = ((-r[f].f) + align - 1) / align * align;
+    const long long pitch = ((long long)front + r[f].l + 1 + align - 1) / align * align;
+    long long s[3] = {0, 0, 0};
+    s[f] = 1;
+    long long acc = pitch;
+    for (int q = f - 1; q >= 0; --q) { s[q] = acc; acc *= r[q].n(); }
+    bytes = size_t(acc) * sizeof(T);
+    MPDX_CUDA(cudaMalloc(&base, bytes));
+    MPDX_CUDA(cudaMemset(base, 0, bytes));
+    long long off = front;
+    for (int q = 0; q < f; ++q) off += (long long)(-r[q].f) * s[q];
+    v.o = static_cast<T *>(base) + off;
+    v.s0 = s[0]; v.s1 = s[1]; v.s2 = s[2];
+    // indices of unused dimensions are always 0; give them stride 0
+    for (int q = nd; q < 3; ++q) (q == 0 ? v.s0 : q == 1 ? v.s1 : v.s2) = 0;
+  }
+};
+
+inline unsigned ceil_div(long long a, long long b) { return unsigned((a + b - 1) / b); }
+
+}  // namespace mpdx

@@ -1,0 +1,398 @@
+// Solver handles and the C ABI (include/mpdx.h).
+//
+// A handle owns the device fields of one solver (libmpdata++'s sharedmem),
+// a CUDA stream, and small scratch buffers.  Host data enters and leaves only
+// through mpdx_set_field / mpdx_get_field / mpdx_stats.
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "boussinesq.cuh"
+#include "fused.cuh"
+#include "general.cuh"
+#include "stats.cuh"
+
+namespace mpdx {
+
+// ---------------------------------------------------------------------------
+// host <-> field transfers: contiguous staging buffer on the device, then a
+// gather/scatter kernel between C-ordered views and the padded halo'ed field.
+template <class T>
+__global__ void k_view_copy(dfield<T> f, T *buf, int e0, int e1, int e2, int o0, int o1, int o2, bool to_field) {
+  const long long tot = (long long)e0 * e1 * e2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int c = int(q % e2);
+    const long long r = q / e2;
+    const int b = int(r % e1), a = int(r / e1);
+    T &x = f(a + o0, b + o1, c + o2);
+    if (to_field) x = buf[q];
+    else buf[q] = x;
+  }
+}
+
+struct solver_base {
+  virtual ~solver_base() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int dtype = 8;
+  virtual void set_field(int kind, int idx, const void *src, bool device) = 0;
+  virtual void get_field(int kind, int idx, void *dst, bool device) = 0;
+  virtual void view_extent(int kind, int idx, int ex[3]) = 0;
+  virtual void advance(long long nt) = 0;
+  virtual void stats(mpdx_step_stats *out) = 0;
+};
+
+// common transfer machinery for solvers built on mpdata_state<T>
+template <class T>
+struct transfer {
+  T *staging = nullptr;
+  size_t cap = 0;
+  ~transfer() { if (staging) cudaFree(staging); }
+  void ensure(size_t n) {
+    if (n <= cap) return;
+    if (staging) cudaFree(staging);
+    staging = nullptr;
+    MPDX_CUDA(cudaMalloc(&staging, n * sizeof(T)));
+    cap = n;
+  }
+  // view (e0 x e1 x e2) at field offset (o0, o1, o2)
+  void put(cudaStream_t s, field<T> &f, const void *src, bool device, const int ex[3], const int off[3]) {
+    const size_t n = size_t(ex[0]) * ex[1] * ex[2];
+    const T *dsrc = static_cast<const T *>(src);
+    if (!device) {
+      ensure(n);
+      MPDX_CUDA(cudaMemcpyAsync(staging, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+      dsrc = staging;
+    }
+    k_view_copy<T><<<std::max(1u, std::min(ceil_div(n, 256), 65535u * 4)), 256, 0, s>>>(
+        f.v, const_cast<T *>(dsrc), ex[0], ex[1], ex[2], off[0], off[1], off[2], true);
+    MPDX_LAUNCH_CHECK();
+    MPDX_CUDA(cudaStreamSynchronize(s));
+  }
+  void get(cudaStream_t s, field<T> &f, void *dst, bool device, const int ex[3], const int off[3]) {
+    const size_t n = size_t(ex[0]) * ex[1] * ex[2];
+    T *ddst = static_cast<T *>(dst);
+    if (!device) { ensure(n); ddst = staging; }
+    k_view_copy<T><<<std::max(1u, std::min(ceil_div(n, 256), 65535u * 4)), 256, 0, s>>>(
+        f.v, ddst, ex[0], ex[1], ex[2], off[0], off[1], off[2], false);
+    MPDX_LAUNCH_CHECK();
+    if (!device) MPDX_CUDA(cudaMemcpyAsync(dst, staging, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    MPDX_CUDA(cudaStreamSynchronize(s));
+  }
+};
+
+template <class T>
+struct mpdata_solver : solver_base {
+  mpdata_state<T> st;
+  general<T> gen{&st};
+  transfer<T> xfer;
+  stats_engine<T> stat;
+  fused_engine<T> fus;
+  int path = MPDX_PATH_AUTO, last_path = MPDX_PATH_GENERAL;
+  double *scratch = nullptr;
+
+  mpdata_solver(const mpdx_config &c) {
+    dtype = sizeof(T);
+    MPDX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    st.stream = stream;
+    st.setup(c.n_dims, c.grid, c.n_eqns, unsigned(c.opts), c.n_iters, c.bcs);
+    st.max_abs_div_eps = c.max_abs_div_eps < 0 ? std::numeric_limits<T>::epsilon() : T(c.max_abs_div_eps);
+    path = c.path;
+    MPDX_CUDA(cudaMalloc(&scratch, 64));
+    fus.init(st);
+    if (path == MPDX_PATH_FUSED && !fus.configurable(st))
+      throw error(MPDX_E_UNSUPPORTED, "fused path requested but not available for this configuration");
+  }
+  ~mpdata_solver() override { if (scratch) cudaFree(scratch); }
+
+  void view(int kind, int idx, int ex[3], int off[3], field<T> *&f) {
+    if (kind == MPDX_FIELD_ADVECTEE) {
+      if (idx < 0 || idx >= st.n_eqns) throw error(MPDX_E_ARG, "equation index out of range");
+      for (int q = 0; q < 3; ++q) { ex[q] = st.n[q]; off[q] = 0; }
+      f = &st.psi[idx][st.tl[idx]];
+      return;
+    }
+    if (kind == MPDX_FIELD_ADVECTOR) {
+      if (idx < 0 || idx >= st.nd) throw error(MPDX_E_ARG, "advector component out of range");
+      st.advector_extent(idx, ex);
+      off[0] = -1; off[1] = idx == 1 ? -1 : 0; off[2] = idx == 2 ? -1 : 0;
+      f = &st.GC[idx];
+      return;
+    }
+    throw error(MPDX_E_ARG, "field kind not available for this solver");
+  }
+  void view_extent(int kind, int idx, int ex[3]) override {
+    int off[3]; field<T> *f; view(kind, idx, ex, off, f);
+  }
+  void set_field(int kind, int idx, const void *src, bool device) override {
+    int ex[3], off[3]; field<T> *f;
+    view(kind, idx, ex, off, f);
+    xfer.put(stream, *f, src, device, ex, off);
+    fus.invalidate();
+  }
+  void get_field(int kind, int idx, void *dst, bool device) override {
+    int ex[3], off[3]; field<T> *f;
+    view(kind, idx, ex, off, f);
+    xfer.get(stream, *f, dst, device, ex, off);
+  }
+  void advance(long long nt) override {
+    if (nt <= 0) return;
+    if (st.timestep == 0) gen.ante_loop(scratch);
+    bool use_fused = false;
+    if (path != MPDX_PATH_GENERAL && fus.configurable(st)) {
+      use_fused = fus.seams_consistent(st, scratch);
+      if (!use_fused && path == MPDX_PATH_FUSED)
+        throw error(MPDX_E_UNSUPPORTED, "fused path requested but the periodic seams of the fields are inconsistent");
+    }
+    last_path = use_fused ? MPDX_PATH_FUSED : MPDX_PATH_GENERAL;
+    for (long long t = 0; t < nt; ++t) {
+      if (use_fused) fus.step(st);
+      else gen.step();
+      ++st.timestep;
+    }
+  }
+  void stats(mpdx_step_stats *out) override {
+    std::memset(out, 0, sizeof(*out));
+    out->timestep = st.timestep;
+    stat.reduce(st, st.psi[0][st.tl[0]], out);
+    out->path = last_path;
+  }
+};
+
+// Boussinesq handle (solvers::boussinesq with GCR pressure solve)
+template <class T>
+struct boussinesq_solver : solver_base {
+  std::unique_ptr<boussinesq<T>> b;
+  transfer<T> xfer;
+  stats_engine<T> stat;
+  explicit boussinesq_solver(const mpdx_config &c) {
+    dtype = sizeof(T);
+    MPDX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    b.reset(new boussinesq<T>(c, stream));
+  }
+  void view(int kind, int idx, int ex[3], int off[3], field<T> *&f) {
+    auto &st = b->st;
+    for (int q = 0; q < 3; ++q) { ex[q] = st.n[q]; off[q] = 0; }
+    if (kind == MPDX_FIELD_ADVECTEE) {
+      if (idx < 0 || idx >= st.n_eqns) throw error(MPDX_E_ARG, "equation index out of range");
+      f = &st.psi[idx][st.tl[idx]];
+      return;
+    }
+    if (kind == MPDX_FIELD_SCLR_ARRAY) {
+      if (idx != MPDX_SCLR_THT_E) throw error(MPDX_E_ARG, "unknown scalar array");
+      f = &b->tht_e;
+      return;
+    }
+    if (kind == MPDX_FIELD_PRESSURE) { f = b->phi_field(); if (!f) throw error(MPDX_E_ARG, "pressure stored in FP64; use the FP64 accessor"); return; }
+    throw error(MPDX_E_ARG, "field kind not available for this solver");
+  }
+  void view_extent(int kind, int idx, int ex[3]) override {
+    int off[3]; field<T> *f; view(kind, idx, ex, off, f);
+  }
+  void set_field(int kind, int idx, const void *src, bool device) override {
+    int ex[3], off[3]; field<T> *f;
+    view(kind, idx, ex, off, f);
+    xfer.put(stream, *f, src, device, ex, off);
+  }
+  void get_field(int kind, int idx, void *dst, bool device) override {
+    int ex[3], off[3]; field<T> *f;
+    view(kind, idx, ex, off, f);
+    xfer.get(stream, *f, dst, device, ex, off);
+  }
+  void advance(long long nt) override { b->advance(nt); }
+  void stats(mpdx_step_stats *out) override {
+    std::memset(out, 0, sizeof(*out));
+    auto &st = b->st;
+    out->timestep = st.timestep;
+    out->time = double(st.timestep) * b->dt;
+    stat.reduce(st, st.psi[b->ix_tht][st.tl[b->ix_tht]], out);
+    out->gcr_iters = b->iters;
+    out->gcr_iters_total = b->iters_total;
+    out->gcr_residual = b->last_residual;
+    out->path = MPDX_PATH_GENERAL;
+  }
+};
+
+}  // namespace mpdx
+
+struct mpdx_solver {
+  std::unique_ptr<mpdx::solver_base> impl;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+mpdx_status guarded(mpdx_handle h, F f) {
+  if (!h || !h->impl) return MPDX_E_ARG;
+  try {
+    f();
+    h->impl->err.clear();
+    return MPDX_OK;
+  } catch (const mpdx::error &e) {
+    h->impl->err = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    h->impl->err = e.what();
+    return MPDX_E_ARG;
+  }
+}
+
+void validate(const mpdx_config &c) {
+  using namespace mpdx;
+  if (c.n_dims < 1 || c.n_dims > 3) throw error(MPDX_E_ARG, "n_dims must be 1, 2 or 3");
+  for (int d = 0; d < c.n_dims; ++d)
+    if (c.grid[d] < 1) throw error(MPDX_E_GRID, "libmpdata++: bogus grid size");
+  if (c.dtype != 4 && c.dtype != 8) throw error(MPDX_E_ARG, "dtype must be 4 or 8");
+  if (c.n_eqns < 1) throw error(MPDX_E_ARG, "n_eqns must be positive");
+  if (c.n_iters < 1) throw error(MPDX_E_ARG, "n_iters must be positive");
+  const unsigned o = unsigned(c.opts);
+  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga;
+  if (o & ~built)
+    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot(1D) pfc npa iga)");
+  if ((o & o_iga) && (o & o_abs)) throw error(MPDX_E_ARG, "abs & iga options are mutually exclusive");
+  if ((o & o_tot) && c.n_dims > 1) throw error(MPDX_E_UNSUPPORTED, "tot option is built for 1D only on this backend");
+  for (int q = 0; q < 2 * c.n_dims; ++q) {
+    const int k = c.bcs[q];
+    if (k != MPDX_BC_CYCLIC && k != MPDX_BC_OPEN && k != MPDX_BC_RIGID) throw error(MPDX_E_ARG, "unknown boundary kind");
+    if (k == MPDX_BC_RIGID && c.solver != MPDX_SOLVER_BOUSSINESQ)
+      throw error(MPDX_E_UNSUPPORTED, "rigid boundaries are built for the Boussinesq solver only");
+  }
+}
+}  // namespace
+
+extern "C" {
+
+void mpdx_config_default(mpdx_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->solver = MPDX_SOLVER_MPDATA;
+  c->n_dims = 1;
+  c->n_eqns = 1;
+  c->grid[0] = c->grid[1] = c->grid[2] = 1;
+  c->opts = mpdx::o_iga | mpdx::o_fct;  // ct_params_default_t::opts (opts.hpp:83)
+  c->n_iters = 2;                       // mpdata_common.hpp:77
+  c->dtype = 8;
+  c->dt = 0;
+  c->di = c->dj = c->dk = 1;
+  c->max_abs_div_eps = -1;
+  c->path = MPDX_PATH_AUTO;
+  c->prs_scheme = MPDX_PRS_CR;
+  c->prs_k_iters = 4;                   // ct_params_default_t::prs_k_iters (opts.hpp:91)
+  c->prs_tol = 1e-7;
+  c->g = 9.81;                          // boussinesq_common.hpp:34
+  c->tht_ref = 0;
+  c->ix_u = 0; c->ix_v = -1; c->ix_w = 1; c->ix_tht = 2;
+  c->precond = MPDX_PRECOND_IDENTITY;
+  c->prs_fp64 = 0;
+}
+
+mpdx_status mpdx_create(const mpdx_config *cfg, mpdx_handle *out) {
+  g_create_error.clear();
+  if (!cfg || !out) { g_create_error = "null argument"; return MPDX_E_ARG; }
+  *out = nullptr;
+  try {
+    validate(*cfg);
+    auto h = std::make_unique<mpdx_solver>();
+    if (cfg->solver == MPDX_SOLVER_BOUSSINESQ) {
+      if (cfg->dtype == 8) h->impl.reset(new mpdx::boussinesq_solver<double>(*cfg));
+      else h->impl.reset(new mpdx::boussinesq_solver<float>(*cfg));
+    } else {
+      if (cfg->dtype == 8) h->impl.reset(new mpdx::mpdata_solver<double>(*cfg));
+      else h->impl.reset(new mpdx::mpdata_solver<float>(*cfg));
+    }
+    *out = h.release();
+    return MPDX_OK;
+  } catch (const mpdx::error &e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    return MPDX_E_ARG;
+  }
+}
+
+const char *mpdx_create_error(void) { return g_create_error.c_str(); }
+
+static void strided_pack(const void *src, void *dst, const int ex[3], const int64_t *st, int es, bool pack) {
+  // pack: strided src -> C-ordered dst;  !pack: C-ordered src -> strided dst
+  size_t q = 0;
+  const char *s = static_cast<const char *>(src);
+  char *d = static_cast<char *>(dst);
+  for (int a = 0; a < ex[0]; ++a)
+    for (int b = 0; b < ex[1]; ++b)
+      for (int c = 0; c < ex[2]; ++c, ++q) {
+        const int64_t o = (int64_t(a) * st[0] + int64_t(b) * st[1] + int64_t(c) * st[2]) * es;
+        if (pack) std::memcpy(d + q * es, s + o, es);
+        else std::memcpy(d + o, s + q * es, es);
+      }
+}
+
+mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, const int64_t *strides) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    if (!strides) { h->impl->set_field(kind, idx, host, false); return; }
+    int ex[3];
+    h->impl->view_extent(kind, idx, ex);
+    const int es = h->impl->dtype;
+    std::vector<char> tmp(size_t(ex[0]) * ex[1] * ex[2] * es);
+    strided_pack(host, tmp.data(), ex, strides, es, true);
+    h->impl->set_field(kind, idx, tmp.data(), false);
+  });
+}
+
+mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const int64_t *strides) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    if (!strides) { h->impl->get_field(kind, idx, host, false); return; }
+    int ex[3];
+    h->impl->view_extent(kind, idx, ex);
+    const int es = h->impl->dtype;
+    std::vector<char> tmp(size_t(ex[0]) * ex[1] * ex[2] * es);
+    h->impl->get_field(kind, idx, tmp.data(), false);
+    strided_pack(tmp.data(), host, ex, strides, es, false);
+  });
+}
+
+mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev) {
+  return guarded(h, [&] {
+    if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    h->impl->set_field(kind, idx, dev, true);
+  });
+}
+
+mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev) {
+  return guarded(h, [&] {
+    if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    h->impl->get_field(kind, idx, dev, true);
+  });
+}
+
+mpdx_status mpdx_advance(mpdx_handle h, int64_t nt) {
+  return guarded(h, [&] { h->impl->advance(nt); });
+}
+
+mpdx_status mpdx_sync(mpdx_handle h) {
+  return guarded(h, [&] { MPDX_CUDA(cudaStreamSynchronize(h->impl->stream)); });
+}
+
+mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
+  return guarded(h, [&] {
+    if (!out) throw mpdx::error(MPDX_E_ARG, "null output");
+    h->impl->stats(out);
+  });
+}
+
+void *mpdx_stream(mpdx_handle h) { return (h && h->impl) ? (void *)h->impl->stream : nullptr; }
+
+const char *mpdx_last_error(mpdx_handle h) { return (h && h->impl) ? h->impl->err.c_str() : "invalid handle"; }
+
+void mpdx_destroy(mpdx_handle h) {
+  if (!h) return;
+  if (h->impl && h->impl->stream) cudaStreamSynchronize(h->impl->stream);
+  delete h;
+}
+
+}  // extern "C"

@@ -180,11 +180,13 @@ def periodic_curl_3d(n, seed, n_modes=8, cmax=0.4, dtype=np.float32):
             a += amp * np.cos(2 * math.pi * (kv[0] * I + kv[1] * J + kv[2] * K) / P + ph)
         A.append(a)
     Ax, Ay, Az = A
-    r = lambda x, ax: np.roll(x, -1, ax)
-    # Ax on x-edges (i+1/2, j-1/2, k-1/2) etc.; face flux = circulation around the face
-    fx = (r(Az, 1) - Az) - (r(Ay, 2) - Ay)        # face (i+1/2, j, k) stored at (i, j, k) after shift below
-    fy = (r(Ax, 2) - Ax) - (r(Az, 0) - Az)
-    fz = (r(Ay, 0) - Ay) - (r(Ax, 1) - Ax)
+    # A on cell edges: Ax[i,j,k] at (i, j+1/2, k+1/2), Ay at (i+1/2, j, k+1/2), Az at (i+1/2, j+1/2, k);
+    # the flux through each face is the circulation of A around it, so the
+    # discrete divergence of every cell vanishes identically
+    b = lambda x, ax: np.roll(x, 1, ax)   # x[i-1]
+    fx = (Az - b(Az, 1)) - (Ay - b(Ay, 2))   # face (i+1/2, j, k)
+    fy = (Ax - b(Ax, 2)) - (Az - b(Az, 0))   # face (i, j+1/2, k)
+    fz = (Ay - b(Ay, 0)) - (Ax - b(Ax, 1))   # face (i, j, k+1/2)
     s = cmax / max(np.abs(fx).max(), np.abs(fy).max(), np.abs(fz).max())
     fx, fy, fz = [(f * s).astype(dtype).astype(np.float64) for f in (fx, fy, fz)]
     a0 = (np.arange(n) - 1) % P

@@ -56,9 +56,15 @@ struct arr {
     v.assign(size_t(s0) * size_t(r0.l - r0.f + 1), std::numeric_limits<T>::quiet_NaN());
   }
   inline T &operator()(int i, int j, int k) {
+#ifdef ORACLE_BOUNDS
+    if (!has(i, j, k)) throw std::runtime_error("oracle: index out of bounds");
+#endif
     return v[size_t((i - lo[0]) * s0 + (j - lo[1]) * s1 + (k - lo[2]))];
   }
   inline const T &operator()(int i, int j, int k) const {
+#ifdef ORACLE_BOUNDS
+    if (!has(i, j, k)) throw std::runtime_error("oracle: index out of bounds");
+#endif
     return v[size_t((i - lo[0]) * s0 + (j - lo[1]) * s1 + (k - lo[2]))];
   }
   bool has(int i, int j, int k) const {

@@ -1,0 +1,103 @@
+"""CPU-side checks of the C ABI: the library loads, exports every entry point
+that include/mpdx.h declares, its structs match the header's layout, and
+argument validation (which runs before any CUDA call) reports the reference's
+errors.  No kernel is launched here."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from libmpdataxx_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "mpdx.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(mpdx_[a-z_]+)\s*\(", txt)))
+
+
+def test_header_declares_python_binding_exports():
+    assert declared() == sorted(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.SO_PATH], capture_output=True, text=True, check=True).stdout
+    syms = set(re.findall(r" T (mpdx_\w+)", out))
+    for name in declared():
+        assert name in syms, name
+        assert hasattr(L, name)
+
+
+def test_struct_layout_matches_header():
+    src = f"""
+    #include <stdio.h>
+    #include <stddef.h>
+    #include "{HEADER}"
+    int main() {{
+      printf("%zu %zu %zu %zu\\n", sizeof(mpdx_config), offsetof(mpdx_config, prs_fp64),
+             sizeof(mpdx_step_stats), offsetof(mpdx_step_stats, path));
+      return 0;
+    }}"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-std=c99", "-o", exe, c], check=True)
+        vals = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals == [ctypes.sizeof(_lib.Config), _lib.Config.prs_fp64.offset,
+                    ctypes.sizeof(_lib.StepStats), _lib.StepStats.path.offset]
+
+
+def _cfg(**kw):
+    L = _lib.lib()
+    c = _lib.Config()
+    L.mpdx_config_default(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "grid":
+            for q, g in enumerate(v):
+                c.grid[q] = g
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def _create(c):
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    rc = L.mpdx_create(ctypes.byref(c), ctypes.byref(h))
+    msg = L.mpdx_create_error().decode()
+    if h:
+        L.mpdx_destroy(h)
+    return rc, msg
+
+
+def test_defaults_follow_reference():
+    c = _cfg()
+    from libmpdataxx_b200 import opts as o
+    assert c.opts == o.iga | o.fct and c.n_iters == 2 and c.prs_k_iters == 4 and c.g == 9.81
+
+
+def test_bogus_grid_size():
+    rc, msg = _create(_cfg(n_dims=2, grid=(0, 5, 1)))
+    assert rc == _lib.MPDX_E_GRID and msg == "libmpdata++: bogus grid size"
+
+
+def test_unsupported_option_rejected():
+    from libmpdataxx_b200 import opts as o
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.nug))
+    assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    rc, _ = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.iga | o.abs))
+    assert rc == _lib.MPDX_E_ARG
+
+
+def test_null_arguments():
+    L = _lib.lib()
+    assert L.mpdx_create(None, None) == _lib.MPDX_E_ARG
+    assert L.mpdx_advance(None, 1) == _lib.MPDX_E_ARG
+    assert L.mpdx_last_error(None) == b"invalid handle"

@@ -1,0 +1,141 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+FP64 results must match the oracle to 1e-12 relative (max |gpu - oracle| /
+max |oracle|), as the reference's own solver would on the same inputs; FP32
+results are compared with a tolerance stated per test and their error
+against an FP64 run is reported."""
+import numpy as np
+import pytest
+
+from libmpdataxx_b200 import bcond, concurr, opts as o, setups, solvers
+from oracle import Oracle
+from runners import load
+
+pytestmark = pytest.mark.gpu
+
+RTOL64 = 1e-12
+
+
+def make_run(grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64, path="general", max_abs_div_eps=None):
+    nd = len(grid)
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = dtype
+    ct.n_dims = nd
+    ct.n_eqns = n_eqns
+    ct.opts = opts
+    p = solvers.mpdata.rt_params_t(grid_size=list(grid), n_iters=n_iters, max_abs_div_eps=max_abs_div_eps)
+    bcs = bcs or ["cyclic"] * (2 * nd)
+    return concurr.cuda(solvers.mpdata(ct), *[getattr(bcond, b) for b in bcs], p=p, path=path)
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def random_setup(grid, bcs, seed, signed=False):
+    rng = np.random.default_rng(seed)
+    nd = len(grid)
+    psi = rng.uniform(0.5, 2.0, size=grid)
+    if signed:
+        psi = psi * np.where(rng.uniform(size=grid) < 0.3, -1.0, 1.0)
+    if nd == 1:
+        adv = [np.full(grid, 0.4)]
+    elif nd == 2:
+        adv = list(setups.periodic_curl_2d(grid[0], grid[1], seed, cmax=0.45))
+    else:
+        assert grid[0] == grid[1] == grid[2]
+        adv = list(setups.periodic_curl_3d(grid[0], seed, cmax=0.3, dtype=np.float64))
+    if all(b == "cyclic" for b in bcs):
+        psi = setups.wrap_periodic(psi[tuple(slice(0, g - 1) for g in grid)])
+    return {"grid": tuple(grid), "bcs": bcs, "advectee": [psi], "advector": adv}
+
+
+CASES = []
+for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
+    for bc in ("cyclic", "open"):
+        for opts, iters in [(0, 1), (0, 2), (o.fct, 2), (o.iga, 2), (o.iga | o.fct, 2), (o.fct, 3), (0, 3),
+                            (o.abs, 2), (o.abs | o.fct, 2), (o.pfc, 2), (o.npa | o.fct, 2)]:
+            CASES.append((nd, grid, bc, opts, iters))
+CASES.append((1, (37,), "cyclic", o.iga | o.tot, 2))
+CASES.append((1, (37,), "open", o.iga | o.tot | o.fct, 2))
+CASES.append((1, (37,), "cyclic", o.tot, 3))
+
+
+@pytest.mark.parametrize("nd,grid,bc,opts,iters", CASES)
+def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
+    bcs = [bc] * (2 * nd)
+    s = random_setup(grid, bcs, seed=nd * 100 + iters, signed=bool(opts & (o.abs | o.iga)))
+    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=1e-10)
+    load(orc, s)
+    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=1e-10)
+    run.set_advectee(s["advectee"][0])
+    for d, a in enumerate(s["advector"]):
+        run.set_advector(a, d)
+    for chunk in (1, 4):
+        orc.advance(chunk)
+        run.advance(chunk)
+        assert rel_err(run.advectee(), orc.advectee()) <= RTOL64
+
+
+def test_advector_view_roundtrip():
+    grid = (6, 7, 5)
+    run = make_run(grid, o.fct, max_abs_div_eps=1.0)
+    rng = np.random.default_rng(0)
+    for d in range(3):
+        a = rng.normal(size=run._shape(1, d))
+        run.set_advector(a, d)
+        np.testing.assert_array_equal(run.advector(d), a)
+
+
+def test_mirror_semantics():
+    """advectee() is a writable mirror: writes are seen by the next advance."""
+    s = setups.cone_bugs()
+    run = make_run(s["grid"], o.fct)
+    run.advectee()[...] = s["advectee"][0]
+    run.advector(0)[...] = s["advector"][0]
+    run.advector(1)[...] = s["advector"][1]
+    run.advance(2)
+    orc = Oracle(s["grid"], o.fct, bcs=s["bcs"])
+    load(orc, s)
+    orc.advance(2)
+    assert rel_err(run.advectee(), orc.advectee()) <= RTOL64
+
+
+def test_divergent_advector_raises():
+    s = setups.cone_bugs()
+    run = make_run(s["grid"], o.fct)
+    run.set_advectee(s["advectee"][0])
+    run.set_advector(s["advector"][0] + np.linspace(0, 0.1, s["grid"][0])[:, None], 0)
+    run.set_advector(s["advector"][1], 1)
+    with pytest.raises(RuntimeError, match="initial advector field is divergent"):
+        run.advance(1)
+
+
+def test_cone_bugs_fp32_exact_min():
+    """tests/unit/cone_bugs: FP32 fct never goes below the background."""
+    s = setups.cone_bugs()
+    run = make_run(s["grid"], o.fct, dtype=np.float32)
+    run.set_advectee(s["advectee"][0])
+    for d, a in enumerate(s["advector"]):
+        run.set_advector(a, d)
+    run.advance(s["nt"])
+    assert run.advectee().min() - 1 == 0
+
+
+def test_stats_mass_conserved():
+    grid = (33, 33)
+    s = random_setup(grid, ["cyclic"] * 4, seed=7)
+    run = make_run(grid, o.iga | o.fct, max_abs_div_eps=1e-10)
+    run.set_advectee(s["advectee"][0])
+    for d, a in enumerate(s["advector"]):
+        run.set_advector(a, d)
+    m0 = run.stats()["mass"]
+    run.advance(20)
+    st = run.stats()
+    assert st["timestep"] == 20
+    assert abs(st["mass"] - m0) <= 1e-12 * abs(m0)
+    psi = run.advectee()
+    assert st["min"] == psi.min() and st["max"] == psi.max()
