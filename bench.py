@@ -1,0 +1,307 @@
+"""Benchmark: MPDATA step throughput (cell-updates/s) against the HBM roofline.
+
+Workload (N = 1): 3D MPDATA, 512^3 cyclic, FP32 advection with FP64 mass sums,
+opts fct|iga, n_iters = 2, a divergence-free random-Fourier flow scaled to max
+Courant 0.4 and 5 Gaussian blobs (libmpdataxx_b200/workloads.py).  One step =
+one MPDATA+FCT step of the whole grid (one fused kernel launch).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun, one process per GPU) every rank advances its own replica
+(the path does not shard on one GPU: "replicas only"); value = all ranks' cell
+updates / the slowest rank's device time.
+
+--impl reference times the reference's CPU path on this host's cores: the CPU
+restatement in oracle/ (the reference itself cannot be built here: it needs
+Blitz++ and Boost), compiled with the reference's release flags plus OpenMP,
+on the same 512^3 configuration.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = 20  # FP32: psi^n 4 + GC 3 x 4 + psi^{n+1} 4
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        rows = [r for r in self.samples if len(r) >= 9]
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def build_run(w, dtype, torch):
+    from libmpdataxx_b200 import bcond, concurr, opts, solvers
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = {"float32": "float32", "float64": "float64"}[dtype]
+    ct.n_dims = 3
+    ct.n_eqns = 1
+    ct.opts = opts.fct | opts.iga
+    p = solvers.mpdata.rt_params_t(grid_size=list(w["grid"]), n_iters=2, max_abs_div_eps=1e-6)
+    run = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * 6, p=p)
+    from libmpdataxx_b200 import _lib
+    run.set_field_device(_lib.FIELD_ADVECTEE, 0, w["advectee"][0].data_ptr())
+    for d, a in enumerate(w["advector"]):
+        run.set_field_device(_lib.FIELD_ADVECTOR, d, a.data_ptr())
+    return run
+
+
+def cpu_baseline(n=160, steps=3):
+    """Oracle (CPU restatement, -Ofast + OpenMP on all host threads) on a
+    bounded sample: n^3 of the same configuration, `steps` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from libmpdataxx_b200 import opts, setups
+    from oracle import Oracle
+    gx, gy, gz = setups.periodic_curl_3d(n, 3, cmax=0.4, dtype=np.float32)
+    rng = np.random.default_rng(4)
+    psi = setups.wrap_periodic(rng.uniform(0, 1, size=(n - 1,) * 3))
+    orc = Oracle((n,) * 3, opts.fct | opts.iga, n_iters=2, dtype=np.float32, fast=True, max_abs_div_eps=1e-6)
+    orc.set_advectee(psi)
+    for d, a in enumerate((gx, gy, gz)):
+        orc.set_advector(a, d)
+    orc.advance(1)  # ante-loop checks and first touch
+    t0 = time.perf_counter()
+    orc.advance(steps)
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n ** 3 * steps / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{n}^3 fct|iga n_iters=2 FP32, {steps} steps, {dt:.1f} s, oracle -Ofast+OpenMP"}
+
+
+def reference_arm(args, rank):
+    """Each step advances a bounded sample of the workload: the same
+    configuration on an n_ref^3 grid (default 256^3, 1/8 of the cells), so that
+    K steps of the CPU path finish within minutes; the metric is per cell."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from libmpdataxx_b200 import opts, setups
+    from oracle import Oracle
+    n = args.n_ref
+    gx, gy, gz = setups.periodic_curl_3d(n, 3, cmax=0.4, dtype=np.float32)
+    rng = np.random.default_rng(4)
+    psi = setups.wrap_periodic(rng.uniform(0, 1, size=(n - 1,) * 3).astype(np.float32))
+    orc = Oracle((n,) * 3, opts.fct | opts.iga, n_iters=2, dtype=np.float32, fast=True, max_abs_div_eps=1e-6)
+    orc.set_advectee(psi)
+    for d, a in enumerate((gx, gy, gz)):
+        orc.set_advector(a, d)
+    for _ in range(args.warmup):
+        orc.advance(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.advance(1)
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = n ** 3 * args.steps / dt
+    line = {"impl": "reference", "metric": "cell-updates/s per MPDATA step", "value": value,
+            "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"3D MPDATA {args.n}^3 cyclic fct|iga n_iters=2 float32 (FP64 mass sums)",
+                       "grid": [args.n] * 3, "sample_grid": [n] * 3},
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": f"{n}^3 grid per step (bounded sample of the {args.n}^3 workload); CPU restatement of the reference "
+                                       "(reference unbuildable here: Blitz++/Boost absent), -Ofast + OpenMP"},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--n-ref", type=int, default=256)
+    ap.add_argument("--dtype", default="float32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from libmpdataxx_b200 import _lib, workloads
+    w = workloads.advection_3d(n=args.n, dtype=args.dtype)
+    run = build_run(w, args.dtype, torch)
+    n_cells = float(args.n) ** 3
+    stream = torch.cuda.ExternalStream(run.stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        run.advance(1)
+    run.sync()
+    assert run.stats()["path"] == _lib.PATH_FUSED, "fused path not taken"
+
+    # device-timed region: inputs resident in HBM, one fused launch per step
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            run.advance(1)
+            ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms_total = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * n_cells * args.steps / (ms_total / 1e3)
+
+    # end-to-end through the public API: every step uploads its inputs from
+    # pinned host memory, advances one step and reads the result back
+    host_in = [a.cpu().pin_memory() for a in w["advectee"] + w["advector"]]
+    host_out = torch.empty_like(w["advectee"][0], device="cpu").pin_memory()
+    itemsize = host_out.element_size()
+    h2d = sum(t.numel() for t in host_in) * itemsize
+    d2h = host_out.numel() * itemsize
+    e2e_steps = max(2, min(args.steps, 5))
+    run.sync()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        run.set_field(_lib.FIELD_ADVECTEE, 0, host_in[0].numpy())
+        for d in range(3):
+            run.set_field(_lib.FIELD_ADVECTOR, d, host_in[1 + d].numpy())
+        run.advance(1)
+        run.L.mpdx_get_field(run.h, _lib.FIELD_ADVECTEE, 0, host_out.data_ptr(), None)
+    run.sync()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n_cells * e2e_steps / e2e_s
+
+    if rank != 0:
+        return
+    hbm, src = peaks()
+    avg_launch_ms = statistics.mean(per)
+    achieved = BYTES_PER_CELL * n_cells / (avg_launch_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        key = f"fused3d_{args.dtype}_{args.n}"
+        if key in tj:
+            traffic = tj[key]
+    line = {
+        "metric": "cell-updates/s per MPDATA step", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.dtype == "float32" else "f64",
+        "data": "synthetic",
+        "config": {"workload": f"3D MPDATA {args.n}^3 cyclic fct|iga n_iters=2 {args.dtype} (FP64 mass sums)",
+                   "grid": [args.n] * 3, "opts": "fct|iga", "n_iters": 2, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 ({BYTES_PER_CELL * n_cells / 1e9:.2f} GB per step)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_source": src,
+                     "bytes_per_launch": BYTES_PER_CELL * n_cells, "avg_launch_ms": avg_launch_ms},
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line))
+    run.close()
+
+
+if __name__ == "__main__":
+    main()

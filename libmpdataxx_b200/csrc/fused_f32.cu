@@ -1,0 +1,9 @@
+// FP32 instantiation of the fused kernels (FMA contraction allowed).
+#include "fused_impl.cuh"
+
+namespace mpdx {
+template bool fused_configurable<float>(const mpdata_state<float> &);
+template void fused3d_launch<float>(mpdata_state<float> &, int, cudaStream_t);
+template void fused2d_launch<float>(mpdata_state<float> &, int, cudaStream_t);
+template bool fused_seams_consistent<float>(mpdata_state<float> &, double *);
+}  // namespace mpdx

@@ -1,0 +1,10 @@
+// FP64 instantiation of the fused kernels, compiled without FMA contraction so
+// that it reproduces the reference-structured path (and the reference) bitwise.
+#include "fused_impl.cuh"
+
+namespace mpdx {
+template bool fused_configurable<double>(const mpdata_state<double> &);
+template void fused3d_launch<double>(mpdata_state<double> &, int, cudaStream_t);
+template void fused2d_launch<double>(mpdata_state<double> &, int, cudaStream_t);
+template bool fused_seams_consistent<double>(mpdata_state<double> &, double *);
+}  // namespace mpdx

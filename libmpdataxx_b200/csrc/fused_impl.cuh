@@ -1,0 +1,157 @@
+// Launchers of the fused MPDATA kernels and the periodic-seam check.
+// Included once per real type (fused_f32.cu, fused_f64.cu) so that each type
+// gets its own compiler flags.
+#pragma once
+
+#include "fused.cuh"
+#include "fused2d.cuh"
+#include "fused3d.cuh"
+
+namespace mpdx {
+
+template <class T> struct tiles;
+template <> struct tiles<float> {
+  static constexpr int TY = 16, TZ = 32, NT3 = 256, LX3 = 128;   // 3D column tile, planes per CTA
+  static constexpr int NT2 = 256, LX2 = 64;                      // 2D strip width (threads), rows per CTA
+};
+template <> struct tiles<double> {
+  static constexpr int TY = 8, TZ = 32, NT3 = 256, LX3 = 128;
+  static constexpr int NT2 = 256, LX2 = 64;
+};
+
+template <class T>
+bool fused_configurable(const mpdata_state<T> &st) {
+  for (int d = 0; d < st.nd; ++d)
+    if (st.bcs[d][0] != MPDX_BC_CYCLIC || st.bcs[d][1] != MPDX_BC_CYCLIC) return false;
+  if (st.opts & ~(o_fct | o_iga)) return false;
+  if (st.nd == 3) {
+    return st.n_iters == 2 && st.n[0] - 1 >= 5 && st.n[1] - 1 >= tiles<T>::TY + 3 &&
+           st.n[2] - 1 >= tiles<T>::TZ + 3;
+  }
+  if (st.nd == 2) {
+    const bool ok_iters = st.n_iters == 2 || (st.n_iters == 3 && !(st.opts & o_iga));
+    return ok_iters && st.n[0] - 1 >= 2 && st.n[1] - 1 >= 2;
+  }
+  return false;
+}
+
+template <class K>
+static void set_smem(K kernel, size_t bytes) {
+  MPDX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+template <class T, bool IGA, bool FCT>
+static void launch3(const f3::args<T> &a, cudaStream_t s, dim3 grid) {
+  constexpr int TY = tiles<T>::TY, TZ = tiles<T>::TZ, NT = tiles<T>::NT3;
+  auto kern = f3::k_fused3d<T, IGA, FCT, TY, TZ, NT>;
+  const size_t bytes = size_t(f3::layout<TY, TZ>::total) * sizeof(T);
+  static bool attr = false;
+  if (!attr) { set_smem(kern, bytes); attr = true; }
+  kern<<<grid, NT, bytes, s>>>(a);
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
+  constexpr int TY = tiles<T>::TY, TZ = tiles<T>::TZ, LX = tiles<T>::LX3;
+  f3::args<T> a;
+  a.in = st.psi[e][st.tl[e]].v;
+  a.out = st.psi[e][st.tl[e] ^ 1].v;
+  a.g0 = st.GC[0].v; a.g1 = st.GC[1].v; a.g2 = st.GC[2].v;
+  a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1; a.P2 = st.n[2] - 1;
+  a.n0 = st.n[0]; a.n1 = st.n[1]; a.n2 = st.n[2];
+  a.LX = LX;
+  a.tiles_z = (a.P2 + TZ - 1) / TZ;
+  const int tiles_y = (a.P1 + TY - 1) / TY;
+  dim3 grid(tiles_y * a.tiles_z, (a.P0 + LX - 1) / LX);
+  const bool iga = st.opts & o_iga, fct = st.opts & o_fct;
+  if (iga && fct) launch3<T, true, true>(a, s, grid);
+  else if (iga) launch3<T, true, false>(a, s, grid);
+  else if (fct) launch3<T, false, true>(a, s, grid);
+  else launch3<T, false, false>(a, s, grid);
+}
+
+template <class T, int NI, bool IGA, bool FCT>
+static void launch2(const f2::prob<T> &a, cudaStream_t s) {
+  constexpr int NT = tiles<T>::NT2, LX = tiles<T>::LX2, H = NI == 3 ? 6 : 4;
+  auto kern = f2::k_fused2d<T, NI, IGA, FCT, NT, H>;
+  const size_t bytes = size_t(f2::rows<NI, FCT>::total) * NT * sizeof(T);
+  static bool attr = false;
+  if (!attr) { set_smem(kern, bytes); attr = true; }
+  dim3 grid((a.P1 + (NT - 2 * H) - 1) / (NT - 2 * H), (a.P0 + LX - 1) / LX);
+  kern<<<grid, NT, bytes, s>>>(a, LX);
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void fused2d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
+  f2::prob<T> a;
+  a.in = st.psi[e][st.tl[e]].v;
+  a.out = st.psi[e][st.tl[e] ^ 1].v;
+  a.g0 = st.GC[0].v; a.g1 = st.GC[1].v;
+  a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1;
+  a.n0 = st.n[0]; a.n1 = st.n[1];
+  const bool iga = st.opts & o_iga, fct = st.opts & o_fct;
+  if (st.n_iters == 3) {
+    if (fct) launch2<T, 3, false, true>(a, s);
+    else launch2<T, 3, false, false>(a, s);
+  } else {
+    if (iga && fct) launch2<T, 2, true, true>(a, s);
+    else if (iga) launch2<T, 2, true, false>(a, s);
+    else if (fct) launch2<T, 2, false, true>(a, s);
+    else launch2<T, 2, false, false>(a, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// seam check: the duplicate point n-1 must equal point 0 along every periodic
+// axis, for the advectees and for the transverse axes of the advector faces.
+template <class T>
+__device__ __forceinline__ bool same_bits(T a, T b) {
+  if (sizeof(T) == 8) return __double_as_longlong(double(a)) == __double_as_longlong(double(b));
+  return __float_as_int(float(a)) == __float_as_int(float(b));
+}
+
+// compare f(.., n_ax-1, ..) with f(.., 0, ..) over the box e0 x e1 x e2 (axis ax collapsed)
+template <class T>
+__global__ void k_seam(dfield<T> f, int ax, int last, int e0, int e1, int e2, unsigned *flag) {
+  const long long tot = (long long)e0 * e1 * e2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    int c = int(q % e2);
+    const long long r = q / e2;
+    int b = int(r % e1), a = int(r / e1);
+    int i0 = a, j0 = b, k0 = c, i1 = a, j1 = b, k1 = c;
+    if (ax == 0) { i0 = 0; i1 = last; }
+    if (ax == 1) { j0 = 0; j1 = last; }
+    if (ax == 2) { k0 = 0; k1 = last; }
+    if (!same_bits(f(i0, j0, k0), f(i1, j1, k1))) atomicOr(flag, 1u);
+  }
+}
+
+template <class T>
+bool fused_seams_consistent(mpdata_state<T> &st, double *scratch) {
+  unsigned *flag = reinterpret_cast<unsigned *>(scratch);
+  MPDX_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), st.stream));
+  auto check = [&](const field<T> &f, int ax, int face_ax) {
+    int e[3];
+    for (int d = 0; d < 3; ++d) e[d] = d < st.nd ? st.n[d] : 1;
+    if (face_ax >= 0) e[face_ax] = st.n[face_ax] - 1;  // unique faces 0..n-2
+    e[ax] = 1;
+    const long long tot = (long long)e[0] * e[1] * e[2];
+    unsigned g = ceil_div(tot, 256);
+    if (g > 4096) g = 4096;
+    k_seam<T><<<g, 256, 0, st.stream>>>(f.v, ax, st.n[ax] - 1, e[0], e[1], e[2], flag);
+    MPDX_LAUNCH_CHECK();
+  };
+  for (int q = 0; q < st.n_eqns; ++q)
+    for (int ax = 0; ax < st.nd; ++ax) check(st.psi[q][st.tl[q]], ax, -1);
+  for (int d = 0; d < st.nd; ++d)
+    for (int ax = 0; ax < st.nd; ++ax)
+      if (ax != d) check(st.GC[d], ax, d);
+  unsigned h = 0;
+  MPDX_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, st.stream));
+  MPDX_CUDA(cudaStreamSynchronize(st.stream));
+  return h == 0;
+}
+
+}  // namespace mpdx

@@ -162,22 +162,23 @@ def periodic_curl_2d(nx, ny, seed, n_modes=8, cmax=0.5, dtype=np.float64):
 
 def periodic_curl_3d(n, seed, n_modes=8, cmax=0.4, dtype=np.float32):
     """Divergence-free 3D Courant field: discrete curl of a vector potential A
-    (3 components of random Fourier modes periodic on (n-1)^3, integer
-    wave-vectors in [1, 4]^3, N(0,1) amplitudes, U[0, 2pi) phases), computed in
-    FP64 on cell edges so that the face fluxes have zero discrete divergence.
-    Returns (gx, gy, gz) in advector view layout."""
+    (3 components of random Fourier modes periodic on the (n-1)-cell torus,
+    integer wave-vectors in [1, 4]^3, N(0,1) amplitudes, U[0, 2pi) phases),
+    computed in FP64 on cell edges so that the face fluxes have zero discrete
+    divergence.  n is an int (cube) or a 3-tuple.  Returns (gx, gy, gz) in
+    advector view layout."""
+    n0, n1, n2 = (n, n, n) if np.isscalar(n) else tuple(n)
     rng = np.random.default_rng(seed)
-    P = n - 1
-    idx = np.arange(P, dtype=np.float64)
-    I, J, K = np.meshgrid(idx, idx, idx, indexing="ij")
+    P = (n0 - 1, n1 - 1, n2 - 1)
+    I, J, K = np.meshgrid(*[np.arange(p, dtype=np.float64) for p in P], indexing="ij")
     A = []
     for _c in range(3):
-        a = np.zeros((P, P, P))
+        a = np.zeros(P)
         for _ in range(n_modes):
             kv = rng.integers(1, 5, size=3)
             amp = rng.normal()
             ph = rng.uniform(0, 2 * math.pi)
-            a += amp * np.cos(2 * math.pi * (kv[0] * I + kv[1] * J + kv[2] * K) / P + ph)
+            a += amp * np.cos(2 * math.pi * (kv[0] * I / P[0] + kv[1] * J / P[1] + kv[2] * K / P[2]) + ph)
         A.append(a)
     Ax, Ay, Az = A
     # A on cell edges: Ax[i,j,k] at (i, j+1/2, k+1/2), Ay at (i+1/2, j, k+1/2), Az at (i+1/2, j+1/2, k);
@@ -189,13 +190,15 @@ def periodic_curl_3d(n, seed, n_modes=8, cmax=0.4, dtype=np.float32):
     fz = (Ay - b(Ay, 0)) - (Ax - b(Ax, 1))   # face (i, j, k+1/2)
     s = cmax / max(np.abs(fx).max(), np.abs(fy).max(), np.abs(fz).max())
     fx, fy, fz = [(f * s).astype(dtype).astype(np.float64) for f in (fx, fy, fz)]
-    a0 = (np.arange(n) - 1) % P
-    a1 = (np.arange(n + 1) - 1) % P
-    b = np.arange(n) % P
-    bm = (np.arange(n) - 1) % P
-    gx = fx[np.ix_(a0, b, b)]
-    gy = fy[np.ix_(a1, bm, b)]
-    gz = fz[np.ix_(a1, b, bm)]
+    a0 = (np.arange(n0) - 1) % P[0]
+    a1 = (np.arange(n0 + 1) - 1) % P[0]
+    j_ = np.arange(n1) % P[1]
+    jm = (np.arange(n1) - 1) % P[1]
+    k_ = np.arange(n2) % P[2]
+    km = (np.arange(n2) - 1) % P[2]
+    gx = fx[np.ix_(a0, j_, k_)]
+    gy = fy[np.ix_(a1, jm, k_)]
+    gz = fz[np.ix_(a1, j_, km)]
     return gx, gy, gz
 
 

@@ -83,6 +83,15 @@ template <> struct pi<3, 0> { static inline void m(int a, int b, int c, int &i, 
 template <> struct pi<3, 1> { static inline void m(int a, int b, int c, int &i, int &j, int &k) { i = c; j = a; k = b; } };
 template <> struct pi<3, 2> { static inline void m(int a, int b, int c, int &i, int &j, int &k) { i = b; j = c; k = a; } };
 
+// inverse: physical (i, j, k) -> frame (a, b, c)
+template <int ND, int D> struct ipi;
+template <> struct ipi<1, 0> { static inline void m(int i, int, int, int &a, int &b, int &c) { a = i; b = 0; c = 0; } };
+template <> struct ipi<2, 0> { static inline void m(int i, int j, int, int &a, int &b, int &c) { a = i; b = j; c = 0; } };
+template <> struct ipi<2, 1> { static inline void m(int i, int j, int, int &a, int &b, int &c) { a = j; b = i; c = 0; } };
+template <> struct ipi<3, 0> { static inline void m(int i, int j, int k, int &a, int &b, int &c) { a = i; b = j; c = k; } };
+template <> struct ipi<3, 1> { static inline void m(int i, int j, int k, int &a, int &b, int &c) { a = j; b = k; c = i; } };
+template <> struct ipi<3, 2> { static inline void m(int i, int j, int k, int &a, int &b, int &c) { a = k; b = i; c = j; } };
+
 template <int ND, int D, class T>
 inline T &P(arr<T> &A, int a, int b = 0, int c = 0) {
   int i, j, k; pi<ND, D>::m(a, b, c, i, j, k); return A(i, j, k);
@@ -166,6 +175,22 @@ struct mpdata {
   // threads pay off only on large grids; loops are elementwise, so results do not depend on it
   bool big() const { return long(n[0]) * n[1] * n[2] >= (1L << 17); }
   void alloc_sclr(arr<T> &a) { a.alloc(sr(0), sr(1), sr(2)); }
+  // visit a frame box (a in ra, b in rb, c in rc) in memory order (k fastest);
+  // every visit is independent, so the order does not change results
+  template <int ND, int D, class F> void box(rng ra, rng rb, rng rc, F f) {
+    rng ph[3] = {{0, 0}, {0, 0}, {0, 0}};
+    ph[D] = ra;
+    if (ND >= 2) ph[(D + 1) % ND] = rb;
+    if (ND >= 3) ph[(D + 2) % ND] = rc;
+#pragma omp parallel for schedule(static) if (big())
+    for (int i = ph[0].f; i <= ph[0].l; ++i)
+      for (int j = ph[1].f; j <= ph[1].l; ++j)
+        for (int k = ph[2].f; k <= ph[2].l; ++k) {
+          int a, b, c;
+          ipi<ND, D>::m(i, j, k, a, b, c);
+          f(a, b, c);
+        }
+  }
   void alloc_vctr(vctr<T> &v) {  // rng_vctr along its own axis: i^h^(halo-1)
     for (int c = 0; c < nd; ++c) {
       rng r[3] = {sr(0), sr(1), sr(2)};
@@ -397,26 +422,21 @@ struct mpdata {
   template <int D> void antidiff3(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
     const arr<T> &Gd = G[D], &G1 = G[(D + 1) % 3], &G2 = G[(D + 2) % 3];
     const rng ra = im[D], rb = ir[(D + 1) % 3], rc = ir[(D + 2) % 3];
-#pragma omp parallel for schedule(static) if (big())
-    for (int a = ra.f; a <= ra.l; ++a)
-      for (int b = rb.f; b <= rb.l; ++b)
-        for (int c = rc.f; c <= rc.l; ++c) {
+    box<3, D>(ra, rb, rc, [&](int a, int b, int c) {
           const T C = P<3, D>(Gd, a, b, c);
           const T gc1 = (P<3, D>(G1, a + 1, b, c) + P<3, D>(G1, a, b, c) + P<3, D>(G1, a + 1, b - 1, c) + P<3, D>(G1, a, b - 1, c)) / T(4);
           const T gc2 = (P<3, D>(G2, a + 1, b, c) + P<3, D>(G2, a, b, c) + P<3, D>(G2, a + 1, b, c - 1) + P<3, D>(G2, a, b, c - 1)) / T(4);
           P<3, D>(res, a, b, c) =
               std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<3, D>(p, a, b, c)
               - C / T(2) * (gc1 * ndy<3, D>(p, a, b, c) + gc2 * ndz<3, D>(p, a, b, c)) / T(1);
-        }
+        });
   }
 
   // ---- donor-cell flux over faces ra (frame a) x rb x rc (make_flux, donorcell_formulae.hpp:36-79) ----
   template <int ND, int D> void make_flux(arr<T> &F, const arr<T> &p, const arr<T> &C, rng ra, rng rb, rng rc) {
-#pragma omp parallel for schedule(static) if (big())
-    for (int a = ra.f; a <= ra.l; ++a)
-      for (int b = rb.f; b <= rb.l; ++b)
-        for (int c = rc.f; c <= rc.l; ++c)
-          P<ND, D>(F, a, b, c) = Fdc(opts, P<ND, D>(p, a, b, c), P<ND, D>(p, a + 1, b, c), P<ND, D>(C, a, b, c));
+    box<ND, D>(ra, rb, rc, [&](int a, int b, int c) {
+      P<ND, D>(F, a, b, c) = Fdc(opts, P<ND, D>(p, a, b, c), P<ND, D>(p, a + 1, b, c), P<ND, D>(C, a, b, c));
+    });
   }
   void fluxes(vctr<T> &F, const arr<T> &p, const vctr<T> &C, bool extended) {
     // extended: ranges im^1 x j^1 x k^1 (fct_adjust_antidiff); else im x j x k
@@ -453,6 +473,7 @@ struct mpdata {
   void fct_init(int e) {
     const arr<T> &p = psi[e][tl[e]];
     rng r0 = ext(ir[0], 1), r1 = nd > 1 ? ext(ir[1], 1) : rng{0, 0}, r2 = nd > 2 ? ext(ir[2], 1) : rng{0, 0};
+#pragma omp parallel for schedule(static) if (big())
     for (int i = r0.f; i <= r0.l; ++i)
       for (int j = r1.f; j <= r1.l; ++j)
         for (int k = r2.f; k <= r2.l; ++k) {
@@ -518,10 +539,7 @@ struct mpdata {
     const rng rb = ND > 1 ? ir[(D + 1) % ND] : rng{0, 0};
     const rng rc = ND > 2 ? ir[(D + 2) % ND] : rng{0, 0};
     const bool absv = (opts & o_abs) && !(opts & o_iga);
-#pragma omp parallel for schedule(static) if (big())
-    for (int a = ra.f; a <= ra.l; ++a)
-      for (int b = rb.f; b <= rb.l; ++b)
-        for (int c = rc.f; c <= rc.l; ++c) {
+    box<ND, D>(ra, rb, rc, [&](int a, int b, int c) {
           const T C = P<ND, D>(corr, a, b, c);
           const T bd0 = P<ND, D>(beta_dn, a, b, c), bu1 = P<ND, D>(beta_up, a + 1, b, c);
           const T bu0 = P<ND, D>(beta_up, a, b, c), bd1 = P<ND, D>(beta_dn, a + 1, b, c);
@@ -530,7 +548,7 @@ struct mpdata {
           else if (C > 0) lim = P<ND, D>(p, a, b, c) > 0 ? std::min(T(1), std::min(bd0, bu1)) : std::min(T(1), std::min(bu0, bd1));
           else lim = P<ND, D>(p, a + 1, b, c) > 0 ? std::min(T(1), std::min(bu0, bd1)) : std::min(T(1), std::min(bd0, bu1));
           P<ND, D>(out, a, b, c) = C * lim;
-        }
+        });
   }
 
   // fct_adjust_antidiff (mpdata_fct_{1,2,3}d.hpp)
