@@ -11,11 +11,11 @@ namespace mpdx {
 
 template <class T> struct tiles;
 template <> struct tiles<float> {
-  static constexpr int TY = 16, TZ = 32, NT3 = 256, LX3 = 128;   // 3D column tile, planes per CTA
-  static constexpr int NT2 = 256, LX2 = 64;                      // 2D strip width (threads), rows per CTA
+  static constexpr int CR = 32, LX3 = 64;   // 3D canvas rows (x 64 columns), planes per CTA
+  static constexpr int NT2 = 256, LX2 = 64; // 2D strip width (threads), rows per CTA
 };
 template <> struct tiles<double> {
-  static constexpr int TY = 8, TZ = 32, NT3 = 256, LX3 = 128;
+  static constexpr int CR = 16, LX3 = 64;
   static constexpr int NT2 = 256, LX2 = 64;
 };
 
@@ -24,10 +24,7 @@ bool fused_configurable(const mpdata_state<T> &st) {
   for (int d = 0; d < st.nd; ++d)
     if (st.bcs[d][0] != MPDX_BC_CYCLIC || st.bcs[d][1] != MPDX_BC_CYCLIC) return false;
   if (st.opts & ~(o_fct | o_iga)) return false;
-  if (st.nd == 3) {
-    return st.n_iters == 2 && st.n[0] - 1 >= 5 && st.n[1] - 1 >= tiles<T>::TY + 3 &&
-           st.n[2] - 1 >= tiles<T>::TZ + 3;
-  }
+  if (st.nd == 3) return st.n_iters == 2 && st.n[0] - 1 >= 2 && st.n[1] - 1 >= 2 && st.n[2] - 1 >= 2;
   if (st.nd == 2) {
     const bool ok_iters = st.n_iters == 2 || (st.n_iters == 3 && !(st.opts & o_iga));
     return ok_iters && st.n[0] - 1 >= 2 && st.n[1] - 1 >= 2;
@@ -42,18 +39,20 @@ static void set_smem(K kernel, size_t bytes) {
 
 template <class T, bool IGA, bool FCT>
 static void launch3(const f3::args<T> &a, cudaStream_t s, dim3 grid) {
-  constexpr int TY = tiles<T>::TY, TZ = tiles<T>::TZ, NT = tiles<T>::NT3;
-  auto kern = f3::k_fused3d<T, IGA, FCT, TY, TZ, NT>;
-  const size_t bytes = size_t(f3::layout<TY, TZ>::total) * sizeof(T);
+  constexpr int CR = tiles<T>::CR;
+  using C = f3::canvas<CR>;
+  auto kern = f3::k_fused3d<T, IGA, FCT, CR>;
+  const size_t bytes = size_t(C::total) * C::N * sizeof(T);
   static bool attr = false;
   if (!attr) { set_smem(kern, bytes); attr = true; }
-  kern<<<grid, NT, bytes, s>>>(a);
+  kern<<<grid, C::NT, bytes, s>>>(a);
   MPDX_LAUNCH_CHECK();
 }
 
 template <class T>
 void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
-  constexpr int TY = tiles<T>::TY, TZ = tiles<T>::TZ, LX = tiles<T>::LX3;
+  using C = f3::canvas<tiles<T>::CR>;
+  constexpr int LX = tiles<T>::LX3;
   f3::args<T> a;
   a.in = st.psi[e][st.tl[e]].v;
   a.out = st.psi[e][st.tl[e] ^ 1].v;
@@ -61,8 +60,8 @@ void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
   a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1; a.P2 = st.n[2] - 1;
   a.n0 = st.n[0]; a.n1 = st.n[1]; a.n2 = st.n[2];
   a.LX = LX;
-  a.tiles_z = (a.P2 + TZ - 1) / TZ;
-  const int tiles_y = (a.P1 + TY - 1) / TY;
+  a.tiles_z = (a.P2 + C::TZ - 1) / C::TZ;
+  const int tiles_y = (a.P1 + C::TY - 1) / C::TY;
   dim3 grid(tiles_y * a.tiles_z, (a.P0 + LX - 1) / LX);
   const bool iga = st.opts & o_iga, fct = st.opts & o_fct;
   if (iga && fct) launch3<T, true, true>(a, s, grid);
