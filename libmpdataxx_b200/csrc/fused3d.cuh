@@ -69,9 +69,12 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // quad formulae --------------------------------------------------------------
+// donor-cell flux pos(C) psi_l + neg(C) psi_r (donorcell_formulae.hpp:25-34),
+// evaluated as C * (C > 0 ? psi_l : psi_r): one of the two products is an
+// exact zero, so both forms give the same value for finite operands
 template <class T>
 __device__ __forceinline__ q4<T> qflux(const q4<T> &pl, const q4<T> &pr, const q4<T> &c) {
-  return qd::fma(qd::pos(c), pl, qd::neg(c) * pr);
+  return c * qd::sel_pos(c, pl, pr);
 }
 template <class T, bool IGA>
 __device__ __forceinline__ q4<T> qndx(const q4<T> &p1, const q4<T> &p0) {  // formulae_mpdata_psi_3d.hpp:262-318
@@ -105,6 +108,14 @@ struct args {
   int tiles_z;      // tiles along k
 };
 
+// slot bookkeeping of a ring of NS planes: base = slot of the oldest plane in use
+template <int NS>
+struct ring {
+  int base;
+  __device__ __forceinline__ int at(int i) const { const int v = base + i; return v >= NS ? v - NS : v; }
+  __device__ __forceinline__ void next() { base = base + 1 == NS ? 0 : base + 1; }
+};
+
 template <int CR>
 struct canvas {
   static constexpr int CC = 64, N = CR * CC, TY = CR - 6, TZ = 56, NT = CR * 16;
@@ -112,7 +123,7 @@ struct canvas {
   // plus the one being prefetched (cp.async, one step ahead)
   static constexpr int NS0 = 5, NG0 = 4, NG1 = 3;
   static constexpr int S0 = 0, G0 = S0 + NS0, G1 = G0 + NG0, G2 = G1 + NG1, S1 = G2 + NG1, CY = S1 + 3,
-                       BU = CY + 1, BD = BU + 2, FY = BD + 2, total = FY + 1;
+                       BU = CY + 2, BD = BU + 2, total = BD + 2;
 };
 
 // asynchronous copy of one quad of field f (plane x, canvas row offset `ro`,
@@ -150,8 +161,9 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
   const int r = 2 * (tid >> 5) + (lane >> 4);   // canvas row
   const int q = lane & 15;                      // quad within the row
   const int me = r * C::CC + 4 * q;             // canvas offset of the own quad
-  // rows r+1 / r-1; the outermost rows reuse their own (they are halo)
-  const int upc = r < CR - 1 ? me + C::CC : me, dnc = r > 0 ? me - C::CC : me;
+  // canvas offset of row r+d (the outermost rows stand in for missing ones: they are halo)
+  auto R = [&](int d) { const int rr = r + d; return rr >= 0 && rr < CR ? me + d * C::CC : me; };
+  const int up = R(1), dn = R(-1);
 
   const int tile = blockIdx.x;
   const int j0 = (tile / A.tiles_z) * C::TY, k0 = (tile % A.tiles_z) * C::TZ;
@@ -168,10 +180,10 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
   const long long ro_g1 = (long long)jg * A.g1.s1, ro_g2 = (long long)jg * A.g2.s1;
 
   auto plane = [&](int base, int nslots, int x) { return sm + (base + ((x % nslots) + nslots) % nslots) * N; };
-  auto cp_in = [&](int x) { gcopy(plane(C::S0, C::NS0, x) + me, A.in, pmod(x, A.P0), ro_in, kb, contig, kc); };
-  auto cp_g0 = [&](int x) { gcopy(plane(C::G0, C::NG0, x) + me, A.g0, pmod(x, A.P0), ro_g0, kb, contig, kc); };
-  auto cp_g1 = [&](int x) { gcopy(plane(C::G1, C::NG1, x) + me, A.g1, pmod(x, A.P0), ro_g1, kb, contig, kc); };
-  auto cp_g2 = [&](int x) { gcopy(plane(C::G2, C::NG1, x) + me, A.g2, pmod(x, A.P0), ro_g2, kb, contig, kc); };
+  auto cp_in = [&](T *dst, int x) { gcopy(dst + me, A.in, pmod(x, A.P0), ro_in, kb, contig, kc); };
+  auto cp_g0 = [&](T *dst, int x) { gcopy(dst + me, A.g0, pmod(x, A.P0), ro_g0, kb, contig, kc); };
+  auto cp_g1 = [&](T *dst, int x) { gcopy(dst + me, A.g1, pmod(x, A.P0), ro_g1, kb, contig, kc); };
+  auto cp_g2 = [&](T *dst, int x) { gcopy(dst + me, A.g2, pmod(x, A.P0), ro_g2, kb, contig, kc); };
 
   for (int p = tid; p < C::total * N; p += C::NT) sm[p] = T(0);
   __syncthreads();
@@ -179,58 +191,78 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
   const int ts = x0 - 3;
   // prologue: everything step ts reads (psi^n planes ts-1..ts+2, GC_x faces
   // ts-1..ts+1, GC_y/GC_z planes ts..ts+1); each step then prefetches one plane ahead
-  for (int x = ts - 1; x <= ts + 2; ++x) cp_in(x);
-  for (int x = ts - 1; x <= ts + 1; ++x) cp_g0(x);
-  for (int x = ts; x <= ts + 1; ++x) { cp_g1(x); cp_g2(x); }
+  for (int x = ts - 1; x <= ts + 2; ++x) cp_in(plane(C::S0, C::NS0, x), x);
+  for (int x = ts - 1; x <= ts + 1; ++x) cp_g0(plane(C::G0, C::NG0, x), x);
+  for (int x = ts; x <= ts + 1; ++x) { cp_g1(plane(C::G1, C::NG1, x), x); cp_g2(plane(C::G2, C::NG1, x), x); }
   cp_commit();
 
   const Q zero = qd::bc<T>(T(0));
   Q p_m = zero, p_c = zero;  // own psi1 at planes t-1, t
   Q cx_m = zero, cy_m = zero, cz_m = zero, bu_m = zero, bd_m = zero, fx_prev = zero;
+  // ring slots of the oldest plane each step reads: psi^n and GC_x from t-1,
+  // GC_y / GC_z from t, psi1 / C~_y / betas from t-1
+  auto slot0 = [](int x, int n) { return ((x % n) + n) % n; };
+  ring<C::NS0> r_s0{slot0(ts - 1, C::NS0)};
+  ring<C::NG0> r_g0{slot0(ts - 1, C::NG0)};
+  ring<C::NG1> r_g1{slot0(ts, C::NG1)};
+  ring<3> r_s1{slot0(ts - 1, 3)};
+  ring<2> r_2{slot0(ts - 1, 2)};
 
+  // Two barriers per step: one before the step reads the planes of the
+  // previous step, one after psi1(t+1) is stored.  The y-face pseudo-velocity
+  // and the y-face flux below the own row, which the FCT sums need, are
+  // recomputed by the thread rather than exchanged.
   for (int t = ts; t <= x1; ++t) {
     cp_wait_all();
     __syncthreads();
-    cp_in(t + 3);
-    cp_g0(t + 2);
-    cp_g1(t + 2);
-    cp_g2(t + 2);
+    T *const s0b = sm + C::S0 * N, *const g0b = sm + C::G0 * N, *const g1b = sm + C::G1 * N, *const g2b = sm + C::G2 * N;
+    cp_in(s0b + r_s0.at(4) * N, t + 3);
+    cp_g0(g0b + r_g0.at(3) * N, t + 2);
+    cp_g1(g1b + r_g1.at(2) * N, t + 2);
+    cp_g2(g2b + r_g1.at(2) * N, t + 2);
     cp_commit();
-    T *S0m = plane(C::S0, C::NS0, t - 1), *S0c = plane(C::S0, C::NS0, t), *S0p = plane(C::S0, C::NS0, t + 1);
-    T *S0pp = plane(C::S0, C::NS0, t + 2);
-    T *G0m = plane(C::G0, C::NG0, t - 1), *G0c = plane(C::G0, C::NG0, t), *G0p = plane(C::G0, C::NG0, t + 1);
-    T *G1c = plane(C::G1, C::NG1, t), *G1p = plane(C::G1, C::NG1, t + 1);
-    T *G2c = plane(C::G2, C::NG1, t), *G2p = plane(C::G2, C::NG1, t + 1);
-    T *S1m = plane(C::S1, 3, t - 1), *S1c = plane(C::S1, 3, t), *S1p = plane(C::S1, 3, t + 1);
-    T *CY = sm + C::CY * N, *FY = sm + C::FY * N;
-    T *BUc = plane(C::BU, 2, t), *BDc = plane(C::BD, 2, t), *BUm = plane(C::BU, 2, t - 1), *BDm = plane(C::BD, 2, t - 1);
+    const T *S0m = s0b + r_s0.at(0) * N, *S0c = s0b + r_s0.at(1) * N, *S0p = s0b + r_s0.at(2) * N;
+    const T *S0pp = s0b + r_s0.at(3) * N;
+    const T *G0m = g0b + r_g0.at(0) * N, *G0c = g0b + r_g0.at(1) * N, *G0p = g0b + r_g0.at(2) * N;
+    const T *G1c = g1b + r_g1.at(0) * N, *G1p = g1b + r_g1.at(1) * N;
+    const T *G2c = g2b + r_g1.at(0) * N, *G2p = g2b + r_g1.at(1) * N;
+    T *const s1b = sm + C::S1 * N;
+    const T *S1m = s1b + r_s1.at(0) * N, *S1c = s1b + r_s1.at(1) * N;
+    T *S1p = s1b + r_s1.at(2) * N;
+    const int sc = r_2.at(1) * N, sm1 = r_2.at(0) * N;
+    T *CYc = sm + C::CY * N + sc, *BUc = sm + C::BU * N + sc, *BDc = sm + C::BD * N + sc;
+    const T *CYm = sm + C::CY * N + sm1, *BUm = sm + C::BU * N + sm1, *BDm = sm + C::BD * N + sm1;
+    r_s0.next(); r_g0.next(); r_g1.next(); r_s1.next(); r_2.next();
 
-    // ---- A: psi1 at plane t+1 ----
-    Q p_p;
-    {
-      const Q c = qd::lds(S0p + me), s0c = qd::lds(S0c + me), s0pp = qd::lds(S0pp + me);
-      const Q g0c = qd::lds(G0c + me), g0p = qd::lds(G0p + me), g1p = qd::lds(G1p + me), g2p = qd::lds(G2p + me);
-      const Q fxp = qflux(c, s0pp, g0p), fxm = qflux(s0c, c, g0c);
-      const Q fyp = qflux(c, qd::lds(S0p + upc), g1p), fym = qflux(qd::lds(S0p + dnc), c, qd::lds(G1p + dnc));
+    // ---- A: psi1 at plane t+1 (mpdata_osc_3d.hpp:181-197) ----
+    auto psi1_row = [&](int o, int om, int op) {  // canvas offsets of the row and its neighbours
+      const Q c = qd::lds(S0p + o);
+      const Q fxp = qflux(c, qd::lds(S0pp + o), qd::lds(G0p + o));
+      const Q fxm = qflux(qd::lds(S0c + o), c, qd::lds(G0c + o));
+      const Q fyp = qflux(c, qd::lds(S0p + op), qd::lds(G1p + o));
+      const Q fym = qflux(qd::lds(S0p + om), c, qd::lds(G1p + om));
+      const Q g2p = qd::lds(G2p + o);
       const Q fzp = qflux(c, qd::kp1(c), g2p), fzm = qflux(qd::km1(c), c, qd::km1(g2p));
-      p_p = c + ((((-fxp) + fxm) + ((-fyp) + fym)) + ((-fzp) + fzm));
-      qd::sts(S1p + me, p_p);
-    }
+      return c + ((((-fxp) + fxm) + ((-fyp) + fym)) + ((-fzp) + fzm));
+    };
+    const Q p_p = psi1_row(me, dn, up);
+    qd::sts(S1p + me, p_p);
     __syncthreads();
+    const Q pp_up = qd::lds(S1p + up), pp_dn = qd::lds(S1p + dn);
 
-    // ---- B: C~ on x-face t+1/2, y- and z-faces of plane t ----
+    // ---- B: C~ on the own x-face t+1/2, y-face j+1/2 and z-faces of plane t ----
+    const Q pc_up = qd::lds(S1c + up), pc_dn = qd::lds(S1c + dn);
     Q cx_c, cy_c, cz_c;
     {
-      const Q pc_up = qd::lds(S1c + upc), pc_dn = qd::lds(S1c + dnc), pm_up = qd::lds(S1m + upc);
-      const Q pp_up = qd::lds(S1p + upc), pp_dn = qd::lds(S1p + dnc);
+      const Q pm_up = qd::lds(S1m + up);
       const Q g0c = qd::lds(G0c + me), g0m = qd::lds(G0m + me);
-      const Q g1c = qd::lds(G1c + me), g1p = qd::lds(G1p + me), g2c = qd::lds(G2c + me), g2p = qd::lds(G2p + me);
-      const Q g1c_dn = qd::lds(G1c + dnc);
+      const Q g1c = qd::lds(G1c + me), g1c_dn = qd::lds(G1c + dn), g2c = qd::lds(G2c + me);
       // x-face (frame a = x, b = y, c = z)
       {
+        const Q g2p = qd::lds(G2p + me);
         const Q ny = qnd4<T, IGA>(pp_up, pc_up, pp_dn, pc_dn);
         const Q nz = qnd4<T, IGA>(qd::kp1(p_p), qd::kp1(p_c), qd::km1(p_p), qd::km1(p_c));
-        const Q gc1 = avg4(g1p, g1c, qd::lds(G1p + dnc), g1c_dn);
+        const Q gc1 = avg4(qd::lds(G1p + me), g1c, qd::lds(G1p + dn), g1c_dn);
         const Q gc2 = avg4(g2p, g2c, qd::km1(g2p), qd::km1(g2c));
         cx_c = qadiff(g0c, gc1, gc2, qndx<T, IGA>(p_p, p_c), ny, nz);
       }
@@ -238,11 +270,11 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
       {
         const Q ny = qnd4<T, IGA>(qd::kp1(pc_up), qd::kp1(p_c), qd::km1(pc_up), qd::km1(p_c));
         const Q nz = qnd4<T, IGA>(pp_up, p_p, pm_up, p_m);
-        const Q g2c_up = qd::lds(G2c + upc);
+        const Q g2c_up = qd::lds(G2c + up);
         const Q gc1 = avg4(g2c_up, g2c, qd::km1(g2c_up), qd::km1(g2c));
-        const Q gc2 = avg4(qd::lds(G0c + upc), g0c, qd::lds(G0m + upc), g0m);
+        const Q gc2 = avg4(qd::lds(G0c + up), g0c, qd::lds(G0m + up), g0m);
         cy_c = qadiff(g1c, gc1, gc2, qndx<T, IGA>(pc_up, p_c), ny, nz);
-        qd::sts(CY + me, cy_c);
+        qd::sts(CYc + me, cy_c);
       }
       // z-face k+1/2 (frame a = z, b = x, c = y)
       {
@@ -253,22 +285,31 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
         cz_c = qadiff(g2c, gc1, gc2, qndx<T, IGA>(qd::kp1(p_c), p_c), ny, nz);
       }
     }
-    __syncthreads();
 
-    // ---- C: betas at plane t ----
+    // ---- C: betas at plane t (formulae_mpdata_fct_3d.hpp:48-143) ----
     Q bu_c = zero, bd_c = zero;
     if (FCT) {
+      // C~ on the y-face j-1/2 below the own row, recomputed (frame a = y at row r-1)
+      Q cy_dn;
+      {
+        const Q pm_dn = qd::lds(S1m + dn), g2c = qd::lds(G2c + me), g2c_dn = qd::lds(G2c + dn);
+        const Q ny = qnd4<T, IGA>(qd::kp1(p_c), qd::kp1(pc_dn), qd::km1(p_c), qd::km1(pc_dn));
+        const Q nz = qnd4<T, IGA>(p_p, pp_dn, p_m, pm_dn);
+        const Q gc1 = avg4(g2c, g2c_dn, qd::km1(g2c), qd::km1(g2c_dn));
+        const Q gc2 = avg4(qd::lds(G0c + me), qd::lds(G0c + dn), qd::lds(G0m + me), qd::lds(G0m + dn));
+        cy_dn = qadiff(qd::lds(G1c + dn), gc1, gc2, qndx<T, IGA>(p_c, pc_dn), ny, nz);
+      }
       // psi_min / psi_max of psi^n over the 7-point stencil at plane t (mpdata_fct_3d.hpp:31-55)
       Q mnq, mxq;
       {
         const Q s0c = qd::lds(S0c + me), s0p = qd::lds(S0p + me), s0m = qd::lds(S0m + me);
-        const Q yp = qd::lds(S0c + upc), ym = qd::lds(S0c + dnc), zp = qd::kp1(s0c), zm = qd::km1(s0c);
+        const Q yp = qd::lds(S0c + up), ym = qd::lds(S0c + dn), zp = qd::kp1(s0c), zm = qd::km1(s0c);
         mnq = qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(s0c, s0p), s0m), yp), ym), zp), zm);
         mxq = qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(s0c, s0p), s0m), yp), ym), zp), zm);
       }
       const Q c = p_c;
-      const Q xp = p_p, xm = p_m, yp = qd::lds(S1c + upc), ym = qd::lds(S1c + dnc), zp = qd::kp1(c), zm = qd::km1(c);
-      Q fxm = cx_m, fxp = cx_c, fym = qd::lds(CY + dnc), fyp = cy_c, fzm = qd::km1(cz_c), fzp = cz_c;
+      const Q xp = p_p, xm = p_m, yp = pc_up, ym = pc_dn, zp = qd::kp1(c), zm = qd::km1(c);
+      Q fxm = cx_m, fxp = cx_c, fym = cy_dn, fyp = cy_c, fzm = qd::km1(cz_c), fzp = cz_c;
       if (!IGA) {
         fxm = qflux(xm, c, fxm); fxp = qflux(c, xp, fxp);
         fym = qflux(ym, c, fym); fyp = qflux(c, yp, fyp);
@@ -284,33 +325,32 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
       qd::sts(BUc + me, bu_c);
       qd::sts(BDc + me, bd_c);
     }
-    __syncthreads();
 
-    // ---- D: limited pseudo-velocities and fluxes at plane t-1 ----
-    Q fxx, fzz;
+    // ---- D: limited fluxes at plane t-1 (formulae_mpdata_fct_3d.hpp:148-250) ----
+    Q fxx, fyu, fyd, fzz;
     {
-      Q Cx = cx_m, Cy = cy_m, Cz = cz_m;
+      Q Cx = cx_m, Cy = cy_m, Cyd = qd::lds(CYm + dn), Cz = cz_m;
       if (FCT) {
+        const Q bu_dn = qd::lds(BUm + dn), bd_dn = qd::lds(BDm + dn);
         Cx = Cx * qd::qlim(Cx, bd_m, bu_c, bu_m, bd_c);
-        Cy = Cy * qd::qlim(Cy, bd_m, qd::lds(BUm + upc), bu_m, qd::lds(BDm + upc));
+        Cy = Cy * qd::qlim(Cy, bd_m, qd::lds(BUm + up), bu_m, qd::lds(BDm + up));
+        Cyd = Cyd * qd::qlim(Cyd, bd_dn, bu_m, bu_dn, bd_m);
         Cz = Cz * qd::qlim(Cz, bd_m, qd::kp1(bu_m), bu_m, qd::kp1(bd_m));
       }
       if (IGA) {
-        fxx = Cx; fzz = Cz;
-        qd::sts(FY + me, Cy);
+        fxx = Cx; fyu = Cy; fyd = Cyd; fzz = Cz;
       } else {
         fxx = qflux(p_m, p_c, Cx);
+        fyu = qflux(p_m, qd::lds(S1m + up), Cy);
+        fyd = qflux(qd::lds(S1m + dn), p_m, Cyd);
         fzz = qflux(p_m, qd::kp1(p_m), Cz);
-        qd::sts(FY + me, qflux(p_m, qd::lds(S1m + upc), Cy));
       }
     }
-    __syncthreads();
 
     // ---- E: psi^{n+1} at plane t-1 ----
     {
       const int x = t - 1;
-      const Q fy = qd::lds(FY + me), fyd = qd::lds(FY + dnc);
-      const Q v = p_m + ((((-fxx) + fx_prev) + ((-fy) + fyd)) + ((-fzz) + qd::km1(fzz)));
+      const Q v = p_m + ((((-fxx) + fx_prev) + ((-fyu) + fyd)) + ((-fzz) + qd::km1(fzz)));
       fx_prev = fxx;
       const int jrow = j0 - 3 + r;
       if (x >= x0 && x < x1 && r >= 3 && r < CR - 3 && jrow < A.P1 && q >= 1 && q < 15) {

@@ -9,9 +9,12 @@
 
 namespace mpdx {
 
+#ifndef MPDX_LX3
+#define MPDX_LX3 64  // planes per CTA of the 3D kernel (4 warm-up planes per chunk)
+#endif
 template <class T> struct tiles;
 template <> struct tiles<float> {
-  static constexpr int CR = 32, LX3 = 64;   // 3D canvas rows (x 64 columns), planes per CTA
+  static constexpr int CR = 32, LX3 = MPDX_LX3;   // 3D canvas rows (x 64 columns), planes per CTA
   static constexpr int NT2 = 256, LX2 = 64; // 2D strip width (threads), rows per CTA
 };
 template <> struct tiles<double> {

@@ -1,6 +1,8 @@
 // Four consecutive cells along k held by one thread ("quad"), with the
-// elementwise arithmetic of the MPDATA formulae.  FP32 quads use the paired
-// FP32 instructions of sm_100 (add/mul/fma on float2); FP64 quads use plain
+// elementwise arithmetic of the MPDATA formulae.  FP32 quads use one FP32
+// instruction per element by default (MPDX_QUAD_PAIRED=1 selects the paired
+// float2 add/mul/fma of sm_100 instead; measured slower here because the
+// shifted quads of the k-stencils need re-pairing moves); FP64 quads use plain
 // double arithmetic (the FP64 translation unit is compiled without FMA
 // contraction, so every operation rounds exactly as the reference's does).
 #pragma once
@@ -37,19 +39,39 @@ __device__ __forceinline__ q4<float> shr(const q4<float> &v, float right) { retu
 __device__ __forceinline__ q4<double> shl(const q4<double> &v, double left) { return {left, v.x, v.y, v.z}; }
 __device__ __forceinline__ q4<double> shr(const q4<double> &v, double right) { return {v.y, v.z, v.w, right}; }
 
-// arithmetic
+// arithmetic (MPDX_QUAD_PAIRED = 0 selects one FP32 instruction per element)
+#ifndef MPDX_QUAD_PAIRED
+#define MPDX_QUAD_PAIRED 0
+#endif
+#if MPDX_QUAD_PAIRED
 __device__ __forceinline__ q4<float> operator+(const q4<float> &p, const q4<float> &q) { return {__fadd2_rn(p.a, q.a), __fadd2_rn(p.b, q.b)}; }
 __device__ __forceinline__ q4<float> operator-(const q4<float> &p, const q4<float> &q) {
   return {__fadd2_rn(p.a, make_float2(-q.a.x, -q.a.y)), __fadd2_rn(p.b, make_float2(-q.b.x, -q.b.y))};
 }
 __device__ __forceinline__ q4<float> operator*(const q4<float> &p, const q4<float> &q) { return {__fmul2_rn(p.a, q.a), __fmul2_rn(p.b, q.b)}; }
+#else
+__device__ __forceinline__ q4<float> operator+(const q4<float> &p, const q4<float> &q) {
+  return mk(p.a.x + q.a.x, p.a.y + q.a.y, p.b.x + q.b.x, p.b.y + q.b.y);
+}
+__device__ __forceinline__ q4<float> operator-(const q4<float> &p, const q4<float> &q) {
+  return mk(p.a.x - q.a.x, p.a.y - q.a.y, p.b.x - q.b.x, p.b.y - q.b.y);
+}
+__device__ __forceinline__ q4<float> operator*(const q4<float> &p, const q4<float> &q) {
+  return mk(p.a.x * q.a.x, p.a.y * q.a.y, p.b.x * q.b.x, p.b.y * q.b.y);
+}
+#endif
 __device__ __forceinline__ q4<float> operator/(const q4<float> &p, const q4<float> &q) {
   return mk(__fdiv_rn(p.a.x, q.a.x), __fdiv_rn(p.a.y, q.a.y), __fdiv_rn(p.b.x, q.b.x), __fdiv_rn(p.b.y, q.b.y));
 }
 __device__ __forceinline__ q4<float> operator-(const q4<float> &p) { return mk(-p.a.x, -p.a.y, -p.b.x, -p.b.y); }
 // p * q + r with one rounding per element (FP32 only; the FP64 path never fuses)
 __device__ __forceinline__ q4<float> fma(const q4<float> &p, const q4<float> &q, const q4<float> &r) {
+#if MPDX_QUAD_PAIRED
   return {__ffma2_rn(p.a, q.a, r.a), __ffma2_rn(p.b, q.b, r.b)};
+#else
+  return mk(__fmaf_rn(p.a.x, q.a.x, r.a.x), __fmaf_rn(p.a.y, q.a.y, r.a.y), __fmaf_rn(p.b.x, q.b.x, r.b.x),
+            __fmaf_rn(p.b.y, q.b.y, r.b.y));
+#endif
 }
 
 __device__ __forceinline__ q4<double> operator+(const q4<double> &p, const q4<double> &q) { return {p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w}; }
@@ -91,7 +113,16 @@ MPDX_Q_MAP2(qmax, fmax(x, y))
 // FCT limiter factor of GC_mono: C > 0 ? min(1, bd_l, bu_r) : min(1, bu_l, bd_r)
 template <class T>
 __device__ __forceinline__ T lim1(T C, T bdl, T bur, T bul, T bdr) {
-  return C > T(0) ? fmin(T(1), fmin(bdl, bur)) : fmin(T(1), fmin(bul, bdr));
+  const bool p = C > T(0);
+  return fmin(T(1), fmin(p ? bdl : bul, p ? bur : bdr));
+}
+// elementwise C > 0 ? a : b
+template <class T> __device__ __forceinline__ T sel1(T c, T a, T b) { return c > T(0) ? a : b; }
+__device__ __forceinline__ q4<float> sel_pos(const q4<float> &c, const q4<float> &a, const q4<float> &b) {
+  return mk(sel1(c.a.x, a.a.x, b.a.x), sel1(c.a.y, a.a.y, b.a.y), sel1(c.b.x, a.b.x, b.b.x), sel1(c.b.y, a.b.y, b.b.y));
+}
+__device__ __forceinline__ q4<double> sel_pos(const q4<double> &c, const q4<double> &a, const q4<double> &b) {
+  return {sel1(c.x, a.x, b.x), sel1(c.y, a.y, b.y), sel1(c.z, a.z, b.z), sel1(c.w, a.w, b.w)};
 }
 __device__ __forceinline__ q4<float> qlim(const q4<float> &C, const q4<float> &bdl, const q4<float> &bur,
                                           const q4<float> &bul, const q4<float> &bdr) {
