@@ -142,6 +142,21 @@ const char *mpdx_create_error(void);
 
 void mpdx_destroy(mpdx_handle h);
 
+/* FP64 compensated sum over [0,m0) x [0,m1) x [0,m2), minimum and maximum over
+ * [0,n0) x [0,n1) x [0,n2) of a caller-owned device array (dtype 4 or 8,
+ * element strides), written as three doubles to the device buffer dev_out,
+ * asynchronously on `stream` (a cudaStream_t; NULL for the legacy stream).
+ *
+ * No counterpart in the reference.  It allocates nothing: for callers that
+ * cannot allocate device memory where they need these numbers (device memory
+ * owned by a caching or pooled allocator, fixed memory budgets).  Its scratch
+ * is one fixed-size array in device memory: at most 8192 points along axis 0
+ * (larger extents return MPDX_E_ARG with the reason in err).  The first call
+ * on a device looks up that array's address and should come before any stream
+ * capture; calls on one device that overlap on the GPU race on the array. */
+mpdx_status mpdx_field_stats_noalloc(const void *dev_field, int dtype, const int64_t *n, const int64_t *strides,
+                                     const int64_t *m, double *dev_out, void *stream, char *err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

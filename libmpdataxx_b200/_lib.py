@@ -23,7 +23,7 @@ SCLR_THT_E = 0
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
            "mpdx_get_field_device", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
-           "mpdx_create_error", "mpdx_destroy"]
+           "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc"]
 
 
 class Config(ctypes.Structure):
