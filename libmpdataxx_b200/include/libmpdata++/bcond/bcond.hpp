@@ -1,0 +1,18 @@
+// Boundary-condition kinds (libmpdata++/bcond/detail/bcond_common.hpp bcond_e).
+#pragma once
+
+#include <mpdx.h>
+
+namespace libmpdataxx {
+namespace bcond {
+enum bcond_e { null, cyclic, open, rigid };
+inline int to_c(bcond_e b) {
+  switch (b) {
+    case cyclic: return MPDX_BC_CYCLIC;
+    case open: return MPDX_BC_OPEN;
+    case rigid: return MPDX_BC_RIGID;
+    default: return -1;
+  }
+}
+}  // namespace bcond
+}  // namespace libmpdataxx

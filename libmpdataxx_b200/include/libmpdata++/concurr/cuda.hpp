@@ -1,0 +1,176 @@
+// concurr::cuda<solver_t, bcxl, bcxr[, bcyl, bcyr[, bczl, bczr]]>: the B200
+// backend of the libmpdata++ run API (header-only; links libmpdx.so).
+//
+// Drop-in for concurr::{serial,openmp,threads} (concurr/detail/concurr_common.hpp:122-454):
+//
+//   using run_t = concurr::cuda<solvers::mpdata<ct_params_t>, bcond::cyclic, bcond::cyclic>;
+//   typename run_t::rt_params_t p;  p.grid_size = {601};
+//   run_t run(p);
+//   run.advectee() = [](int i) { return i <= 75 || i >= 125 ? 2. : 4.; };
+//   run.advector() = -.75;
+//   run.advance(1200);
+//
+// Fields live on the device.  advectee()/advector()/sclr_array() return
+// writable views of host mirrors: a mirror is downloaded when first handed
+// out after a step, and every mirror handed out is uploaded before the next
+// advance(), so writes through a view behave as writes into the reference's
+// Blitz++ views.  Data otherwise leaves the GPU only when a view is requested.
+// Hooks run on the host once per step (rank 0 only: there is one GPU).
+#pragma once
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <mpdx.h>
+
+#include "../bcond/bcond.hpp"
+#include "../opts.hpp"
+#include "any.hpp"
+
+namespace libmpdataxx {
+namespace concurr {
+
+namespace detail {
+// exception text of each status, as the reference throws them
+inline void check(mpdx_handle h, mpdx_status rc) {
+  if (rc == MPDX_OK) return;
+  switch (rc) {
+    case MPDX_E_GRID: throw std::runtime_error("libmpdata++: bogus grid size");
+    case MPDX_E_DIVERGENT: throw std::runtime_error("libmpdata++: initial advector field is divergent");
+    case MPDX_E_PRS_STUCK: throw std::runtime_error("libmpdata++: stuck in pressure solver");
+    default: throw std::runtime_error(std::string("libmpdata++ (cuda backend): ") + (h ? mpdx_last_error(h) : mpdx_create_error()));
+  }
+}
+}  // namespace detail
+
+template <class solver_t, bcond::bcond_e bcxl, bcond::bcond_e bcxr, bcond::bcond_e bcyl = bcond::null,
+          bcond::bcond_e bcyr = bcond::null, bcond::bcond_e bczl = bcond::null, bcond::bcond_e bczr = bcond::null>
+class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
+ public:
+  using real_t = typename solver_t::real_t;
+  enum { n_dims = solver_t::n_dims };
+  enum { n_eqns = solver_t::n_eqns };
+  using rt_params_t = typename solver_t::rt_params_t;
+  using arr_t = host_view<real_t, n_dims>;
+  using ct_params_t = typename solver_t::ct_params_t_;
+
+  static_assert(n_dims >= 1 && n_dims <= 3, "n_dims must be 1, 2 or 3");
+  static_assert(bcxl != bcond::null && bcxr != bcond::null, "x boundary conditions are required");
+  static_assert(n_dims < 2 || (bcyl != bcond::null && bcyr != bcond::null), "y boundary conditions are required");
+  static_assert(n_dims < 3 || (bczl != bcond::null && bczr != bcond::null), "z boundary conditions are required");
+  static_assert(!opts::isset(ct_params_t::opts, opts::nug | opts::dfl | opts::khn | opts::div_2nd | opts::div_3rd |
+                                                    opts::div_3rd_dt | opts::fot),
+                "MPDATA option not built on this backend (built: fct abs tot(1D) pfc npa iga)");
+
+  explicit cuda(const rt_params_t &p) : p_(p) {
+    mpdx_config c;
+    mpdx_config_default(&c);
+    c.n_dims = n_dims;
+    c.n_eqns = n_eqns;
+    for (int d = 0; d < 3; ++d) c.grid[d] = d < n_dims ? p.grid_size[d] : 1;
+    c.opts = uint64_t(ct_params_t::opts);
+    c.n_iters = p.n_iters;
+    c.dtype = int(sizeof(real_t));
+    const bcond::bcond_e b[6] = {bcxl, bcxr, bcyl, bcyr, bczl, bczr};
+    for (int q = 0; q < 2 * n_dims; ++q) c.bcs[q] = bcond::to_c(b[q]);
+    c.dt = double(p.dt);
+    c.di = p.di != 0 ? double(p.di) : 1.0;
+    c.dj = p.dj != 0 ? double(p.dj) : 1.0;
+    c.dk = p.dk != 0 ? double(p.dk) : 1.0;
+    c.max_abs_div_eps = double(p.max_abs_div_eps);
+    solver_t::fill(c, p);
+    detail::check(nullptr, mpdx_create(&c, &h_));
+  }
+  ~cuda() override {
+    if (h_) mpdx_destroy(h_);
+  }
+  cuda(const cuda &) = delete;
+  cuda &operator=(const cuda &) = delete;
+
+  // accessors (concurr_common.hpp:387-433)
+  arr_t advectee(int e = 0) override { return view(MPDX_FIELD_ADVECTEE, e); }
+  arr_t advector(int d = 0) override { return view(MPDX_FIELD_ADVECTOR, d); }
+  arr_t sclr_array(const std::string &name, int = 0) override {
+    if (name != "tht_e") throw std::out_of_range("libmpdata++: unknown scalar array " + name);
+    return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_E);
+  }
+
+  // run.advance(nt) (concurr_common.hpp:380-385); hooks, if set, run after every step
+  void advance(int nt) override {
+    flush();
+    if (!hook_) {
+      detail::check(h_, mpdx_advance(h_, nt));
+      invalidate_state();
+      return;
+    }
+    for (int t = 0; t < nt && !panic_; ++t) {
+      detail::check(h_, mpdx_advance(h_, 1));
+      invalidate_state();
+      hook_(*this);
+      flush();
+    }
+  }
+
+  real_t min(int e = 0) override { return libmpdataxx::min(advectee(e)); }
+  real_t max(int e = 0) override { return libmpdataxx::max(advectee(e)); }
+  real_t time() const override { return real_t(stats().timestep) * p_.dt; }
+  bool *panic_ptr() override { return &panic_; }
+
+  // device-side statistics: timestep, FP64 mass, min/max, pressure-solver counters
+  mpdx_step_stats stats() const {
+    mpdx_step_stats s;
+    detail::check(h_, mpdx_stats(h_, &s));
+    return s;
+  }
+  // per-step host hook (stands in for overriding hook_post_step in a subclass)
+  template <class F> void hook_post_step(F f) { hook_ = f; }
+  mpdx_handle handle() const { return h_; }
+
+ private:
+  struct mirror {
+    std::vector<real_t> buf;
+    bool fresh = false;
+  };
+
+  arr_t view(int kind, int idx) {
+    std::array<int, n_dims> ext, lb;
+    for (int d = 0; d < n_dims; ++d) {
+      ext[d] = p_.grid_size[d];
+      lb[d] = 0;
+    }
+    if (kind == MPDX_FIELD_ADVECTOR) {
+      if (idx > 0) ext[0] += 1;  // view extents (sharedmem.hpp:431-456, 543-577)
+      lb[0] = -1;
+    }
+    size_t n = 1;
+    for (int d = 0; d < n_dims; ++d) n *= size_t(ext[d]);
+    mirror &m = mirrors_[{kind, idx}];
+    if (m.buf.size() != n) m.buf.assign(n, real_t(0));
+    if (!m.fresh) {
+      detail::check(h_, mpdx_get_field(h_, kind, idx, m.buf.data(), nullptr));
+      m.fresh = true;
+    }
+    return arr_t(m.buf.data(), lb, ext);
+  }
+  void flush() {
+    for (auto &kv : mirrors_)
+      if (kv.second.fresh) detail::check(h_, mpdx_set_field(h_, kv.first.first, kv.first.second, kv.second.buf.data(), nullptr));
+  }
+  void invalidate_state() {
+    for (auto &kv : mirrors_)
+      if (kv.first.first == MPDX_FIELD_ADVECTEE) kv.second.fresh = false;
+  }
+
+  rt_params_t p_;
+  mpdx_handle h_ = nullptr;
+  std::map<std::pair<int, int>, mirror> mirrors_;
+  std::function<void(cuda &)> hook_;
+  bool panic_ = false;
+};
+
+}  // namespace concurr
+}  // namespace libmpdataxx
