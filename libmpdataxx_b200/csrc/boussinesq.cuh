@@ -1,23 +1,72 @@
-// Boussinesq solver with GCR pressure solve (declarations).
+// Boussinesq solver with GCR(k) pressure solve (solvers::boussinesq, iles,
+// trapezoidal right-hand side, explicit buoyancy) on the device.
 #pragma once
 
-#include "state.cuh"
+#include <vector>
+
+#include "general.cuh"
 
 namespace mpdx {
 
+constexpr int kGcrMaxK = 8;        // largest k of GCR(k) built
+constexpr int kRedBlocks = 296;    // reduction grid: 2 x 148 SMs (fixed shape => reproducible sums)
+constexpr int kRedThreads = 256;
+constexpr int kRedSlots = kGcrMaxK + 2;
+
+// GCR scalars that live on the device.  beta, alpha and tmp_den persist from
+// solve to solve as the reference's members do (mpdata_rhs_vip_prs_gcrk.hpp:25-27).
 template <class T>
+struct gcr_dev {
+  T beta;
+  T alpha[kGcrMaxK];
+  T tmp_den[kGcrMaxK];
+  T pend_den, pend_num;  // sums produced with a new search direction, consumed by the next update
+  T mean;                // ini_pressure: mean of Phi
+  double residual;       // max|err| at the last convergence check
+  int converged, done, stuck, cur;
+  long long iters;
+  unsigned int arrive;   // last-block ticket of the running reduction
+};
+
+// T: type of the advected state (real_t); P: type of the pressure solve
+// (Phi, the GCR fields and scalars) -- T itself, or double under FP32 advection.
+template <class T, class P>
 struct boussinesq {
   mpdata_state<T> st;
-  field<T> tht_e;
+  general<T> gen{&st};
+  field<T> stash[3], vip_rhs[3], rhs[4], tht_e;
+  field<P> Phi, err[2], lap_err;
+  std::vector<field<P>> p_err, lap_p_err;
   double dt = 0;
-  int ix_tht = 0;
-  long long iters = 0, iters_total = 0;
+  T dtT = 0, g = 0, tht_ref = 0;
+  double dijk[3] = {1, 1, 1};
+  P err_tol = 0;
+  int k_iters = 1, vip[3] = {0, 1, 2}, ix_w = 1, ix_tht = 2;
+  T dt_stash0 = 0;
+  long long iters = 0, iters_total = 0, predicted = 8;
   double last_residual = 0;
-  boussinesq(const mpdx_config &, cudaStream_t) {
-    throw error(MPDX_E_UNSUPPORTED, "Boussinesq solver not built yet");
-  }
-  field<T> *phi_field() { return nullptr; }
-  void advance(long long) {}
+  gcr_dev<P> *dev = nullptr;
+  gcr_dev<P> *hdev = nullptr;  // pinned host copy for the convergence read-back
+  double *part = nullptr;      // per-block partial results of the running reduction
+  double *scratch = nullptr;
+  int *vip_dev = nullptr;      // vip[] on the device
+
+  boussinesq(const mpdx_config &c, cudaStream_t s);
+  ~boussinesq();
+  boussinesq(const boussinesq &) = delete;
+  boussinesq &operator=(const boussinesq &) = delete;
+  field<P> *phi_field() { return &Phi; }
+  void advance(long long nt);
+
+ private:
+  field<T> &vips(int d) { return st.psi[vip[d]][st.tl[vip[d]]]; }
+  void ante_loop();
+  void step();
+  void pressure_solve();  // pressure_solver_update up to the final gradient
 };
+
+extern template struct boussinesq<float, float>;
+extern template struct boussinesq<float, double>;
+extern template struct boussinesq<double, double>;
 
 }  // namespace mpdx

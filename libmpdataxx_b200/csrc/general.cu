@@ -1,6 +1,6 @@
 // Reference-structured MPDATA path: one kernel per libmpdata++ formula and one
 // small kernel per halo fill, launched in the order the reference's solvers call
-// them.  It covers every dimension, the cyclic and open boundary conditions
+// them.  It covers every dimension, the cyclic, open and rigid boundary conditions
 // and the MPDATA options that the fused kernels do not, and it is the FP64
 // parity path (this file is compiled with --fmad=false so that FP64 results
 // follow the reference's rounding).
@@ -8,7 +8,7 @@
 // Reference call structure mirrored here:
 //   advop            libmpdata++/solvers/detail/mpdata_osc_{1,2,3}d.hpp
 //   fct_init / fct_adjust_antidiff   mpdata_fct_{1,2,3}d.hpp
-//   halo exchanges   solvers/detail/solver_{1,2,3}d.hpp, bcond/{cyclic,open}_{1,2,3}d.hpp
+//   halo exchanges   solvers/detail/solver_{1,2,3}d.hpp, bcond/{cyclic,open,rigid}_{1,2,3}d.hpp
 #include <cfloat>
 
 #include "general.cuh"
@@ -324,6 +324,28 @@ __global__ void k_zero_div(dfield<T> Ad, dfield<T> A1, dfield<T> A2, int nd, int
   }
 }
 
+// rigid walls (bcond/rigid_{2,3}d.hpp), halo position f + t, t in [0, cnt):
+//   mode 0 (scalar mirror):   A(f+t) = A(src0 + sgn*t)
+//   mode 1 (pressure):        A(f+t) = 2 A(edge) - A(src0 + sgn*t)
+//   mode 2 (negated mirror):  A(f+t) = -A(src0 + sgn*t)
+template <class T>
+__global__ void k_halo_rigid(dfield<T> A, int nd, int d, int mode, int f, int cnt, int src0, int sgn, int edge,
+                             int bf, int nb, int cf, int nc) {
+  const long long tot = (long long)cnt * nb * nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int c = cf + int(q % nc);
+    const long long r = q / nc;
+    const int b = bf + int(r % nb);
+    const int t = int(r / nb);
+    const T m = PR(A, nd, d, src0 + sgn * t, b, c);
+    T v;
+    if (mode == 0) v = m;
+    else if (mode == 1) v = T(2) * PR(A, nd, d, edge, b, c) - m;
+    else v = -m;
+    PR(A, nd, d, f + t, b, c) = v;
+  }
+}
+
 static unsigned grid_for(long long tot) {
   unsigned g = ceil_div(tot, 256);
   if (g > 65535u * 8u) g = 65535u * 8u;
@@ -349,6 +371,10 @@ void general<T>::fill_sclr(int d, int side, field<T> &A, rng rb, rng rc, bool de
     // zero-gradient (open_{1,2,3}d.hpp fill_halos_sclr)
     const int f = side == 0 ? -H : n, e = side == 0 ? 0 : n - 1;
     k_halo_set<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, f, H, e, !deriv, T(0), rb.f, rb.n(), rc.f, rc.n());
+  } else if (kind == MPDX_BC_RIGID) {
+    // mirror about the wall point: A(-m) = A(m), A(n-1+m) = A(n-1-m)  (rigid_2d.hpp:16-24, 124-132)
+    if (side == 0) k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, 0, -H, H, H, -1, 0, rb.f, rb.n(), rc.f, rc.n());
+    else k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, 0, n, H, n - 2, -1, 0, rb.f, rb.n(), rc.f, rc.n());
   } else {
     throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for scalars on this path");
   }
@@ -356,10 +382,52 @@ void general<T>::fill_sclr(int d, int side, field<T> &A, rng rb, rng rc, bool de
 }
 
 template <class T>
-void general<T>::fill_vctr_nrml(int d, int side, field<T> &A, rng rb, rng rc) {
+void general<T>::fill_pres(int d, int side, field<T> &A, rng rb, rng rc) {
   auto &S = *s;
   const int kind = S.bcs[d][side];
   if (kind == MPDX_BC_CYCLIC) { fill_sclr(d, side, A, rb, rc); return; }
+  if (kind != MPDX_BC_RIGID) throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for pressure on this path");
+  const int nd = S.nd, H = S.H, n = S.n[d];
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  const long long tot = (long long)H * rb.n() * rc.n();
+  // A(-m) = 2 A(0) - A(m);  A(n-1+m) = 2 A(n-1) - A(n-1-m)  (rigid_2d.hpp:26-35, 134-143)
+  if (side == 0) k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, 1, -H, H, H, -1, 0, rb.f, rb.n(), rc.f, rc.n());
+  else k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(A.v, nd, d, 1, n, H, n - 2, -1, n - 1, rb.f, rb.n(), rc.f, rc.n());
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::set_edge_pres(int d, int side, field<T> &A, rng rb, rng rc) {
+  auto &S = *s;
+  if (S.bcs[d][side] != MPDX_BC_RIGID) return;  // no-op for cyclic (cyclic_2d.hpp:42)
+  const int nd = S.nd;
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  const int e = side == 0 ? 0 : S.n[d] - 1;  // rigid_2d.hpp:52-56, 148-152
+  k_halo_set<T><<<grid_for((long long)rb.n() * rc.n()), 256, 0, S.stream>>>(A.v, nd, d, e, 1, 0, false, T(0), rb.f, rb.n(), rc.f, rc.n());
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::fill_flux(int d, int side, field<T> *AV, rng rb, rng rc) {
+  auto &S = *s;
+  if (S.bcs[d][side] != MPDX_BC_RIGID) return;  // no-op for cyclic and open
+  const int nd = S.nd, n = S.n[d];
+  if (nd < 2) rb = {0, 0};
+  if (nd < 3) rc = {0, 0};
+  // F(-1) = -F(0);  F(n-1) = -F(n-2)  (rigid_2d.hpp:74-79, 170-175)
+  const long long tot = (long long)rb.n() * rc.n();
+  if (side == 0) k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, nd, d, 2, -1, 1, 0, 1, 0, rb.f, rb.n(), rc.f, rc.n());
+  else k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, nd, d, 2, n - 1, 1, n - 2, 1, 0, rb.f, rb.n(), rc.f, rc.n());
+  MPDX_LAUNCH_CHECK();
+}
+
+template <class T>
+void general<T>::fill_vctr_nrml(int d, int side, field<T> &A, rng rb, rng rc) {
+  auto &S = *s;
+  const int kind = S.bcs[d][side];
+  if (kind == MPDX_BC_CYCLIC || kind == MPDX_BC_RIGID) { fill_sclr(d, side, A, rb, rc); return; }  // rigid: as scalars
   if (kind != MPDX_BC_OPEN) throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for vectors on this path");
   const int nd = S.nd, H = S.H, n = S.n[d];
   if (nd < 2) rb = {0, 0};
@@ -386,6 +454,19 @@ void general<T>::fill_vctr_alng(int d, int side, field<T> *AV, rng rb, rng rc, b
     return;
   }
   if (cyclic_only) return;
+  if (kind == MPDX_BC_RIGID) {
+    // zero normal velocity at the wall point (rigid_2d.hpp:58-66, 154-162):
+    // left  GC(-m) = -GC(m-1) for m = H .. 1 (.. 2 with ad);
+    // right GC(n-1+a+t) = -GC(n-2-t), t = 0 .. H-1-a, a = ad (the reference's counter starts at 1 either way)
+    const int a = ad ? 1 : 0;
+    const long long tot = (long long)(H - a) * rb.n() * rc.n();
+    if (H - a > 0) {
+      if (side == 0) k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, nd, d, 2, -H, H - a, H - 1, -1, 0, rb.f, rb.n(), rc.f, rc.n());
+      else k_halo_rigid<T><<<grid_for(tot), 256, 0, S.stream>>>(AV[d].v, nd, d, 2, n - 1 + a, H - a, n - 2, -1, 0, rb.f, rb.n(), rc.f, rc.n());
+      MPDX_LAUNCH_CHECK();
+    }
+    return;
+  }
   if (kind != MPDX_BC_OPEN) throw error(MPDX_E_UNSUPPORTED, "boundary condition not supported for vectors on this path");
   if (nd == 1) {  // open_1d.hpp:36-40, 66-70
     int f, cnt, src;
@@ -475,6 +556,59 @@ void general<T>::xchng_vctr_nrml(field<T> *AV, int ex) {
   for (int q = 0; q < 2; ++q) fill_vctr_nrml(2, q, AV[1], ext(ext(ir[0], ex), 1), exh(ext(ir[1], ex)));
   for (int q = 0; q < 2; ++q) fill_vctr_nrml(0, q, AV[2], ext(ext(ir[1], ex), 1), exh(ext(ir[2], ex)));
   for (int q = 0; q < 2; ++q) fill_vctr_nrml(1, q, AV[2], exh(ext(ir[2], ex)), ext(ext(ir[0], ex), 1));
+}
+
+template <class T>
+void general<T>::xchng_flux(field<T> *AV) {  // solver_2d.hpp:90-101, solver_3d.hpp:105-118
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) { for (int q = 0; q < 2; ++q) fill_flux(0, q, AV, {0, 0}, {0, 0}); return; }
+  if (S.nd == 2) {
+    for (int q = 0; q < 2; ++q) fill_flux(0, q, AV, ir[1], {0, 0});
+    for (int q = 0; q < 2; ++q) fill_flux(1, q, AV, ir[0], {0, 0});
+    return;
+  }
+  for (int q = 0; q < 2; ++q) fill_flux(0, q, AV, ir[1], ir[2]);
+  for (int q = 0; q < 2; ++q) fill_flux(1, q, AV, ir[2], ir[0]);
+  for (int q = 0; q < 2; ++q) fill_flux(2, q, AV, ir[0], ir[1]);
+}
+
+template <class T>
+void general<T>::xchng_pres(field<T> &A, int ex) {  // solver_2d.hpp:204-220, solver_3d.hpp:288-307
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) { for (int q = 0; q < 2; ++q) fill_pres(0, q, A, {0, 0}, {0, 0}); return; }
+  if (S.nd == 2) {
+    for (int q = 0; q < 2; ++q) fill_pres(0, q, A, ext(ir[1], ex), {0, 0});
+    for (int q = 0; q < 2; ++q) fill_pres(1, q, A, ext(ir[0], ex), {0, 0});
+    return;
+  }
+  for (int q = 0; q < 2; ++q) fill_pres(0, q, A, ext(ir[1], ex), ext(ir[2], ex));
+  for (int q = 0; q < 2; ++q) fill_pres(1, q, A, ext(ir[2], ex), ext(ir[0], ex));
+  for (int q = 0; q < 2; ++q) fill_pres(2, q, A, ext(ir[0], ex), ext(ir[1], ex));
+}
+
+template <class T>
+void general<T>::set_edges(field<T> *const *AV) {  // solver_2d.hpp:222-237, solver_3d.hpp:309-326
+  auto &S = *s;
+  const rng *ir = S.ir;
+  if (S.nd == 1) { for (int q = 0; q < 2; ++q) set_edge_pres(0, q, *AV[0], {0, 0}, {0, 0}); return; }
+  if (S.nd == 2) {
+    for (int q = 0; q < 2; ++q) set_edge_pres(0, q, *AV[0], ir[1], {0, 0});
+    for (int q = 0; q < 2; ++q) set_edge_pres(1, q, *AV[1], ir[0], {0, 0});
+    return;
+  }
+  for (int q = 0; q < 2; ++q) set_edge_pres(0, q, *AV[0], ir[1], ir[2]);
+  for (int q = 0; q < 2; ++q) set_edge_pres(1, q, *AV[1], ir[2], ir[0]);
+  for (int q = 0; q < 2; ++q) set_edge_pres(2, q, *AV[2], ir[0], ir[1]);
+}
+
+template <class T>
+bool general<T>::any_rigid() const {
+  for (int d = 0; d < s->nd; ++d)
+    for (int q = 0; q < 2; ++q)
+      if (s->bcs[d][q] == MPDX_BC_RIGID) return true;
+  return false;
 }
 
 template <class T>
@@ -574,6 +708,7 @@ void general<T>::advop_nd(int e) {
     field<T> *flx = S.flux;
     if (!(S.opts & o_iga) || iter == 0) fluxes_nd<ND>(S.flux, p, GCit(iter), false);
     else flx = GCit(iter);
+    if (any_rigid()) xchng_flux(flx);  // mpdata_osc_2d.hpp:154-155 (a no-op without rigid walls)
     const dfield<T> z = flx[0].v;
     launch_frame<ND, 0>(S.stream, op_donorcell<ND, T>{S.psi[e][S.tl[e] ^ 1].v, p.v, flx[0].v, ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z},
                         S.ir[0], ND > 1 ? S.ir[1] : rng{0, 0}, ND > 2 ? S.ir[2] : rng{0, 0});

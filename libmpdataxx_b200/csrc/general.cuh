@@ -25,6 +25,14 @@ struct general {
   void fill_sclr(int d, int side, field<T> &A, rng rb, rng rc, bool deriv = false);
   void fill_vctr_nrml(int d, int side, field<T> &A, rng rb, rng rc);
   void fill_vctr_alng(int d, int side, field<T> *AV, rng rb, rng rc, bool ad, bool cyclic_only);
+  // pressure-solver exchanges (solver_{2,3}d.hpp xchng_pres / set_edges / xchng_flux)
+  void xchng_pres(field<T> &A, int ex);
+  void set_edges(field<T> *const *AV);
+  void xchng_flux(field<T> *AV);
+  void fill_pres(int d, int side, field<T> &A, rng rb, rng rc);
+  void set_edge_pres(int d, int side, field<T> &A, rng rb, rng rc);
+  void fill_flux(int d, int side, field<T> *AV, rng rb, rng rc);
+  bool any_rigid() const;
 
  private:
   field<T> *GC_unco(int iter);

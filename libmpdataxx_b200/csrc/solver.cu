@@ -6,6 +6,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "boussinesq.cuh"
@@ -162,16 +163,17 @@ struct mpdata_solver : solver_base {
   }
 };
 
-// Boussinesq handle (solvers::boussinesq with GCR pressure solve)
-template <class T>
+// Boussinesq handle (solvers::boussinesq with GCR pressure solve); P is the
+// type of the pressure solve (T, or double under FP32 advection with prs_fp64)
+template <class T, class P>
 struct boussinesq_solver : solver_base {
-  std::unique_ptr<boussinesq<T>> b;
+  std::unique_ptr<boussinesq<T, P>> b;
   transfer<T> xfer;
   stats_engine<T> stat;
   explicit boussinesq_solver(const mpdx_config &c) {
     dtype = sizeof(T);
     MPDX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    b.reset(new boussinesq<T>(c, stream));
+    b.reset(new boussinesq<T, P>(c, stream));
   }
   void view(int kind, int idx, int ex[3], int off[3], field<T> *&f) {
     auto &st = b->st;
@@ -186,7 +188,10 @@ struct boussinesq_solver : solver_base {
       f = &b->tht_e;
       return;
     }
-    if (kind == MPDX_FIELD_PRESSURE) { f = b->phi_field(); if (!f) throw error(MPDX_E_ARG, "pressure stored in FP64; use the FP64 accessor"); return; }
+    if (kind == MPDX_FIELD_PRESSURE) {
+      if constexpr (std::is_same<T, P>::value) { f = b->phi_field(); return; }
+      throw error(MPDX_E_ARG, "the pressure is held in FP64 in this configuration and has no real_t view");
+    }
     throw error(MPDX_E_ARG, "field kind not available for this solver");
   }
   void view_extent(int kind, int idx, int ex[3]) override {
@@ -258,8 +263,6 @@ void validate(const mpdx_config &c) {
   for (int q = 0; q < 2 * c.n_dims; ++q) {
     const int k = c.bcs[q];
     if (k != MPDX_BC_CYCLIC && k != MPDX_BC_OPEN && k != MPDX_BC_RIGID) throw error(MPDX_E_ARG, "unknown boundary kind");
-    if (k == MPDX_BC_RIGID && c.solver != MPDX_SOLVER_BOUSSINESQ)
-      throw error(MPDX_E_UNSUPPORTED, "rigid boundaries are built for the Boussinesq solver only");
   }
 }
 }  // namespace
@@ -297,8 +300,9 @@ mpdx_status mpdx_create(const mpdx_config *cfg, mpdx_handle *out) {
     validate(*cfg);
     auto h = std::make_unique<mpdx_solver>();
     if (cfg->solver == MPDX_SOLVER_BOUSSINESQ) {
-      if (cfg->dtype == 8) h->impl.reset(new mpdx::boussinesq_solver<double>(*cfg));
-      else h->impl.reset(new mpdx::boussinesq_solver<float>(*cfg));
+      if (cfg->dtype == 8) h->impl.reset(new mpdx::boussinesq_solver<double, double>(*cfg));
+      else if (cfg->prs_fp64) h->impl.reset(new mpdx::boussinesq_solver<float, double>(*cfg));
+      else h->impl.reset(new mpdx::boussinesq_solver<float, float>(*cfg));
     } else {
       if (cfg->dtype == 8) h->impl.reset(new mpdx::mpdata_solver<double>(*cfg));
       else h->impl.reset(new mpdx::mpdata_solver<float>(*cfg));

@@ -32,7 +32,7 @@ struct mpdata_state {
     return h;
   }
   rng sr(int d) const { return d < nd ? ext(ir[d], H) : rng{0, 0}; }
-  void alloc_sclr(field<T> &f) { rng r[3] = {sr(0), sr(1), sr(2)}; f.alloc(nd, r); }
+  template <class U> void alloc_sclr(field<U> &f) { rng r[3] = {sr(0), sr(1), sr(2)}; f.alloc(nd, r); }
   void alloc_vctr(field<T> *v) {
     for (int c = 0; c < nd; ++c) {
       rng r[3] = {sr(0), sr(1), sr(2)};

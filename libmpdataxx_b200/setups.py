@@ -208,3 +208,49 @@ def wrap_periodic(u):
     for ax in range(u.ndim):
         u = np.concatenate([u, np.take(u, [0], axis=ax)], axis=ax)
     return u
+
+
+# --- tests/paper_2015_GMD/8_boussinesq_2d/boussinesq_2d.cpp:17-117 ------------
+def boussinesq_2d(nx=201, ny=201, r0=250.0):
+    """Buoyant thermal (Smolarkiewicz & Pudykiewicz 1992, fig. 3): equations
+    (u, w, tht), cyclic in x and y, cr pressure solver, 800 steps."""
+    dx = 10.0
+    tht_ref = 300.0
+    i, j = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(ny, dtype=np.float64), indexing="ij")
+    tht = tht_ref + np.where((i * dx - 4 * r0) ** 2 + (j * dx - 1.04 * r0) ** 2 <= r0 ** 2, 0.5, 0.0)
+    return {"grid": (nx, ny), "bcs": ["cyclic"] * 4, "advectee": [np.zeros((nx, ny)), np.zeros((nx, ny)), tht],
+            "tht_e": np.full((nx, ny), tht_ref), "dt": 0.75, "dx": (dx, dx, 1.0), "tht_ref": tht_ref, "g": 9.81,
+            "prs_tol": 1e-7, "nt": 800, "prs_k": 1}
+
+
+def boussinesq_stats(tht, u, w, tht_ref, init):
+    """The statistics printed by tests/paper_2015_GMD/8_boussinesq_2d/boussinesq_stats.hpp:58-118:
+    sums leave out the first row and column (duplicated cyclic edge)."""
+    pert = (tht - tht_ref)[1:, 1:]
+    s2 = float((((init - tht_ref)[1:, 1:]) ** 2).sum())
+    return {"min(tht)": float(tht.min()), "max(tht)": float(tht.max()),
+            "max(velocity)": float(np.sqrt(u ** 2 + w ** 2).max()),
+            "error_2": (float((pert ** 2).sum()) - s2) / s2 * 100}
+
+
+def boussinesq_bubble_3d(nx=256, ny=256, nz=128, seed=6, dx=10.0, n_bv=0.01, dtype=np.float64):
+    """Stably stratified 3D thermal: tht_e(z) = 300 exp(N^2 z / g), zero wind,
+    a +0.5 K sphere of radius 0.1 nx dx centred at (Lx/2, Ly/2, Lz/4) plus
+    seeded uniform noise of +-0.01 K; x and y cyclic, z rigid.  Equations
+    (u, v, w, tht)."""
+    g, tref = 9.81, 300.0
+    rng = np.random.default_rng(seed)
+    i, j, k = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(ny, dtype=np.float64),
+                          np.arange(nz, dtype=np.float64), indexing="ij")
+    z = k * dx
+    tht_e = tref * np.exp(n_bv ** 2 * z / g)
+    r = 0.1 * nx * dx
+    inside = (i * dx - 0.5 * (nx - 1) * dx) ** 2 + (j * dx - 0.5 * (ny - 1) * dx) ** 2 + (z - 0.25 * (nz - 1) * dx) ** 2 <= r * r
+    tht = tht_e + np.where(inside, 0.5, 0.0) + rng.uniform(-0.01, 0.01, size=(nx, ny, nz))
+    # duplicated-endpoint convention of the cyclic axes
+    tht[-1, :, :] = tht[0, :, :]
+    tht[:, -1, :] = tht[:, 0, :]
+    zero = np.zeros((nx, ny, nz))
+    return {"grid": (nx, ny, nz), "bcs": ["cyclic", "cyclic", "cyclic", "cyclic", "rigid", "rigid"],
+            "advectee": [zero, zero.copy(), zero.copy(), tht.astype(dtype)], "tht_e": tht_e.astype(dtype),
+            "dt": 0.75, "dx": (dx, dx, dx), "tht_ref": tref, "g": g, "prs_tol": 1e-7, "prs_k": 1}

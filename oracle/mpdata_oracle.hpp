@@ -229,12 +229,46 @@ struct mpdata {
         rng h = side == 0 ? left_halo_sclr(d) : rght_halo_sclr(d);
         int e = side == 0 ? 0 : n[d] - 1;
         for (int i = h.f; i <= h.l; ++i) PR(A, nd, d, i, b, c) = deriv ? T(0) : PR(A, nd, d, e, b, c);
+      } else if (kind == bc_rigid) {
+        // mirror about the edge point (rigid_2d.hpp:16-24, 124-132; rigid_3d.hpp:30-38)
+        if (side == 0) { for (int m = 1; m <= H; ++m) PR(A, nd, d, -m, b, c) = PR(A, nd, d, m, b, c); }
+        else { for (int m = 1; m <= H; ++m) PR(A, nd, d, n[d] - 1 + m, b, c) = PR(A, nd, d, n[d] - 1 - m, b, c); }
       } else throw std::runtime_error("oracle: bcond kind not supported for scalars");
+    });
+  }
+  // fill_halos_pres: cyclic as scalars; rigid one-sided-derivative extrapolation
+  // (rigid_2d.hpp:26-35, 134-143; rigid_3d.hpp:40-49)
+  void fill_pres(int d, int side, arr<T> &A, rng rb, rng rc) {
+    const int kind = bcs[d][side];
+    if (kind == bc_cyclic) { fill_sclr(d, side, A, rb, rc); return; }
+    if (kind != bc_rigid) throw std::runtime_error("oracle: bcond kind not supported for pressure");
+    each(rb, rc, [&](int b, int c) {
+      if (side == 0) {
+        for (int m = H; m >= 1; --m) PR(A, nd, d, -m, b, c) = T(2) * PR(A, nd, d, 0, b, c) - PR(A, nd, d, m, b, c);
+      } else {
+        const int e = n[d] - 1;
+        for (int m = 1; m <= H; ++m) PR(A, nd, d, e + m, b, c) = T(2) * PR(A, nd, d, e, b, c) - PR(A, nd, d, e - m, b, c);
+      }
+    });
+  }
+  // set_edge_pres: zero on a rigid wall point, no-op otherwise (rigid_2d.hpp:52-56, 148-152)
+  void set_edge_pres(int d, int side, arr<T> &A, rng rb, rng rc) {
+    if (bcs[d][side] != bc_rigid) return;
+    const int e = side == 0 ? 0 : n[d] - 1;
+    each(rb, rc, [&](int b, int c) { PR(A, nd, d, e, b, c) = T(0); });
+  }
+  // fill_halos_flux: antisymmetric face next to a rigid wall, no-op otherwise
+  // (rigid_2d.hpp:74-79, 170-175; rigid_3d.hpp:73-78)
+  void fill_flux(int d, int side, vctr<T> &AV, rng rb, rng rc) {
+    if (bcs[d][side] != bc_rigid) return;
+    each(rb, rc, [&](int b, int c) {
+      if (side == 0) PR(AV[d], nd, d, -1, b, c) = -PR(AV[d], nd, d, 0, b, c);
+      else PR(AV[d], nd, d, n[d] - 1, b, c) = -PR(AV[d], nd, d, n[d] - 2, b, c);
     });
   }
   void fill_vctr_nrml(int d, int side, arr<T> &A, rng rb, rng rc) {
     const int kind = bcs[d][side];
-    if (kind == bc_cyclic) { fill_sclr(d, side, A, rb, rc); return; }
+    if (kind == bc_cyclic || kind == bc_rigid) { fill_sclr(d, side, A, rb, rc); return; }  // rigid: "intentional sclr"
     if (kind == bc_open) {
       rng h = side == 0 ? left_halo_sclr(d) : rght_halo_sclr(d);
       each(rb, rc, [&](int b, int c) { for (int i = h.f; i <= h.l; ++i) PR(A, nd, d, i, b, c) = T(0); });
@@ -254,6 +288,16 @@ struct mpdata {
       return;
     }
     if (cyclic_only) return;  // fill_halos_vctr_alng_cyclic is a no-op for non-cyclic bconds
+    if (kind == bc_rigid) {  // zero normal velocity on the wall point (rigid_2d.hpp:58-66, 154-162)
+      each(rb, rc, [&](int b, int c) {
+        if (side == 0) { for (int m = H; m >= (ad ? 2 : 1); --m) PR(AV[d], nd, d, -m, b, c) = -PR(AV[d], nd, d, m - 1, b, c); }
+        else {  // the counter starts at 1 also when ad skips the first halo face
+          const int a0 = ad ? 1 : 0;
+          for (int t = 0; t < H - a0; ++t) PR(AV[d], nd, d, n[d] - 1 + a0 + t, b, c) = -PR(AV[d], nd, d, n[d] - 2 - t, b, c);
+        }
+      });
+      return;
+    }
     if (kind != bc_open) throw std::runtime_error("oracle: bcond kind not supported for vectors");
     if (nd == 1) {  // open_1d.hpp:36-40, 66-70
       if (side == 0) { rng h = left_halo_vctr(0); T v = AV[0](left_intr_vctr(0).f, 0, 0);
@@ -342,6 +386,43 @@ struct mpdata {
     for (int s = 0; s < 2; ++s) fill_vctr_nrml(2, s, AV[1], ext(ext(ir[0], ex), 1), exh(ext(ir[1], ex)));
     for (int s = 0; s < 2; ++s) fill_vctr_nrml(0, s, AV[2], ext(ext(ir[1], ex), 1), exh(ext(ir[2], ex)));
     for (int s = 0; s < 2; ++s) fill_vctr_nrml(1, s, AV[2], exh(ext(ir[2], ex)), ext(ext(ir[0], ex), 1));
+  }
+
+  // solver_2d.hpp:90-101, solver_3d.hpp:105-118
+  void xchng_flux(vctr<T> &AV) {
+    if (nd == 1) { for (int s = 0; s < 2; ++s) fill_flux(0, s, AV, {0, 0}, {0, 0}); return; }
+    if (nd == 2) {
+      for (int s = 0; s < 2; ++s) fill_flux(0, s, AV, ir[1], {0, 0});
+      for (int s = 0; s < 2; ++s) fill_flux(1, s, AV, ir[0], {0, 0});
+      return;
+    }
+    for (int s = 0; s < 2; ++s) fill_flux(0, s, AV, ir[1], ir[2]);
+    for (int s = 0; s < 2; ++s) fill_flux(1, s, AV, ir[2], ir[0]);
+    for (int s = 0; s < 2; ++s) fill_flux(2, s, AV, ir[0], ir[1]);
+  }
+  // solver_2d.hpp:204-220, solver_3d.hpp:288-307
+  void xchng_pres(arr<T> &A, int ex = 0) {
+    if (nd == 1) { for (int s = 0; s < 2; ++s) fill_pres(0, s, A, {0, 0}, {0, 0}); return; }
+    if (nd == 2) {
+      for (int s = 0; s < 2; ++s) fill_pres(0, s, A, ext(ir[1], ex), {0, 0});
+      for (int s = 0; s < 2; ++s) fill_pres(1, s, A, ext(ir[0], ex), {0, 0});
+      return;
+    }
+    for (int s = 0; s < 2; ++s) fill_pres(0, s, A, ext(ir[1], ex), ext(ir[2], ex));
+    for (int s = 0; s < 2; ++s) fill_pres(1, s, A, ext(ir[2], ex), ext(ir[0], ex));
+    for (int s = 0; s < 2; ++s) fill_pres(2, s, A, ext(ir[0], ex), ext(ir[1], ex));
+  }
+  // solver_2d.hpp:222-237, solver_3d.hpp:309-326 (the sign argument is unused by every bcond here)
+  void set_edges(const std::array<arr<T> *, 3> &AV) {
+    if (nd == 1) { for (int s = 0; s < 2; ++s) set_edge_pres(0, s, *AV[0], {0, 0}, {0, 0}); return; }
+    if (nd == 2) {
+      for (int s = 0; s < 2; ++s) set_edge_pres(0, s, *AV[0], ir[1], {0, 0});
+      for (int s = 0; s < 2; ++s) set_edge_pres(1, s, *AV[1], ir[0], {0, 0});
+      return;
+    }
+    for (int s = 0; s < 2; ++s) set_edge_pres(0, s, *AV[0], ir[1], ir[2]);
+    for (int s = 0; s < 2; ++s) set_edge_pres(1, s, *AV[1], ir[2], ir[0]);
+    for (int s = 0; s < 2; ++s) set_edge_pres(2, s, *AV[2], ir[0], ir[1]);
   }
 
   // ---- mpdata_common.hpp:40-60 ----
@@ -581,9 +662,10 @@ struct mpdata {
         if (opts & o_fct) fct_adjust_antidiff(e, iter);
       }
       const arr<T> &p = psi[e][tl[e]];
-      const vctr<T> *flx = &flux;
+      vctr<T> *flx = &flux;
       if (!(opts & o_iga) || iter == 0) fluxes(flux, p, GCit(iter), false);
       else flx = &GCit(iter);
+      xchng_flux(*flx);  // mpdata_osc_2d.hpp:154-155
       donorcell_sum(psi[e][(tl[e] + 1) % 2], p, *flx);
     }
   }

@@ -55,7 +55,7 @@ def random_setup(grid, bcs, seed, signed=False):
 
 CASES = []
 for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
-    for bc in ("cyclic", "open"):
+    for bc in ("cyclic", "open", "rigid"):
         for opts, iters in [(0, 1), (0, 2), (o.fct, 2), (o.iga, 2), (o.iga | o.fct, 2), (o.fct, 3), (0, 3),
                             (o.abs, 2), (o.abs | o.fct, 2), (o.pfc, 2), (o.npa | o.fct, 2)]:
             CASES.append((nd, grid, bc, opts, iters))
@@ -68,9 +68,13 @@ CASES.append((1, (37,), "cyclic", o.tot, 3))
 def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
     bcs = [bc] * (2 * nd)
     s = random_setup(grid, bcs, seed=nd * 100 + iters, signed=bool(opts & (o.abs | o.iga)))
-    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=1e-10)
+    # rigid walls mirror the normal Courant number with a sign flip, so a field that
+    # is not zero on the wall faces fails the reference's divergence guard; the
+    # guard is lifted for those cases (the numerics under test do not depend on it)
+    eps = 1e30 if bc == "rigid" else 1e-10
+    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)
     load(orc, s)
-    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=1e-10)
+    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)
     run.set_advectee(s["advectee"][0])
     for d, a in enumerate(s["advector"]):
         run.set_advector(a, d)

@@ -88,3 +88,42 @@ def test_divergent_advector_raises():
 def test_bogus_grid_raises():
     with pytest.raises(RuntimeError, match="bogus grid size"):
         Oracle((0, 4), o.fct)
+
+
+# --- tests/paper_2015_GMD/8_boussinesq_2d: stats.txt.gz every 10 steps ---------
+def _bq_golden_check(orc, s, rows):
+    from libmpdataxx_b200.setups import boussinesq_stats
+    init = s["advectee"][2]
+    for row in rows:
+        orc.advance(row["timestep"] - orc.timestep)
+        st = boussinesq_stats(orc.advectee(2), orc.advectee(0), orc.advectee(1), s["tht_ref"], init)
+        for key, v in st.items():
+            # stats.txt prints std::scientific with 6 digits after the point
+            assert float("%.6e" % v) == row[key], (row["timestep"], key, v, row[key])
+
+
+def test_boussinesq_2d_golden_first_steps():
+    from libmpdataxx_b200.setups import boussinesq_2d
+    from runners import bq_oracle
+    s = boussinesq_2d()
+    rows = golden()["boussinesq_2d"]["rows"]
+    _bq_golden_check(bq_oracle(s), s, [r for r in rows if r["timestep"] <= 30])
+
+
+@pytest.mark.slow
+def test_boussinesq_2d_golden_800_steps():
+    from libmpdataxx_b200.setups import boussinesq_2d
+    from runners import bq_oracle
+    s = boussinesq_2d()
+    _bq_golden_check(bq_oracle(s), s, golden()["boussinesq_2d"]["rows"])
+
+
+def test_boussinesq_pressure_solver_stuck():
+    """More than 10000 GCR iterations throw the reference's error (mpdata_rhs_vip_prs_common.hpp:118-122)."""
+    from libmpdataxx_b200.setups import boussinesq_2d
+    from runners import bq_oracle
+    s = boussinesq_2d(nx=17, ny=17, r0=30.0)
+    s["prs_tol"] = 1e-300
+    orc = bq_oracle(s)
+    with pytest.raises(RuntimeError, match="stuck in pressure solver"):
+        orc.advance(1)
