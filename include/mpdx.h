@@ -157,6 +157,66 @@ void mpdx_destroy(mpdx_handle h);
 mpdx_status mpdx_field_stats_noalloc(const void *dev_field, int dtype, const int64_t *n, const int64_t *strides,
                                      const int64_t *m, double *dev_out, void *stream, char *err, int errlen);
 
+/* ---- Batched advance of independent 2D problems ----
+ *
+ * No counterpart in the reference, where every run object advances alone.  A
+ * batch groups existing handles (2D, same dtype, opts and n_iters, one
+ * equation, cyclic boundaries, opts within fct/iga) and advances all of them
+ * together: MPDX_BATCH_PERSISTENT runs one persistent fused launch per step,
+ * whose tile shape an autotuner picks by timing the first steps (results do
+ * not depend on it), captured with the next steps in a CUDA graph;
+ * MPDX_BATCH_PER_PROBLEM launches the fused kernel once per problem per step.
+ * The handles stay usable (fields, stats) between batched advances; the batch
+ * must be destroyed before its handles.  Errors of mpdx_batch_create are in
+ * mpdx_create_error(). */
+typedef struct mpdx_batch *mpdx_batch_handle;
+enum { MPDX_BATCH_PERSISTENT = 0, MPDX_BATCH_PER_PROBLEM = 1 };
+
+typedef struct {
+  int n_problems;
+  int64_t cells;        /* sum over the problems of n0 x n1 */
+  int mode;             /* MPDX_BATCH_* */
+  int tile_nt, tile_lx; /* tile chosen by the autotuner (0 until tuning ends) */
+  int grid;             /* resident CTAs of the persistent launch */
+  int n_candidates;     /* tile candidates timed by the autotuner */
+  double tune_ms[8];    /* measured ms of one batched step per candidate (0 = not measured yet) */
+} mpdx_batch_info;
+
+mpdx_status mpdx_batch_create(const mpdx_handle *handles, int n, int mode, mpdx_batch_handle *out);
+mpdx_status mpdx_batch_advance(mpdx_batch_handle b, int64_t nt);
+mpdx_status mpdx_batch_get_info(mpdx_batch_handle b, mpdx_batch_info *out);
+mpdx_status mpdx_batch_sync(mpdx_batch_handle b);
+const char *mpdx_batch_last_error(mpdx_batch_handle b);
+void mpdx_batch_destroy(mpdx_batch_handle b);
+
+/* ---- Learned GCR preconditioner network on its own ----
+ *
+ * No counterpart in the reference.  A linear 4-level 3D (or 2D) U-net that maps
+ * a residual field to a search direction, with BF16 tensor-core convolutions
+ * (architecture in libmpdataxx_b200/csrc/precond.cu).  grid: points per axis;
+ * wrap[d] = 1 pads axis d cyclically, 0 with zeros; channels: the four levels'
+ * channel counts (8, 16, 32 or 64; level 0 at most 16).  Parameters are FP32
+ * in the order e0 e1 e2 e3 m3 d2 d1 d0 q, each weight (cout, taps, cin) followed
+ * by its bias (cout); taps run over offsets -1..1 with the last axis fastest.
+ * Host arrays are C-ordered over the grid.  Errors of create are in
+ * mpdx_pcnet_create_error(). */
+typedef struct mpdx_pcnet *mpdx_pcnet_handle;
+mpdx_status mpdx_pcnet_create(int nd, const int *grid, const int *wrap, const int *channels, uint64_t seed,
+                              mpdx_pcnet_handle *out);
+const char *mpdx_pcnet_create_error(void);
+int64_t mpdx_pcnet_num_params(mpdx_pcnet_handle h);
+mpdx_status mpdx_pcnet_set_params(mpdx_pcnet_handle h, const float *host);
+mpdx_status mpdx_pcnet_get_params(mpdx_pcnet_handle h, float *host);
+/* q = net(r) */
+mpdx_status mpdx_pcnet_forward(mpdx_pcnet_handle h, const float *r_host, float *q_host);
+/* gradient of sum(dq * net(r)) with respect to every parameter */
+mpdx_status mpdx_pcnet_backward(mpdx_pcnet_handle h, const float *r_host, const float *dq_host, float *grad_host);
+/* one Adam step (weights only; the biases stay as they are) on mean((net(r) - target)^2) */
+mpdx_status mpdx_pcnet_train_step(mpdx_pcnet_handle h, const float *r_host, const float *target_host, float lr,
+                                  double *loss);
+const char *mpdx_pcnet_last_error(mpdx_pcnet_handle h);
+void mpdx_pcnet_destroy(mpdx_pcnet_handle h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,12 @@ SCLR_THT_E = 0
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
            "mpdx_get_field_device", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
-           "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc"]
+           "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc", "mpdx_batch_create", "mpdx_batch_advance",
+           "mpdx_batch_get_info", "mpdx_batch_sync", "mpdx_batch_last_error", "mpdx_batch_destroy",
+           "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
+           "mpdx_pcnet_get_params", "mpdx_pcnet_forward", "mpdx_pcnet_backward", "mpdx_pcnet_train_step",
+           "mpdx_pcnet_last_error", "mpdx_pcnet_destroy"]
+BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 
 
 class Config(ctypes.Structure):
@@ -42,6 +47,12 @@ class StepStats(ctypes.Structure):
     _fields_ = [("timestep", ctypes.c_int64), ("time", ctypes.c_double), ("mass", ctypes.c_double),
                 ("min", ctypes.c_double), ("max", ctypes.c_double), ("gcr_iters", ctypes.c_int64),
                 ("gcr_iters_total", ctypes.c_int64), ("gcr_residual", ctypes.c_double), ("path", ctypes.c_int)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("n_problems", ctypes.c_int), ("cells", ctypes.c_int64), ("mode", ctypes.c_int),
+                ("tile_nt", ctypes.c_int), ("tile_lx", ctypes.c_int), ("grid", ctypes.c_int),
+                ("n_candidates", ctypes.c_int), ("tune_ms", ctypes.c_double * 8)]
 
 
 _lib = None
@@ -79,6 +90,38 @@ def lib():
     L.mpdx_last_error.restype = ctypes.c_char_p
     L.mpdx_destroy.argtypes = [vp]
     L.mpdx_destroy.restype = None
+    L.mpdx_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.mpdx_batch_create.restype = ctypes.c_int
+    L.mpdx_batch_advance.argtypes = [vp, ctypes.c_int64]
+    L.mpdx_batch_advance.restype = ctypes.c_int
+    L.mpdx_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
+    L.mpdx_batch_get_info.restype = ctypes.c_int
+    L.mpdx_batch_sync.argtypes = [vp]
+    L.mpdx_batch_sync.restype = ctypes.c_int
+    L.mpdx_batch_last_error.argtypes = [vp]
+    L.mpdx_batch_last_error.restype = ctypes.c_char_p
+    L.mpdx_batch_destroy.argtypes = [vp]
+    L.mpdx_batch_destroy.restype = None
+    ip, fp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
+    L.mpdx_pcnet_create.argtypes = [ctypes.c_int, ip, ip, ip, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.mpdx_pcnet_create.restype = ctypes.c_int
+    L.mpdx_pcnet_create_error.argtypes = []
+    L.mpdx_pcnet_create_error.restype = ctypes.c_char_p
+    L.mpdx_pcnet_num_params.argtypes = [vp]
+    L.mpdx_pcnet_num_params.restype = ctypes.c_int64
+    for f in ("mpdx_pcnet_set_params", "mpdx_pcnet_get_params"):
+        getattr(L, f).argtypes = [vp, fp]
+        getattr(L, f).restype = ctypes.c_int
+    L.mpdx_pcnet_forward.argtypes = [vp, fp, fp]
+    L.mpdx_pcnet_forward.restype = ctypes.c_int
+    L.mpdx_pcnet_backward.argtypes = [vp, fp, fp, fp]
+    L.mpdx_pcnet_backward.restype = ctypes.c_int
+    L.mpdx_pcnet_train_step.argtypes = [vp, fp, fp, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
+    L.mpdx_pcnet_train_step.restype = ctypes.c_int
+    L.mpdx_pcnet_last_error.argtypes = [vp]
+    L.mpdx_pcnet_last_error.restype = ctypes.c_char_p
+    L.mpdx_pcnet_destroy.argtypes = [vp]
+    L.mpdx_pcnet_destroy.restype = None
     _lib = L
     return L
 

@@ -40,56 +40,86 @@ namespace bq {
 
 struct geom {
   int nd, n[3], bc[3][2];
-  double dx[3];  // converted to the arithmetic type where used
+  int nf, nrows;            // points along the last axis; rows = all other axes
+  double dxd[3], rdxd[3];   // spacing and RN(1/spacing), FP64
+  float dxf[3], rdxf[3];    // the same in FP32
   long long cells;
+  template <class T> __device__ __forceinline__ T dx(int d) const { if constexpr (sizeof(T) == 4) return dxf[d]; else return dxd[d]; }
+  template <class T> __device__ __forceinline__ T rdx(int d) const { if constexpr (sizeof(T) == 4) return rdxf[d]; else return rdxd[d]; }
 };
 
-__device__ __forceinline__ void ijk_of(const geom &g, long long q, int &i, int &j, int &k) {
-  k = int(q % g.n[2]);
-  const long long r = q / g.n[2];
-  j = int(r % g.n[1]);
-  i = int(r / g.n[1]);
+// Every interior point once: threadIdx.x runs along the last (contiguous)
+// axis, threadIdx.y and the blocks over the rows of the other axes.
+template <class F>
+__device__ __forceinline__ void for_interior(const geom &g, F &&fn) {
+  for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < g.nrows; row += gridDim.x * blockDim.y) {
+    int i = row, j = 0;
+    if (g.nd == 3) { i = row / g.n[1]; j = row - i * g.n[1]; }
+    for (int f = threadIdx.x; f < g.nf; f += blockDim.x) {
+      if (g.nd == 3) fn(i, j, f);
+      else fn(i, f, 0);
+    }
+  }
 }
 
-// plain field and err + beta * lap_p (the updated error, evaluated where it is read)
+// Field accessors by linear element offset.  Every pressure-type field of a
+// solver has the same layout (same halo ranges and padding), so one offset
+// addresses the same point in each of them.
 template <class T>
 struct fld {
-  dfield<T> a;
-  __device__ __forceinline__ T operator()(int i, int j, int k) const { return a(i, j, k); }
+  const T *o;
+  __device__ __forceinline__ T operator()(long long q) const { return o[q]; }
 };
+// err + beta * lap_p: the updated error, evaluated where it is read
 template <class T>
 struct fld_axpy {
-  dfield<T> x, y;
+  const T *x, *y;
   T b;
-  __device__ __forceinline__ T operator()(int i, int j, int k) const { return x(i, j, k) + b * y(i, j, k); }
+  __device__ __forceinline__ T operator()(long long q) const { return x[q] + b * y[q]; }
 };
 
-// value at the point whose coordinate d is replaced by q (q inside [0, n))
-template <class T, class F>
-__device__ __forceinline__ T at(const F &A, int d, int i, int j, int k, int q) {
-  return d == 0 ? A(q, j, k) : (d == 1 ? A(i, q, k) : A(i, j, q));
+template <class T>
+__device__ __forceinline__ long long off3(const dfield<T> &f, int i, int j, int k) {
+  return (long long)i * f.s0 + (long long)j * f.s1 + (long long)k * f.s2;
 }
-
-// A at coordinate q in [-2, n+1] along d with the pressure halo rule
-// (cyclic_2d.hpp:35-38 -> fill_halos_sclr; rigid_2d.hpp:26-35, 134-143)
-template <class T, class F>
-__device__ __forceinline__ T aval(const F &A, const geom &g, int d, int i, int j, int k, int q) {
-  const int n = g.n[d];
-  if (q >= 0 && q < n) return at<T>(A, d, i, j, k, q);
-  const int side = q < 0 ? 0 : 1;
-  if (g.bc[d][side] == MPDX_BC_CYCLIC) return at<T>(A, d, i, j, k, q < 0 ? q + n - 1 : q - (n - 1));
-  const int e = side == 0 ? 0 : n - 1, m = side == 0 ? -q : q - (n - 1);
-  return T(2) * at<T>(A, d, i, j, k, e) - at<T>(A, d, i, j, k, side == 0 ? m : n - 1 - m);
+template <class T>
+__device__ __forceinline__ long long stride(const dfield<T> &f, int d) {
+  return d == 0 ? f.s0 : (d == 1 ? f.s1 : f.s2);
 }
 
 __device__ __forceinline__ bool rigid_edge(const geom &g, int d, int q) {
   return (q == 0 && g.bc[d][0] == MPDX_BC_RIGID) || (q == g.n[d] - 1 && g.bc[d][1] == MPDX_BC_RIGID);
 }
 
-// grad_d A at interior coordinate q (nabla_formulae.hpp:18-41)
+// Where coordinate q along axis d (q in [-2, n+1]) takes its value from under
+// the pressure halo fill (cyclic_2d.hpp:35-38 -> fill_halos_sclr; rigid_2d.hpp:
+// 26-35, 134-143): the point qa itself, or 2 x (point qa) - (point qb).
+__device__ __forceinline__ void pres_src(const geom &g, int d, int q, int &qa, int &qb) {
+  const int n = g.n[d];
+  qa = q; qb = -1;
+  if (q >= 0 && q < n) return;
+  const int side = q < 0 ? 0 : 1;
+  const int kind = side == 0 ? g.bc[d][0] : g.bc[d][1];
+  if (kind == MPDX_BC_CYCLIC) { qa = q < 0 ? q + n - 1 : q - (n - 1); return; }
+  qa = side == 0 ? 0 : n - 1;
+  qb = side == 0 ? -q : 2 * (n - 1) - q;
+}
+
+// A at coordinate q of the line through `base` along d (line element q at base + q * sd)
 template <class T, class F>
-__device__ __forceinline__ T grad(const F &A, const geom &g, int d, int i, int j, int k, int q) {
-  return (aval<T>(A, g, d, i, j, k, q + 1) - aval<T>(A, g, d, i, j, k, q - 1)) / T(g.dx[d]) / T(2);
+__device__ __forceinline__ T aval(const F &A, const geom &g, int d, long long base, long long sd, int q) {
+  int qa, qb;
+  pres_src(g, d, q, qa, qb);
+  T v = A(base + qa * sd);
+  if (qb >= 0) v = T(2) * v - A(base + qb * sd);
+  return v;
+}
+
+// grad_d A at interior coordinate q (nabla_formulae.hpp:18-41):
+// (x(i+1) - x(i-1)) / dx / 2; halving is exact, so it is a multiplication by 0.5
+template <class T, class F>
+__device__ __forceinline__ T grad(const F &A, const geom &g, int d, long long base, long long sd, int q) {
+  return mpdx::qdiv<T>(aval<T>(A, g, d, base, sd, q + 1) - aval<T>(A, g, d, base, sd, q - 1), g.dx<T>(d), g.rdx<T>(d)) * T(0.5);
 }
 
 struct no_u {};
@@ -102,32 +132,44 @@ template <class T> struct is_vec<vec_u<T>> : std::true_type {};
 
 // lap_tmp[d] at interior coordinate q: grad, minus u (err_init), zero on a rigid wall (set_edges)
 template <class T, class F, class U>
-__device__ __forceinline__ T lt(const F &A, const U &u, const geom &g, int d, int i, int j, int k, int q) {
+__device__ __forceinline__ T lt(const F &A, const U &u, const geom &g, int d, long long base, long long sd,
+                                long long ubase, long long usd, int q) {
   if (rigid_edge(g, d, q)) return T(0);
-  T v = grad<T>(A, g, d, i, j, k, q);
-  if constexpr (is_vec<U>::value) {
-    const auto &ud = u.u[d];
-    v -= T(d == 0 ? ud(q, j, k) : (d == 1 ? ud(i, q, k) : ud(i, j, q)));
-  }
+  T v = grad<T>(A, g, d, base, sd, q);
+  if constexpr (is_vec<U>::value) v -= T(u.u[d].o[ubase + q * usd]);
   return v;
 }
 // lap_tmp[d] at coordinate q in [-1, n] (its own pressure halo fill)
 template <class T, class F, class U>
-__device__ __forceinline__ T LT(const F &A, const U &u, const geom &g, int d, int i, int j, int k, int q) {
-  const int n = g.n[d];
-  if (q >= 0 && q < n) return lt<T>(A, u, g, d, i, j, k, q);
-  const int side = q < 0 ? 0 : 1;
-  if (g.bc[d][side] == MPDX_BC_CYCLIC) return lt<T>(A, u, g, d, i, j, k, q < 0 ? q + n - 1 : q - (n - 1));
-  const int e = side == 0 ? 0 : n - 1, m = side == 0 ? -q : q - (n - 1);
-  return T(2) * lt<T>(A, u, g, d, i, j, k, e) - lt<T>(A, u, g, d, i, j, k, side == 0 ? m : n - 1 - m);
+__device__ __forceinline__ T LT(const F &A, const U &u, const geom &g, int d, long long base, long long sd,
+                                long long ubase, long long usd, int q) {
+  int qa, qb;
+  pres_src(g, d, q, qa, qb);
+  T v = lt<T>(A, u, g, d, base, sd, ubase, usd, qa);
+  if (qb >= 0) v = T(2) * v - lt<T>(A, u, g, d, base, sd, ubase, usd, qb);
+  return v;
 }
 // lap(A) at interior point (i, j, k): div(grad A [- u]) (mpdata_rhs_vip_prs_common.hpp:49-84,
-// nabla_formulae.hpp:184-215)
+// nabla_formulae.hpp:184-215).  `lay` is the layout shared by A's fields.
 template <class T, class F, class U>
-__device__ __forceinline__ T lap(const F &A, const U &u, const geom &g, int i, int j, int k) {
-  T r = (LT<T>(A, u, g, 0, i, j, k, i + 1) - LT<T>(A, u, g, 0, i, j, k, i - 1)) / T(g.dx[0]) / T(2)
-      + (LT<T>(A, u, g, 1, i, j, k, j + 1) - LT<T>(A, u, g, 1, i, j, k, j - 1)) / T(g.dx[1]) / T(2);
-  if (g.nd == 3) r = r + (LT<T>(A, u, g, 2, i, j, k, k + 1) - LT<T>(A, u, g, 2, i, j, k, k - 1)) / T(g.dx[2]) / T(2);
+__device__ __forceinline__ T lap(const F &A, const dfield<T> &lay, const U &u, const geom &g, int i, int j, int k) {
+  const int c[3] = {i, j, k};
+  const long long o = off3(lay, i, j, k);
+  T r = T(0);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (d >= g.nd) break;
+    const long long sd = stride(lay, d);
+    const long long base = o - c[d] * sd;
+    long long ubase = 0, usd = 0;
+    if constexpr (is_vec<U>::value) {
+      usd = stride(u.u[d], d);
+      ubase = off3(u.u[d], i, j, k) - c[d] * usd;
+    }
+    const T term = mpdx::qdiv<T>(LT<T>(A, u, g, d, base, sd, ubase, usd, c[d] + 1) - LT<T>(A, u, g, d, base, sd, ubase, usd, c[d] - 1),
+                                 g.dx<T>(d), g.rdx<T>(d)) * T(0.5);
+    r = d == 0 ? term : r + term;
+  }
   return r;
 }
 
@@ -161,19 +203,24 @@ __device__ __forceinline__ void warp_mm(double &mx, double &mn) {
 // block to arrive; there tot[] and mx/mn hold the grid results in every thread.
 // Fixed tree: per-thread strided sums, warp shuffle tree, warps in order, blocks
 // in order -> the same bits on every run.
-__device__ bool grid_reduce(dd *acc, int ns, bool mm, double &mx, double &mn, double *part, unsigned *arrive) {
+template <int NS, bool MM>
+__device__ __forceinline__ bool grid_reduce(dd (&acc)[NS], double &mx, double &mn, double *part, unsigned *arrive) {
+  constexpr int ns = NS;
+  constexpr bool mm = MM;
   __shared__ dd wsum[kRedThreads / 32];
   __shared__ double wmx[kRedThreads / 32], wmn[kRedThreads / 32];
   __shared__ bool last;
   __shared__ dd bsum[kRedSlots];
   __shared__ double bmx, bmn;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+  const int lane = tid & 31, w = tid >> 5, nw = nthr >> 5;
   double *mine = part + size_t(blockIdx.x) * kRedSlots * 2;
+#pragma unroll
   for (int s = 0; s < ns; ++s) {
     const dd v = warp_sum(acc[s]);
     if (lane == 0) wsum[w] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       dd t = wsum[0];
       for (int q = 1; q < nw; ++q) t = dd_add(t, wsum[q]);
       mine[2 * s] = t.s;
@@ -181,11 +228,11 @@ __device__ bool grid_reduce(dd *acc, int ns, bool mm, double &mx, double &mn, do
     }
     __syncthreads();
   }
-  if (mm) {
+  if constexpr (mm) {
     warp_mm(mx, mn);
     if (lane == 0) { wmx[w] = mx; wmn[w] = mn; }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       double a = wmx[0], b = wmn[0];
       for (int q = 1; q < nw; ++q) { a = fmax(a, wmx[q]); b = fmin(b, wmn[q]); }
       mine[2 * (kRedSlots - 1)] = a;
@@ -194,29 +241,30 @@ __device__ bool grid_reduce(dd *acc, int ns, bool mm, double &mx, double &mn, do
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1;
+  if (tid == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1;
   __syncthreads();
   if (!last) return false;
   __threadfence();
+#pragma unroll
   for (int s = 0; s < ns; ++s) {
     dd v{0.0, 0.0};
-    for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) {
+    for (int b = tid; b < int(gridDim.x); b += nthr) {
       const double *p = part + size_t(b) * kRedSlots * 2 + 2 * s;
       v = dd_add(v, dd{__ldcg(p), __ldcg(p + 1)});
     }
     v = warp_sum(v);
     if (lane == 0) wsum[w] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       dd t = wsum[0];
       for (int q = 1; q < nw; ++q) t = dd_add(t, wsum[q]);
       bsum[s] = t;
     }
     __syncthreads();
   }
-  if (mm) {
+  if constexpr (mm) {
     double a = -DBL_MAX, b = DBL_MAX;
-    for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) {
+    for (int q = tid; q < int(gridDim.x); q += nthr) {
       const double *p = part + size_t(q) * kRedSlots * 2 + 2 * (kRedSlots - 1);
       a = fmax(a, __ldcg(p));
       b = fmin(b, __ldcg(p + 1));
@@ -224,7 +272,7 @@ __device__ bool grid_reduce(dd *acc, int ns, bool mm, double &mx, double &mn, do
     warp_mm(a, b);
     if (lane == 0) { wmx[w] = a; wmn[w] = b; }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       double x = wmx[0], y = wmn[0];
       for (int q = 1; q < nw; ++q) { x = fmax(x, wmx[q]); y = fmin(y, wmn[q]); }
       bmx = x; bmn = y;
@@ -232,8 +280,9 @@ __device__ bool grid_reduce(dd *acc, int ns, bool mm, double &mx, double &mn, do
     __syncthreads();
     mx = bmx; mn = bmn;
   }
+#pragma unroll
   for (int s = 0; s < ns; ++s) acc[s] = bsum[s];
-  if (threadIdx.x == 0) *arrive = 0u;
+  if (tid == 0) *arrive = 0u;
   return true;
 }
 
@@ -249,30 +298,26 @@ __global__ void k_gcr_reset(gcr_dev<T> *dv) {
 
 // err = lap(Phi) with err_init (u = the velocity being projected)
 template <class P, class T>
-__global__ void k_err_init(geom g, dfield<P> phi, vec_u<T> u, dfield<P> err) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
-    err(i, j, k) = lap<P>(fld<P>{phi}, u, g, i, j, k);
-  }
+__global__ void __launch_bounds__(kRedThreads, 4) k_err_init(geom g, dfield<P> phi, vec_u<T> u, dfield<P> err) {
+  for_interior(g, [&](int i, int j, int k) {
+    err(i, j, k) = lap<P>(fld<P>{phi.o}, phi, u, g, i, j, k);
+    });
 }
 
 // loop_init: p_0 = err, lap_p_0 = lap(p_0); sums of the first beta
 template <class T>
-__global__ void k_gcr_init(geom g, dfield<T> err, dfield<T> p0, dfield<T> lp0, gcr_dev<T> *dv, double *part) {
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_init(geom g, dfield<T> err, dfield<T> p0, dfield<T> lp0, gcr_dev<T> *dv, double *part) {
   dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+  for_interior(g, [&](int i, int j, int k) {
     const T e = err(i, j, k);
-    const T l = lap<T>(fld<T>{err}, no_u{}, g, i, j, k);
+    const T l = lap<T>(fld<T>{err.o}, err, no_u{}, g, i, j, k);
     p0(i, j, k) = e;
     lp0(i, j, k) = l;
     acc[0] = dd_add(acc[0], dd{double(T(l * l)), 0.0});
     acc[1] = dd_add(acc[1], dd{double(T(e * l)), 0.0});
-  }
+    });
   double mx = 0, mn = 0;
-  if (grid_reduce(acc, 2, false, mx, mn, part, &dv->arrive) && threadIdx.x == 0) {
+  if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     dv->pend_den = T(ddv(acc[0]));
     dv->pend_num = T(ddv(acc[1]));
   }
@@ -283,92 +328,122 @@ struct dirs {
   dfield<T> p[kGcrMaxK], lp[kGcrMaxK];
 };
 
-// inner step v, first half (mpdata_rhs_vip_prs_gcrk.hpp:43-64)
-template <class T>
-__global__ void k_gcr_update(geom g, int v, T err_tol, dfield<T> phi, dfield<T> err0, dfield<T> err1, dfield<T> lap_err,
-                             dirs<T> D, gcr_dev<T> *dv, double *part) {
+// inner step v = NV - 1, first half (mpdata_rhs_vip_prs_gcrk.hpp:43-64)
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol, dfield<T> phi, dfield<T> err0, dfield<T> err1,
+                                                               dfield<T> lap_err, dirs<T> D, gcr_dev<T> *dv, double *part) {
+  constexpr int v = NV - 1;
   if (dv->done) return;
   const int cur = dv->cur;
   const dfield<T> ea = cur ? err1 : err0, eb = cur ? err0 : err1;
   const T den = dv->pend_den;
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;  // beta keeps its value when tmp_den is 0
-  if (blockIdx.x == 0 && threadIdx.x == 0) { dv->tmp_den[v] = den; dv->beta = b; }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
   const dfield<T> pv = D.p[v], lpv = D.lp[v];
-  const fld_axpy<T> enew{ea, lpv, b};
-  dd acc[kGcrMaxK];
-  for (int l = 0; l <= v; ++l) acc[l] = dd{0.0, 0.0};
+  dfield<T> lps[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
+  const fld_axpy<T> enew{ea.o, lpv.o, b};
+  dd acc[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
   double mx = -DBL_MAX, mn = DBL_MAX;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+  for_interior(g, [&](int i, int j, int k) {
     phi(i, j, k) = phi(i, j, k) + b * pv(i, j, k);
-    const T e = enew(i, j, k);
+    const T e = enew(off3(ea, i, j, k));
     eb(i, j, k) = e;
     mx = fmax(mx, double(e));
     mn = fmin(mn, double(e));
-    const T le = lap<T>(enew, no_u{}, g, i, j, k);
+    const T le = lap<T>(enew, ea, no_u{}, g, i, j, k);
     lap_err(i, j, k) = le;
-    for (int l = 0; l <= v; ++l) acc[l] = dd_add(acc[l], dd{double(T(le * D.lp[l](i, j, k))), 0.0});
-  }
-  if (grid_reduce(acc, v + 1, true, mx, mn, part, &dv->arrive) && threadIdx.x == 0) {
+#pragma unroll
+    for (int l = 0; l < NV; ++l) acc[l] = dd_add(acc[l], dd{double(T(le * lps[l](i, j, k))), 0.0});
+  });
+  if (grid_reduce<NV, true>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     const T amx = fabs(T(mx)), amn = fabs(T(mn));
     const T error = amx < amn ? amn : amx;  // std::max(|max|, |min|)
     dv->residual = double(error);
     if (error <= err_tol) dv->converged = 1;
-    for (int l = 0; l <= v; ++l) {
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
       const T dl = l == v ? den : dv->tmp_den[l];
       if (dl != T(0)) dv->alpha[l] = -T(ddv(acc[l])) / dl;
     }
   }
 }
 
-// inner step v, second half: next search direction (mpdata_rhs_vip_prs_gcrk.hpp:66-92)
-template <class T>
-__global__ void k_gcr_direction(geom g, int v, int kk, dfield<T> err0, dfield<T> err1, dfield<T> lap_err, dirs<T> D,
-                                gcr_dev<T> *dv, double *part) {
+// inner step v = NV - 1, second half: next search direction (mpdata_rhs_vip_prs_gcrk.hpp:66-92)
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk, dfield<T> err0, dfield<T> err1,
+                                                                  dfield<T> lap_err, dirs<T> D, gcr_dev<T> *dv, double *part) {
+  constexpr int v = NV - 1;
   if (dv->done) return;
   const int cur = dv->cur;
   const dfield<T> e = cur ? err0 : err1;  // the error written by k_gcr_update
-  T a[kGcrMaxK];
-  for (int l = 0; l <= v; ++l) a[l] = dv->alpha[l];
-  const int dst = v < kk - 1 ? v + 1 : 0;
-  const dfield<T> pd = D.p[dst], lpd = D.lp[dst];
+  T a[NV];
+  dfield<T> ps[NV], lps[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) { a[l] = dv->alpha[l]; ps[l] = D.p[l]; lps[l] = D.lp[l]; }
+  const bool restart = v == kk - 1;
+  const dfield<T> pd = restart ? D.p[0] : D.p[NV < kGcrMaxK ? NV : 0], lpd = restart ? D.lp[0] : D.lp[NV < kGcrMaxK ? NV : 0];
   dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+  for_interior(g, [&](int i, int j, int k) {
     const T ev = e(i, j, k);
     T pn, ln;
-    if (v < kk - 1) {
+    if (!restart) {
       pn = ev;
       ln = lap_err(i, j, k);
-      for (int l = 0; l <= v; ++l) {
-        pn = pn + a[l] * D.p[l](i, j, k);
-        ln = ln + a[l] * D.lp[l](i, j, k);
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        pn = pn + a[l] * ps[l](i, j, k);
+        ln = ln + a[l] * lps[l](i, j, k);
       }
     } else {
-      pn = ev + a[0] * D.p[0](i, j, k);
-      ln = lap_err(i, j, k) + a[0] * D.lp[0](i, j, k);
-      for (int l = 1; l <= v; ++l) {
-        pn = pn + a[l] * D.p[l](i, j, k);
-        ln = ln + a[l] * D.lp[l](i, j, k);
+      pn = ev + a[0] * ps[0](i, j, k);
+      ln = lap_err(i, j, k) + a[0] * lps[0](i, j, k);
+#pragma unroll
+      for (int l = 1; l < NV; ++l) {
+        pn = pn + a[l] * ps[l](i, j, k);
+        ln = ln + a[l] * lps[l](i, j, k);
       }
     }
     pd(i, j, k) = pn;
     lpd(i, j, k) = ln;
     acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
     acc[1] = dd_add(acc[1], dd{double(T(ev * ln)), 0.0});
-  }
+  });
   double mx = 0, mn = 0;
-  if (grid_reduce(acc, 2, false, mx, mn, part, &dv->arrive) && threadIdx.x == 0) {
+  if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     dv->pend_den = T(ddv(acc[0]));
     dv->pend_num = T(ddv(acc[1]));
     dv->cur = 1 - cur;
-    if (v == kk - 1) {  // end of one loop body (mpdata_rhs_vip_prs_common.hpp:111-125)
+    if (restart) {  // end of one loop body (mpdata_rhs_vip_prs_common.hpp:111-125)
       dv->iters += 1;
       if (dv->converged) dv->done = 1;
       if (dv->iters > 10000) { dv->stuck = 1; dv->done = 1; }
     }
+  }
+}
+
+// one inner step of GCR(k), NV = v + 1 known at compile time
+template <class T, int NV>
+void launch_inner(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi, dfield<T> e0,
+                  dfield<T> e1, dfield<T> le, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
+  k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part);
+  k_gcr_direction<T, NV><<<G, blk, 0, s>>>(g, kk, e0, e1, le, D, dv, part);
+}
+template <class T>
+void launch_inner(int v, unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi,
+                  dfield<T> e0, dfield<T> e1, dfield<T> le, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
+  switch (v + 1) {
+    case 1: launch_inner<T, 1>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 2: launch_inner<T, 2>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 3: launch_inner<T, 3>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 4: launch_inner<T, 4>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 5: launch_inner<T, 5>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 6: launch_inner<T, 6>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    case 7: launch_inner<T, 7>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
+    default: launch_inner<T, 8>(G, blk, s, g, kk, err_tol, phi, e0, e1, le, D, dv, part); break;
   }
 }
 
@@ -381,13 +456,14 @@ enum { APPLY_PROJECT = 0, APPLY_RHS = 1, APPLY_FINISH = 2 };
 // (PROJECT), vip_rhs -= grad Phi (RHS, hook_ante_loop), or pressure_solver_apply +
 // set_edges + vip_rhs = (vip_rhs + u) / (dt / 2) (FINISH, vip_rhs_impl_fnlz)
 template <class T, class P>
-__global__ void k_apply_grad(geom g, int mode, dfield<P> phi, vec_u<T> vel, vec_u<T> vr, T hdt) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+__global__ void __launch_bounds__(kRedThreads, 4) k_apply_grad(geom g, int mode, dfield<P> phi, vec_u<T> vel, vec_u<T> vr, T hdt) {
+  for_interior(g, [&](int i, int j, int k) {
     const int c[3] = {i, j, k};
-    for (int d = 0; d < g.nd; ++d) {
-      const P gd = grad<P>(fld<P>{phi}, g, d, i, j, k, c[d]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.nd) break;
+      const long long sd = stride(phi, d);
+      const P gd = grad<P>(fld<P>{phi.o}, g, d, off3(phi, i, j, k) - c[d] * sd, sd, c[d]);
       if (mode == APPLY_RHS) {
         vr.u[d](i, j, k) = T(P(vr.u[d](i, j, k)) - gd);
         continue;
@@ -400,7 +476,7 @@ __global__ void k_apply_grad(geom g, int mode, dfield<P> phi, vec_u<T> vel, vec_
         vr.u[d](i, j, k) = r / hdt;
       }
     }
-  }
+    });
 }
 
 template <class T>
@@ -411,15 +487,13 @@ struct eqns {
 // extrp (mpdata_rhs_vip_common.hpp:120-153): stash = -beta stash + (1 + beta) u
 template <class T>
 __global__ void k_extrp(geom g, vec_u<T> stash, vec_u<T> vel, T b) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
-    for (int d = 0; d < g.nd; ++d) {
+  for_interior(g, [&](int i, int j, int k) {
+    _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
       T s = stash.u[d](i, j, k) * -b;
       s = s + (T(1) + b) * vel.u[d](i, j, k);
       stash.u[d](i, j, k) = s;
     }
-  }
+    });
 }
 
 // intrp<d> (mpdata_rhs_vip.hpp:122-143): GC = dt / di * 0.5 * (u(i) + u(i+1)) over a box
@@ -438,16 +512,14 @@ __global__ void k_intrp(dfield<T> gc, dfield<T> src, int d, T c, int i0, int j0,
 // hook_ante_step: fill_stash, apply_rhs(dt / 2), vip_rhs_apply
 template <class T>
 __global__ void k_ante_step(geom g, int ne, eqns<T> E, const int *vip, vec_u<T> stash, vec_u<T> vr, T dt2, T hdt) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
-    for (int d = 0; d < g.nd; ++d) stash.u[d](i, j, k) = E.psi[vip[d]](i, j, k);
-    for (int e = 0; e < ne; ++e) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
-    for (int d = 0; d < g.nd; ++d) {
+  for_interior(g, [&](int i, int j, int k) {
+    _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) stash.u[d](i, j, k) = E.psi[vip[d]](i, j, k);
+    _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
+    _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
       E.psi[vip[d]](i, j, k) = E.psi[vip[d]](i, j, k) + hdt * vr.u[d](i, j, k);
       vr.u[d](i, j, k) = T(0);
     }
-  }
+    });
 }
 
 // update_rhs (rhs = 0; rhs[w] += g (tht - tht_e) / Tht_ref), then (post step)
@@ -455,46 +527,40 @@ __global__ void k_ante_step(geom g, int ne, eqns<T> E, const int *vip, vec_u<T> 
 template <class T>
 __global__ void k_rhs(geom g, int ne, int post, eqns<T> E, const int *vip, int iw, int ith, dfield<T> the, T grav,
                       T tref, T dt2, vec_u<T> vr) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
-    for (int e = 0; e < ne; ++e) E.rhs[e](i, j, k) = T(0);
+  for_interior(g, [&](int i, int j, int k) {
+    _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.rhs[e](i, j, k) = T(0);
     E.rhs[iw](i, j, k) = T(0) + grav * (E.psi[ith](i, j, k) - the(i, j, k)) / tref;
     if (post) {
-      for (int e = 0; e < ne; ++e) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
-      for (int d = 0; d < g.nd; ++d) vr.u[d](i, j, k) = -E.psi[vip[d]](i, j, k);
+      _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
+      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) vr.u[d](i, j, k) = -E.psi[vip[d]](i, j, k);
     } else {
-      for (int d = 0; d < g.nd; ++d) vr.u[d](i, j, k) = T(0);
+      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) vr.u[d](i, j, k) = T(0);
     }
-  }
+    });
 }
 
 // ini_pressure, first part: Phi = -sum_d 0.5 u_d^2 and its mean
 template <class T, class P>
 __global__ void k_phi_ini(geom g, dfield<P> phi, vec_u<T> vel, gcr_dev<P> *dv, double *part, double npoints) {
   dd acc[1] = {{0.0, 0.0}};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+  for_interior(g, [&](int i, int j, int k) {
     P p = P(0);
-    for (int d = 0; d < g.nd; ++d) {
+    _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
       const P v = P(vel.u[d](i, j, k));
       p = p - P(0.5) * (v * v);
     }
     phi(i, j, k) = p;
     acc[0] = dd_add(acc[0], dd{double(p), 0.0});
-  }
+    });
   double mx = 0, mn = 0;
-  if (grid_reduce(acc, 1, false, mx, mn, part, &dv->arrive) && threadIdx.x == 0) dv->mean = P(ddv(acc[0])) / P(npoints);
+  if (grid_reduce<1, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) dv->mean = P(ddv(acc[0])) / P(npoints);
 }
 template <class P>
 __global__ void k_phi_sub_mean(geom g, dfield<P> phi, const gcr_dev<P> *dv) {
   const P m = dv->mean;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < g.cells; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(g, q, i, j, k);
+  for_interior(g, [&](int i, int j, int k) {
     phi(i, j, k) = phi(i, j, k) - m;
-  }
+    });
 }
 
 }  // namespace bq
@@ -511,13 +577,19 @@ bq::geom make_geom(const mpdata_state<T> &st, const double *dijk) {
     g.n[d] = st.n[d];
     g.bc[d][0] = st.bcs[d][0];
     g.bc[d][1] = st.bcs[d][1];
-    g.dx[d] = dijk[d];
+    g.dxd[d] = dijk[d];
+    g.rdxd[d] = 1.0 / dijk[d];                  // RN(1/dx) in FP64
+    g.dxf[d] = float(dijk[d]);
+    g.rdxf[d] = 1.0f / float(dijk[d]);          // RN(1/dx) in FP32
   }
   g.cells = st.cells();
+  g.nf = st.n[st.nd - 1];
+  g.nrows = int(g.cells / g.nf);
   return g;
 }
-unsigned red_grid(long long cells) {
-  long long b = (cells + kRedThreads - 1) / kRedThreads;
+const dim3 kBlk(32, kRedThreads / 32);  // 32 points along the contiguous axis x 8 rows
+unsigned red_grid(const bq::geom &g) {
+  const long long b = (g.nrows + kBlk.y - 1) / kBlk.y;
   return unsigned(std::max(1LL, std::min<long long>(b, kRedBlocks)));
 }
 }  // namespace
@@ -586,7 +658,7 @@ boussinesq<T, P>::~boussinesq() {
 template <class T, class P>
 void boussinesq<T, P>::pressure_solve() {
   const auto gm = make_geom(st, dijk);
-  const unsigned G = red_grid(gm.cells);
+  const unsigned G = red_grid(gm);
   cudaStream_t s = st.stream;
   bq::vec_u<T> u;
   for (int d = 0; d < 3; ++d) u.u[d] = d < st.nd ? vips(d).v : vips(0).v;
@@ -596,16 +668,15 @@ void boussinesq<T, P>::pressure_solve() {
     D.lp[v] = lap_p_err[std::min(v, k_iters - 1)].v;
   }
   bq::k_gcr_reset<P><<<1, 1, 0, s>>>(dev);
-  bq::k_err_init<P, T><<<G, kRedThreads, 0, s>>>(gm, Phi.v, u, err[0].v);
-  bq::k_gcr_init<P><<<G, kRedThreads, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+  bq::k_err_init<P, T><<<G, kBlk, 0, s>>>(gm, Phi.v, u, err[0].v);
+  bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
   MPDX_LAUNCH_CHECK();
   long long launched = 0;
   for (;;) {
     const long long batch = launched == 0 ? std::max(1LL, predicted) : std::max(4LL, predicted / 4);
     for (long long b = 0; b < batch; ++b)
       for (int v = 0; v < k_iters; ++v) {
-        bq::k_gcr_update<P><<<G, kRedThreads, 0, s>>>(gm, v, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
-        bq::k_gcr_direction<P><<<G, kRedThreads, 0, s>>>(gm, v, k_iters, err[0].v, err[1].v, lap_err.v, D, dev, part);
+        bq::launch_inner<P>(v, G, kBlk, s, gm, k_iters, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
       }
     MPDX_LAUNCH_CHECK();
     launched += batch;
@@ -623,7 +694,7 @@ void boussinesq<T, P>::pressure_solve() {
 template <class T, class P>
 void boussinesq<T, P>::ante_loop() {
   const auto gm = make_geom(st, dijk);
-  const unsigned G = red_grid(gm.cells);
+  const unsigned G = red_grid(gm);
   cudaStream_t s = st.stream;
   bq::vec_u<T> u, vr;
   for (int d = 0; d < 3; ++d) {
@@ -633,7 +704,7 @@ void boussinesq<T, P>::ante_loop() {
   // initial projection (mpdata_rhs_vip_prs_common.hpp:130-146); save_edges is a no-op here
   MPDX_CUDA(cudaMemsetAsync(Phi.base, 0, Phi.bytes, s));
   pressure_solve();
-  bq::k_apply_grad<T, P><<<G, kRedThreads, 0, s>>>(gm, bq::APPLY_PROJECT, Phi.v, u, vr, T(0));
+  bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(gm, bq::APPLY_PROJECT, Phi.v, u, vr, T(0));
   MPDX_LAUNCH_CHECK();
   // mpdata_rhs_vip_common.hpp:283-302: GC = 0, stash = 0, parent hooks, vip_rhs = 0
   for (int d = 0; d < st.nd; ++d) {
@@ -649,20 +720,20 @@ void boussinesq<T, P>::ante_loop() {
   }
   // update_rhs(dt / 2, at = 0); update_rhs's halo exchange of every equation is
   // left out: the next read of any halo is preceded by its own exchange
-  bq::k_rhs<T><<<G, kRedThreads, 0, s>>>(gm, st.n_eqns, 0, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
+  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 0, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
   // ini_pressure (mpdata_rhs_vip_prs_common.hpp:86-97), then vip_rhs -= grad Phi
   double npoints = 1;
   for (int d = 0; d < st.nd; ++d) npoints *= st.n[d];
-  bq::k_phi_ini<T, P><<<G, kRedThreads, 0, s>>>(gm, Phi.v, u, dev, part, npoints);
-  bq::k_phi_sub_mean<P><<<G, kRedThreads, 0, s>>>(gm, Phi.v, dev);
-  bq::k_apply_grad<T, P><<<G, kRedThreads, 0, s>>>(gm, bq::APPLY_RHS, Phi.v, u, vr, T(0));
+  bq::k_phi_ini<T, P><<<G, kBlk, 0, s>>>(gm, Phi.v, u, dev, part, npoints);
+  bq::k_phi_sub_mean<P><<<G, kBlk, 0, s>>>(gm, Phi.v, dev);
+  bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(gm, bq::APPLY_RHS, Phi.v, u, vr, T(0));
   MPDX_LAUNCH_CHECK();
 }
 
 template <class T, class P>
 void boussinesq<T, P>::step() {
   const auto gm = make_geom(st, dijk);
-  const unsigned G = red_grid(gm.cells);
+  const unsigned G = red_grid(gm);
   cudaStream_t s = st.stream;
   bq::vec_u<T> u, vr, sh;
   for (int d = 0; d < 3; ++d) {
@@ -671,7 +742,7 @@ void boussinesq<T, P>::step() {
   }
   // calc_gc: extrapolate_in_time + interpolate_in_space
   const T b = dt_stash0 > T(0) ? dtT / (2 * dt_stash0) : T(0);
-  bq::k_extrp<T><<<G, kRedThreads, 0, s>>>(gm, sh, u, b);
+  bq::k_extrp<T><<<G, kBlk, 0, s>>>(gm, sh, u, b);
   MPDX_LAUNCH_CHECK();
   const int ex = st.H - 1;
   for (int d = 0; d < st.nd; ++d) gen.xchng_pres(stash[d], ex);
@@ -694,7 +765,7 @@ void boussinesq<T, P>::step() {
     E.psi[e] = st.psi[ee][st.tl[ee]].v;
     E.rhs[e] = rhs[ee].v;
   }
-  bq::k_ante_step<T><<<G, kRedThreads, 0, s>>>(gm, st.n_eqns, E, vip_dev, sh, vr, dtT / 2, T(0.5) * dtT);
+  bq::k_ante_step<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, E, vip_dev, sh, vr, dtT / 2, T(0.5) * dtT);
   MPDX_LAUNCH_CHECK();
   // advection of every equation
   gen.step();
@@ -703,10 +774,10 @@ void boussinesq<T, P>::step() {
   // hook_post_step
   for (int d = 0; d < 3; ++d) u.u[d] = vips(d < st.nd ? d : 0).v;
   for (int e = 0; e < 4; ++e) E.psi[e] = st.psi[e < st.n_eqns ? e : 0][st.tl[e < st.n_eqns ? e : 0]].v;
-  bq::k_rhs<T><<<G, kRedThreads, 0, s>>>(gm, st.n_eqns, 1, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
+  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 1, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
   MPDX_LAUNCH_CHECK();
   pressure_solve();
-  bq::k_apply_grad<T, P><<<G, kRedThreads, 0, s>>>(gm, bq::APPLY_FINISH, Phi.v, u, vr, T(0.5) * dtT);
+  bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(gm, bq::APPLY_FINISH, Phi.v, u, vr, T(0.5) * dtT);
   MPDX_LAUNCH_CHECK();
 }
 

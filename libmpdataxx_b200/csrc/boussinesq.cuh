@@ -9,7 +9,7 @@
 namespace mpdx {
 
 constexpr int kGcrMaxK = 8;        // largest k of GCR(k) built
-constexpr int kRedBlocks = 296;    // reduction grid: 2 x 148 SMs (fixed shape => reproducible sums)
+constexpr int kRedBlocks = 1184;   // largest reduction grid: 8 x 148 SMs (a fixed shape per grid size => reproducible sums)
 constexpr int kRedThreads = 256;
 constexpr int kRedSlots = kGcrMaxK + 2;
 

@@ -6,4 +6,6 @@ template bool fused_configurable<float>(const mpdata_state<float> &);
 template void fused3d_launch<float>(mpdata_state<float> &, int, cudaStream_t);
 template void fused2d_launch<float>(mpdata_state<float> &, int, cudaStream_t);
 template bool fused_seams_consistent<float>(mpdata_state<float> &, double *);
+template int fused2d_batched<float>(int, int, bool, bool, const f2::prob<float> *, const f2::item *, int, int *, int,
+                                     cudaStream_t, bool);
 }  // namespace mpdx

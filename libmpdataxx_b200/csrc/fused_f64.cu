@@ -7,4 +7,6 @@ template bool fused_configurable<double>(const mpdata_state<double> &);
 template void fused3d_launch<double>(mpdata_state<double> &, int, cudaStream_t);
 template void fused2d_launch<double>(mpdata_state<double> &, int, cudaStream_t);
 template bool fused_seams_consistent<double>(mpdata_state<double> &, double *);
+template int fused2d_batched<double>(int, int, bool, bool, const f2::prob<double> *, const f2::item *, int, int *, int,
+                                     cudaStream_t, bool);
 }  // namespace mpdx

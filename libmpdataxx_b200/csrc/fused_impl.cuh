@@ -6,6 +6,7 @@
 #include "fused.cuh"
 #include "fused2d.cuh"
 #include "fused3d.cuh"
+#include "fused2d_batch.cuh"
 
 namespace mpdx {
 
@@ -102,6 +103,49 @@ void fused2d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
     else if (iga) launch2<T, 2, true, false>(a, s);
     else if (fct) launch2<T, 2, false, true>(a, s);
     else launch2<T, 2, false, false>(a, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// batched persistent launch (fused2d_batch.cuh)
+template <class T, int NI, bool IGA, bool FCT, int NT>
+static int batched_do(const f2::prob<T> *probs, const f2::item *items, int n_items, int *counter, int grid,
+                      cudaStream_t s, bool occupancy_only) {
+  constexpr int H = NI == 3 ? 6 : 4;
+  auto kern = f2::k_fused2d_batched<T, NI, IGA, FCT, NT, H>;
+  const size_t bytes = size_t(f2::rows<NI, FCT>::total) * NT * sizeof(T);
+  static bool attr = false;
+  if (!attr) { set_smem(kern, bytes); attr = true; }
+  if (occupancy_only) {
+    int occ = 0;
+    MPDX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, bytes));
+    return occ;
+  }
+  kern<<<grid, NT, bytes, s>>>(probs, items, n_items, counter);
+  MPDX_LAUNCH_CHECK();
+  return 0;
+}
+
+template <class T, int NT>
+static int batched_nt(int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
+                      int *counter, int grid, cudaStream_t s, bool occ) {
+  if (ni == 3) {
+    if (fct) return batched_do<T, 3, false, true, NT>(probs, items, n_items, counter, grid, s, occ);
+    return batched_do<T, 3, false, false, NT>(probs, items, n_items, counter, grid, s, occ);
+  }
+  if (iga && fct) return batched_do<T, 2, true, true, NT>(probs, items, n_items, counter, grid, s, occ);
+  if (iga) return batched_do<T, 2, true, false, NT>(probs, items, n_items, counter, grid, s, occ);
+  if (fct) return batched_do<T, 2, false, true, NT>(probs, items, n_items, counter, grid, s, occ);
+  return batched_do<T, 2, false, false, NT>(probs, items, n_items, counter, grid, s, occ);
+}
+
+template <class T>
+int fused2d_batched(int tile, int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
+                    int *counter, int grid, cudaStream_t s, bool occ) {
+  switch (kBatchTiles[tile].nt) {
+    case 128: return batched_nt<T, 128>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
+    case 256: return batched_nt<T, 256>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
+    default: return batched_nt<T, 512>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
   }
 }
 

@@ -72,7 +72,10 @@ struct field {
   }
   ~field() { if (base) cudaFree(base); }
 
-  void alloc(int nd_, const rng *rr) {
+  // `stream` is the stream every later use of the field is ordered on: the zero fill
+  // goes there too (a legacy-stream memset would not be ordered with work on
+  // a non-blocking stream)
+  void alloc(int nd_, const rng *rr, cudaStream_t stream) {
     nd = nd_;
     for (int q = 0; q < 3; ++q) r[q] = q < nd ? rr[q] : rng{0, 0};
     const int align = int(128 / sizeof(T));
@@ -85,7 +88,7 @@ struct field {
     for (int q = f - 1; q >= 0; --q) { s[q] = acc; acc *= r[q].n(); }
     bytes = size_t(acc) * sizeof(T);
     MPDX_CUDA(cudaMalloc(&base, bytes));
-    MPDX_CUDA(cudaMemset(base, 0, bytes));
+    MPDX_CUDA(cudaMemsetAsync(base, 0, bytes, stream));
     long long off = front;
     for (int q = 0; q < f; ++q) off += (long long)(-r[q].f) * s[q];
     v.o = static_cast<T *>(base) + off;
@@ -96,5 +99,18 @@ struct field {
 };
 
 inline unsigned ceil_div(long long a, long long b) { return unsigned((a + b - 1) / b); }
+
+// a / b, correctly rounded, from y = RN(1/b): q = RN(a y), r = a - b q (exact
+// with one FMA), result RN(q + r y) -- Markstein's correction step (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000 processor",
+// IBM J. Res. Dev. 34(1), 1990).  Equals the IEEE quotient for operands away
+// from overflow and underflow (checked against the '/' operator by
+// tests/cuda/qdiv_check.cu); a zero numerator gives +0.
+template <class T>
+__device__ __forceinline__ T qdiv(T a, T b, T y) {
+  const T q = a * y;
+  const T r = fma(-q, b, a);
+  return fma(r, y, q);
+}
 
 }  // namespace mpdx

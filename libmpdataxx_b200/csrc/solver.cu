@@ -4,6 +4,7 @@
 // a CUDA stream, and small scratch buffers.  Host data enters and leaves only
 // through mpdx_set_field / mpdx_get_field / mpdx_stats.
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -11,6 +12,7 @@
 
 #include "boussinesq.cuh"
 #include "fused.cuh"
+#include "fused2d_batch.cuh"
 #include "general.cuh"
 #include "stats.cuh"
 
@@ -221,6 +223,189 @@ struct boussinesq_solver : solver_base {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Batched advance of independent 2D problems (one persistent launch per step)
+
+struct batch_base {
+  virtual ~batch_base() = default;
+  virtual void advance(long long nt) = 0;
+  virtual void info(mpdx_batch_info *out) = 0;
+  virtual void sync() = 0;
+  std::string err;
+};
+
+template <class T>
+struct batch_impl : batch_base {
+  std::vector<mpdata_solver<T> *> hs;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_done = nullptr, ev_a = nullptr, ev_b = nullptr;
+  int mode = MPDX_BATCH_PERSISTENT, ni = 2;
+  bool iga = false, fct = false;
+  int tile = -1, items_tile = -1, n_items = 0, grid = 0, n_sm = 0, next_candidate = 0;
+  double tune_ms[kNumBatchTiles] = {};
+  f2::prob<T> *probs_dev = nullptr;  // [2][n]: step parity 0 and 1
+  f2::item *items_dev = nullptr;
+  size_t items_cap = 0;
+  int *counter = nullptr;            // one per parity
+  cudaGraphExec_t graph = nullptr;   // two steps (parity 0, then 1)
+  long long cells = 0;
+
+  batch_impl(const std::vector<mpdata_solver<T> *> &v, int mode_) : hs(v), mode(mode_) {
+    const auto &s0 = hs[0]->st;
+    ni = s0.n_iters; iga = s0.opts & o_iga; fct = s0.opts & o_fct;
+    for (size_t p = 0; p < hs.size(); ++p) {
+      const auto &st = hs[p]->st;
+      if (st.nd != 2) throw error(MPDX_E_UNSUPPORTED, "batched advance is built for 2D problems");
+      if (st.opts != s0.opts || st.n_iters != s0.n_iters)
+        throw error(MPDX_E_ARG, "all problems of a batch need the same opts and n_iters");
+      if (st.n_eqns != 1) throw error(MPDX_E_UNSUPPORTED, "batched problems advect one equation each");
+      if (!fused_configurable(st))
+        throw error(MPDX_E_UNSUPPORTED, "batched advance needs cyclic boundaries and opts within {fct, iga} (n_iters 2, or 3 without iga)");
+      for (size_t q = 0; q < p; ++q)
+        if (hs[q] == hs[p]) throw error(MPDX_E_ARG, "a problem appears twice in the batch");
+      cells += st.cells();
+    }
+    MPDX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    MPDX_CUDA(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    MPDX_CUDA(cudaEventCreate(&ev_a));
+    MPDX_CUDA(cudaEventCreate(&ev_b));
+    MPDX_CUDA(cudaMalloc(&probs_dev, 2 * hs.size() * sizeof(f2::prob<T>)));
+    MPDX_CUDA(cudaMalloc(&counter, 2 * sizeof(int)));
+    int dev = 0;
+    MPDX_CUDA(cudaGetDevice(&dev));
+    MPDX_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  }
+  ~batch_impl() override {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (probs_dev) cudaFree(probs_dev);
+    if (items_dev) cudaFree(items_dev);
+    if (counter) cudaFree(counter);
+    if (ev_done) cudaEventDestroy(ev_done);
+    if (ev_a) cudaEventDestroy(ev_a);
+    if (ev_b) cudaEventDestroy(ev_b);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  void use_tile(int t) {
+    if (t == items_tile) return;
+    std::vector<int> P0(hs.size()), P1(hs.size());
+    for (size_t p = 0; p < hs.size(); ++p) { P0[p] = hs[p]->st.n[0] - 1; P1[p] = hs[p]->st.n[1] - 1; }
+    const auto items = fused2d_batch_items(t, ni, P0, P1);
+    if (items.size() > items_cap) {
+      if (items_dev) cudaFree(items_dev);
+      items_dev = nullptr;
+      MPDX_CUDA(cudaMalloc(&items_dev, items.size() * sizeof(f2::item)));
+      items_cap = items.size();
+    }
+    MPDX_CUDA(cudaMemcpyAsync(items_dev, items.data(), items.size() * sizeof(f2::item), cudaMemcpyHostToDevice, stream));
+    MPDX_CUDA(cudaStreamSynchronize(stream));
+    n_items = int(items.size());
+    const int occ = fused2d_batched<T>(t, ni, iga, fct, nullptr, nullptr, 0, nullptr, 0, stream, true);
+    grid = std::max(1, occ) * n_sm;
+    items_tile = t;
+  }
+  void one_step(int parity) {
+    MPDX_CUDA(cudaMemsetAsync(counter + parity, 0, sizeof(int), stream));
+    fused2d_batched<T>(items_tile, ni, iga, fct, probs_dev + parity * hs.size(), items_dev, n_items, counter + parity,
+                       grid, stream, false);
+  }
+  void capture() {
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    MPDX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    one_step(0);
+    one_step(1);
+    MPDX_CUDA(cudaStreamEndCapture(stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    MPDX_CUDA(e);
+  }
+
+  void advance(long long nt) override {
+    if (nt <= 0) return;
+    for (size_t p = 0; p < hs.size(); ++p) {
+      auto *h = hs[p];
+      MPDX_CUDA(cudaStreamSynchronize(h->stream));
+      try {
+        if (h->st.timestep == 0) h->gen.ante_loop(h->scratch);
+      } catch (const error &e) {
+        throw error(e.code, std::string(e.what()) + " (batch problem " + std::to_string(p) + ")");
+      }
+      if (!h->fus.seams_consistent(h->st, h->scratch))
+        throw error(MPDX_E_UNSUPPORTED, "batched advance: the periodic seams of the fields of problem " + std::to_string(p) +
+                                            " are inconsistent");
+    }
+    // problem descriptors for both step parities, from the current time levels
+    std::vector<f2::prob<T>> pr(2 * hs.size());
+    for (size_t p = 0; p < hs.size(); ++p) {
+      auto &st = hs[p]->st;
+      for (int par = 0; par < 2; ++par) {
+        f2::prob<T> a;
+        a.in = st.psi[0][st.tl[0] ^ par].v;
+        a.out = st.psi[0][st.tl[0] ^ par ^ 1].v;
+        a.g0 = st.GC[0].v; a.g1 = st.GC[1].v;
+        a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1;
+        a.n0 = st.n[0]; a.n1 = st.n[1];
+        pr[par * hs.size() + p] = a;
+      }
+    }
+    MPDX_CUDA(cudaMemcpyAsync(probs_dev, pr.data(), pr.size() * sizeof(f2::prob<T>), cudaMemcpyHostToDevice, stream));
+    long long s = 0;
+    if (mode == MPDX_BATCH_PER_PROBLEM) {
+      for (; s < nt; ++s)
+        for (auto *h : hs) {
+          fused2d_launch(h->st, 0, stream);
+          h->st.tl[0] ^= 1;
+        }
+    } else {
+      // autotuning: one timed step per candidate tile, then the fastest one in a graph
+      while (s < nt && tile < 0) {
+        const int c = next_candidate++;
+        use_tile(c);
+        MPDX_CUDA(cudaEventRecord(ev_a, stream));
+        one_step(int(s & 1));
+        MPDX_CUDA(cudaEventRecord(ev_b, stream));
+        MPDX_CUDA(cudaEventSynchronize(ev_b));
+        float ms = 0;
+        MPDX_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
+        tune_ms[c] = ms;
+        ++s;
+        if (next_candidate == kNumBatchTiles) {
+          int best = 0;
+          for (int q = 1; q < kNumBatchTiles; ++q)
+            if (tune_ms[q] < tune_ms[best]) best = q;
+          tile = best;
+          use_tile(best);
+          capture();
+        }
+      }
+      if (s < nt && (s & 1)) one_step(1), ++s;
+      for (; s + 2 <= nt; s += 2) MPDX_CUDA(cudaGraphLaunch(graph, stream));
+      if (s < nt) one_step(0), ++s;
+      for (auto *h : hs) h->st.tl[0] ^= int(nt & 1);
+    }
+    for (auto *h : hs) {
+      h->st.timestep += nt;
+      h->last_path = MPDX_PATH_FUSED;
+    }
+    MPDX_CUDA(cudaEventRecord(ev_done, stream));
+    for (auto *h : hs) MPDX_CUDA(cudaStreamWaitEvent(h->stream, ev_done, 0));
+  }
+
+  void sync() override { MPDX_CUDA(cudaStreamSynchronize(stream)); }
+
+  void info(mpdx_batch_info *out) override {
+    std::memset(out, 0, sizeof(*out));
+    out->n_problems = int(hs.size());
+    out->cells = cells;
+    out->mode = mode;
+    if (tile >= 0) { out->tile_nt = kBatchTiles[tile].nt; out->tile_lx = kBatchTiles[tile].lx; out->grid = grid; }
+    out->n_candidates = kNumBatchTiles;
+    for (int q = 0; q < kNumBatchTiles && q < 8; ++q) out->tune_ms[q] = tune_ms[q];
+  }
+};
+
 }  // namespace mpdx
 
 struct mpdx_solver {
@@ -392,6 +577,81 @@ mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
 void *mpdx_stream(mpdx_handle h) { return (h && h->impl) ? (void *)h->impl->stream : nullptr; }
 
 const char *mpdx_last_error(mpdx_handle h) { return (h && h->impl) ? h->impl->err.c_str() : "invalid handle"; }
+
+}  // extern "C"
+
+struct mpdx_batch {
+  std::unique_ptr<mpdx::batch_base> impl;
+};
+
+extern "C" {
+
+mpdx_status mpdx_batch_create(const mpdx_handle *handles, int n, int mode, mpdx_batch_handle *out) {
+  g_create_error.clear();
+  if (!handles || !out || n < 1) { g_create_error = "null argument or empty batch"; return MPDX_E_ARG; }
+  *out = nullptr;
+  try {
+    if (mode != MPDX_BATCH_PERSISTENT && mode != MPDX_BATCH_PER_PROBLEM) throw mpdx::error(MPDX_E_ARG, "unknown batch mode");
+    const int dtype = handles[0] && handles[0]->impl ? handles[0]->impl->dtype : 0;
+    auto collect = [&](auto *tag) {
+      using S = std::remove_pointer_t<decltype(tag)>;
+      std::vector<S *> v;
+      for (int p = 0; p < n; ++p) {
+        if (!handles[p] || !handles[p]->impl) throw mpdx::error(MPDX_E_ARG, "null handle in batch");
+        auto *sp = dynamic_cast<S *>(handles[p]->impl.get());
+        if (!sp) throw mpdx::error(MPDX_E_ARG, "batch members must be MPDATA solvers of the same dtype");
+        v.push_back(sp);
+      }
+      return v;
+    };
+    auto b = std::make_unique<mpdx_batch>();
+    if (dtype == 8) b->impl.reset(new mpdx::batch_impl<double>(collect((mpdx::mpdata_solver<double> *)nullptr), mode));
+    else if (dtype == 4) b->impl.reset(new mpdx::batch_impl<float>(collect((mpdx::mpdata_solver<float> *)nullptr), mode));
+    else throw mpdx::error(MPDX_E_ARG, "null handle in batch");
+    *out = b.release();
+    return MPDX_OK;
+  } catch (const mpdx::error &e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    return MPDX_E_ARG;
+  }
+}
+
+static mpdx_status batch_guarded(mpdx_batch_handle b, const std::function<void()> &f) {
+  if (!b || !b->impl) return MPDX_E_ARG;
+  try {
+    f();
+    b->impl->err.clear();
+    return MPDX_OK;
+  } catch (const mpdx::error &e) {
+    b->impl->err = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    b->impl->err = e.what();
+    return MPDX_E_ARG;
+  }
+}
+
+mpdx_status mpdx_batch_advance(mpdx_batch_handle b, int64_t nt) {
+  return batch_guarded(b, [&] { b->impl->advance(nt); });
+}
+
+mpdx_status mpdx_batch_get_info(mpdx_batch_handle b, mpdx_batch_info *out) {
+  return batch_guarded(b, [&] {
+    if (!out) throw mpdx::error(MPDX_E_ARG, "null output");
+    b->impl->info(out);
+  });
+}
+
+mpdx_status mpdx_batch_sync(mpdx_batch_handle b) {
+  return batch_guarded(b, [&] { b->impl->sync(); });
+}
+
+const char *mpdx_batch_last_error(mpdx_batch_handle b) { return (b && b->impl) ? b->impl->err.c_str() : "invalid batch"; }
+
+void mpdx_batch_destroy(mpdx_batch_handle b) { delete b; }
 
 void mpdx_destroy(mpdx_handle h) {
   if (!h) return;

@@ -32,12 +32,12 @@ struct mpdata_state {
     return h;
   }
   rng sr(int d) const { return d < nd ? ext(ir[d], H) : rng{0, 0}; }
-  template <class U> void alloc_sclr(field<U> &f) { rng r[3] = {sr(0), sr(1), sr(2)}; f.alloc(nd, r); }
+  template <class U> void alloc_sclr(field<U> &f) { rng r[3] = {sr(0), sr(1), sr(2)}; f.alloc(nd, r, stream); }
   void alloc_vctr(field<T> *v) {
     for (int c = 0; c < nd; ++c) {
       rng r[3] = {sr(0), sr(1), sr(2)};
       r[c] = ext(exh(ir[c]), H - 1);  // i^h^(halo-1)  (solver_common.hpp:370-371)
-      v[c].alloc(nd, r);
+      v[c].alloc(nd, r, stream);
     }
   }
 

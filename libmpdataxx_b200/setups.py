@@ -254,3 +254,21 @@ def boussinesq_bubble_3d(nx=256, ny=256, nz=128, seed=6, dx=10.0, n_bv=0.01, dty
     return {"grid": (nx, ny, nz), "bcs": ["cyclic", "cyclic", "cyclic", "cyclic", "rigid", "rigid"],
             "advectee": [zero, zero.copy(), zero.copy(), tht.astype(dtype)], "tht_e": tht_e.astype(dtype),
             "dt": 0.75, "dx": (dx, dx, dx), "tht_ref": tref, "g": g, "prs_tol": 1e-7, "prs_k": 1}
+
+
+def batched_problems(n=256, seed=5, lo=64, hi=1024, dtype=np.float32, cmax=0.5):
+    """Independent 2D cyclic problems of uneven sizes: side lengths drawn
+    uniformly from [lo, hi] per axis (seed), each with its own divergence-free
+    random-Fourier Courant field (seed 1000 + p, max |C| = cmax) and an
+    i.i.d. log-normal(0, 1) advectee (seed 2000 + p).  Returns a list of
+    set-ups in the reference's accessor conventions."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, size=(n, 2))
+    out = []
+    for p, (nx, ny) in enumerate(sizes):
+        nx, ny = int(nx), int(ny)
+        gx, gy = periodic_curl_2d(nx, ny, 1000 + p, cmax=cmax, dtype=dtype)
+        psi = np.random.default_rng(2000 + p).lognormal(0.0, 1.0, size=(nx - 1, ny - 1))
+        out.append({"grid": (nx, ny), "bcs": ["cyclic"] * 4, "advectee": [wrap_periodic(psi).astype(dtype)],
+                    "advector": [gx.astype(dtype), gy.astype(dtype)]})
+    return out

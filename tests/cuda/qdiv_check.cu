@@ -1,0 +1,44 @@
+// Checks mpdx::qdiv (reciprocal times Markstein correction) against the CUDA
+// '/' operator on random operands over many binades, FP64 and FP32.  Prints
+// the number of mismatches per type and exits non-zero if there is any.
+#include <cstdio>
+
+#include "../../libmpdataxx_b200/csrc/mpdx_common.cuh"
+
+__device__ unsigned long long xs(unsigned long long &s) { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return s; }
+
+template <class T>
+__global__ void k_check(const T *bs, int nb, long long per_thread, unsigned long long *bad) {
+  unsigned long long s = 0x9E3779B97F4A7C15ull ^ (blockIdx.x * 1315423911ull + threadIdx.x * 2654435761ull + 1);
+  unsigned long long nbad = 0;
+  for (int t = 0; t < nb; ++t) {
+    const T b = bs[t], y = T(1) / b;
+    for (long long i = 0; i < per_thread; ++i) {
+      const unsigned long long r = xs(s);
+      const double u = double(r >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+      const T a = T(ldexp(u, int(r & 63) - 40));
+      if (mpdx::qdiv<T>(a, b, y) != a / b) ++nbad;
+    }
+  }
+  atomicAdd(bad, nbad);
+}
+
+int main() {
+  const double bd[] = {10.0, 0.1, 3.0, 7.3, 1e-3, 123.456, 0.75, 1.0 / 3.0, 12.5, 0.01};
+  const int nb = 10;
+  double *dbd; float *dbf; unsigned long long *dbad;
+  float bf[nb];
+  for (int i = 0; i < nb; ++i) bf[i] = float(bd[i]);
+  cudaMalloc(&dbd, sizeof(bd)); cudaMalloc(&dbf, sizeof(bf)); cudaMalloc(&dbad, 2 * sizeof(unsigned long long));
+  cudaMemcpy(dbd, bd, sizeof(bd), cudaMemcpyHostToDevice);
+  cudaMemcpy(dbf, bf, sizeof(bf), cudaMemcpyHostToDevice);
+  cudaMemset(dbad, 0, 2 * sizeof(unsigned long long));
+  k_check<double><<<148 * 4, 256>>>(dbd, nb, 1000, dbad);
+  k_check<float><<<148 * 4, 256>>>(dbf, nb, 1000, dbad + 1);
+  unsigned long long bad[2] = {1, 1};
+  const cudaError_t e = cudaMemcpy(bad, dbad, sizeof(bad), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { std::printf("CUDA error: %s\n", cudaGetErrorString(e)); return 2; }
+  const long long n = 148LL * 4 * 256 * 1000 * nb;
+  std::printf("qdiv vs '/': %lld operand pairs per type, mismatches fp64 %llu fp32 %llu\n", n, bad[0], bad[1]);
+  return (bad[0] || bad[1]) ? 1 : 0;
+}

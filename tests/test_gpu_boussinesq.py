@@ -125,3 +125,17 @@ def test_boussinesq_fp64_pressure_is_not_viewed_as_fp32():
     out = np.empty((17, 15), dtype=np.float32)
     rc = run.L.mpdx_get_field(run.h, _lib.FIELD_PRESSURE, 0, out.ctypes.data, None)
     assert rc == _lib.MPDX_E_ARG
+
+
+def test_reciprocal_division_matches_cuda_division(tmp_path):
+    """The pressure operators divide by the grid spacing with mpdx::qdiv
+    (reciprocal + Markstein correction); it must return the IEEE quotient."""
+    import os
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "qdiv_check")
+    subprocess.run(["nvcc", "-std=c++17", "-O3", "--fmad=false", "-gencode", "arch=compute_100a,code=sm_100a",
+                    os.path.join(here, "cuda", "qdiv_check.cu"), "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr

@@ -1,0 +1,53 @@
+"""The preconditioner network's CPU oracle: its analytic gradients must agree
+with finite differences (this pins the oracle before it checks the GPU)."""
+import numpy as np
+import pytest
+
+import precond_oracle as po
+
+
+@pytest.mark.parametrize("grid,wrap", [((9, 7, 6), (True, True, False)), ((11, 10), (True, False, False))])
+def test_gradients_match_finite_differences(grid, wrap):
+    nd = len(grid)
+    ch = (2, 3, 4, 5)
+    P = po.init_params(nd, ch, seed=1)
+    rng = np.random.default_rng(2)
+    for k in P:
+        if k.startswith("b_"):
+            P[k] = rng.normal(size=P[k].shape) * 0.1
+    r = rng.normal(size=grid)
+    w = rng.normal(size=grid)  # loss = sum(w * q)
+    wrap3 = tuple(wrap) + (False,) * (3 - len(wrap))
+    q, c = po.forward(r, P, grid, wrap3, ch)
+    G = po.backward(w, c, P, grid, wrap3)
+
+    def loss(P2, r2):
+        return float((w * po.forward(r2, P2, grid, wrap3, ch)[0]).sum())
+
+    eps = 1e-6
+    for name in ["W_e0", "W_e3", "W_m3", "W_d2", "W_d0", "W_q", "b_e1", "b_d1", "b_q"]:
+        flat = P[name].reshape(-1)
+        for idx in rng.choice(flat.size, size=min(4, flat.size), replace=False):
+            Pp = {k: v.copy() for k, v in P.items()}
+            Pm = {k: v.copy() for k, v in P.items()}
+            Pp[name].reshape(-1)[idx] += eps
+            Pm[name].reshape(-1)[idx] -= eps
+            fd = (loss(Pp, r) - loss(Pm, r)) / (2 * eps)
+            assert abs(fd - G[name].reshape(-1)[idx]) <= 1e-6 * max(1.0, abs(fd)), (name, idx, fd, G[name].reshape(-1)[idx])
+    for idx in rng.choice(r.size, size=4, replace=False):
+        rp, rm = r.copy(), r.copy()
+        rp.reshape(-1)[idx] += eps
+        rm.reshape(-1)[idx] -= eps
+        fd = (loss(P, rp) - loss(P, rm)) / (2 * eps)
+        assert abs(fd - G["r"].reshape(-1)[idx]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_network_is_linear_and_shapes():
+    grid = (12, 9, 5)
+    P = po.init_params(3, seed=0)
+    r = np.random.default_rng(0).normal(size=grid)
+    q1, _ = po.forward(r, P, grid, (True, True, False))
+    q2, _ = po.forward(3.0 * r, P, grid, (True, True, False))
+    assert q1.shape == grid
+    assert np.allclose(q2, 3.0 * q1)  # zero biases at initialisation
+    assert po.level_shapes(grid) == [(12, 9, 5), (6, 5, 3), (3, 3, 2), (2, 2, 1)]
