@@ -11,6 +11,11 @@ For N > 1 (torchrun, one process per GPU) every rank advances its own replica
 (the path does not shard on one GPU: "replicas only"); value = all ranks' cell
 updates / the slowest rank's device time.
 
+With N = 1 the line also carries "batched_2d" (256 uneven 2D problems in one
+persistent launch vs one launch per problem) and "gcr" (3D Boussinesq pressure
+solves to max|err| <= 1e-7/dt: iterations and device time per solve, plain GCR
+vs GCR with the learned preconditioner trained on the first solves).
+
 --impl reference times the reference's CPU path on this host's cores: the CPU
 restatement in oracle/ (the reference itself cannot be built here: it needs
 Blitz++ and Boost), compiled with the reference's release flags plus OpenMP,
@@ -145,6 +150,86 @@ def cpu_baseline(n=160, steps=3):
             "sample": f"{n}^3 fct|iga n_iters=2 FP32, {steps} steps, {dt:.1f} s, oracle -Ofast+OpenMP"}
 
 
+def batched_extra(n_problems=256, steps=50):
+    """C4: independent 2D fct problems of uneven sizes, one persistent launch per
+    step in a CUDA graph (autotuned tile) vs one launch per problem per step."""
+    import numpy as np
+    from libmpdataxx_b200 import bcond, concurr, opts, setups, solvers
+    probs = setups.batched_problems(n=n_problems)
+    cells = sum(s["grid"][0] * s["grid"][1] for s in probs)
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = np.float32
+    ct.n_dims = 2
+    ct.n_eqns = 1
+    ct.opts = opts.fct
+    out = {"workload": f"{n_problems} cyclic 2D fct problems, sides 64..1024, FP32", "cells_per_step": cells}
+    for mode, k in (("persistent", steps), ("per_problem", max(5, steps // 5))):
+        runs = []
+        for s in probs:
+            p = solvers.mpdata.rt_params_t(grid_size=list(s["grid"]), n_iters=2, max_abs_div_eps=1e-6)
+            r = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * 4, p=p, path="fused")
+            r.set_advectee(s["advectee"][0])
+            for d, a in enumerate(s["advector"]):
+                r.set_advector(a, d)
+            runs.append(r)
+        b = concurr.batch(runs, mode=mode)
+        b.advance(10)  # first steps include the autotuner
+        b.sync()
+        t0 = time.perf_counter()
+        b.advance(k)
+        b.sync()
+        dt = (time.perf_counter() - t0) / k
+        out[mode] = {"ms_per_step": dt * 1e3, "cell_updates_per_s": cells / dt}
+        if mode == "persistent":
+            i = b.info()
+            out["tile"] = {"nt": i["tile_nt"], "lx": i["tile_lx"], "grid": i["grid"], "tune_ms": i["tune_ms"]}
+        b.close()
+        for r in runs:
+            r.close()
+    out["speedup_vs_per_problem"] = out["persistent"]["cell_updates_per_s"] / out["per_problem"]["cell_updates_per_s"]
+    return out
+
+
+def gcr_extra(grid=(256, 256, 128), record=30, train=400, compare=5):
+    """C5: 3D Boussinesq, FP32 advection with FP64 GCR (cr) to max|err| <= 1e-7/dt;
+    pairs from the first `record` plain solves train the learned preconditioner,
+    then `compare` solves each, plain and learned: iterations and device time per solve."""
+    import numpy as np
+    from libmpdataxx_b200 import setups
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from runners import bq_run
+    s = setups.boussinesq_bubble_3d(*grid)
+    run = bq_run(s, dtype=np.float32, prs_fp64=True)
+    run.precond_record(record)
+    run.advance(record)
+    run.sync()
+    t0 = time.perf_counter()
+    loss = run.precond_train(train, lr=2e-3)
+    t_train = time.perf_counter() - t0
+
+    def solves(k):
+        it, ms = [], []
+        for _ in range(k):
+            run.advance(1)
+            st = run.stats()
+            it.append(st["gcr_iters"])
+            ms.append(st["gcr_ms"])
+        return it, ms
+
+    it_p, ms_p = solves(compare)
+    run.precond_enable(True)
+    it_l, ms_l = solves(compare)
+    run.close()
+    return {"workload": f"3D Boussinesq {grid[0]}x{grid[1]}x{grid[2]}, x/y cyclic, z rigid, FP32 advection, FP64 GCR (cr), prs_tol 1e-7",
+            "plain": {"iters_per_solve": statistics.mean(it_p), "ms_per_solve": statistics.mean(ms_p)},
+            "learned": {"iters_per_solve": statistics.mean(it_l), "ms_per_solve": statistics.mean(ms_l)},
+            "time_to_tol_speedup": statistics.mean(ms_p) / statistics.mean(ms_l),
+            "training": {"pairs": record, "adam_steps": train, "final_loss": loss, "seconds": t_train}}
+
+
 def reference_arm(args, rank):
     """Each step advances a bounded sample of the workload: the same
     configuration on an n_ref^3 grid (default 256^3, 1/8 of the cells), so that
@@ -194,6 +279,7 @@ def main():
     ap.add_argument("--n-ref", type=int, default=256)
     ap.add_argument("--dtype", default="float32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched-2D and Boussinesq/GCR measurements")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
@@ -299,6 +385,9 @@ def main():
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+    if world == 1 and not args.no_extras:
+        line["batched_2d"] = batched_extra()
+        line["gcr"] = gcr_extra()
     print(json.dumps(line))
     run.close()
 

@@ -98,6 +98,8 @@ typedef struct {
   int64_t gcr_iters_total; /* since creation */
   double gcr_residual;     /* max|err| at the end of the last pressure solve */
   int path;                /* path used by the last advance (MPDX_PATH_GENERAL/FUSED) */
+  double gcr_ms;           /* device time of the last pressure solve, start to max|err| <= prs_tol / dt */
+  int gcr_fallback;        /* 1 if the last solve left the learned preconditioner for plain GCR */
 } mpdx_step_stats;
 
 /* Fill *cfg with the reference defaults (opts = iga|fct, n_iters = 2, ...). */
@@ -188,6 +190,26 @@ mpdx_status mpdx_batch_get_info(mpdx_batch_handle b, mpdx_batch_info *out);
 mpdx_status mpdx_batch_sync(mpdx_batch_handle b);
 const char *mpdx_batch_last_error(mpdx_batch_handle b);
 void mpdx_batch_destroy(mpdx_batch_handle b);
+
+/* ---- Learned preconditioner inside a Boussinesq solver's GCR ----
+ *
+ * No counterpart in the reference (its cr / gcrk solvers use no
+ * preconditioner).  FP64 pressure solves only (dtype 8, or prs_fp64).
+ * mpdx_precond_record keeps the (initial residual, correction Phi_end -
+ * Phi_start) pair of each of the next max_pairs pressure solves on the device;
+ * mpdx_precond_train runs `steps` Adam steps of the network on randomly drawn
+ * pairs (each normalised by its residual's max-norm) and returns the mean loss
+ * of the last tenth; mpdx_precond_enable switches GCR to the flexible form whose
+ * search directions start from the network's output instead of the residual.
+ * The stopping test (max|err| <= prs_tol / dt) is unchanged: only the
+ * iteration count changes.  Weights are exchanged in the mpdx_pcnet layout. */
+mpdx_status mpdx_precond_record(mpdx_handle h, int64_t max_pairs);
+mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t seed, double *final_loss);
+mpdx_status mpdx_precond_enable(mpdx_handle h, int on);
+int64_t mpdx_precond_pairs(mpdx_handle h);
+int64_t mpdx_precond_num_params(mpdx_handle h);
+mpdx_status mpdx_precond_get_params(mpdx_handle h, float *host);
+mpdx_status mpdx_precond_set_params(mpdx_handle h, const float *host);
 
 /* ---- Learned GCR preconditioner network on its own ----
  *

@@ -27,7 +27,9 @@ EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_fie
            "mpdx_batch_get_info", "mpdx_batch_sync", "mpdx_batch_last_error", "mpdx_batch_destroy",
            "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
            "mpdx_pcnet_get_params", "mpdx_pcnet_forward", "mpdx_pcnet_backward", "mpdx_pcnet_train_step",
-           "mpdx_pcnet_last_error", "mpdx_pcnet_destroy"]
+           "mpdx_pcnet_last_error", "mpdx_pcnet_destroy", "mpdx_precond_record", "mpdx_precond_train",
+           "mpdx_precond_enable", "mpdx_precond_pairs", "mpdx_precond_num_params", "mpdx_precond_get_params",
+           "mpdx_precond_set_params"]
 BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 
 
@@ -46,7 +48,8 @@ class Config(ctypes.Structure):
 class StepStats(ctypes.Structure):
     _fields_ = [("timestep", ctypes.c_int64), ("time", ctypes.c_double), ("mass", ctypes.c_double),
                 ("min", ctypes.c_double), ("max", ctypes.c_double), ("gcr_iters", ctypes.c_int64),
-                ("gcr_iters_total", ctypes.c_int64), ("gcr_residual", ctypes.c_double), ("path", ctypes.c_int)]
+                ("gcr_iters_total", ctypes.c_int64), ("gcr_residual", ctypes.c_double), ("path", ctypes.c_int),
+                ("gcr_ms", ctypes.c_double), ("gcr_fallback", ctypes.c_int)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -122,6 +125,20 @@ def lib():
     L.mpdx_pcnet_last_error.restype = ctypes.c_char_p
     L.mpdx_pcnet_destroy.argtypes = [vp]
     L.mpdx_pcnet_destroy.restype = None
+    L.mpdx_precond_record.argtypes = [vp, ctypes.c_int64]
+    L.mpdx_precond_record.restype = ctypes.c_int
+    L.mpdx_precond_train.argtypes = [vp, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.mpdx_precond_train.restype = ctypes.c_int
+    L.mpdx_precond_enable.argtypes = [vp, ctypes.c_int]
+    L.mpdx_precond_enable.restype = ctypes.c_int
+    L.mpdx_precond_pairs.argtypes = [vp]
+    L.mpdx_precond_pairs.restype = ctypes.c_int64
+    L.mpdx_precond_num_params.argtypes = [vp]
+    L.mpdx_precond_num_params.restype = ctypes.c_int64
+    L.mpdx_precond_get_params.argtypes = [vp, fp]
+    L.mpdx_precond_get_params.restype = ctypes.c_int
+    L.mpdx_precond_set_params.argtypes = [vp, fp]
+    L.mpdx_precond_set_params.restype = ctypes.c_int
     _lib = L
     return L
 

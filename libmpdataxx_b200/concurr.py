@@ -159,6 +159,36 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_stats(self.h, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in _lib.StepStats._fields_}
 
+    # -- learned GCR preconditioner (Boussinesq solvers; no counterpart in the reference) --
+    def precond_record(self, max_pairs):
+        """Keep the (initial residual, correction) pair of each of the next max_pairs pressure solves."""
+        _check(self.L, self.h, self.L.mpdx_precond_record(self.h, int(max_pairs)))
+
+    def precond_pairs(self):
+        return int(self.L.mpdx_precond_pairs(self.h))
+
+    def precond_train(self, steps, lr=1e-3, seed=0):
+        """Adam steps of the network on the recorded pairs; returns the mean loss of the last tenth."""
+        loss = ctypes.c_double()
+        _check(self.L, self.h, self.L.mpdx_precond_train(self.h, int(steps), float(lr), int(seed), ctypes.byref(loss)))
+        return loss.value
+
+    def precond_enable(self, on=True):
+        """GCR search directions from the network's output (flexible GCR) instead of the residual."""
+        _check(self.L, self.h, self.L.mpdx_precond_enable(self.h, 1 if on else 0))
+
+    def precond_params(self):
+        n = int(self.L.mpdx_precond_num_params(self.h))
+        if n < 0:
+            raise _lib.MpdxError(_lib.MPDX_E_UNSUPPORTED, self.L.mpdx_last_error(self.h).decode())
+        out = np.empty(n, dtype=np.float32)
+        _check(self.L, self.h, self.L.mpdx_precond_get_params(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_precond_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.L, self.h, self.L.mpdx_precond_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
     def min(self, e=0):
         return float(self.advectee(e).min())
 

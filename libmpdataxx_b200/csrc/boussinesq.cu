@@ -34,6 +34,7 @@
 #include <type_traits>
 
 #include "boussinesq.cuh"
+#include "precond.cuh"
 
 namespace mpdx {
 namespace bq {
@@ -448,6 +449,206 @@ void launch_inner(int v, unsigned G, dim3 blk, cudaStream_t s, const geom &g, in
 }
 
 // ---------------------------------------------------------------------------
+// GCR(k) with a preconditioner M (the learned network): directions start from
+// q = M(err) instead of err (flexible GCR); err is updated with the exact
+// lap of each direction, so the stopping test is the reference's.  The
+// error is updated in place (no stencil reads it in the same kernel).
+
+// loop_init: p_0 = M(err) (already written by the network), lap_p_0 = lap(p_0); first beta sums
+template <class T>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_init_pc(geom g, dfield<T> err, dfield<T> p0, dfield<T> lp0,
+                                                                gcr_dev<T> *dv, double *part) {
+  dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  for_interior(g, [&](int i, int j, int k) {
+    const T l = lap<T>(fld<T>{p0.o}, p0, no_u{}, g, i, j, k);
+    lp0(i, j, k) = l;
+    acc[0] = dd_add(acc[0], dd{double(T(l * l)), 0.0});
+    acc[1] = dd_add(acc[1], dd{double(T(err(i, j, k) * l)), 0.0});
+  });
+  double mx = 0, mn = 0;
+  if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
+    dv->pend_den = T(ddv(acc[0]));
+    dv->pend_num = T(ddv(acc[1]));
+  }
+}
+
+// step v = NV - 1: Phi += beta p_v, err += beta lap_p_v, convergence test
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_tol, dfield<T> phi, dfield<T> err,
+                                                                  dirs<T> D, gcr_dev<T> *dv, double *part) {
+  constexpr int v = NV - 1;
+  if (dv->done) return;
+  const T den = dv->pend_den;
+  const T b = den != T(0) ? -dv->pend_num / den : dv->beta;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
+  const dfield<T> pv = D.p[v], lpv = D.lp[v];
+  dd acc[1] = {{0.0, 0.0}};
+  double mx = -DBL_MAX, mn = DBL_MAX;
+  for_interior(g, [&](int i, int j, int k) {
+    phi(i, j, k) = phi(i, j, k) + b * pv(i, j, k);
+    const T e = err(i, j, k) + b * lpv(i, j, k);
+    err(i, j, k) = e;
+    mx = fmax(mx, double(e));
+    mn = fmin(mn, double(e));
+  });
+  if (grid_reduce<1, true>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
+    const T amx = fabs(T(mx)), amn = fabs(T(mn));
+    const T error = amx < amn ? amn : amx;
+    dv->residual = double(error);
+    if (error <= err_tol) dv->converged = 1;
+  }
+}
+
+// lq = lap(q), alpha_l = -<lq, lap_p_l> / tmp_den[l]
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_lapq(geom g, dfield<T> q, dfield<T> lq, dirs<T> D, gcr_dev<T> *dv,
+                                                             double *part) {
+  if (dv->done) return;
+  dfield<T> lps[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
+  dd acc[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
+  for_interior(g, [&](int i, int j, int k) {
+    const T l = lap<T>(fld<T>{q.o}, q, no_u{}, g, i, j, k);
+    lq(i, j, k) = l;
+#pragma unroll
+    for (int m = 0; m < NV; ++m) acc[m] = dd_add(acc[m], dd{double(T(l * lps[m](i, j, k))), 0.0});
+  });
+  double mx = 0, mn = 0;
+  if (grid_reduce<NV, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const T dl = dv->tmp_den[l];
+      if (dl != T(0)) dv->alpha[l] = -T(ddv(acc[l])) / dl;
+    }
+  }
+}
+
+// next direction from q and lq; beta sums with the current error
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction_pc(geom g, int kk, dfield<T> err, dfield<T> q, dfield<T> lq,
+                                                                     dirs<T> D, gcr_dev<T> *dv, double *part) {
+  constexpr int v = NV - 1;
+  if (dv->done) return;
+  T a[NV];
+  dfield<T> ps[NV], lps[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) { a[l] = dv->alpha[l]; ps[l] = D.p[l]; lps[l] = D.lp[l]; }
+  const bool restart = v == kk - 1;
+  const dfield<T> pd = restart ? D.p[0] : D.p[NV < kGcrMaxK ? NV : 0], lpd = restart ? D.lp[0] : D.lp[NV < kGcrMaxK ? NV : 0];
+  dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  for_interior(g, [&](int i, int j, int k) {
+    T pn = q(i, j, k), ln = lq(i, j, k);
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      pn = pn + a[l] * ps[l](i, j, k);
+      ln = ln + a[l] * lps[l](i, j, k);
+    }
+    pd(i, j, k) = pn;
+    lpd(i, j, k) = ln;
+    acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
+    acc[1] = dd_add(acc[1], dd{double(T(err(i, j, k) * ln)), 0.0});
+  });
+  double mx = 0, mn = 0;
+  if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
+    dv->pend_den = T(ddv(acc[0]));
+    dv->pend_num = T(ddv(acc[1]));
+    if (restart) {
+      dv->iters += 1;
+      if (dv->converged) dv->done = 1;
+      if (dv->iters > 10000) { dv->stuck = 1; dv->done = 1; }
+    }
+  }
+}
+
+template <class T, int NV>
+void launch_pc_update(unsigned G, dim3 blk, cudaStream_t s, const geom &g, T err_tol, dfield<T> phi, dfield<T> err,
+                      const dirs<T> &D, gcr_dev<T> *dv, double *part) {
+  k_gcr_update_pc<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, err, D, dv, part);
+}
+template <class T, int NV>
+void launch_pc_direction(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, dfield<T> err, dfield<T> q,
+                         dfield<T> lq, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
+  k_gcr_lapq<T, NV><<<G, blk, 0, s>>>(g, q, lq, D, dv, part);
+  k_gcr_direction_pc<T, NV><<<G, blk, 0, s>>>(g, kk, err, q, lq, D, dv, part);
+}
+#define MPDX_NV_SWITCH(v, CALL)                     \
+  switch ((v) + 1) {                                \
+    case 1: CALL(1); break;                         \
+    case 2: CALL(2); break;                         \
+    case 3: CALL(3); break;                         \
+    case 4: CALL(4); break;                         \
+    case 5: CALL(5); break;                         \
+    case 6: CALL(6); break;                         \
+    case 7: CALL(7); break;                         \
+    default: CALL(8); break;                        \
+  }
+
+// training pairs: a field's interior as a compact FP32 array, or the difference of two fields
+template <class T>
+__global__ void k_to_compact(geom g, dfield<T> a, dfield<T> b, float *out) {
+  for_interior(g, [&](int i, int j, int k) {
+    const long long v = ((long long)i * g.n[1] + j) * g.n[2] + k;
+    out[v] = b.o ? float(a(i, j, k) - b(i, j, k)) : float(a(i, j, k));
+  });
+}
+template <class T>
+__global__ void k_copy_field(geom g, dfield<T> src, dfield<T> dst) {
+  for_interior(g, [&](int i, int j, int k) { dst(i, j, k) = src(i, j, k); });
+}
+// pair normalisation: s = max|r|, then r / s and t / s
+__global__ void k_absmax(const float *x, long long n, float *s) {
+  float m = 0.f;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(x[q]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned *>(s), __float_as_uint(m));  // non-negative floats order as their bits
+}
+// training in the operator's norm: d = q - t; z = lap(d) with loss += sum z^2 / n and
+// dz = (2 / n) z (scale_out); then dq = lap(dz) (lap is symmetric up to the rigid-wall rows)
+__global__ void k_sub(const float *a, float ca, const float *b, long long n, float *o) {  // o = ca * a - b
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) o[q] = ca * a[q] - b[q];
+}
+__global__ void k_sumsq(const float *x, long long n, double *out) {
+  double sq = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    sq += double(x[q]) * double(x[q]);
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, sq);
+}
+// r / rms(r), t / rms(r) with rms from the sum of squares in *ss
+__global__ void k_scale_rms(const float *r, const float *t, long long n, const double *ss, float *ro, float *to) {
+  const double rms = sqrt(*ss / double(n));
+  const float inv = rms > 0.0 ? float(1.0 / rms) : 1.f;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    ro[q] = r[q] * inv;
+    to[q] = t[q] * inv;
+  }
+}
+__global__ void __launch_bounds__(kRedThreads, 4) k_lap_compact(geom g, const float *x, float *out, double *loss, float scale_out) {
+  const dfield<float> lay{const_cast<float *>(x), (long long)g.n[1] * g.n[2], g.n[2], g.nd == 3 ? 1 : 0};
+  double sq = 0.0;
+  for_interior(g, [&](int i, int j, int k) {
+    const float z = lap<float>(fld<float>{x}, lay, no_u{}, g, i, j, k);
+    out[off3(lay, i, j, k)] = scale_out * z;
+    sq += double(z) * double(z);
+  });
+  if (loss) {
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0) atomicAdd(loss, sq / double(g.cells));
+  }
+}
+__global__ void k_scale2(const float *r, const float *t, long long n, const float *s, float *ro, float *to) {
+  const float inv = *s > 0.f ? 1.f / *s : 1.f;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    ro[q] = r[q] * inv;
+    to[q] = t[q] * inv;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pointwise stages
 
 enum { APPLY_PROJECT = 0, APPLY_RHS = 1, APPLY_FINISH = 2 };
@@ -598,7 +799,7 @@ template <class T, class P>
 boussinesq<T, P>::boussinesq(const mpdx_config &c, cudaStream_t s) {
   if (c.n_dims < 2) throw error(MPDX_E_UNSUPPORTED, "the Boussinesq solver needs 2 or 3 dimensions");
   if (c.n_eqns != c.n_dims + 1) throw error(MPDX_E_ARG, "the Boussinesq solver advects n_dims + 1 equations (velocities and theta)");
-  if (c.precond != MPDX_PRECOND_IDENTITY) throw error(MPDX_E_UNSUPPORTED, "preconditioner not built");
+  if (c.precond != MPDX_PRECOND_IDENTITY && c.precond != MPDX_PRECOND_LEARNED) throw error(MPDX_E_ARG, "unknown preconditioner");
   if (c.dt <= 0) throw error(MPDX_E_ARG, "dt must be positive");
   if (c.tht_ref == 0) throw error(MPDX_E_ARG, "Tht_ref must be non-zero");
   for (int q = 0; q < 2 * c.n_dims; ++q)
@@ -651,6 +852,9 @@ boussinesq<T, P>::~boussinesq() {
   if (part) cudaFree(part);
   if (scratch) cudaFree(scratch);
   if (vip_dev) cudaFree(vip_dev);
+  for (float *p : {pairs, tr_r, tr_t, tr_q, tr_z, tr_dq}) if (p) cudaFree(p);
+  if (tr_loss) cudaFree(tr_loss);
+  for (cudaEvent_t e : ev_solve) if (e) cudaEventDestroy(e);
 }
 
 // pressure_solver_update (mpdata_rhs_vip_prs_common.hpp:99-123) without the final
@@ -667,29 +871,199 @@ void boussinesq<T, P>::pressure_solve() {
     D.p[v] = p_err[std::min(v, k_iters - 1)].v;
     D.lp[v] = lap_p_err[std::min(v, k_iters - 1)].v;
   }
+  if (!ev_solve[0]) { MPDX_CUDA(cudaEventCreate(&ev_solve[0])); MPDX_CUDA(cudaEventCreate(&ev_solve[1])); }
+  MPDX_CUDA(cudaEventRecord(ev_solve[0], s));
+  // recording: the pair (residual, Phi_end - Phi) at the start and at up to
+  // kSnaps later iterations of this plain solve
+  const bool rec = pairs && n_pairs < max_pairs && !(use_net && net);
+  long long rec_slots[1 + kSnaps];
+  int n_rec = 0;
+  if (rec) {
+    rec_slots[n_rec++] = n_pairs++;
+    bq::k_copy_field<P><<<G, kBlk, 0, s>>>(gm, Phi.v, snap[0].v);
+  }
   bq::k_gcr_reset<P><<<1, 1, 0, s>>>(dev);
   bq::k_err_init<P, T><<<G, kBlk, 0, s>>>(gm, Phi.v, u, err[0].v);
-  bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+  if (rec) bq::k_to_compact<P><<<G, kBlk, 0, s>>>(gm, err[0].v, dfield<P>{}, pairs + size_t(rec_slots[0]) * 2 * gm.cells);
+  bool pcnd = use_net && net;
+  fell_back = false;
+  if (pcnd) {
+    if constexpr (std::is_same<P, double>::value) {
+      const auto &e = err[0].v;
+      net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, p_err[0].v.o, nullptr);
+    }
+    bq::k_gcr_init_pc<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+  } else {
+    bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+  }
   MPDX_LAUNCH_CHECK();
   long long launched = 0;
   for (;;) {
-    const long long batch = launched == 0 ? std::max(1LL, predicted) : std::max(4LL, predicted / 4);
+    long long batch = launched == 0 ? std::max(1LL, predicted) : std::max(4LL, predicted / 4);
+    if (rec) batch = std::min(batch, 16LL);  // snapshots are taken between batches
     for (long long b = 0; b < batch; ++b)
       for (int v = 0; v < k_iters; ++v) {
-        bq::launch_inner<P>(v, G, kBlk, s, gm, k_iters, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
+        if (!pcnd) {
+          bq::launch_inner<P>(v, G, kBlk, s, gm, k_iters, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
+          continue;
+        }
+        // preconditioned step: update, q = M(err) (skipped once converged), lap(q), new direction
+#define MPDX_PC_UPD(NV) bq::launch_pc_update<P, NV>(G, kBlk, s, gm, err_tol, Phi.v, err[0].v, D, dev, part)
+#define MPDX_PC_DIR(NV) bq::launch_pc_direction<P, NV>(G, kBlk, s, gm, k_iters, err[0].v, q_f.v, lq_f.v, D, dev, part)
+        MPDX_NV_SWITCH(v, MPDX_PC_UPD)
+        if constexpr (std::is_same<P, double>::value) {
+          const auto &e = err[0].v;
+          net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, q_f.v.o, &dev->done);
+        }
+        MPDX_NV_SWITCH(v, MPDX_PC_DIR)
+#undef MPDX_PC_UPD
+#undef MPDX_PC_DIR
       }
     MPDX_LAUNCH_CHECK();
     launched += batch;
+    MPDX_CUDA(cudaEventRecord(ev_solve[1], s));
     MPDX_CUDA(cudaMemcpyAsync(hdev, dev, sizeof(gcr_dev<P>), cudaMemcpyDeviceToHost, s));
     MPDX_CUDA(cudaStreamSynchronize(s));
     if (hdev->stuck) throw error(MPDX_E_PRS_STUCK, "libmpdata++: stuck in pressure solver");
     if (hdev->done) break;
+    if (rec && n_rec < 1 + kSnaps && n_pairs < max_pairs && hdev->iters >= 16LL << (n_rec - 1)) {
+      const auto &e = err[hdev->cur].v;  // the current error after the last inner step
+      rec_slots[n_rec] = n_pairs++;
+      bq::k_to_compact<P><<<G, kBlk, 0, s>>>(gm, e, dfield<P>{}, pairs + size_t(rec_slots[n_rec]) * 2 * gm.cells);
+      bq::k_copy_field<P><<<G, kBlk, 0, s>>>(gm, Phi.v, snap[n_rec].v);
+      MPDX_LAUNCH_CHECK();
+      ++n_rec;
+    }
+    if (pcnd && hdev->iters > std::max(20LL, 2 * last_plain_iters)) {
+      // the learned directions are not converging: continue from the current
+      // iterate with plain GCR (directions restart from the residual)
+      bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+      MPDX_LAUNCH_CHECK();
+      pcnd = false;
+      fell_back = true;
+      ++fallbacks;
+    }
+  }
+  {
+    float ms = 0;
+    MPDX_CUDA(cudaEventElapsedTime(&ms, ev_solve[0], ev_solve[1]));
+    last_solve_ms = ms;
   }
   iters = hdev->iters;
   iters_total += iters;
+  if (!(use_net && net)) last_plain_iters = iters;
   last_residual = hdev->residual;
   predicted = std::max(1LL, iters);
+  for (int q = 0; q < n_rec; ++q)  // corrections Phi_end - Phi_snapshot
+    bq::k_to_compact<P><<<G, kBlk, 0, s>>>(gm, Phi.v, snap[q].v, pairs + (size_t(rec_slots[q]) * 2 + 1) * gm.cells);
+  MPDX_LAUNCH_CHECK();
 }
+template <class T, class P>
+void boussinesq<T, P>::ensure_net() {
+  if (net) return;
+  if constexpr (!std::is_same<P, double>::value) {
+    throw error(MPDX_E_UNSUPPORTED, "the learned preconditioner needs the FP64 pressure solve (dtype 8, or prs_fp64)");
+  } else {
+    int grid[3], wrap[3];
+    for (int d = 0; d < 3; ++d) {
+      grid[d] = d < st.nd ? st.n[d] : 1;
+      wrap[d] = d < st.nd ? (st.bcs[d][0] == MPDX_BC_CYCLIC ? 1 : 0) : 1;
+    }
+    net.reset(new pc::net(st.nd, grid, wrap, pc_channels, 12345, st.stream));
+    st.alloc_sclr(q_f);
+    st.alloc_sclr(lq_f);
+  }
+}
+
+template <class T, class P>
+void boussinesq<T, P>::precond_record(long long n) {
+  if constexpr (!std::is_same<P, double>::value) {
+    (void)n;
+    throw error(MPDX_E_UNSUPPORTED, "the learned preconditioner needs the FP64 pressure solve (dtype 8, or prs_fp64)");
+  } else {
+    if (n < 0) throw error(MPDX_E_ARG, "negative pair count");
+    if (pairs) { cudaFree(pairs); pairs = nullptr; }
+    max_pairs = n;
+    n_pairs = 0;
+    if (n == 0) return;
+    const size_t vox = size_t(st.cells());
+    MPDX_CUDA(cudaMalloc(&pairs, size_t(n) * 2 * vox * sizeof(float)));
+    for (auto &f : snap)
+      if (!f.base) st.alloc_sclr(f);
+  }
+}
+
+template <class T, class P>
+double boussinesq<T, P>::precond_train(long long steps, double lr, unsigned long long seed) {
+  if constexpr (!std::is_same<P, double>::value) {
+    (void)steps; (void)lr; (void)seed;
+    throw error(MPDX_E_UNSUPPORTED, "the learned preconditioner needs the FP64 pressure solve (dtype 8, or prs_fp64)");
+  } else {
+    if (n_pairs < 1) throw error(MPDX_E_ARG, "no recorded pressure solves to train on (call precond_record first)");
+    ensure_net();
+    const long long vox = st.cells();
+    if (!tr_r) {
+      for (float **b : {&tr_r, &tr_t, &tr_q, &tr_z, &tr_dq}) MPDX_CUDA(cudaMalloc(b, vox * sizeof(float)));
+      MPDX_CUDA(cudaMalloc(&tr_loss, 4 * sizeof(double)));
+    }
+    const auto gm = make_geom(st, dijk);
+    const unsigned G = red_grid(gm);
+    cudaStream_t s = st.stream;
+    // output scale: A^-1 amplifies the residual by orders of magnitude, so the
+    // network learns q with c * q ~ correction, c = rms(correction) / rms(residual)
+    // over the recorded pairs (GCR itself is indifferent to the scale of q)
+    if (out_scale <= 0) {
+      double rr = 0, dd = 0;
+      for (long long k = 0; k < n_pairs; ++k) {
+        const float *r = pairs + size_t(k) * 2 * vox, *d = r + vox;
+        MPDX_CUDA(cudaMemsetAsync(tr_loss, 0, 2 * sizeof(double), s));
+        bq::k_sumsq<<<296, 256, 0, s>>>(r, vox, tr_loss);
+        bq::k_sumsq<<<296, 256, 0, s>>>(d, vox, tr_loss + 1);
+        double h[2];
+        MPDX_CUDA(cudaMemcpyAsync(h, tr_loss, sizeof(h), cudaMemcpyDeviceToHost, s));
+        MPDX_CUDA(cudaStreamSynchronize(s));
+        rr += h[0]; dd += h[1];
+      }
+      out_scale = rr > 0 ? std::sqrt(dd / rr) : 1.0;
+    }
+    const float c = float(out_scale);
+    // loss: mean((A (c net(r) - t))^2) = mean((c A net(r) + r)^2) for a pair (r, t),
+    // A t = -r, each pair divided by rms(r): the relative squared residual left by c net(r)
+    unsigned long long x = seed * 6364136223846793005ull + 1442695040888963407ull;
+    double tail = 0;
+    long long tail_n = 0;
+    for (long long it = 0; it < steps; ++it) {
+      x = x * 6364136223846793005ull + 1442695040888963407ull;
+      const long long k = (long long)((x >> 33) % (unsigned long long)n_pairs);
+      const float *r = pairs + size_t(k) * 2 * vox, *d = r + vox;
+      MPDX_CUDA(cudaMemsetAsync(tr_loss, 0, 2 * sizeof(double), s));
+      bq::k_sumsq<<<296, 256, 0, s>>>(r, vox, tr_loss);
+      bq::k_scale_rms<<<1184, 256, 0, s>>>(r, d, vox, tr_loss, tr_r, tr_t);
+      net->forward_compact(tr_r, tr_q);
+      bq::k_sub<<<1184, 256, 0, s>>>(tr_q, c, tr_t, vox, tr_z);
+      bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_z, tr_dq, tr_loss + 1, float(2.0 / double(vox)) * c);
+      bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_dq, tr_z, nullptr, 1.f);
+      MPDX_LAUNCH_CHECK();
+      net->backward(tr_r, tr_z, net->grad);
+      net->adam_step(float(lr));
+      if (it >= steps - std::max(1LL, steps / 10)) {
+        double l = 0;
+        MPDX_CUDA(cudaMemcpyAsync(&l, tr_loss + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MPDX_CUDA(cudaStreamSynchronize(s));
+        tail += l;
+        ++tail_n;
+      }
+    }
+    return tail_n ? tail / double(tail_n) : 0.0;
+  }
+}
+
+template <class T, class P>
+void boussinesq<T, P>::precond_enable(bool on) {
+  if (on) ensure_net();
+  use_net = on;
+}
+
 
 template <class T, class P>
 void boussinesq<T, P>::ante_loop() {

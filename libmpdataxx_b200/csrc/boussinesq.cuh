@@ -4,7 +4,10 @@
 
 #include <vector>
 
+#include <memory>
+
 #include "general.cuh"
+#include "precond.cuh"
 
 namespace mpdx {
 
@@ -44,12 +47,32 @@ struct boussinesq {
   int k_iters = 1, vip[3] = {0, 1, 2}, ix_w = 1, ix_tht = 2;
   T dt_stash0 = 0;
   long long iters = 0, iters_total = 0, predicted = 8;
-  double last_residual = 0;
+  double last_residual = 0, last_solve_ms = 0;
+  cudaEvent_t ev_solve[2] = {nullptr, nullptr};
   gcr_dev<P> *dev = nullptr;
   gcr_dev<P> *hdev = nullptr;  // pinned host copy for the convergence read-back
   double *part = nullptr;      // per-block partial results of the running reduction
   double *scratch = nullptr;
   int *vip_dev = nullptr;      // vip[] on the device
+
+  // learned preconditioner (FP64 pressure solve only): the network, whether GCR
+  // uses it, and the recorded (initial residual, correction) pairs of solves
+  std::unique_ptr<pc::net> net;
+  bool use_net = false;
+  static constexpr int kSnaps = 3;  // recorded pairs per solve beyond the initial one (iterations 16, 32, 64)
+  field<P> q_f, lq_f, snap[1 + kSnaps];
+  float *pairs = nullptr, *tr_r = nullptr, *tr_t = nullptr, *tr_q = nullptr, *tr_z = nullptr, *tr_dq = nullptr;
+  double out_scale = 0;
+  double *tr_loss = nullptr;
+  long long last_plain_iters = 250, fallbacks = 0;
+  bool fell_back = false;
+  long long max_pairs = 0, n_pairs = 0;
+  int pc_channels[4] = {8, 16, 32, 64};
+
+  void precond_record(long long max_pairs);
+  double precond_train(long long steps, double lr, unsigned long long seed);
+  void precond_enable(bool on);
+  void ensure_net();
 
   boussinesq(const mpdx_config &c, cudaStream_t s);
   ~boussinesq();

@@ -444,7 +444,8 @@ __global__ void k_endl_reduce(const float *part, int nblk, int ntaps, int cy, in
 // pooling / up-sampling and their adjoints, conversions
 
 // coarse[P][c] = mean over fine p with floor(p/2) = P
-__global__ void k_pool(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y) {
+__global__ void k_pool(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y, const int *skip_flag) {
+  if (skip_flag && *skip_flag) return;
   for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < cg.vox * C; P += (long long)gridDim.x * blockDim.x) {
     const int c = int(P % C);
     const long long V = P / C;
@@ -464,7 +465,8 @@ __global__ void k_pool(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y)
   }
 }
 // fine[p][c] = coarse[floor(p/2)][c]
-__global__ void k_up(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y) {
+__global__ void k_up(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y, const int *skip_flag) {
+  if (skip_flag && *skip_flag) return;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < f.vox * C; q += (long long)gridDim.x * blockDim.x) {
     const int c = int(q % C);
     const long long v = q / C;
@@ -761,7 +763,7 @@ static void forward_impl(net &N, const double *rf, long long s0, long long s1, l
   MPDX_LAUNCH_CHECK();
   // encoder
   for (int l = 1; l < 4; ++l) {
-    k_pool<<<gsz(G[l].vox * N.ch[l - 1]), 256, 0, s>>>(G[l - 1], G[l], N.ch[l - 1], a_e[l - 1], a_p[l]);
+    k_pool<<<gsz(G[l].vox * N.ch[l - 1]), 256, 0, s>>>(G[l - 1], G[l], N.ch[l - 1], a_e[l - 1], a_p[l], skip);
     conv_tc<ND>(N.cin[l], N.cout[l], G[l], a_p[l], wf[l], conv_out{a_e[l], nullptr, P + N.b_off[l], nullptr}, skip, s);
   }
   conv_tc<ND>(N.cin[4], N.cout[4], G[3], a_e[3], wf[4], conv_out{a_m3, nullptr, P + N.b_off[4], nullptr}, skip, s);
@@ -769,7 +771,7 @@ static void forward_impl(net &N, const double *rf, long long s0, long long s1, l
   const uint16_t *coarse = a_m3;
   for (int q = 5; q <= 7; ++q) {
     const int l = N.level[q];
-    k_up<<<gsz(G[l].vox * N.cin[q]), 256, 0, s>>>(G[l], G[l + 1], N.cin[q], coarse, a_u[l]);
+    k_up<<<gsz(G[l].vox * N.cin[q]), 256, 0, s>>>(G[l], G[l + 1], N.cin[q], coarse, a_u[l], skip);
     conv_tc<ND>(N.cin[q], N.cout[q], G[l], a_u[l], wf[q], conv_out{a_d[l], nullptr, P + N.b_off[q], a_e[l]}, skip, s);
     coarse = a_d[l];
   }
@@ -874,16 +876,21 @@ double net::train_step(const float *r, const float *target, float lr) {
   MPDX_CUDA(cudaMemsetAsync(loss_dev, 0, sizeof(double), s));
   k_mse<<<gsz(L[0].vox), 256, 0, s>>>(q32, target, L[0].vox, dq32, loss_dev);
   backward(r, dq32, grad);
+  adam_step(lr);
+  double loss = 0;
+  MPDX_CUDA(cudaMemcpyAsync(&loss, loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MPDX_CUDA(cudaStreamSynchronize(s));
+  return loss;
+}
+
+void net::adam_step(float lr) {
+  cudaStream_t s = stream;
   ++adam_t;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - std::pow(b1, float(adam_t)), c2 = 1.f - std::pow(b2, float(adam_t));
   k_adam<<<gsz(n_params), 256, 0, s>>>(params, grad, adam_m, adam_v, n_params, lr, b1, b2, 1e-8f, c1, c2, wmask);
   MPDX_LAUNCH_CHECK();
   sync_weights();
-  double loss = 0;
-  MPDX_CUDA(cudaMemcpyAsync(&loss, loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
-  MPDX_CUDA(cudaStreamSynchronize(s));
-  return loss;
 }
 
 }  // namespace pc

@@ -51,6 +51,7 @@ class net {
   // one Adam step on the mean squared error between forward_compact(r) and target
   double train_step(const float *r, const float *target, float lr);
   void sync_weights();  // FP32 master -> BF16 fragments
+  void adam_step(float lr);  // one Adam step with the gradient in `grad`
 
   float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   long long adam_t = 0;

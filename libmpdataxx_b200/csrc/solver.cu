@@ -46,6 +46,13 @@ struct solver_base {
   virtual void view_extent(int kind, int idx, int ex[3]) = 0;
   virtual void advance(long long nt) = 0;
   virtual void stats(mpdx_step_stats *out) = 0;
+  // learned GCR preconditioner (Boussinesq solvers only)
+  virtual void precond_record(long long) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
+  virtual double precond_train(long long, double, unsigned long long) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
+  virtual void precond_enable(bool) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
+  virtual long long precond_pairs() { return 0; }
+  virtual long long precond_num_params() { return 0; }
+  virtual void precond_params(float *, const float *) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
 };
 
 // common transfer machinery for solvers built on mpdata_state<T>
@@ -210,6 +217,19 @@ struct boussinesq_solver : solver_base {
     xfer.get(stream, *f, dst, device, ex, off);
   }
   void advance(long long nt) override { b->advance(nt); }
+  void precond_record(long long n) override { b->precond_record(n); }
+  double precond_train(long long steps, double lr, unsigned long long seed) override { return b->precond_train(steps, lr, seed); }
+  void precond_enable(bool on) override { b->precond_enable(on); }
+  long long precond_pairs() override { return b->n_pairs; }
+  long long precond_num_params() override {
+    b->ensure_net();
+    return b->net->n_params;
+  }
+  void precond_params(float *get, const float *set) override {
+    b->ensure_net();
+    if (get) b->net->get_params(get);
+    if (set) b->net->set_params(set);
+  }
   void stats(mpdx_step_stats *out) override {
     std::memset(out, 0, sizeof(*out));
     auto &st = b->st;
@@ -219,6 +239,8 @@ struct boussinesq_solver : solver_base {
     out->gcr_iters = b->iters;
     out->gcr_iters_total = b->iters_total;
     out->gcr_residual = b->last_residual;
+    out->gcr_ms = b->last_solve_ms;
+    out->gcr_fallback = b->fell_back ? 1 : 0;
     out->path = MPDX_PATH_GENERAL;
   }
 };
@@ -652,6 +674,42 @@ mpdx_status mpdx_batch_sync(mpdx_batch_handle b) {
 const char *mpdx_batch_last_error(mpdx_batch_handle b) { return (b && b->impl) ? b->impl->err.c_str() : "invalid batch"; }
 
 void mpdx_batch_destroy(mpdx_batch_handle b) { delete b; }
+
+mpdx_status mpdx_precond_record(mpdx_handle h, int64_t max_pairs) {
+  return guarded(h, [&] { h->impl->precond_record(max_pairs); });
+}
+
+mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t seed, double *final_loss) {
+  return guarded(h, [&] {
+    const double l = h->impl->precond_train(steps, lr, seed);
+    if (final_loss) *final_loss = l;
+  });
+}
+
+mpdx_status mpdx_precond_enable(mpdx_handle h, int on) {
+  return guarded(h, [&] { h->impl->precond_enable(on != 0); });
+}
+
+int64_t mpdx_precond_pairs(mpdx_handle h) { return (h && h->impl) ? h->impl->precond_pairs() : -1; }
+
+int64_t mpdx_precond_num_params(mpdx_handle h) {
+  if (!h || !h->impl) return -1;
+  try { return h->impl->precond_num_params(); } catch (const std::exception &e) { h->impl->err = e.what(); return -1; }
+}
+
+mpdx_status mpdx_precond_get_params(mpdx_handle h, float *host) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null buffer");
+    h->impl->precond_params(host, nullptr);
+  });
+}
+
+mpdx_status mpdx_precond_set_params(mpdx_handle h, const float *host) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null buffer");
+    h->impl->precond_params(nullptr, host);
+  });
+}
 
 void mpdx_destroy(mpdx_handle h) {
   if (!h) return;

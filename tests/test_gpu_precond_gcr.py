@@ -1,0 +1,65 @@
+"""GCR with the learned preconditioner inside the Boussinesq solver.
+
+Pairs recorded from plain solves train the network on the GPU; with it
+enabled the pressure solves stop at the same tolerance in fewer iterations,
+and the flow stays the one plain GCR produces (to the solver tolerance)."""
+import numpy as np
+import pytest
+
+from libmpdataxx_b200 import setups
+from runners import bq_run
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def bubble(n=(48, 48, 24)):
+    return setups.boussinesq_bubble_3d(*n)
+
+
+@pytest.mark.parametrize("dtype,prs_fp64", [(np.float64, False), (np.float32, True)])
+def test_learned_gcr_fewer_iterations_same_flow(dtype, prs_fp64):
+    s = bubble()
+    plain = bq_run(s, dtype=dtype, prs_fp64=prs_fp64)
+    learn = bq_run(s, dtype=dtype, prs_fp64=prs_fp64)
+    learn.precond_record(40)
+    plain.advance(12)
+    learn.advance(12)
+    assert 12 < learn.precond_pairs() <= 40  # initial residuals plus later iterations of each solve
+    loss = learn.precond_train(600, lr=2e-3)
+    print("final training loss", loss)
+    learn.precond_enable(True)
+    it_p, it_l = [], []
+    for _ in range(6):
+        plain.advance(1)
+        learn.advance(1)
+        sp, sl = plain.stats(), learn.stats()
+        it_p.append(sp["gcr_iters"])
+        it_l.append(sl["gcr_iters"])
+        print("fallback", sl["gcr_fallback"], "ms plain %.2f learned %.2f" % (sp["gcr_ms"], sl["gcr_ms"]))
+        tol = s["prs_tol"] / s["dt"]
+        assert sl["gcr_residual"] <= tol * (1 + 1e-6)
+    print("iterations plain", it_p, "learned", it_l)
+    assert sum(it_l) < 0.8 * sum(it_p)
+    for e in range(4):
+        a, b = learn.advectee(e).astype(np.float64), plain.advectee(e).astype(np.float64)
+        scale = np.abs(b).max() if e < 3 else 1.0
+        print("eqn", e, "max diff", np.abs(a - b).max(), "scale", scale)
+        assert np.abs(a - b).max() <= (1e-3 * max(scale, 1e-3) if e < 3 else 1e-4)
+
+
+def test_precond_params_roundtrip_and_requires_fp64():
+    s = bubble((24, 24, 12))
+    run = bq_run(s)
+    p = run.precond_params()
+    p2 = p * 0.5
+    run.set_precond_params(p2)
+    np.testing.assert_array_equal(run.precond_params(), p2)
+    r32 = bq_run(s, dtype=np.float32)  # FP32 pressure solve: no learned preconditioner
+    with pytest.raises(RuntimeError, match="FP64 pressure"):
+        r32.precond_record(2)
+    with pytest.raises(RuntimeError, match="no recorded"):
+        run.precond_train(5)
