@@ -606,10 +606,12 @@ net::net(int nd_, const int *grid, const int *wrap_, const int *ch_, uint64_t se
   }
   n_params = off;
   alloc_all();
-  // initialisation: N(0, 1 / fan-in) weights, zero biases
+  // initialisation: N(0, 1 / fan-in) weights, zero biases, and a zero output
+  // layer, so that an untrained network returns 0 and training starts from
+  // "no correction" (relative residual 1)
   std::vector<float> h(n_params, 0.f);
   std::mt19937_64 rng(seed);
-  for (int q = 0; q < kLayers; ++q) {
+  for (int q = 0; q < kLayers - 1; ++q) {
     std::normal_distribution<double> nd01(0.0, 1.0 / std::sqrt(double(ntaps * cin[q])));
     for (long long x = 0; x < (long long)cout[q] * ntaps * cin[q]; ++x) h[w_off[q] + x] = float(nd01(rng));
   }

@@ -23,9 +23,10 @@ def test_forward_and_gradients_match_oracle(grid, wrap, ch):
     p = net.params()
     P = unpack(p, nd, ch)
     rng = np.random.default_rng(4)
-    for k in P:  # non-zero biases exercise the bias paths
+    for k in P:  # non-zero biases exercise the bias paths; the output layer starts at zero
         if k.startswith("b_"):
             P[k] = rng.normal(size=P[k].shape) * 0.05
+    P["W_q"] = rng.normal(size=P["W_q"].shape) / np.sqrt(P["W_q"].shape[1] * P["W_q"].shape[2])
     net.set_params(pack(P, nd, ch))
     P = unpack(net.params(), nd, ch)
     r = rng.normal(size=grid).astype(np.float32)
