@@ -208,10 +208,9 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
   ring<3> r_s1{slot0(ts - 1, 3)};
   ring<2> r_2{slot0(ts - 1, 2)};
 
-  // Two barriers per step: one before the step reads the planes of the
-  // previous step, one after psi1(t+1) is stored.  The y-face pseudo-velocity
-  // and the y-face flux below the own row, which the FCT sums need, are
-  // recomputed by the thread rather than exchanged.
+  // Barriers per step: one before the step reads the planes of the previous
+  // step, one after psi1(t+1) is stored, and (FCT) one after the y-face
+  // pseudo-velocities are stored, so that each row reads the face below it.
   for (int t = ts; t <= x1; ++t) {
     cp_wait_all();
     __syncthreads();
@@ -289,16 +288,9 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
     // ---- C: betas at plane t (formulae_mpdata_fct_3d.hpp:48-143) ----
     Q bu_c = zero, bd_c = zero;
     if (FCT) {
-      // C~ on the y-face j-1/2 below the own row, recomputed (frame a = y at row r-1)
-      Q cy_dn;
-      {
-        const Q pm_dn = qd::lds(S1m + dn), g2c = qd::lds(G2c + me), g2c_dn = qd::lds(G2c + dn);
-        const Q ny = qnd4<T, IGA>(qd::kp1(p_c), qd::kp1(pc_dn), qd::km1(p_c), qd::km1(pc_dn));
-        const Q nz = qnd4<T, IGA>(p_p, pp_dn, p_m, pm_dn);
-        const Q gc1 = avg4(g2c, g2c_dn, qd::km1(g2c), qd::km1(g2c_dn));
-        const Q gc2 = avg4(qd::lds(G0c + me), qd::lds(G0c + dn), qd::lds(G0m + me), qd::lds(G0m + dn));
-        cy_dn = qadiff(qd::lds(G1c + dn), gc1, gc2, qndx<T, IGA>(p_c, pc_dn), ny, nz);
-      }
+      // C~ on the y-face j-1/2 below the own row: stored by row r-1 in stage B
+      __syncthreads();
+      const Q cy_dn = qd::lds(CYc + dn);
       // psi_min / psi_max of psi^n over the 7-point stencil at plane t (mpdata_fct_3d.hpp:31-55)
       Q mnq, mxq;
       {
