@@ -151,7 +151,35 @@ __device__ __forceinline__ T ndz(unsigned o, const dfield<T> &p, int a, int b, i
   return nd4(o, P<ND, D>(p, a + 1, b, c + 1), P<ND, D>(p, a, b, c + 1), P<ND, D>(p, a + 1, b, c - 1), P<ND, D>(p, a, b, c - 1));
 }
 
-// antidiffusive velocity (formulae_mpdata_{1,2,3}d.hpp antidiff, standard form)
+// third-order terms (formulae_mpdata_hot_{1,2,3}d.hpp, G = 1): four-point second
+// derivatives 2 (pa - pb - pc + pd) / (pa + pb + pc + pd) (ndxx/ndxy/ndxz_psi,
+// formulae_mpdata_psi_{1,2,3}d.hpp), the eight-corner ndyz_psi (psi_3d.hpp:697-790)
+// and their Courant-number coefficients
+template <class T>
+__device__ __forceinline__ T nd2(unsigned o, T pa, T pb, T pc, T pd) {
+  if (o & o_iga) return T(2) * (pa - pb - pc + pd) / T(4);
+  if (o & o_abs) { pa = fabs(pa); pb = fabs(pb); pc = fabs(pc); pd = fabs(pd); }
+  return T(2) * frac(o, pa - pb - pc + pd, pa + pb + pc + pd);
+}
+template <int D, class T>
+__device__ __forceinline__ T ndyz(unsigned o, const dfield<T> &p, int a, int b, int c) {
+  T q[8] = {P<3, D>(p, a + 1, b + 1, c + 1), P<3, D>(p, a + 1, b - 1, c - 1), P<3, D>(p, a + 1, b + 1, c - 1),
+            P<3, D>(p, a + 1, b - 1, c + 1), P<3, D>(p, a, b + 1, c + 1),     P<3, D>(p, a, b - 1, c - 1),
+            P<3, D>(p, a, b + 1, c - 1),     P<3, D>(p, a, b - 1, c + 1)};
+  if (o & o_iga) return (q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7]) / T(8);
+  if (o & o_abs) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) q[t] = fabs(q[t]);
+  }
+  return frac(o, q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7], q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + q[7]);
+}
+template <class T> __device__ __forceinline__ T cxx(T C) { return (T(3) * C * fabs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6); }
+template <class T> __device__ __forceinline__ T cxy(T C, T g) { return (fabs(C) - T(2) * (C * C) / T(1)) * g / T(2); }
+template <class T> __device__ __forceinline__ T cyz(T C, T g1, T g2) { return T(-2) * C * g1 * g2 / T(3) / T(1); }
+
+// antidiffusive velocity (formulae_mpdata_{1,2,3}d.hpp antidiff, standard form).
+// TOT and DFL are added only when their options are set (the reference adds an
+// integer zero otherwise, which changes at most the sign of a zero result).
 template <int ND, int D, class T>
 struct op_antidiff {
   dfield<T> res, psi, G0, G1, G2;  // G0 = GC[D], G1 = GC[D+1], G2 = GC[D+2]
@@ -159,25 +187,43 @@ struct op_antidiff {
   __device__ void operator()(int a, int b, int c) const {
     const T C = P<ND, D>(G0, a, b, c);
     T r = fabs(C) / T(2) * (T(1) - fabs(C) / T(1)) * ndx<ND, D>(o, psi, a, b, c);
+    const T xx = (o & o_tot) ? nd2(o, P<ND, D>(psi, a + 2, b, c), P<ND, D>(psi, a + 1, b, c), P<ND, D>(psi, a, b, c),
+                                   P<ND, D>(psi, a - 1, b, c)) : T(0);
     if (ND == 1) {
-      if (o & o_tot) {  // TOT (formulae_mpdata_hot_1d.hpp:19-52)
-        const T pa = psi(a + 2, 0, 0), pb = psi(a + 1, 0, 0), pc = psi(a, 0, 0), pd = psi(a - 1, 0, 0);
-        T xx;
-        if (o & o_iga) xx = T(2) * (pa - pb - pc + pd) / T(4);
-        else if (o & o_abs) xx = T(2) * frac(o, fabs(pa) - fabs(pb) - fabs(pc) + fabs(pd), fabs(pa) + fabs(pb) + fabs(pc) + fabs(pd));
-        else xx = T(2) * frac(o, pa - pb - pc + pd, pa + pb + pc + pd);
-        const T coeff = (T(3) * C * fabs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6);
-        r = r + xx * coeff;
-      }
+      if (o & o_tot) r = r + xx * cxx(C);  // formulae_mpdata_hot_1d.hpp:19-52
     } else if (ND == 2) {
       // GC1_bar_xy (formulae_mpdata_gc_2d.hpp:76-90)
       const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
       r = r - C * gc1 / T(2) * ndy<ND, D>(o, psi, a, b, c);
+      if (o & o_tot) {  // formulae_mpdata_hot_2d.hpp:52-80
+        const T xy = nd2(o, P<ND, D>(psi, a + 1, b + 1, c), P<ND, D>(psi, a, b + 1, c), P<ND, D>(psi, a + 1, b - 1, c), P<ND, D>(psi, a, b - 1, c));
+        r = r + (xx * cxx(C) + xy * cxy(C, gc1));
+      }
     } else {
       // GC1_bar_xy, GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
       const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
       const T gc2 = (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) + P<ND, D>(G2, a + 1, b, c - 1) + P<ND, D>(G2, a, b, c - 1)) / T(4);
       r = r - C / T(2) * (gc1 * ndy<ND, D>(o, psi, a, b, c) + gc2 * ndz<ND, D>(o, psi, a, b, c)) / T(1);
+      if (o & o_tot) {  // formulae_mpdata_hot_3d.hpp:97-110
+        const T xy = nd2(o, P<ND, D>(psi, a + 1, b + 1, c), P<ND, D>(psi, a, b + 1, c), P<ND, D>(psi, a + 1, b - 1, c), P<ND, D>(psi, a, b - 1, c));
+        const T xz = nd2(o, P<ND, D>(psi, a + 1, b, c + 1), P<ND, D>(psi, a, b, c + 1), P<ND, D>(psi, a + 1, b, c - 1), P<ND, D>(psi, a, b, c - 1));
+        r = r + (xx * cxx(C) + xy * cxy(C, gc1) + xz * cxy(C, gc2) + ndyz<D>(o, psi, a, b, c) * cyz(C, gc1, gc2));
+      }
+    }
+    if (o & o_dfl) {  // divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp)
+      T d;
+      if (ND == 1) {
+        d = T(-0.5) * C / T(2) * (P<ND, D>(G0, a + 1, b, c) - P<ND, D>(G0, a - 1, b, c));
+        if (o & o_iga) d = d * T(0.5) * (P<ND, D>(psi, a + 1, b, c) + P<ND, D>(psi, a, b, c));
+      } else {
+        T s = (P<ND, D>(G0, a + 1, b, c) - P<ND, D>(G0, a - 1, b, c))
+            + (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) - P<ND, D>(G1, a + 1, b - 1, c) - P<ND, D>(G1, a, b - 1, c));
+        if (ND == 3)
+          s = s + (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) - P<ND, D>(G2, a + 1, b, c - 1) - P<ND, D>(G2, a, b, c - 1));
+        d = T(-0.25) * C / T(1) * s;
+        if (o & o_iga) d = d * ((P<ND, D>(psi, a + 1, b, c) + P<ND, D>(psi, a, b, c)) / T(2));
+      }
+      r = r + d;
     }
     P<ND, D>(res, a, b, c) = r;
   }
@@ -701,7 +747,10 @@ void general<T>::advop_nd(int e) {
       xchng_sclr(S.psi[e][S.tl[e]], S.H);
       field<T> *corr = GC_corr(iter);
       antidiff_nd<ND>(corr, S.psi[e][S.tl[e]], GC_unco(iter));
-      if (!(S.opts & o_fct) && iter != S.n_iters - 1) xchng_vctr_nrml(corr, 0);
+      if (!(S.opts & o_fct) && iter != S.n_iters - 1) {
+        xchng_vctr_nrml(corr, 0);
+        if (S.opts & o_dfl) xchng_vctr_alng(corr, false);  // mpdata_osc_1d.hpp:82-88, _2d.hpp:120-124, _3d.hpp:138-142
+      }
       if (S.opts & o_fct) fct_adjust_nd<ND>(e, iter);
     }
     field<T> &p = S.psi[e][S.tl[e]];

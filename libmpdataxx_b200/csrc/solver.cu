@@ -462,11 +462,10 @@ void validate(const mpdx_config &c) {
   if (c.n_eqns < 1) throw error(MPDX_E_ARG, "n_eqns must be positive");
   if (c.n_iters < 1) throw error(MPDX_E_ARG, "n_iters must be positive");
   const unsigned o = unsigned(c.opts);
-  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga;
+  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl;
   if (o & ~built)
-    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot(1D) pfc npa iga)");
+    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl)");
   if ((o & o_iga) && (o & o_abs)) throw error(MPDX_E_ARG, "abs & iga options are mutually exclusive");
-  if ((o & o_tot) && c.n_dims > 1) throw error(MPDX_E_UNSUPPORTED, "tot option is built for 1D only on this backend");
   for (int q = 0; q < 2 * c.n_dims; ++q) {
     const int k = c.bcs[q];
     if (k != MPDX_BC_CYCLIC && k != MPDX_BC_OPEN && k != MPDX_BC_RIGID) throw error(MPDX_E_ARG, "unknown boundary kind");

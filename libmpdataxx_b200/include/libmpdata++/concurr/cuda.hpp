@@ -62,9 +62,9 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   static_assert(bcxl != bcond::null && bcxr != bcond::null, "x boundary conditions are required");
   static_assert(n_dims < 2 || (bcyl != bcond::null && bcyr != bcond::null), "y boundary conditions are required");
   static_assert(n_dims < 3 || (bczl != bcond::null && bczr != bcond::null), "z boundary conditions are required");
-  static_assert(!opts::isset(ct_params_t::opts, opts::nug | opts::dfl | opts::khn | opts::div_2nd | opts::div_3rd |
+  static_assert(!opts::isset(ct_params_t::opts, opts::nug | opts::khn | opts::div_2nd | opts::div_3rd |
                                                     opts::div_3rd_dt | opts::fot),
-                "MPDATA option not built on this backend (built: fct abs tot(1D) pfc npa iga)");
+                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl)");
 
   explicit cuda(const rt_params_t &p) : p_(p) {
     mpdx_config c;

@@ -62,7 +62,8 @@ def rotating_cone(nx=101, ny=101):
             "dt": dt}
 
 
-CONE_CASES = {"basic": (0, 2), "fct": (o.fct, 2), "iga_fct": (o.iga | o.fct, 2)}
+CONE_CASES = {"basic": (0, 2), "fct": (o.fct, 2), "iga_fct": (o.iga | o.fct, 2),
+              "iga_tot_fct": (o.iga | o.tot | o.fct, 2), "iters3_tot_fct": (o.tot | o.fct, 3)}
 
 
 def cone_stats(psi_init, psi_final, nt, dt):

@@ -462,27 +462,69 @@ struct mpdata {
     if (opts & o_abs) { pa = std::abs(pa); pb = std::abs(pb); pc = std::abs(pc); pd = std::abs(pd); }
     return frac(opts, pa + pb - pc - pd, pa + pb + pc + pd);
   }
-  // 1D ndxx_psi (formulae_mpdata_psi_1d.hpp:110-161) and TOT (formulae_mpdata_hot_1d.hpp:19-52)
-  T ndxx1(const arr<T> &p, int i) const {
-    T a = p(i + 2, 0, 0), b = p(i + 1, 0, 0), c = p(i, 0, 0), d = p(i - 1, 0, 0);
-    if (opts & o_iga) return T(2) * (a - b - c + d) / T(4);
-    if (opts & o_abs) { a = std::abs(a); b = std::abs(b); c = std::abs(c); d = std::abs(d); }
-    return T(2) * frac(opts, a - b - c + d, a + b + c + d);
+  // ---- third-order terms (formulae_mpdata_hot_{1,2,3}d.hpp), G = 1 ----
+  // four-point second derivatives at (a+1/2): 2 (pa - pb - pc + pd) / (pa + pb + pc + pd)
+  // (ndxx_psi: psi_1d.hpp:110-161, psi_2d.hpp:246-300, psi_3d.hpp:469-541;
+  //  ndxy_psi / ndxz_psi: psi_2d.hpp:305-359, psi_3d.hpp:545-695)
+  T nd2(T pa, T pb, T pc, T pd) const {
+    if (opts & o_iga) return T(2) * (pa - pb - pc + pd) / T(4);
+    if (opts & o_abs) { pa = std::abs(pa); pb = std::abs(pb); pc = std::abs(pc); pd = std::abs(pd); }
+    return T(2) * frac(opts, pa - pb - pc + pd, pa + pb + pc + pd);
   }
-  T tot1(const arr<T> &p, const arr<T> &G0, int i) const {
-    if (!(opts & o_tot)) return T(0);
-    const T C = G0(i, 0, 0);
-    const T coeff = (T(3) * C * std::abs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6);
-    return ndxx1(p, i) * coeff;
+  template <int ND, int D> T ndxx(const arr<T> &p, int a, int b, int c) const {
+    return nd2(P<ND, D>(p, a + 2, b, c), P<ND, D>(p, a + 1, b, c), P<ND, D>(p, a, b, c), P<ND, D>(p, a - 1, b, c));
+  }
+  template <int ND, int D> T ndxy(const arr<T> &p, int a, int b, int c) const {
+    return nd2(P<ND, D>(p, a + 1, b + 1, c), P<ND, D>(p, a, b + 1, c), P<ND, D>(p, a + 1, b - 1, c), P<ND, D>(p, a, b - 1, c));
+  }
+  template <int D> T ndxz(const arr<T> &p, int a, int b, int c) const {
+    return nd2(P<3, D>(p, a + 1, b, c + 1), P<3, D>(p, a, b, c + 1), P<3, D>(p, a + 1, b, c - 1), P<3, D>(p, a, b, c - 1));
+  }
+  // ndyz_psi (psi_3d.hpp:697-790): eight corners, no factor 2
+  template <int D> T ndyz(const arr<T> &p, int a, int b, int c) const {
+    T q[8] = {P<3, D>(p, a + 1, b + 1, c + 1), P<3, D>(p, a + 1, b - 1, c - 1), P<3, D>(p, a + 1, b + 1, c - 1),
+              P<3, D>(p, a + 1, b - 1, c + 1), P<3, D>(p, a, b + 1, c + 1),     P<3, D>(p, a, b - 1, c - 1),
+              P<3, D>(p, a, b + 1, c - 1),     P<3, D>(p, a, b - 1, c + 1)};
+    const T num = q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7];
+    if (opts & o_iga) return num / T(8);
+    if (opts & o_abs) for (T &v : q) v = std::abs(v);
+    return frac(opts, q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7],
+                q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + q[7]);
+  }
+  // coefficients (hot_1d.hpp:19-40, hot_2d.hpp:21-50, hot_3d.hpp:21-95)
+  static T cxx(T C) { return (T(3) * C * std::abs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6); }
+  static T cxy(T C, T g) { return (std::abs(C) - T(2) * (C * C) / T(1)) * g / T(2); }
+  static T cyz(T C, T g1, T g2) { return T(-2) * C * g1 * g2 / T(3) / T(1); }
+
+  // ---- divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp), G = 1 ----
+  // -C/4 (div of the advector around the face) [x psi_bar_x with iga]; 1D: -C/2/(1+1) dC
+  template <int ND, int D> T dfl(const arr<T> &p, const arr<T> &Gd, const arr<T> &G1, const arr<T> &G2, int a, int b, int c) const {
+    const T C = P<ND, D>(Gd, a, b, c);
+    T r;
+    if (ND == 1) {
+      r = T(-0.5) * C / T(2) * (P<ND, D>(Gd, a + 1, b, c) - P<ND, D>(Gd, a - 1, b, c));
+      if (opts & o_iga) r = r * T(0.5) * (P<ND, D>(p, a + 1, b, c) + P<ND, D>(p, a, b, c));
+      return r;
+    }
+    T s = (P<ND, D>(Gd, a + 1, b, c) - P<ND, D>(Gd, a - 1, b, c))
+        + (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) - P<ND, D>(G1, a + 1, b - 1, c) - P<ND, D>(G1, a, b - 1, c));
+    if (ND == 3)
+      s = s + (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) - P<ND, D>(G2, a + 1, b, c - 1) - P<ND, D>(G2, a, b, c - 1));
+    r = T(-0.25) * C / T(1) * s;
+    if (opts & o_iga) r = r * ((P<ND, D>(p, a + 1, b, c) + P<ND, D>(p, a, b, c)) / T(2));
+    return r;
   }
 
   // ---- antidiffusive velocity ----
+  // The reference adds TOT and DFL as integer zeros when the options are off;
+  // they are left out here (x + 0 differs from x only in the sign of a zero).
   // 1D: formulae_mpdata_1d.hpp:186-210
   void antidiff1(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
     for (int i = im[0].f; i <= im[0].l; ++i) {
       const T C = G[0](i, 0, 0);
       T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<1, 0>(p, i, 0, 0);
-      r = r + tot1(p, G[0], i);
+      if (opts & o_tot) r = r + ndxx<1, 0>(p, i, 0, 0) * cxx(C);
+      if (opts & o_dfl) r = r + dfl<1, 0>(p, G[0], G[0], G[0], i, 0, 0);
       res(i, 0, 0) = r;
     }
   }
@@ -494,9 +536,11 @@ struct mpdata {
       for (int b = rb.f; b <= rb.l; ++b) {
         const T C = P<2, D>(Gd, a, b);
         const T gc1 = (P<2, D>(Gt, a + 1, b) + P<2, D>(Gt, a, b) + P<2, D>(Gt, a + 1, b - 1) + P<2, D>(Gt, a, b - 1)) / T(4);
-        P<2, D>(res, a, b) =
-            std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<2, D>(p, a, b, 0)
+        T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<2, D>(p, a, b, 0)
             - C * gc1 / T(2) * ndy<2, D>(p, a, b, 0);
+        if (opts & o_tot) r = r + (ndxx<2, D>(p, a, b, 0) * cxx(C) + ndxy<2, D>(p, a, b, 0) * cxy(C, gc1));
+        if (opts & o_dfl) r = r + dfl<2, D>(p, Gd, Gt, Gt, a, b, 0);
+        P<2, D>(res, a, b) = r;
       }
   }
   // 3D: formulae_mpdata_3d.hpp:254-295 with GC1_bar_xy / GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
@@ -507,9 +551,13 @@ struct mpdata {
           const T C = P<3, D>(Gd, a, b, c);
           const T gc1 = (P<3, D>(G1, a + 1, b, c) + P<3, D>(G1, a, b, c) + P<3, D>(G1, a + 1, b - 1, c) + P<3, D>(G1, a, b - 1, c)) / T(4);
           const T gc2 = (P<3, D>(G2, a + 1, b, c) + P<3, D>(G2, a, b, c) + P<3, D>(G2, a + 1, b, c - 1) + P<3, D>(G2, a, b, c - 1)) / T(4);
-          P<3, D>(res, a, b, c) =
-              std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<3, D>(p, a, b, c)
+          T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<3, D>(p, a, b, c)
               - C / T(2) * (gc1 * ndy<3, D>(p, a, b, c) + gc2 * ndz<3, D>(p, a, b, c)) / T(1);
+          if (opts & o_tot)
+            r = r + (ndxx<3, D>(p, a, b, c) * cxx(C) + ndxy<3, D>(p, a, b, c) * cxy(C, gc1)
+                     + ndxz<D>(p, a, b, c) * cxy(C, gc2) + ndyz<D>(p, a, b, c) * cyz(C, gc1, gc2));
+          if (opts & o_dfl) r = r + dfl<3, D>(p, Gd, G1, G2, a, b, c);
+          P<3, D>(res, a, b, c) = r;
         });
   }
 
@@ -658,7 +706,10 @@ struct mpdata {
         if (nd == 1) antidiff1(corr[0], p, unco);
         else if (nd == 2) { antidiff2<0>(corr[0], p, unco); antidiff2<1>(corr[1], p, unco); }
         else { antidiff3<0>(corr[0], p, unco); antidiff3<1>(corr[1], p, unco); antidiff3<2>(corr[2], p, unco); }
-        if (!(opts & o_fct) && iter != n_iters - 1) xchng_vctr_nrml(corr);
+        if (!(opts & o_fct) && iter != n_iters - 1) {
+          xchng_vctr_nrml(corr);
+          if (opts & o_dfl) xchng_vctr_alng(corr);  // mpdata_osc_1d.hpp:82-88, _2d.hpp:120-124, _3d.hpp:138-142
+        }
         if (opts & o_fct) fct_adjust_antidiff(e, iter);
       }
       const arr<T> &p = psi[e][tl[e]];

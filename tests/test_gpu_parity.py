@@ -62,6 +62,29 @@ for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
 CASES.append((1, (37,), "cyclic", o.iga | o.tot, 2))
 CASES.append((1, (37,), "open", o.iga | o.tot | o.fct, 2))
 CASES.append((1, (37,), "cyclic", o.tot, 3))
+# third-order terms in 2D and 3D (formulae_mpdata_hot_{2,3}d.hpp)
+for nd, grid in [(2, (19, 23)), (3, (13, 13, 13))]:
+    for bc in ("cyclic", "open", "rigid"):
+        for opts, iters in [(o.iga | o.tot, 2), (o.tot, 2), (o.abs | o.tot, 2), (o.iga | o.tot | o.fct, 2),
+                            (o.tot | o.fct, 3)]:
+            CASES.append((nd, grid, bc, opts, iters))
+
+# divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp) on a divergent advector
+DFL_CASES = []
+for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
+    for bc in ("cyclic", "open", "rigid"):
+        for opts, iters in [(o.dfl, 2), (o.iga | o.dfl, 2), (o.dfl | o.fct, 2), (o.iga | o.dfl | o.fct, 2),
+                            (o.dfl, 3), (o.iga | o.tot | o.dfl | o.fct, 3)]:
+            DFL_CASES.append((nd, grid, bc, opts, iters))
+
+
+@pytest.mark.parametrize("nd,grid,bc,opts,iters", DFL_CASES)
+def test_dfl_fp64_matches_oracle(nd, grid, bc, opts, iters):
+    bcs = [bc] * (2 * nd)
+    s = random_setup(grid, bcs, seed=nd * 100 + iters + 7, signed=bool(opts & o.iga))
+    rng = np.random.default_rng(nd * 10 + iters)
+    s["advector"] = [a + 0.05 * rng.uniform(-1.0, 1.0, np.shape(a)) for a in s["advector"]]
+    _check_parity(s, grid, bcs, opts, iters, eps=None)
 
 
 @pytest.mark.parametrize("nd,grid,bc,opts,iters", CASES)
@@ -71,7 +94,10 @@ def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
     # rigid walls mirror the normal Courant number with a sign flip, so a field that
     # is not zero on the wall faces fails the reference's divergence guard; the
     # guard is lifted for those cases (the numerics under test do not depend on it)
-    eps = 1e30 if bc == "rigid" else 1e-10
+    _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10)
+
+
+def _check_parity(s, grid, bcs, opts, iters, eps):
     orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)
     load(orc, s)
     run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)

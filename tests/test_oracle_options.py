@@ -1,0 +1,75 @@
+"""The oracle's third-order terms (tot) and divergent-flow correction (dfl)
+across dimensions.
+
+No golden data of the reference pins dfl, nor tot in 3D (the rotating-cone
+goldens pin tot in 2D, test_oracle_golden.py).  These restatements are checked
+for consistency instead: a problem that is uniform along y (and z), with zero
+transverse Courant numbers, must evolve exactly as the 1D problem does -- the
+2D/3D formulae (formulae_mpdata_{hot,dfl}_{2,3}d.hpp) reduce to the 1D ones
+(formulae_mpdata_{hot,dfl}_1d.hpp) when every transverse difference vanishes,
+and they do so bit for bit because the extra terms are exact zeros and the
+constant factors (-0.5/2 against -0.25/1, 0.5 (a + b) against (a + b)/2) round
+identically.  The transverse boundaries are cyclic: an open boundary fills its
+halo faces by the zero-divergence condition (open_2d.hpp fill_halos_vctr_alng),
+which makes the transverse Courant numbers of a divergent flow non-zero there.
+Along x an open boundary fills 1D and 2D halos differently as well (open_1d.hpp
+copies the boundary face, open_2d.hpp the first inner face), so with open x
+boundaries only rows out of the boundaries' reach are compared."""
+import numpy as np
+import pytest
+
+from libmpdataxx_b200 import opts as o
+from oracle import Oracle
+
+NX = 29
+CASES = [(o.dfl, 2), (o.iga | o.dfl, 2), (o.dfl | o.fct, 2), (o.iga | o.dfl | o.fct, 2), (o.dfl, 3),
+         (o.tot, 2), (o.iga | o.tot, 2), (o.abs | o.tot, 2), (o.tot | o.fct, 3), (o.iga | o.tot | o.dfl | o.fct, 2)]
+
+
+def _problem(seed, signed):
+    rng = np.random.default_rng(seed)
+    psi = rng.uniform(0.5, 2.0, NX)
+    if signed:
+        psi *= np.where(rng.uniform(size=NX) < 0.3, -1.0, 1.0)
+    x = np.arange(NX) / (NX - 1)
+    gc = 0.25 + 0.1 * np.sin(2 * np.pi * x) + 0.05 * rng.uniform(-1, 1, NX)  # divergent
+    return psi, gc
+
+
+def _run(grid, bc, opts, iters, psi1, gc1, nt):
+    nd = len(grid)
+    orc = Oracle(grid, opts, n_iters=iters, bcs=[bc] * 2 + ["cyclic"] * (2 * nd - 2), max_abs_div_eps=1e30)
+    orc.set_advectee(np.broadcast_to(psi1.reshape((NX,) + (1,) * (nd - 1)), grid))
+    orc.set_advector(np.broadcast_to(gc1.reshape((NX,) + (1,) * (nd - 1)), grid), 0)
+    for d in range(1, nd):
+        orc.set_advector(np.zeros(orc.advector_shape(d)), d)
+    orc.advance(nt)
+    out = orc.advectee()
+    return out.reshape(NX, -1) if nd > 1 else out.reshape(NX, 1)
+
+
+@pytest.mark.parametrize("bc", ["open", "cyclic"])
+@pytest.mark.parametrize("opts,iters", CASES)
+def test_uniform_transverse_reduces_to_1d(opts, iters, bc):
+    psi, gc = _problem(seed=iters * 31 + opts % 97, signed=bool(opts & (o.abs | o.iga)))
+    nt, rows = (6, slice(None)) if bc == "cyclic" else (2, slice(12, NX - 12))
+    ref = _run((NX,), bc, opts, iters, psi, gc, nt=nt)
+    for grid in [(NX, 5), (NX, 4, 5)]:
+        got = _run(grid, bc, opts, iters, psi, gc, nt=nt)
+        for col in range(got.shape[1]):
+            np.testing.assert_array_equal(got[rows, col], ref[rows, 0])
+
+
+def test_dfl_changes_the_result():
+    """The correction is active: a divergent flow gives a different answer with dfl."""
+    psi, gc = _problem(seed=5, signed=False)
+    a = _run((NX, 5), "open", o.iga, 2, psi, gc, nt=6)
+    b = _run((NX, 5), "open", o.iga | o.dfl, 2, psi, gc, nt=6)
+    assert np.abs(a - b).max() > 1e-6
+
+
+def test_tot_changes_the_result():
+    psi, gc = _problem(seed=6, signed=False)
+    a = _run((NX, 4, 5), "cyclic", o.fct, 2, psi, gc, nt=6)
+    b = _run((NX, 4, 5), "cyclic", o.tot | o.fct, 2, psi, gc, nt=6)
+    assert np.abs(a - b).max() > 1e-6
