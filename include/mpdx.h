@@ -57,7 +57,8 @@ enum {
   MPDX_FIELD_ADVECTEE = 0,   /* idx = equation; interior n0 x n1 x n2 */
   MPDX_FIELD_ADVECTOR = 1,   /* idx = dimension; reference view extents (below) */
   MPDX_FIELD_SCLR_ARRAY = 2, /* idx = MPDX_SCLR_* named scalar array */
-  MPDX_FIELD_PRESSURE = 3    /* Boussinesq: Phi, interior */
+  MPDX_FIELD_PRESSURE = 3,   /* Boussinesq: Phi, interior */
+  MPDX_FIELD_G = 4           /* g_factor() with the nug option: G, interior (sharedmem.hpp:373-380) */
 };
 enum { MPDX_SCLR_THT_E = 0 };
 
@@ -84,6 +85,7 @@ typedef struct {
   int ix_u, ix_v, ix_w, ix_tht;  /* equation indices (ct_params_t::ix); ix_v = -1 in 2D */
   int precond;             /* MPDX_PRECOND_* */
   int prs_fp64;            /* 1: pressure fields in FP64 even when real_t is float */
+  int upwind_filter_freq;  /* rt_params upwind_filter_freq (mpdata_common.hpp:77): every n-th step is upwind only; 0 = never */
 } mpdx_config;
 
 typedef struct mpdx_solver *mpdx_handle;

@@ -17,7 +17,7 @@ SOLVER_MPDATA, SOLVER_BOUSSINESQ = 0, 1
 PRS_CR, PRS_GCRK = 0, 1
 PRECOND_IDENTITY, PRECOND_LEARNED = 0, 1
 PATH_AUTO, PATH_GENERAL, PATH_FUSED = 0, 1, 2
-FIELD_ADVECTEE, FIELD_ADVECTOR, FIELD_SCLR_ARRAY, FIELD_PRESSURE = 0, 1, 2, 3
+FIELD_ADVECTEE, FIELD_ADVECTOR, FIELD_SCLR_ARRAY, FIELD_PRESSURE, FIELD_G = 0, 1, 2, 3, 4
 SCLR_THT_E = 0
 
 # every entry point declared in include/mpdx.h
@@ -42,7 +42,7 @@ class Config(ctypes.Structure):
                 ("prs_k_iters", ctypes.c_int), ("prs_tol", ctypes.c_double), ("g", ctypes.c_double),
                 ("tht_ref", ctypes.c_double), ("ix_u", ctypes.c_int), ("ix_v", ctypes.c_int),
                 ("ix_w", ctypes.c_int), ("ix_tht", ctypes.c_int), ("precond", ctypes.c_int),
-                ("prs_fp64", ctypes.c_int)]
+                ("prs_fp64", ctypes.c_int), ("upwind_filter_freq", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):

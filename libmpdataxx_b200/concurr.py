@@ -61,6 +61,7 @@ class cuda:
         cfg.dk = float(getattr(p, "dk", 1.0) or 1.0)
         eps = getattr(p, "max_abs_div_eps", None)
         cfg.max_abs_div_eps = -1.0 if eps is None else float(eps)
+        cfg.upwind_filter_freq = int(getattr(p, "upwind_filter_freq", 0) or 0)
         cfg.path = {"auto": _lib.PATH_AUTO, "general": _lib.PATH_GENERAL, "fused": _lib.PATH_FUSED}[path]
         if isinstance(solver, _bq):
             solver.fill_config(cfg, p)
@@ -111,6 +112,13 @@ class cuda:
             raise KeyError(name)
         return self._mirror(_lib.FIELD_SCLR_ARRAY, _lib.SCLR_THT_E)
 
+    def g_factor(self):
+        """G of the nug option (sharedmem.hpp:373-380): a writable mirror, uploaded before the next advance."""
+        return self._mirror(_lib.FIELD_G, 0)
+
+    def set_g_factor(self, a):
+        self.set_field(_lib.FIELD_G, 0, a)
+
     def advectee_global(self, e=0):
         return self.advectee(e)
 
@@ -118,8 +126,8 @@ class cuda:
         for (kind, idx), a in self._mirrors.items():
             if (kind, idx) in self._fresh:
                 _check(self.L, self.h, self.L.mpdx_set_field(self.h, kind, idx, np.ascontiguousarray(a).ctypes.data, None))
-        # state fields change on the device; advectors and scalar arrays do not
-        self._fresh = {k for k in self._fresh if k[0] in (_lib.FIELD_ADVECTOR, _lib.FIELD_SCLR_ARRAY)}
+        # state fields change on the device; advectors, scalar arrays and G do not
+        self._fresh = {k for k in self._fresh if k[0] in (_lib.FIELD_ADVECTOR, _lib.FIELD_SCLR_ARRAY, _lib.FIELD_G)}
 
     # -- explicit transfers ---------------------------------------------------
     def set_field(self, kind, idx, a):

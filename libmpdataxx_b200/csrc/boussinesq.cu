@@ -812,6 +812,7 @@ boussinesq<T, P>::boussinesq(const mpdx_config &c, cudaStream_t s) {
   for (int d = 0; d < st.nd; ++d)
     if (st.n[d] < 2 * st.H + 1) throw error(MPDX_E_GRID, "libmpdata++: bogus grid size");
   st.max_abs_div_eps = c.max_abs_div_eps < 0 ? std::numeric_limits<T>::epsilon() : T(c.max_abs_div_eps);
+  st.upwind_filter_freq = c.upwind_filter_freq;
   dt = c.dt;
   dtT = T(c.dt);
   // grid spacings as real_t values (what the reference's rt_params hold), kept in double

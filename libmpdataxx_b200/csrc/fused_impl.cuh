@@ -28,6 +28,7 @@ bool fused_configurable(const mpdata_state<T> &st) {
   for (int d = 0; d < st.nd; ++d)
     if (st.bcs[d][0] != MPDX_BC_CYCLIC || st.bcs[d][1] != MPDX_BC_CYCLIC) return false;
   if (st.opts & ~(o_fct | o_iga)) return false;
+  if (st.upwind_filter_freq > 0) return false;
   if (st.nd == 3) return st.n_iters == 2 && st.n[0] - 1 >= 2 && st.n[1] - 1 >= 2 && st.n[2] - 1 >= 2;
   if (st.nd == 2) {
     const bool ok_iters = st.n_iters == 2 || (st.n_iters == 3 && !(st.opts & o_iga));

@@ -151,7 +151,7 @@ __device__ __forceinline__ T ndz(unsigned o, const dfield<T> &p, int a, int b, i
   return nd4(o, P<ND, D>(p, a + 1, b, c + 1), P<ND, D>(p, a, b, c + 1), P<ND, D>(p, a + 1, b, c - 1), P<ND, D>(p, a, b, c - 1));
 }
 
-// third-order terms (formulae_mpdata_hot_{1,2,3}d.hpp, G = 1): four-point second
+// third-order terms (formulae_mpdata_hot_{1,2,3}d.hpp): four-point second
 // derivatives 2 (pa - pb - pc + pd) / (pa + pb + pc + pd) (ndxx/ndxy/ndxz_psi,
 // formulae_mpdata_psi_{1,2,3}d.hpp), the eight-corner ndyz_psi (psi_3d.hpp:697-790)
 // and their Courant-number coefficients
@@ -173,54 +173,59 @@ __device__ __forceinline__ T ndyz(unsigned o, const dfield<T> &p, int a, int b, 
   }
   return frac(o, q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7], q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + q[7]);
 }
-template <class T> __device__ __forceinline__ T cxx(T C) { return (T(3) * C * fabs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6); }
-template <class T> __device__ __forceinline__ T cxy(T C, T g) { return (fabs(C) - T(2) * (C * C) / T(1)) * g / T(2); }
-template <class T> __device__ __forceinline__ T cyz(T C, T g1, T g2) { return T(-2) * C * g1 * g2 / T(3) / T(1); }
+// (gb = G_bar_x; pow2/pow3 as products)
+template <class T> __device__ __forceinline__ T cxx(T C, T gb) { return (T(3) * C * fabs(C) / gb - T(2) * (C * C * C) / (gb * gb) - C) / T(6); }
+template <class T> __device__ __forceinline__ T cxy(T C, T g, T gb) { return (fabs(C) - T(2) * (C * C) / gb) * g / (T(2) * gb); }
+template <class T> __device__ __forceinline__ T cyz(T C, T g1, T g2, T gb) { return T(-2) * C * g1 * g2 / T(3) / (gb * gb); }
 
 // antidiffusive velocity (formulae_mpdata_{1,2,3}d.hpp antidiff, standard form).
 // TOT and DFL are added only when their options are set (the reference adds an
 // integer zero otherwise, which changes at most the sign of a zero result).
+// With nug, G_bar_x = (G(a+1) + G(a)) / 2 (formulae_mpdata_g_{1,2,3}d.hpp); 1 otherwise.
 template <int ND, int D, class T>
 struct op_antidiff {
   dfield<T> res, psi, G0, G1, G2;  // G0 = GC[D], G1 = GC[D+1], G2 = GC[D+2]
   unsigned o;
+  dfield<T> Gf;  // G factor (nug only)
   __device__ void operator()(int a, int b, int c) const {
     const T C = P<ND, D>(G0, a, b, c);
-    T r = fabs(C) / T(2) * (T(1) - fabs(C) / T(1)) * ndx<ND, D>(o, psi, a, b, c);
+    const T gb = (o & o_nug) ? (P<ND, D>(Gf, a + 1, b, c) + P<ND, D>(Gf, a, b, c)) / T(2) : T(1);
+    T r = fabs(C) / T(2) * (T(1) - fabs(C) / gb) * ndx<ND, D>(o, psi, a, b, c);
     const T xx = (o & o_tot) ? nd2(o, P<ND, D>(psi, a + 2, b, c), P<ND, D>(psi, a + 1, b, c), P<ND, D>(psi, a, b, c),
                                    P<ND, D>(psi, a - 1, b, c)) : T(0);
     if (ND == 1) {
-      if (o & o_tot) r = r + xx * cxx(C);  // formulae_mpdata_hot_1d.hpp:19-52
+      if (o & o_tot) r = r + xx * cxx(C, gb);  // formulae_mpdata_hot_1d.hpp:19-52
     } else if (ND == 2) {
       // GC1_bar_xy (formulae_mpdata_gc_2d.hpp:76-90)
       const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
-      r = r - C * gc1 / T(2) * ndy<ND, D>(o, psi, a, b, c);
+      r = r - C * gc1 / (T(2) * gb) * ndy<ND, D>(o, psi, a, b, c);
       if (o & o_tot) {  // formulae_mpdata_hot_2d.hpp:52-80
         const T xy = nd2(o, P<ND, D>(psi, a + 1, b + 1, c), P<ND, D>(psi, a, b + 1, c), P<ND, D>(psi, a + 1, b - 1, c), P<ND, D>(psi, a, b - 1, c));
-        r = r + (xx * cxx(C) + xy * cxy(C, gc1));
+        r = r + (xx * cxx(C, gb) + xy * cxy(C, gc1, gb));
       }
     } else {
       // GC1_bar_xy, GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
       const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
       const T gc2 = (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) + P<ND, D>(G2, a + 1, b, c - 1) + P<ND, D>(G2, a, b, c - 1)) / T(4);
-      r = r - C / T(2) * (gc1 * ndy<ND, D>(o, psi, a, b, c) + gc2 * ndz<ND, D>(o, psi, a, b, c)) / T(1);
+      r = r - C / T(2) * (gc1 * ndy<ND, D>(o, psi, a, b, c) + gc2 * ndz<ND, D>(o, psi, a, b, c)) / gb;
       if (o & o_tot) {  // formulae_mpdata_hot_3d.hpp:97-110
         const T xy = nd2(o, P<ND, D>(psi, a + 1, b + 1, c), P<ND, D>(psi, a, b + 1, c), P<ND, D>(psi, a + 1, b - 1, c), P<ND, D>(psi, a, b - 1, c));
         const T xz = nd2(o, P<ND, D>(psi, a + 1, b, c + 1), P<ND, D>(psi, a, b, c + 1), P<ND, D>(psi, a + 1, b, c - 1), P<ND, D>(psi, a, b, c - 1));
-        r = r + (xx * cxx(C) + xy * cxy(C, gc1) + xz * cxy(C, gc2) + ndyz<D>(o, psi, a, b, c) * cyz(C, gc1, gc2));
+        r = r + (xx * cxx(C, gb) + xy * cxy(C, gc1, gb) + xz * cxy(C, gc2, gb) + ndyz<D>(o, psi, a, b, c) * cyz(C, gc1, gc2, gb));
       }
     }
     if (o & o_dfl) {  // divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp)
       T d;
       if (ND == 1) {
-        d = T(-0.5) * C / T(2) * (P<ND, D>(G0, a + 1, b, c) - P<ND, D>(G0, a - 1, b, c));
+        const T g2 = (o & o_nug) ? P<ND, D>(Gf, a + 1, b, c) + P<ND, D>(Gf, a, b, c) : T(2);
+        d = T(-0.5) * C / g2 * (P<ND, D>(G0, a + 1, b, c) - P<ND, D>(G0, a - 1, b, c));
         if (o & o_iga) d = d * T(0.5) * (P<ND, D>(psi, a + 1, b, c) + P<ND, D>(psi, a, b, c));
       } else {
         T s = (P<ND, D>(G0, a + 1, b, c) - P<ND, D>(G0, a - 1, b, c))
             + (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) - P<ND, D>(G1, a + 1, b - 1, c) - P<ND, D>(G1, a, b - 1, c));
         if (ND == 3)
           s = s + (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) - P<ND, D>(G2, a + 1, b, c - 1) - P<ND, D>(G2, a, b, c - 1));
-        d = T(-0.25) * C / T(1) * s;
+        d = T(-0.25) * C / gb * s;
         if (o & o_iga) d = d * ((P<ND, D>(psi, a + 1, b, c) + P<ND, D>(psi, a, b, c)) / T(2));
       }
       r = r + d;
@@ -240,16 +245,30 @@ struct op_flux {
   }
 };
 
-// donorcell_sum with G = 1 (donorcell_formulae.hpp:81-165)
+// donorcell_sum (donorcell_formulae.hpp:81-165): divided by G (1 without nug);
+// with khn a Kahan-compensated sum (kahan_sum.hpp:14-27) of psi_old, then
+// -F(+1/2)/G and F(-1/2)/G per dimension
 template <int ND, class T>
 struct op_donorcell {
   dfield<T> pn, po, f0, f1, f2;
+  unsigned o;
+  dfield<T> Gf;
   __device__ void operator()(int i, int j, int k) const {
-    if (ND == 1) pn(i, j, k) = po(i, j, k) + (-f0(i, j, k) + f0(i - 1, j, k)) / T(1);
+    const T g = (o & o_nug) ? Gf(i, j, k) : T(1);
+    if (o & o_khn) {
+      T sum = T(0), c = T(0);
+      auto add = [&](T in) { const T y = in - c; const T t = sum + y; c = (t - sum) - y; sum = t; };
+      add(po(i, j, k));
+      add(-f0(i, j, k) / g);
+      add(f0(i - 1, j, k) / g);
+      if (ND > 1) { add(-f1(i, j, k) / g); add(f1(i, j - 1, k) / g); }
+      if (ND > 2) { add(-f2(i, j, k) / g); add(f2(i, j, k - 1) / g); }
+      pn(i, j, k) = sum;
+    } else if (ND == 1) pn(i, j, k) = po(i, j, k) + (-f0(i, j, k) + f0(i - 1, j, k)) / g;
     else if (ND == 2)
-      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k))) / T(1);
+      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k))) / g;
     else
-      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k)) + (-f2(i, j, k) + f2(i, j, k - 1))) / T(1);
+      pn(i, j, k) = po(i, j, k) + ((-f0(i, j, k) + f0(i - 1, j, k)) + (-f1(i, j, k) + f1(i, j - 1, k)) + (-f2(i, j, k) + f2(i, j, k - 1))) / g;
   }
 };
 
@@ -279,6 +298,7 @@ template <int ND, class T>
 struct op_betas {
   dfield<T> bu, bd, p, pmax, pmin, f0, f1, f2;
   unsigned o;
+  dfield<T> Gf;
   __device__ void operator()(int i, int j, int k) const {
     const T c = p(i, j, k);
     T mx, mn, du, dd;
@@ -300,8 +320,9 @@ struct op_betas {
       dd = (pospart(o, f0(i, j, k)) - negpart(o, f0(i - 1, j, k))) + (pospart(o, f1(i, j, k)) - negpart(o, f1(i, j - 1, k)))
          + (pospart(o, f2(i, j, k)) - negpart(o, f2(i, j, k - 1)));
     }
-    bu(i, j, k) = fct_frac((mx - c) * T(1), du);
-    bd(i, j, k) = fct_frac((c - mn) * T(1), dd);
+    const T g = (o & o_nug) ? Gf(i, j, k) : T(1);  // beta numerators times G (formulae_mpdata_fct_2d.hpp:37, 88)
+    bu(i, j, k) = fct_frac((mx - c) * g, du);
+    bd(i, j, k) = fct_frac((c - mn) * g, dd);
   }
 };
 
@@ -675,14 +696,14 @@ void general<T>::antidiff_nd(field<T> *res, field<T> &psi, field<T> *G) {
   const unsigned o = S.opts;
   const rng *ir = S.ir, *im = S.im;
   if (ND == 1) {
-    launch_frame<1, 0>(S.stream, op_antidiff<1, 0, T>{res[0].v, psi.v, G[0].v, G[0].v, G[0].v, o}, im[0], {0, 0}, {0, 0});
+    launch_frame<1, 0>(S.stream, op_antidiff<1, 0, T>{res[0].v, psi.v, G[0].v, G[0].v, G[0].v, o, S.G.v}, im[0], {0, 0}, {0, 0});
   } else if (ND == 2) {
-    launch_frame<2, 0>(S.stream, op_antidiff<2, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[1].v, o}, im[0], ir[1], {0, 0});
-    launch_frame<2, 1>(S.stream, op_antidiff<2, 1, T>{res[1].v, psi.v, G[1].v, G[0].v, G[0].v, o}, im[1], ir[0], {0, 0});
+    launch_frame<2, 0>(S.stream, op_antidiff<2, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[1].v, o, S.G.v}, im[0], ir[1], {0, 0});
+    launch_frame<2, 1>(S.stream, op_antidiff<2, 1, T>{res[1].v, psi.v, G[1].v, G[0].v, G[0].v, o, S.G.v}, im[1], ir[0], {0, 0});
   } else {
-    launch_frame<3, 0>(S.stream, op_antidiff<3, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[2].v, o}, im[0], ir[1], ir[2]);
-    launch_frame<3, 1>(S.stream, op_antidiff<3, 1, T>{res[1].v, psi.v, G[1].v, G[2].v, G[0].v, o}, im[1], ir[2], ir[0]);
-    launch_frame<3, 2>(S.stream, op_antidiff<3, 2, T>{res[2].v, psi.v, G[2].v, G[0].v, G[1].v, o}, im[2], ir[0], ir[1]);
+    launch_frame<3, 0>(S.stream, op_antidiff<3, 0, T>{res[0].v, psi.v, G[0].v, G[1].v, G[2].v, o, S.G.v}, im[0], ir[1], ir[2]);
+    launch_frame<3, 1>(S.stream, op_antidiff<3, 1, T>{res[1].v, psi.v, G[1].v, G[2].v, G[0].v, o, S.G.v}, im[1], ir[2], ir[0]);
+    launch_frame<3, 2>(S.stream, op_antidiff<3, 2, T>{res[2].v, psi.v, G[2].v, G[0].v, G[1].v, o, S.G.v}, im[2], ir[0], ir[1]);
   }
 }
 
@@ -718,7 +739,7 @@ void general<T>::fct_adjust_nd(int e, int iter) {
   rng r0 = ext(S.ir[0], 1), r1 = ND > 1 ? ext(S.ir[1], 1) : rng{0, 0}, r2 = ND > 2 ? ext(S.ir[2], 1) : rng{0, 0};
   const dfield<T> z = flx[0].v;
   launch_frame<ND, 0>(S.stream, op_betas<ND, T>{S.beta_up.v, S.beta_dn.v, p.v, S.psi_max.v, S.psi_min.v, flx[0].v,
-                                                ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z, S.opts},
+                                                ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z, S.opts, S.G.v},
                       r0, r1, r2);
   const rng *ir = S.ir, *im = S.im;
   if (ND == 1) {
@@ -759,14 +780,17 @@ void general<T>::advop_nd(int e) {
     else flx = GCit(iter);
     if (any_rigid()) xchng_flux(flx);  // mpdata_osc_2d.hpp:154-155 (a no-op without rigid walls)
     const dfield<T> z = flx[0].v;
-    launch_frame<ND, 0>(S.stream, op_donorcell<ND, T>{S.psi[e][S.tl[e] ^ 1].v, p.v, flx[0].v, ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z},
+    launch_frame<ND, 0>(S.stream, op_donorcell<ND, T>{S.psi[e][S.tl[e] ^ 1].v, p.v, flx[0].v, ND > 1 ? flx[1].v : z, ND > 2 ? flx[2].v : z, S.opts, S.G.v},
                         S.ir[0], ND > 1 ? S.ir[1] : rng{0, 0}, ND > 2 ? S.ir[2] : rng{0, 0});
+    // upwind-only step every upwind_filter_freq steps (mpdata_osc_2d.hpp:176-179)
+    if (S.upwind_filter_freq > 0 && S.timestep % S.upwind_filter_freq == 0) break;
   }
 }
 
-// divergence of the advector: max |div GC| over the interior (solver_{2,3}d.hpp max_abs_vctr_div)
+// divergence of the advector: max |div GC| / G over the interior (solver_{2,3}d.hpp max_abs_vctr_div)
 template <class T>
-__global__ void k_max_abs_div(int nd, int n0, int n1, int n2, dfield<T> g0, dfield<T> g1, dfield<T> g2, double *out) {
+__global__ void k_max_abs_div(int nd, int n0, int n1, int n2, dfield<T> g0, dfield<T> g1, dfield<T> g2, bool nug, dfield<T> G,
+                              double *out) {
   double m = 0;
   const long long tot = (long long)n0 * n1 * n2;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
@@ -777,6 +801,7 @@ __global__ void k_max_abs_div(int nd, int n0, int n1, int n2, dfield<T> g0, dfie
     if (nd == 1) v = fabs(g0(i, j, k) - g0(i - 1, j, k));
     else if (nd == 2) v = fabs((g0(i, j, k) - g0(i - 1, j, k)) + (g1(i, j, k) - g1(i, j - 1, k)));
     else v = fabs((g0(i, j, k) - g0(i - 1, j, k)) + (g1(i, j, k) - g1(i, j - 1, k)) + (g2(i, j, k) - g2(i, j, k - 1)));
+    if (nug) v = v / G(i, j, k);
     m = fmax(m, double(v));
   }
   for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
@@ -794,14 +819,30 @@ void general<T>::ante_loop(double *dev_scratch) {
     MPDX_CUDA(cudaMemsetAsync(dev_scratch, 0, sizeof(double), S.stream));
     const dfield<T> z = S.GC[0].v;
     k_max_abs_div<T><<<grid_for(S.cells()), 256, 0, S.stream>>>(S.nd, S.n[0], S.n[1], S.n[2], S.GC[0].v,
-                                                                S.nd > 1 ? S.GC[1].v : z, S.nd > 2 ? S.GC[2].v : z, dev_scratch);
+                                                                S.nd > 1 ? S.GC[1].v : z, S.nd > 2 ? S.GC[2].v : z,
+                                                                (S.opts & o_nug) != 0, S.G.v, dev_scratch);
     MPDX_LAUNCH_CHECK();
     double m = 0;
     MPDX_CUDA(cudaMemcpyAsync(&m, dev_scratch, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     MPDX_CUDA(cudaStreamSynchronize(S.stream));
     if (T(m) > S.max_abs_div_eps) throw error(MPDX_E_DIVERGENT, "libmpdata++: initial advector field is divergent");
   }
+  if (S.opts & o_nug) xchng_sclr(S.G, S.H);  // mpdata_osc_{1,2,3}d.hpp hook_ante_loop
   if (S.nd > 1) xchng_vctr_nrml(S.GC, S.H - 1);
+}
+
+template <class T>
+__global__ void k_fill(T *p, size_t n, T v) {
+  for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n; q += size_t(gridDim.x) * blockDim.x) p[q] = v;
+}
+
+template <class T>
+void general<T>::init_g() {
+  auto &S = *s;
+  if (!(S.opts & o_nug)) return;
+  const size_t n = S.G.bytes / sizeof(T);
+  k_fill<T><<<grid_for((long long)n), 256, 0, S.stream>>>(static_cast<T *>(S.G.base), n, T(1));
+  MPDX_LAUNCH_CHECK();
 }
 
 template <class T>

@@ -15,6 +15,8 @@ struct general {
   // MPDX_E_DIVERGENT), normal-halo fill (solver_common.hpp:191-211,
   // solver_2d.hpp:279-293, mpdata_osc_2d.hpp:40-67).  dev_scratch: one double.
   void ante_loop(double *dev_scratch);
+  // G = 1 everywhere (nug option), before the user sets g_factor()
+  void init_g();
   // one time step of every equation (solver_common.hpp:127-136, 321-331)
   void step();
 

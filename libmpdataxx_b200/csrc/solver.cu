@@ -110,6 +110,8 @@ struct mpdata_solver : solver_base {
     st.stream = stream;
     st.setup(c.n_dims, c.grid, c.n_eqns, unsigned(c.opts), c.n_iters, c.bcs);
     st.max_abs_div_eps = c.max_abs_div_eps < 0 ? std::numeric_limits<T>::epsilon() : T(c.max_abs_div_eps);
+    st.upwind_filter_freq = c.upwind_filter_freq;
+    gen.init_g();
     path = c.path;
     MPDX_CUDA(cudaMalloc(&scratch, 64));
     fus.init(st);
@@ -130,6 +132,12 @@ struct mpdata_solver : solver_base {
       st.advector_extent(idx, ex);
       off[0] = -1; off[1] = idx == 1 ? -1 : 0; off[2] = idx == 2 ? -1 : 0;
       f = &st.GC[idx];
+      return;
+    }
+    if (kind == MPDX_FIELD_G) {
+      if (!(st.opts & o_nug)) throw error(MPDX_E_ARG, "libmpdata++: g_factor() called with nug option unset?");
+      for (int q = 0; q < 3; ++q) { ex[q] = st.n[q]; off[q] = 0; }
+      f = &st.G;
       return;
     }
     throw error(MPDX_E_ARG, "field kind not available for this solver");
@@ -282,7 +290,7 @@ struct batch_impl : batch_base {
         throw error(MPDX_E_ARG, "all problems of a batch need the same opts and n_iters");
       if (st.n_eqns != 1) throw error(MPDX_E_UNSUPPORTED, "batched problems advect one equation each");
       if (!fused_configurable(st))
-        throw error(MPDX_E_UNSUPPORTED, "batched advance needs cyclic boundaries and opts within {fct, iga} (n_iters 2, or 3 without iga)");
+        throw error(MPDX_E_UNSUPPORTED, "batched advance needs cyclic boundaries, opts within {fct, iga} (n_iters 2, or 3 without iga) and no upwind filter");
       for (size_t q = 0; q < p; ++q)
         if (hs[q] == hs[p]) throw error(MPDX_E_ARG, "a problem appears twice in the batch");
       cells += st.cells();
@@ -462,9 +470,12 @@ void validate(const mpdx_config &c) {
   if (c.n_eqns < 1) throw error(MPDX_E_ARG, "n_eqns must be positive");
   if (c.n_iters < 1) throw error(MPDX_E_ARG, "n_iters must be positive");
   const unsigned o = unsigned(c.opts);
-  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl;
+  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl | o_nug | o_khn;
   if (o & ~built)
-    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl)");
+    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl nug khn)");
+  if ((o & o_nug) && c.solver == MPDX_SOLVER_BOUSSINESQ)
+    throw error(MPDX_E_UNSUPPORTED, "nug option is built for solvers::mpdata only on this backend");
+  if (c.upwind_filter_freq < 0) throw error(MPDX_E_ARG, "upwind_filter_freq must be non-negative");
   if ((o & o_iga) && (o & o_abs)) throw error(MPDX_E_ARG, "abs & iga options are mutually exclusive");
   for (int q = 0; q < 2 * c.n_dims; ++q) {
     const int k = c.bcs[q];

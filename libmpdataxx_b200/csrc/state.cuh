@@ -22,6 +22,8 @@ struct mpdata_state {
   std::vector<int> tl;  // time level of psi[e] holding the current state
   field<T> GC[3], tmp0[3], tmp1[3], flux[3], GC_mono[3];
   field<T> psi_min, psi_max, beta_up, beta_dn;
+  field<T> G;                  // G factor with the nug option (sharedmem G); unallocated otherwise
+  int upwind_filter_freq = 0;  // rt_params (mpdata_common.hpp:77): upwind-only step every n-th step
   cudaStream_t stream = nullptr;
   long long timestep = 0;
 
@@ -59,6 +61,7 @@ struct mpdata_state {
       alloc_sclr(psi_min); alloc_sclr(psi_max); alloc_sclr(beta_up); alloc_sclr(beta_dn);
       alloc_vctr(GC_mono);
     }
+    if (opts & o_nug) alloc_sclr(G);  // set to 1 by general<T>::init_g
   }
 
   long long cells() const { return (long long)n[0] * n[1] * n[2]; }

@@ -62,9 +62,8 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   static_assert(bcxl != bcond::null && bcxr != bcond::null, "x boundary conditions are required");
   static_assert(n_dims < 2 || (bcyl != bcond::null && bcyr != bcond::null), "y boundary conditions are required");
   static_assert(n_dims < 3 || (bczl != bcond::null && bczr != bcond::null), "z boundary conditions are required");
-  static_assert(!opts::isset(ct_params_t::opts, opts::nug | opts::khn | opts::div_2nd | opts::div_3rd |
-                                                    opts::div_3rd_dt | opts::fot),
-                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl)");
+  static_assert(!opts::isset(ct_params_t::opts, opts::div_2nd | opts::div_3rd | opts::div_3rd_dt | opts::fot),
+                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl nug khn)");
 
   explicit cuda(const rt_params_t &p) : p_(p) {
     mpdx_config c;
@@ -82,6 +81,7 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
     c.dj = p.dj != 0 ? double(p.dj) : 1.0;
     c.dk = p.dk != 0 ? double(p.dk) : 1.0;
     c.max_abs_div_eps = double(p.max_abs_div_eps);
+    c.upwind_filter_freq = p.upwind_filter_freq;
     solver_t::fill(c, p);
     detail::check(nullptr, mpdx_create(&c, &h_));
   }
@@ -94,6 +94,13 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   // accessors (concurr_common.hpp:387-433)
   arr_t advectee(int e = 0) override { return view(MPDX_FIELD_ADVECTEE, e); }
   arr_t advector(int d = 0) override { return view(MPDX_FIELD_ADVECTOR, d); }
+  // G of the nug option (sharedmem.hpp:373-380); throws without nug, as the reference does
+  arr_t g_factor() override { return view(MPDX_FIELD_G, 0); }
+  // advectee_global_set (concurr_common.hpp:444-453): copy a whole field into the advectee
+  void advectee_global_set(const arr_t &a, int e = 0) override {
+    arr_t v = advectee(e);
+    std::copy(a.data(), a.data() + v.size(), v.data());
+  }
   arr_t sclr_array(const std::string &name, int = 0) override {
     if (name != "tht_e") throw std::out_of_range("libmpdata++: unknown scalar array " + name);
     return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_E);

@@ -135,12 +135,14 @@ struct mpdata {
   unsigned opts = o_iga | o_fct;
   int bcs[3][2] = {{bc_cyclic, bc_cyclic}, {bc_cyclic, bc_cyclic}, {bc_cyclic, bc_cyclic}};
   T max_abs_div_eps = std::numeric_limits<T>::epsilon();
+  int upwind_filter_freq = 0;  // rt_params (mpdata_common.hpp:77): upwind-only step every n-th step
 
   // state
   std::vector<std::array<arr<T>, 2>> psi;  // psi[e][tlev]
   std::vector<int> tl;                     // per-eqn time level n[e] (mod 2)
   vctr<T> GC, tmp0, tmp1, flux, GC_mono;
   arr<T> psi_min, psi_max, beta_up, beta_dn;
+  arr<T> Gf;  // G factor with the nug option (sharedmem G, solver_{1,2,3}d.hpp alloc); 1 elsewhere
   long long timestep = 0;
 
   rng ir[3];  // interior ranges
@@ -169,6 +171,18 @@ struct mpdata {
       alloc_sclr(psi_min); alloc_sclr(psi_max); alloc_sclr(beta_up); alloc_sclr(beta_dn);
       alloc_vctr(GC_mono);
     }
+    if (opts & o_nug) {
+      alloc_sclr(Gf);
+      for (auto &v : Gf.v) v = T(1);
+    }
+  }
+
+  // G and its face average G_bar_x (formulae/common.hpp:127-195, formulae_mpdata_g_{1,2,3}d.hpp);
+  // the reference returns the integer 1 for both without nug
+  T Gc(int i, int j, int k) const { return (opts & o_nug) ? Gf(i, j, k) : T(1); }
+  template <int ND, int D> T Gbar(int a, int b, int c) const {
+    if (!(opts & o_nug)) return T(1);
+    return (P<ND, D>(Gf, a + 1, b, c) + P<ND, D>(Gf, a, b, c)) / T(2);
   }
 
   rng sr(int d) const { return d < nd ? ext(ir[d], H) : rng{0, 0}; }     // rng_sclr
@@ -491,18 +505,20 @@ struct mpdata {
     return frac(opts, q[0] + q[1] - q[2] - q[3] + q[4] + q[5] - q[6] - q[7],
                 q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6] + q[7]);
   }
-  // coefficients (hot_1d.hpp:19-40, hot_2d.hpp:21-50, hot_3d.hpp:21-95)
-  static T cxx(T C) { return (T(3) * C * std::abs(C) / T(1) - T(2) * (C * C * C) / T(1) - C) / T(6); }
-  static T cxy(T C, T g) { return (std::abs(C) - T(2) * (C * C) / T(1)) * g / T(2); }
-  static T cyz(T C, T g1, T g2) { return T(-2) * C * g1 * g2 / T(3) / T(1); }
+  // coefficients (hot_1d.hpp:19-40, hot_2d.hpp:21-50, hot_3d.hpp:21-95); gb = G_bar_x,
+  // pow2/pow3 as products
+  static T cxx(T C, T gb) { return (T(3) * C * std::abs(C) / gb - T(2) * (C * C * C) / (gb * gb) - C) / T(6); }
+  static T cxy(T C, T g, T gb) { return (std::abs(C) - T(2) * (C * C) / gb) * g / (T(2) * gb); }
+  static T cyz(T C, T g1, T g2, T gb) { return T(-2) * C * g1 * g2 / T(3) / (gb * gb); }
 
   // ---- divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp), G = 1 ----
-  // -C/4 (div of the advector around the face) [x psi_bar_x with iga]; 1D: -C/2/(1+1) dC
+  // -C/4/G_bar_x (div of the advector around the face) [x psi_bar_x with iga];
+  // 1D: -C/2/(G(i+1)+G(i)) dC
   template <int ND, int D> T dfl(const arr<T> &p, const arr<T> &Gd, const arr<T> &G1, const arr<T> &G2, int a, int b, int c) const {
     const T C = P<ND, D>(Gd, a, b, c);
     T r;
     if (ND == 1) {
-      r = T(-0.5) * C / T(2) * (P<ND, D>(Gd, a + 1, b, c) - P<ND, D>(Gd, a - 1, b, c));
+      r = T(-0.5) * C / (Gc(a + 1, 0, 0) + Gc(a, 0, 0)) * (P<ND, D>(Gd, a + 1, b, c) - P<ND, D>(Gd, a - 1, b, c));
       if (opts & o_iga) r = r * T(0.5) * (P<ND, D>(p, a + 1, b, c) + P<ND, D>(p, a, b, c));
       return r;
     }
@@ -510,7 +526,7 @@ struct mpdata {
         + (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) - P<ND, D>(G1, a + 1, b - 1, c) - P<ND, D>(G1, a, b - 1, c));
     if (ND == 3)
       s = s + (P<ND, D>(G2, a + 1, b, c) + P<ND, D>(G2, a, b, c) - P<ND, D>(G2, a + 1, b, c - 1) - P<ND, D>(G2, a, b, c - 1));
-    r = T(-0.25) * C / T(1) * s;
+    r = T(-0.25) * C / Gbar<ND, D>(a, b, c) * s;
     if (opts & o_iga) r = r * ((P<ND, D>(p, a + 1, b, c) + P<ND, D>(p, a, b, c)) / T(2));
     return r;
   }
@@ -521,9 +537,9 @@ struct mpdata {
   // 1D: formulae_mpdata_1d.hpp:186-210
   void antidiff1(arr<T> &res, const arr<T> &p, const vctr<T> &G) {
     for (int i = im[0].f; i <= im[0].l; ++i) {
-      const T C = G[0](i, 0, 0);
-      T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<1, 0>(p, i, 0, 0);
-      if (opts & o_tot) r = r + ndxx<1, 0>(p, i, 0, 0) * cxx(C);
+      const T C = G[0](i, 0, 0), gb = Gbar<1, 0>(i, 0, 0);
+      T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / gb) * ndx<1, 0>(p, i, 0, 0);
+      if (opts & o_tot) r = r + ndxx<1, 0>(p, i, 0, 0) * cxx(C, gb);
       if (opts & o_dfl) r = r + dfl<1, 0>(p, G[0], G[0], G[0], i, 0, 0);
       res(i, 0, 0) = r;
     }
@@ -534,11 +550,11 @@ struct mpdata {
     const rng ra = im[D], rb = ir[(D + 1) % 2];
     for (int a = ra.f; a <= ra.l; ++a)
       for (int b = rb.f; b <= rb.l; ++b) {
-        const T C = P<2, D>(Gd, a, b);
+        const T C = P<2, D>(Gd, a, b), gb = Gbar<2, D>(a, b, 0);
         const T gc1 = (P<2, D>(Gt, a + 1, b) + P<2, D>(Gt, a, b) + P<2, D>(Gt, a + 1, b - 1) + P<2, D>(Gt, a, b - 1)) / T(4);
-        T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<2, D>(p, a, b, 0)
-            - C * gc1 / T(2) * ndy<2, D>(p, a, b, 0);
-        if (opts & o_tot) r = r + (ndxx<2, D>(p, a, b, 0) * cxx(C) + ndxy<2, D>(p, a, b, 0) * cxy(C, gc1));
+        T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / gb) * ndx<2, D>(p, a, b, 0)
+            - C * gc1 / (T(2) * gb) * ndy<2, D>(p, a, b, 0);
+        if (opts & o_tot) r = r + (ndxx<2, D>(p, a, b, 0) * cxx(C, gb) + ndxy<2, D>(p, a, b, 0) * cxy(C, gc1, gb));
         if (opts & o_dfl) r = r + dfl<2, D>(p, Gd, Gt, Gt, a, b, 0);
         P<2, D>(res, a, b) = r;
       }
@@ -548,14 +564,14 @@ struct mpdata {
     const arr<T> &Gd = G[D], &G1 = G[(D + 1) % 3], &G2 = G[(D + 2) % 3];
     const rng ra = im[D], rb = ir[(D + 1) % 3], rc = ir[(D + 2) % 3];
     box<3, D>(ra, rb, rc, [&](int a, int b, int c) {
-          const T C = P<3, D>(Gd, a, b, c);
+          const T C = P<3, D>(Gd, a, b, c), gb = Gbar<3, D>(a, b, c);
           const T gc1 = (P<3, D>(G1, a + 1, b, c) + P<3, D>(G1, a, b, c) + P<3, D>(G1, a + 1, b - 1, c) + P<3, D>(G1, a, b - 1, c)) / T(4);
           const T gc2 = (P<3, D>(G2, a + 1, b, c) + P<3, D>(G2, a, b, c) + P<3, D>(G2, a + 1, b, c - 1) + P<3, D>(G2, a, b, c - 1)) / T(4);
-          T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / T(1)) * ndx<3, D>(p, a, b, c)
-              - C / T(2) * (gc1 * ndy<3, D>(p, a, b, c) + gc2 * ndz<3, D>(p, a, b, c)) / T(1);
+          T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / gb) * ndx<3, D>(p, a, b, c)
+              - C / T(2) * (gc1 * ndy<3, D>(p, a, b, c) + gc2 * ndz<3, D>(p, a, b, c)) / gb;
           if (opts & o_tot)
-            r = r + (ndxx<3, D>(p, a, b, c) * cxx(C) + ndxy<3, D>(p, a, b, c) * cxy(C, gc1)
-                     + ndxz<D>(p, a, b, c) * cxy(C, gc2) + ndyz<D>(p, a, b, c) * cyz(C, gc1, gc2));
+            r = r + (ndxx<3, D>(p, a, b, c) * cxx(C, gb) + ndxy<3, D>(p, a, b, c) * cxy(C, gc1, gb)
+                     + ndxz<D>(p, a, b, c) * cxy(C, gc2, gb) + ndyz<D>(p, a, b, c) * cyz(C, gc1, gc2, gb));
           if (opts & o_dfl) r = r + dfl<3, D>(p, Gd, G1, G2, a, b, c);
           P<3, D>(res, a, b, c) = r;
         });
@@ -582,19 +598,31 @@ struct mpdata {
     }
   }
 
-  // ---- donorcell_sum (donorcell_formulae.hpp:81-165), G = 1 ----
+  // ---- donorcell_sum (donorcell_formulae.hpp:81-165), divided by G; Kahan variant with khn ----
   void donorcell_sum(arr<T> &pn, const arr<T> &po, const vctr<T> &f) {
 #pragma omp parallel for schedule(static) if (big())
     for (int i = 0; i < n[0]; ++i)
       for (int j = 0; j < n[1]; ++j)
         for (int k = 0; k < n[2]; ++k) {
-          if (nd == 1)
-            pn(i, j, k) = po(i, j, k) + (-f[0](i, j, k) + f[0](i - 1, j, k)) / T(1);
+          const T g = Gc(i, j, k);
+          if (opts & o_khn) {
+            // Kahan-compensated sum (kahan_sum.hpp:14-27): psi_old, then -F(+1/2)/G and
+            // F(-1/2)/G per dimension
+            T sum = T(0), c = T(0);
+            auto add = [&](T in) { const T y = in - c; const T t = sum + y; c = (t - sum) - y; sum = t; };
+            add(po(i, j, k));
+            add(-f[0](i, j, k) / g);
+            add(f[0](i - 1, j, k) / g);
+            if (nd > 1) { add(-f[1](i, j, k) / g); add(f[1](i, j - 1, k) / g); }
+            if (nd > 2) { add(-f[2](i, j, k) / g); add(f[2](i, j, k - 1) / g); }
+            pn(i, j, k) = sum;
+          } else if (nd == 1)
+            pn(i, j, k) = po(i, j, k) + (-f[0](i, j, k) + f[0](i - 1, j, k)) / g;
           else if (nd == 2)
-            pn(i, j, k) = po(i, j, k) + ((-f[0](i, j, k) + f[0](i - 1, j, k)) + (-f[1](i, j, k) + f[1](i, j - 1, k))) / T(1);
+            pn(i, j, k) = po(i, j, k) + ((-f[0](i, j, k) + f[0](i - 1, j, k)) + (-f[1](i, j, k) + f[1](i, j - 1, k))) / g;
           else
             pn(i, j, k) = po(i, j, k) + ((-f[0](i, j, k) + f[0](i - 1, j, k)) + (-f[1](i, j, k) + f[1](i, j - 1, k))
-                                         + (-f[2](i, j, k) + f[2](i, j, k - 1))) / T(1);
+                                         + (-f[2](i, j, k) + f[2](i, j, k - 1))) / g;
         }
   }
 
@@ -657,8 +685,8 @@ struct mpdata {
                    + (pospart(o, f[1](i, j, k)) - negpart(o, f[1](i, j - 1, k)))
                    + (pospart(o, f[2](i, j, k)) - negpart(o, f[2](i, j, k - 1)));
           }
-          beta_up(i, j, k) = fct_frac((mx - c) * T(1), den_up);
-          beta_dn(i, j, k) = fct_frac((c - mn) * T(1), den_dn);
+          beta_up(i, j, k) = fct_frac((mx - c) * Gc(i, j, k), den_up);
+          beta_dn(i, j, k) = fct_frac((c - mn) * Gc(i, j, k), den_dn);
         }
   }
 
@@ -718,6 +746,8 @@ struct mpdata {
       else flx = &GCit(iter);
       xchng_flux(*flx);  // mpdata_osc_2d.hpp:154-155
       donorcell_sum(psi[e][(tl[e] + 1) % 2], p, *flx);
+      // upwind-only step every upwind_filter_freq steps (mpdata_osc_2d.hpp:176-179)
+      if (upwind_filter_freq > 0 && timestep % upwind_filter_freq == 0) break;
     }
   }
 
@@ -727,9 +757,9 @@ struct mpdata {
       for (int j = 0; j < n[1]; ++j)
         for (int k = 0; k < n[2]; ++k) {
           T v;
-          if (nd == 1) v = std::abs(GC[0](i, 0, 0) - GC[0](i - 1, 0, 0));
-          else if (nd == 2) v = std::abs((GC[0](i, j, 0) - GC[0](i - 1, j, 0)) + (GC[1](i, j, 0) - GC[1](i, j - 1, 0)));
-          else v = std::abs((GC[0](i, j, k) - GC[0](i - 1, j, k)) + (GC[1](i, j, k) - GC[1](i, j - 1, k)) + (GC[2](i, j, k) - GC[2](i, j, k - 1)));
+          if (nd == 1) v = std::abs(GC[0](i, 0, 0) - GC[0](i - 1, 0, 0)) / Gc(i, j, k);
+          else if (nd == 2) v = std::abs((GC[0](i, j, 0) - GC[0](i - 1, j, 0)) + (GC[1](i, j, 0) - GC[1](i, j - 1, 0))) / Gc(i, j, k);
+          else v = std::abs((GC[0](i, j, k) - GC[0](i - 1, j, k)) + (GC[1](i, j, k) - GC[1](i, j - 1, k)) + (GC[2](i, j, k) - GC[2](i, j, k - 1))) / Gc(i, j, k);
           mx = std::max(mx, v);
         }
     return mx;
@@ -742,6 +772,7 @@ struct mpdata {
       if (max_abs_vctr_div() > max_abs_div_eps)
         throw std::runtime_error("libmpdata++: initial advector field is divergent");
     }
+    if (opts & o_nug) xchng_sclr(Gf, H);  // mpdata_osc_{1,2,3}d.hpp hook_ante_loop
     if (nd > 1) xchng_vctr_nrml(GC, H - 1);
   }
 

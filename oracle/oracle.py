@@ -44,6 +44,8 @@ def lib(fast=False):
         getattr(L, f).restype = ctypes.c_int
     L.orc_set_sclr_array.argtypes = [vp, ctypes.c_char_p, dp]
     L.orc_set_sclr_array.restype = ctypes.c_int
+    L.orc_set_param.argtypes = [vp, ctypes.c_char_p, ctypes.c_double]
+    L.orc_set_param.restype = ctypes.c_int
     L.orc_advance.argtypes = [vp, ctypes.c_longlong]
     L.orc_advance.restype = ctypes.c_int
     L.orc_timestep.argtypes = [vp]
@@ -68,7 +70,7 @@ class Oracle:
     """CPU restatement of one concurr run (solvers::mpdata or boussinesq)."""
 
     def __init__(self, grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64,
-                 max_abs_div_eps=None, fast=False, boussinesq=None):
+                 max_abs_div_eps=None, fast=False, boussinesq=None, upwind_filter_freq=0):
         self.L = lib(fast)
         self.grid = tuple(int(g) for g in grid)
         self.nd = len(self.grid)
@@ -88,6 +90,8 @@ class Oracle:
                                                   _dptr(prm), int(boussinesq.get("prs_k", 1)), err, 512)
         if not self.h:
             raise RuntimeError(err.value.decode())
+        if upwind_filter_freq:
+            self._check(self.L.orc_set_param(self.h, b"upwind_filter_freq", float(upwind_filter_freq)))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -125,6 +129,10 @@ class Oracle:
     def set_sclr_array(self, name, a):
         a = np.ascontiguousarray(np.broadcast_to(a, self.grid), dtype=np.float64)
         self._check(self.L.orc_set_sclr_array(self.h, name.encode(), _dptr(a)))
+
+    def set_g_factor(self, a):
+        """g_factor() = a (nug option): G at the interior points."""
+        self.set_sclr_array("G", a)
 
     def advance(self, nt):
         self._check(self.L.orc_advance(self.h, int(nt)))

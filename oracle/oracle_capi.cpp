@@ -22,6 +22,7 @@ struct base_t {
   virtual void advance(long long nt) = 0;
   virtual long long timestep() const = 0;
   virtual void set_sclr(const char *, const double *) { throw std::runtime_error("no such scalar array"); }
+  virtual void set_param(const char *, double) { throw std::runtime_error("no such parameter"); }
   virtual long long last_iters() const { return -1; }
   std::string err;
 };
@@ -51,6 +52,17 @@ struct wrap_t : base_t {
   }
   void advance(long long nt) override { s.advance(nt); }
   long long timestep() const override { return s.timestep; }
+  // g_factor() (sharedmem.hpp:373-380, 458-465, 579-586): interior values of G
+  void set_sclr(const char *name, const double *src) override {
+    if (std::strcmp(name, "G") != 0) throw std::runtime_error("no such scalar array");
+    if (!(s.opts & o_nug)) throw std::runtime_error("libmpdata++: g_factor() called with nug option unset?");
+    size_t q = 0;
+    for (int i = 0; i < s.n[0]; ++i) for (int j = 0; j < s.n[1]; ++j) for (int k = 0; k < s.n[2]; ++k) s.Gf(i, j, k) = T(src[q++]);
+  }
+  void set_param(const char *name, double v) override {
+    if (std::strcmp(name, "upwind_filter_freq") == 0) s.upwind_filter_freq = int(v);
+    else throw std::runtime_error("no such parameter");
+  }
 };
 
 template <class T>
@@ -121,6 +133,7 @@ int orc_get_advectee(void *h, int e, double *dst) { ORC_TRY(static_cast<base_t *
 int orc_set_advector(void *h, int d, const double *src) { ORC_TRY(static_cast<base_t *>(h)->set_advector(d, src)) }
 int orc_get_advector(void *h, int d, double *dst) { ORC_TRY(static_cast<base_t *>(h)->get_advector(d, dst)) }
 int orc_set_sclr_array(void *h, const char *name, const double *src) { ORC_TRY(static_cast<base_t *>(h)->set_sclr(name, src)) }
+int orc_set_param(void *h, const char *name, double v) { ORC_TRY(static_cast<base_t *>(h)->set_param(name, v)) }
 int orc_advance(void *h, long long nt) { ORC_TRY(static_cast<base_t *>(h)->advance(nt)) }
 long long orc_timestep(void *h) { return static_cast<base_t *>(h)->timestep(); }
 long long orc_last_iters(void *h) { return static_cast<base_t *>(h)->last_iters(); }

@@ -90,7 +90,7 @@ def test_bogus_grid_size():
 
 def test_unsupported_option_rejected():
     from libmpdataxx_b200 import opts as o
-    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.nug))
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.div_2nd))
     assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
     rc, _ = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.iga | o.abs))
     assert rc == _lib.MPDX_E_ARG

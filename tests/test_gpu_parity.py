@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 RTOL64 = 1e-12
 
 
-def make_run(grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64, path="general", max_abs_div_eps=None):
+def make_run(grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64, path="general", max_abs_div_eps=None,
+             upwind_filter_freq=0):
     nd = len(grid)
 
     class ct(solvers.ct_params_default_t):
@@ -26,7 +27,8 @@ def make_run(grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64, path="
     ct.n_dims = nd
     ct.n_eqns = n_eqns
     ct.opts = opts
-    p = solvers.mpdata.rt_params_t(grid_size=list(grid), n_iters=n_iters, max_abs_div_eps=max_abs_div_eps)
+    p = solvers.mpdata.rt_params_t(grid_size=list(grid), n_iters=n_iters, max_abs_div_eps=max_abs_div_eps,
+                                   upwind_filter_freq=upwind_filter_freq)
     bcs = bcs or ["cyclic"] * (2 * nd)
     return concurr.cuda(solvers.mpdata(ct), *[getattr(bcond, b) for b in bcs], p=p, path=path)
 
@@ -87,6 +89,42 @@ def test_dfl_fp64_matches_oracle(nd, grid, bc, opts, iters):
     _check_parity(s, grid, bcs, opts, iters, eps=None)
 
 
+# non-unit G (nug, with a spatially varying G), Kahan donor-cell sums (khn) and the upwind filter
+NUG_CASES = []
+for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
+    for bc in ("cyclic", "open", "rigid"):
+        for opts, iters in [(o.nug, 2), (o.nug | o.iga | o.fct, 2), (o.nug | o.fct, 3), (o.nug | o.tot | o.fct, 2),
+                            (o.nug | o.iga | o.tot, 3), (o.khn, 2), (o.khn | o.nug | o.fct, 2)]:
+            NUG_CASES.append((nd, grid, bc, opts, iters))
+
+
+@pytest.mark.parametrize("nd,grid,bc,opts,iters", NUG_CASES)
+def test_nug_khn_fp64_matches_oracle(nd, grid, bc, opts, iters):
+    bcs = [bc] * (2 * nd)
+    s = random_setup(grid, bcs, seed=nd * 100 + iters + 3, signed=bool(opts & o.iga))
+    rng = np.random.default_rng(nd + iters)
+    G = rng.uniform(0.7, 1.3, grid)
+    if bc == "cyclic":
+        G = setups.wrap_periodic(G[tuple(slice(0, g - 1) for g in grid)])
+    if opts & o.nug:
+        s["G"] = G
+    _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10)
+
+
+@pytest.mark.parametrize("nd,grid", [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))])
+@pytest.mark.parametrize("opts,iters,uff", [(o.iga | o.fct, 2, 2), (o.fct, 3, 3), (0, 2, 1)])
+def test_upwind_filter_fp64_matches_oracle(nd, grid, opts, iters, uff):
+    bcs = ["cyclic"] * (2 * nd)
+    s = random_setup(grid, bcs, seed=nd * 100 + iters + 5, signed=bool(opts & o.iga))
+    _check_parity(s, grid, bcs, opts, iters, eps=1e-10, uff=uff)
+
+
+def test_g_factor_needs_nug():
+    run = make_run((8, 8), o.fct)
+    with pytest.raises(RuntimeError, match="g_factor"):
+        run.set_g_factor(np.ones((8, 8)))
+
+
 @pytest.mark.parametrize("nd,grid,bc,opts,iters", CASES)
 def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
     bcs = [bc] * (2 * nd)
@@ -97,13 +135,16 @@ def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
     _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10)
 
 
-def _check_parity(s, grid, bcs, opts, iters, eps):
-    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)
+def _check_parity(s, grid, bcs, opts, iters, eps, uff=0):
+    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps, upwind_filter_freq=uff)
     load(orc, s)
-    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps)
+    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps, upwind_filter_freq=uff)
     run.set_advectee(s["advectee"][0])
     for d, a in enumerate(s["advector"]):
         run.set_advector(a, d)
+    if "G" in s:
+        orc.set_g_factor(s["G"])
+        run.set_g_factor(s["G"])
     for chunk in (1, 4):
         orc.advance(chunk)
         run.advance(chunk)

@@ -73,3 +73,85 @@ def test_tot_changes_the_result():
     a = _run((NX, 4, 5), "cyclic", o.fct, 2, psi, gc, nt=6)
     b = _run((NX, 4, 5), "cyclic", o.tot | o.fct, 2, psi, gc, nt=6)
     assert np.abs(a - b).max() > 1e-6
+
+
+# ---- nug: non-unit G (formulae_mpdata_g_{1,2,3}d.hpp, donorcell_sum / G, betas * G) ----
+def _run_g(grid, opts, iters, psi, adv, G=None, nt=4, bcs=None):
+    nd = len(grid)
+    orc = Oracle(grid, opts, n_iters=iters, bcs=bcs or ["cyclic"] * (2 * nd), max_abs_div_eps=1e30)
+    orc.set_advectee(psi)
+    for d, a in enumerate(adv):
+        orc.set_advector(a, d)
+    if G is not None:
+        orc.set_g_factor(G)
+    orc.advance(nt)
+    return orc.advectee()
+
+
+def _random_2d(seed, grid=(17, 19)):
+    rng = np.random.default_rng(seed)
+    psi = rng.uniform(0.5, 2.0, grid)
+    adv = [rng.uniform(-0.3, 0.3, (grid[0], grid[1])), rng.uniform(-0.3, 0.3, (grid[0] + 1, grid[1]))]
+    return psi, adv
+
+
+@pytest.mark.parametrize("opts,iters", [(0, 2), (o.iga | o.fct, 2), (o.tot | o.fct, 3), (o.iga | o.dfl, 2), (o.khn, 2)])
+def test_nug_with_unit_g_is_plain(opts, iters):
+    """G = 1 everywhere gives the no-nug result bit for bit (every G factor is an exact 1)."""
+    psi, adv = _random_2d(1)
+    a = _run_g(psi.shape, opts, iters, psi, adv)
+    b = _run_g(psi.shape, opts | o.nug, iters, psi, adv, G=np.ones(psi.shape))
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("opts,iters", [(0, 2), (o.iga, 2), (o.tot, 2), (o.iga | o.tot, 3), (o.dfl, 2),
+                                        (o.iga | o.dfl, 2), (o.abs | o.tot, 2), (o.npa, 2), (o.pfc, 3)])
+@pytest.mark.parametrize("nd", [1, 2, 3])
+def test_nug_constant_g_scales_courant_numbers(opts, iters, nd):
+    """With G = 2 everywhere the scheme equals the no-nug scheme on the advector C/2, bit
+    for bit: every G factor then rescales by an exact power of two.  (Not with fct, whose
+    beta denominators add an unscaled epsilon.)"""
+    rng = np.random.default_rng(nd * 7 + iters)
+    grid = {1: (23,), 2: (13, 15), 3: (9, 10, 11)}[nd]
+    psi = rng.uniform(0.5, 2.0, grid)
+    if opts & o.abs:
+        psi *= np.where(rng.uniform(size=grid) < 0.3, -1.0, 1.0)
+    adv = []
+    for d in range(nd):
+        s = list(grid)
+        if d > 0:
+            s[0] += 1
+        adv.append(rng.uniform(-0.6, 0.6, s))
+    a = _run_g(grid, opts, iters, psi, [x / 2 for x in adv])
+    b = _run_g(grid, opts | o.nug, iters, psi, adv, G=np.full(grid, 2.0))
+    np.testing.assert_array_equal(a, b)
+
+
+# ---- khn: Kahan-compensated donor-cell sums (donorcell_formulae.hpp:81-165) ----
+def test_khn_close_to_plain_and_different():
+    psi, adv = _random_2d(2)
+    a = _run_g(psi.shape, o.iga | o.fct, 2, psi, adv)
+    b = _run_g(psi.shape, o.iga | o.fct | o.khn, 2, psi, adv)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+    assert np.abs(a - b).max() > 0
+
+
+# ---- upwind_filter_freq (mpdata_osc_2d.hpp:176-179) ----
+def test_upwind_filter_every_step_is_upwind():
+    psi, adv = _random_2d(3)
+    grid = psi.shape
+    ref = Oracle(grid, o.fct, n_iters=1, max_abs_div_eps=1e30)
+    uf = Oracle(grid, o.fct, n_iters=2, max_abs_div_eps=1e30, upwind_filter_freq=1)
+    mp = Oracle(grid, o.fct, n_iters=2, max_abs_div_eps=1e30, upwind_filter_freq=2)
+    for r in (ref, uf, mp):
+        r.set_advectee(psi)
+        for d, a in enumerate(adv):
+            r.set_advector(a, d)
+    for r in (ref, uf, mp):
+        r.advance(1)
+    np.testing.assert_array_equal(uf.advectee(), ref.advectee())
+    np.testing.assert_array_equal(mp.advectee(), ref.advectee())  # timestep 0 is filtered
+    for r in (ref, uf, mp):
+        r.advance(1)
+    np.testing.assert_array_equal(uf.advectee(), ref.advectee())
+    assert np.abs(mp.advectee() - ref.advectee()).max() > 1e-6      # timestep 1 is full MPDATA
