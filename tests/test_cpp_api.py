@@ -14,11 +14,21 @@ BUILD = os.path.join(ROOT, "tests", "cpp", "_build")
 LIBDIR = os.path.join(ROOT, "libmpdataxx_b200")
 
 
+def _newest_input(src):
+    """mtime of the program's source or of any header it can include (mpdx.h, the C++ API)."""
+    t = os.path.getmtime(src)
+    for top in (os.path.join(LIBDIR, "include"), os.path.join(ROOT, "include")):
+        for d, _, files in os.walk(top):
+            for f in files:
+                t = max(t, os.path.getmtime(os.path.join(d, f)))
+    return t
+
+
 def build(name):
     os.makedirs(BUILD, exist_ok=True)
     exe = os.path.join(BUILD, name)
     src = os.path.join(CPP, name + ".cpp")
-    if not os.path.exists(exe) or os.path.getmtime(exe) < os.path.getmtime(src):
+    if not os.path.exists(exe) or os.path.getmtime(exe) < _newest_input(src):
         subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(LIBDIR, "include"), "-I",
                         os.path.join(ROOT, "include"), src, "-o", exe, "-L", LIBDIR, "-lmpdx",
                         f"-Wl,-rpath,{LIBDIR}"], check=True)
