@@ -193,6 +193,52 @@ def batched_extra(n_problems=256, steps=50):
     return out
 
 
+def rotation_extra(n=1024, steps=200):
+    """C2: 2D n^2 cyclic solid-body rotation of a cone, fct, n_iters=3, in FP32 and
+    FP64 (fused 2D kernel; the FP32 fields, 12 MB, fit in L2): device time per step
+    on the solver's stream, FP32 - FP64 differences, minimum and mass drift."""
+    import numpy as np
+    import torch
+    from libmpdataxx_b200 import _lib, bcond, concurr, opts, solvers, workloads
+    out = {"workload": f"2D {n}^2 cyclic solid-body rotation, cone h=4 r=0.15n, fct, n_iters=3", "steps": steps}
+    fields = {}
+    for dt in ("float32", "float64"):
+        w = workloads.rotation_2d(n, dtype=dt)
+
+        class ct(solvers.ct_params_default_t):
+            pass
+
+        ct.real_t = dt
+        ct.n_dims = 2
+        ct.n_eqns = 1
+        ct.opts = opts.fct
+        p = solvers.mpdata.rt_params_t(grid_size=[n, n], n_iters=3, max_abs_div_eps=1e-6)
+        run = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * 4, p=p)
+        run.set_field_device(_lib.FIELD_ADVECTEE, 0, w["advectee"][0].data_ptr())
+        for d, a in enumerate(w["advector"]):
+            run.set_field_device(_lib.FIELD_ADVECTOR, d, a.data_ptr())
+        m0 = run.stats()["mass"]
+        run.advance(3)
+        run.sync()
+        stream = torch.cuda.ExternalStream(run.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            run.advance(steps)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        st = run.stats()
+        fields[dt] = np.array(run.advectee(), dtype=np.float64)
+        out[dt] = {"ms_per_step": ms, "cell_updates_per_s": n * n / (ms * 1e-3),
+                   "path": "fused" if st["path"] == _lib.PATH_FUSED else "general",
+                   "min": st["min"], "max": st["max"], "mass_rel_drift": (st["mass"] - m0) / m0}
+        run.close()
+    d = fields["float32"] - fields["float64"]
+    out["fp32_vs_fp64"] = {"max_abs": float(np.abs(d).max()), "l2": float(np.sqrt((d * d).mean()))}
+    return out
+
+
 def gcr_extra(grid=(256, 256, 128), record=20, train=400, compare=5):
     """C5: 3D Boussinesq, FP32 advection with FP64 GCR (cr) to max|err| <= 1e-7/dt;
     (residual, correction) pairs from the first `record` plain solves (their start
@@ -282,7 +328,9 @@ def main():
     ap.add_argument("--n-ref", type=int, default=256)
     ap.add_argument("--dtype", default="float32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched-2D and Boussinesq/GCR measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the 2D rotation, batched-2D and Boussinesq/GCR measurements")
+    ap.add_argument("--extra", choices=["rotation_2d", "batched_2d", "gcr"],
+                    help="run only this one extra measurement on one GPU and print its JSON object")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
@@ -291,6 +339,10 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.extra:
+        fn = {"rotation_2d": rotation_extra, "batched_2d": batched_extra, "gcr": gcr_extra}[args.extra]
+        print(json.dumps({args.extra: fn()}))
+        return
     from libmpdataxx_b200 import _lib, workloads
     w = workloads.advection_3d(n=args.n, dtype=args.dtype)
     run = build_run(w, args.dtype, torch)
@@ -389,6 +441,7 @@ def main():
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if world == 1 and not args.no_extras:
+        line["rotation_2d"] = rotation_extra()
         line["batched_2d"] = batched_extra()
         line["gcr"] = gcr_extra()
     print(json.dumps(line))
