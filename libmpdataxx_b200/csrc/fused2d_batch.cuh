@@ -2,26 +2,26 @@
 // independent problems: tile candidates, work lists and the launcher's
 // declaration (definition in fused_impl.cuh).
 //
-// A work item is one strip (NT - 2H columns) x LX rows of one problem; a
-// grid of resident CTAs (SM count x occupancy) takes items from a counter in
-// global memory until the list is exhausted.  Results do not depend on the
-// tile shape: every output point goes through the same arithmetic whatever
-// strip or row chunk computes it, so the tile can be chosen by timing.
+// A work item is one strip (the columns one warp writes) x LX rows of one
+// problem; a grid of resident warps (SM count x occupancy) takes items from a
+// counter in global memory until the list is exhausted.  Results do not depend
+// on the tile shape: every output point goes through the same arithmetic
+// whatever strip or row chunk computes it, so the tile can be chosen by timing.
 #pragma once
 
 #include <algorithm>
 #include <vector>
 
-#include "fused2d.cuh"
+#include "fused2d_warp.cuh"
 
 namespace mpdx {
 
-// tile candidates of the autotuner: strip width (threads) and rows per item
+// tile candidates of the autotuner: threads per item (one warp) and rows per item
 struct batch_tile {
   int nt, lx;
 };
-constexpr int kNumBatchTiles = 6;
-constexpr batch_tile kBatchTiles[kNumBatchTiles] = {{128, 32}, {128, 64}, {256, 32}, {256, 64}, {256, 128}, {512, 64}};
+constexpr int kNumBatchTiles = 4;
+constexpr batch_tile kBatchTiles[kNumBatchTiles] = {{32, 16}, {32, 32}, {32, 64}, {32, 128}};
 
 // launch (or, with occ, return the resident CTAs per SM of) tile candidate
 // `tile` of the persistent kernel; instantiated per real type in fused_f32.cu /
@@ -33,7 +33,7 @@ int fused2d_batched(int tile, int ni, bool iga, bool fct, const f2::prob<T> *pro
 // work list of tile candidate `tile` for problems of periods (P0, P1); larger
 // problems first so that the tail of the list holds the small items
 inline std::vector<f2::item> fused2d_batch_items(int tile, int ni, const std::vector<int> &P0, const std::vector<int> &P1) {
-  const int H = ni == 3 ? 6 : 4, TJ = kBatchTiles[tile].nt - 2 * H, LX = kBatchTiles[tile].lx;
+  const int TJ = ni == 3 ? f2w::shape<3>::WV : f2w::shape<2>::WV, LX = kBatchTiles[tile].lx;
   std::vector<int> order(P0.size());
   for (size_t p = 0; p < order.size(); ++p) order[p] = int(p);
   std::stable_sort(order.begin(), order.end(),

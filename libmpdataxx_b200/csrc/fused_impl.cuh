@@ -4,7 +4,6 @@
 #pragma once
 
 #include "fused.cuh"
-#include "fused2d.cuh"
 #include "fused3d.cuh"
 #include "fused2d_batch.cuh"
 
@@ -16,11 +15,9 @@ namespace mpdx {
 template <class T> struct tiles;
 template <> struct tiles<float> {
   static constexpr int CR = 32, LX3 = MPDX_LX3;   // 3D canvas rows (x 64 columns), planes per CTA
-  static constexpr int NT2 = 256, LX2 = 64; // 2D strip width (threads), rows per CTA
 };
 template <> struct tiles<double> {
   static constexpr int CR = 16, LX3 = 64;
-  static constexpr int NT2 = 256, LX2 = 64;
 };
 
 template <class T>
@@ -75,15 +72,23 @@ void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
   else launch3<T, false, false>(a, s, grid);
 }
 
+// 2D: one warp per strip of 128 columns (fused2d_warp.cuh); rows per warp chosen
+// so that small problems still spread over the GPU (the warm-up rows of every
+// chunk are recomputed, so chunks stay at 16 rows or more)
 template <class T, int NI, bool IGA, bool FCT>
 static void launch2(const f2::prob<T> &a, cudaStream_t s) {
-  constexpr int NT = tiles<T>::NT2, LX = tiles<T>::LX2, H = NI == 3 ? 6 : 4;
-  auto kern = f2::k_fused2d<T, NI, IGA, FCT, NT, H>;
-  const size_t bytes = size_t(f2::rows<NI, FCT>::total) * NT * sizeof(T);
-  static bool attr = false;
-  if (!attr) { set_smem(kern, bytes); attr = true; }
-  dim3 grid((a.P1 + (NT - 2 * H) - 1) / (NT - 2 * H), (a.P0 + LX - 1) / LX);
-  kern<<<grid, NT, bytes, s>>>(a, LX);
+  using S = f2w::shape<NI>;
+  static int n_sm = 0;
+  if (!n_sm) {
+    int dev = 0;
+    MPDX_CUDA(cudaGetDevice(&dev));
+    MPDX_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int n_strips = (a.P1 + S::WV - 1) / S::WV;
+  int LX = 64;
+  while (LX > 16 && (long long)n_strips * ((a.P0 + LX - 1) / LX) < 8LL * n_sm) LX /= 2;
+  const int n_warps = n_strips * ((a.P0 + LX - 1) / LX);
+  f2w::k_fused2d_w<T, NI, IGA, FCT><<<(n_warps + 3) / 4, 128, 0, s>>>(a, LX, n_strips, n_warps);
   MPDX_LAUNCH_CHECK();
 }
 
@@ -108,46 +113,33 @@ void fused2d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
-// batched persistent launch (fused2d_batch.cuh)
-template <class T, int NI, bool IGA, bool FCT, int NT>
+// batched persistent launch (fused2d_batch.cuh): blocks of 4 independent warps
+template <class T, int NI, bool IGA, bool FCT>
 static int batched_do(const f2::prob<T> *probs, const f2::item *items, int n_items, int *counter, int grid,
                       cudaStream_t s, bool occupancy_only) {
-  constexpr int H = NI == 3 ? 6 : 4;
-  auto kern = f2::k_fused2d_batched<T, NI, IGA, FCT, NT, H>;
-  const size_t bytes = size_t(f2::rows<NI, FCT>::total) * NT * sizeof(T);
-  static bool attr = false;
-  if (!attr) { set_smem(kern, bytes); attr = true; }
+  auto kern = f2w::k_fused2d_w_batched<T, NI, IGA, FCT>;
   if (occupancy_only) {
     int occ = 0;
-    MPDX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, bytes));
+    MPDX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0));
     return occ;
   }
-  kern<<<grid, NT, bytes, s>>>(probs, items, n_items, counter);
+  kern<<<grid, 128, 0, s>>>(probs, items, n_items, counter);
   MPDX_LAUNCH_CHECK();
   return 0;
-}
-
-template <class T, int NT>
-static int batched_nt(int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
-                      int *counter, int grid, cudaStream_t s, bool occ) {
-  if (ni == 3) {
-    if (fct) return batched_do<T, 3, false, true, NT>(probs, items, n_items, counter, grid, s, occ);
-    return batched_do<T, 3, false, false, NT>(probs, items, n_items, counter, grid, s, occ);
-  }
-  if (iga && fct) return batched_do<T, 2, true, true, NT>(probs, items, n_items, counter, grid, s, occ);
-  if (iga) return batched_do<T, 2, true, false, NT>(probs, items, n_items, counter, grid, s, occ);
-  if (fct) return batched_do<T, 2, false, true, NT>(probs, items, n_items, counter, grid, s, occ);
-  return batched_do<T, 2, false, false, NT>(probs, items, n_items, counter, grid, s, occ);
 }
 
 template <class T>
 int fused2d_batched(int tile, int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
                     int *counter, int grid, cudaStream_t s, bool occ) {
-  switch (kBatchTiles[tile].nt) {
-    case 128: return batched_nt<T, 128>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
-    case 256: return batched_nt<T, 256>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
-    default: return batched_nt<T, 512>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
+  (void)tile;  // the rows per item are in the work list
+  if (ni == 3) {
+    if (fct) return batched_do<T, 3, false, true>(probs, items, n_items, counter, grid, s, occ);
+    return batched_do<T, 3, false, false>(probs, items, n_items, counter, grid, s, occ);
   }
+  if (iga && fct) return batched_do<T, 2, true, true>(probs, items, n_items, counter, grid, s, occ);
+  if (iga) return batched_do<T, 2, true, false>(probs, items, n_items, counter, grid, s, occ);
+  if (fct) return batched_do<T, 2, false, true>(probs, items, n_items, counter, grid, s, occ);
+  return batched_do<T, 2, false, false>(probs, items, n_items, counter, grid, s, occ);
 }
 
 // ---------------------------------------------------------------------------
