@@ -251,7 +251,7 @@ __device__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
 
 // single problem: warp w takes strip w % n_strips of row chunk w / n_strips
 template <class T, int NI, bool IGA, bool FCT>
-__global__ void __launch_bounds__(128) k_fused2d_w(const f2::prob<T> A, int LX, int n_strips, int n_warps) {
+__global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w(const f2::prob<T> A, int LX, int n_strips, int n_warps) {
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= n_warps) return;
   const int x0 = (w / n_strips) * LX;

@@ -113,4 +113,20 @@ __device__ __forceinline__ T qdiv(T a, T b, T y) {
   return fma(r, y, q);
 }
 
+// a / b in FP32, correctly rounded and without a branch, for normal b whose
+// reciprocal is normal and a quotient that neither overflows nor underflows.
+// y0 = rcp.approx(b) (relative error below 2^-22), two Newton-Raphson steps
+// y <- y + y (1 - b y) leave an error of about 2^-70 relative before the last
+// rounding, below the least distance (about 2^-47 relative) of the reciprocal
+// of a 24-bit number from a rounding midpoint, so y = RN(1/b); Markstein's
+// correction (qdiv) then returns RN(a/b).  Checked against the '/' operator by
+// tests/cuda/qdiv_check.cu.
+__device__ __forceinline__ float rdivf(float a, float b) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+  y = fmaf(fmaf(-b, y, 1.0f), y, y);
+  y = fmaf(fmaf(-b, y, 1.0f), y, y);
+  return qdiv(a, b, y);
+}
+
 }  // namespace mpdx

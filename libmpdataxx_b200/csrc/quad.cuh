@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include "mpdx_common.cuh"
+
 namespace mpdx {
 namespace qd {
 
@@ -60,8 +62,10 @@ __device__ __forceinline__ q4<float> operator*(const q4<float> &p, const q4<floa
   return mk(p.a.x * q.a.x, p.a.y * q.a.y, p.b.x * q.b.x, p.b.y * q.b.y);
 }
 #endif
+// FP32 quotients through mpdx::rdivf (correctly rounded, no slow-path branch):
+// the denominators of the formulae are sums plus FLT_MIN or FLT_EPSILON
 __device__ __forceinline__ q4<float> operator/(const q4<float> &p, const q4<float> &q) {
-  return mk(__fdiv_rn(p.a.x, q.a.x), __fdiv_rn(p.a.y, q.a.y), __fdiv_rn(p.b.x, q.b.x), __fdiv_rn(p.b.y, q.b.y));
+  return mk(rdivf(p.a.x, q.a.x), rdivf(p.a.y, q.a.y), rdivf(p.b.x, q.b.x), rdivf(p.b.y, q.b.y));
 }
 __device__ __forceinline__ q4<float> operator-(const q4<float> &p) { return mk(-p.a.x, -p.a.y, -p.b.x, -p.b.y); }
 // p * q + r with one rounding per element (FP32 only; the FP64 path never fuses)

@@ -1,6 +1,9 @@
 // Checks mpdx::qdiv (reciprocal times Markstein correction) against the CUDA
-// '/' operator on random operands over many binades, FP64 and FP32.  Prints
-// the number of mismatches per type and exits non-zero if there is any.
+// '/' operator on random operands over many binades, FP64 and FP32, and
+// mpdx::rdivf (FP32 quotient from an approximate reciprocal refined twice) on
+// random numerators and denominators over 60 binades each, both signs, plus the
+// FCT beta and frac operand ranges.  Prints the number of mismatches and exits
+// non-zero if there is any.
 #include <cstdio>
 
 #include "../../libmpdataxx_b200/csrc/mpdx_common.cuh"
@@ -23,6 +26,36 @@ __global__ void k_check(const T *bs, int nb, long long per_thread, unsigned long
   atomicAdd(bad, nbad);
 }
 
+// random float with a uniformly random 24-bit significand, exponent in [elo, ehi], random sign
+__device__ float rnd_float(unsigned long long &s, int elo, int ehi, bool sign) {
+  const unsigned long long r = xs(s);
+  const int e = elo + int((r >> 40) % unsigned(ehi - elo + 1));
+  const float m = 1.0f + float(r & 0x7fffff) * (1.0f / 8388608.0f);
+  const float v = ldexpf(m, e);
+  return (sign && (r >> 63)) ? -v : v;
+}
+
+__global__ void k_check_rdiv(long long per_thread, unsigned long long *bad) {
+  unsigned long long s = 0xD1B54A32D192ED03ull ^ (blockIdx.x * 2246822519ull + threadIdx.x * 3266489917ull + 7);
+  unsigned long long nbad = 0;
+  for (long long i = 0; i < per_thread; ++i) {
+    // general operands
+    float a = rnd_float(s, -30, 30, true), b = rnd_float(s, -30, 30, true);
+    if (mpdx::rdivf(a, b) != a / b) ++nbad;
+    // FCT betas: (max - psi) / (sum of fluxes + FLT_EPSILON)
+    a = rnd_float(s, -24, 12, false);
+    b = rnd_float(s, -30, 12, false) + 1.1920929e-7f;
+    if (mpdx::rdivf(a, b) != a / b) ++nbad;
+    // frac: (p1 - p0) / ((p1 + p0) + FLT_MIN)
+    const float p1 = rnd_float(s, -20, 10, false), p0 = rnd_float(s, -20, 10, false);
+    a = p1 - p0;
+    b = (p1 + p0) + 1.17549435e-38f;
+    if (mpdx::rdivf(a, b) != a / b) ++nbad;
+  }
+  if (mpdx::rdivf(0.0f, 1.17549435e-38f) != 0.0f) ++nbad;
+  atomicAdd(bad, nbad);
+}
+
 int main() {
   const double bd[] = {10.0, 0.1, 3.0, 7.3, 1e-3, 123.456, 0.75, 1.0 / 3.0, 12.5, 0.01};
   const int nb = 10;
@@ -35,10 +68,16 @@ int main() {
   cudaMemset(dbad, 0, 2 * sizeof(unsigned long long));
   k_check<double><<<148 * 4, 256>>>(dbd, nb, 1000, dbad);
   k_check<float><<<148 * 4, 256>>>(dbf, nb, 1000, dbad + 1);
-  unsigned long long bad[2] = {1, 1};
-  const cudaError_t e = cudaMemcpy(bad, dbad, sizeof(bad), cudaMemcpyDeviceToHost);
+  unsigned long long *dbad2;
+  cudaMalloc(&dbad2, sizeof(unsigned long long));
+  cudaMemset(dbad2, 0, sizeof(unsigned long long));
+  k_check_rdiv<<<148 * 4, 256>>>(4000, dbad2);
+  unsigned long long bad[2] = {1, 1}, bad2 = 1;
+  cudaError_t e = cudaMemcpy(bad, dbad, sizeof(bad), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&bad2, dbad2, sizeof(bad2), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) { std::printf("CUDA error: %s\n", cudaGetErrorString(e)); return 2; }
   const long long n = 148LL * 4 * 256 * 1000 * nb;
   std::printf("qdiv vs '/': %lld operand pairs per type, mismatches fp64 %llu fp32 %llu\n", n, bad[0], bad[1]);
-  return (bad[0] || bad[1]) ? 1 : 0;
+  std::printf("rdivf vs '/': %lld operand pairs, mismatches %llu\n", 148LL * 4 * 256 * 4000 * 3, bad2);
+  return (bad[0] || bad[1] || bad2) ? 1 : 0;
 }
