@@ -129,7 +129,9 @@ def test_boussinesq_fp64_pressure_is_not_viewed_as_fp32():
 
 def test_reciprocal_division_matches_cuda_division(tmp_path):
     """The pressure operators divide by the grid spacing with mpdx::qdiv
-    (reciprocal + Markstein correction); it must return the IEEE quotient."""
+    (reciprocal + Markstein correction) and the FP32 quad kernels divide with
+    mpdx::rdivf (refined reciprocal + Markstein correction); both must return
+    the IEEE quotient."""
     import os
     import subprocess
     here = os.path.dirname(os.path.abspath(__file__))
