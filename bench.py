@@ -246,10 +246,8 @@ def gcr_extra(grid=(256, 256, 128), record=20, train=400, compare=5):
     solves each, plain and learned: iterations and device time per solve."""
     import numpy as np
     from libmpdataxx_b200 import setups
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from runners import bq_run
     s = setups.boussinesq_bubble_3d(*grid)
-    run = bq_run(s, dtype=np.float32, prs_fp64=True)
+    run = setups.boussinesq_run(s, dtype=np.float32, prs_fp64=True)
     run.precond_record(4 * record)
     run.advance(record)
     run.sync()

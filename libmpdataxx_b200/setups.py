@@ -273,3 +273,40 @@ def batched_problems(n=256, seed=5, lo=64, hi=1024, dtype=np.float32, cmax=0.5):
         out.append({"grid": (nx, ny), "bcs": ["cyclic"] * 4, "advectee": [wrap_periodic(psi).astype(dtype)],
                     "advector": [gx.astype(dtype), gy.astype(dtype)]})
     return out
+
+
+def boussinesq_run(setup, opts=None, n_iters=2, dtype=np.float64, prs_scheme=None, prs_fp64=False):
+    """concurr::cuda<solvers::boussinesq<...>> loaded with a Boussinesq set-up
+    (equations (u, [v,] w, tht) as in the reference's tests, boussinesq_2d.cpp:27-30)."""
+    from . import bcond, concurr, solvers
+    nd = len(setup["grid"])
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = dtype
+    ct.n_dims = nd
+    ct.n_eqns = nd + 1
+    ct.opts = o.iga | o.fct if opts is None else opts
+    ct.rhs_scheme = solvers.trapez
+    k = setup.get("prs_k", 1)
+    ct.prs_scheme = prs_scheme if prs_scheme is not None else (solvers.cr if k == 1 else solvers.gcrk)
+    ct.prs_k_iters = k
+
+    class ix:
+        pass
+
+    ix.vip_i, ix.vip_j = 0, 1
+    if nd == 3:
+        ix.vip_k = 2
+    ix.tht = nd
+    ct.ix = ix
+    p = solvers.boussinesq.rt_params_t(grid_size=list(setup["grid"]), n_iters=n_iters, dt=setup["dt"],
+                                       di=setup["dx"][0], dj=setup["dx"][1], dk=setup["dx"][2],
+                                       prs_tol=setup["prs_tol"], g=setup["g"], Tht_ref=setup["tht_ref"],
+                                       prs_fp64=prs_fp64)
+    run = concurr.cuda(solvers.boussinesq(ct), *[getattr(bcond, b) for b in setup["bcs"]], p=p)
+    run.sclr_array("tht_e")[...] = setup["tht_e"]
+    for e, a in enumerate(setup["advectee"]):
+        run.advectee(e)[...] = a
+    return run
