@@ -157,6 +157,32 @@ __device__ __forceinline__ T lap(const F &A, const dfield<T> &lay, const U &u, c
   const int c[3] = {i, j, k};
   const long long o = off3(lay, i, j, k);
   T r = T(0);
+  // Points whose whole stencil (c - 2 .. c + 2 along every axis) is interior: no halo
+  // rule and no wall applies, so LT(c +- 1) = grad(c +- 1) [- u(c +- 1)] and aval is a
+  // plain read.  Same operations in the same order as the general form below.
+  bool inner = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (d < g.nd) inner = inner && c[d] >= 2 && c[d] <= g.n[d] - 3;
+  if (inner) {
+    const T a0 = A(o);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.nd) break;
+      const long long sd = stride(lay, d);
+      const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
+      T gp = mpdx::qdiv<T>(A(o + 2 * sd) - a0, dx, rdx) * T(0.5);
+      T gm = mpdx::qdiv<T>(a0 - A(o - 2 * sd), dx, rdx) * T(0.5);
+      if constexpr (is_vec<U>::value) {
+        const long long usd = stride(u.u[d], d), uo = off3(u.u[d], i, j, k);
+        gp -= T(u.u[d].o[uo + usd]);
+        gm -= T(u.u[d].o[uo - usd]);
+      }
+      const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
+      r = d == 0 ? term : r + term;
+    }
+    return r;
+  }
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (d >= g.nd) break;
