@@ -399,6 +399,150 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
   }
 }
 
+// 3D form of k_gcr_update.  A block owns a tile of kTJ x kTK (j, k) columns and
+// marches along i over a chunk of planes.  The updated error of plane i+2, on the
+// tile plus a halo of 2, goes to a ring of 4 shared planes; the Laplacian at an
+// interior point then reads its j and k neighbours from the plane of i, its i+2
+// neighbour from the plane of i+2 and its i-2 neighbour from its own registers.
+// Points within 2 of a boundary take the general lap.  The arithmetic of every
+// point is k_gcr_update's (same operations in the same order).
+constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 16;
+static_assert(kTJ * kTK == kRedThreads, "one tile column per thread");
+template <class T, int NV>
+__global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_tol, dfield<T> phi, dfield<T> err0,
+                                                                dfield<T> err1, dfield<T> lap_err, dirs<T> D,
+                                                                gcr_dev<T> *dv, double *part, int chunk) {
+  constexpr int v = NV - 1;
+  if (dv->done) return;
+  const int cur = dv->cur;
+  const dfield<T> ea = cur ? err1 : err0, eb = cur ? err0 : err1;
+  const T den = dv->pend_den;
+  const T b = den != T(0) ? -dv->pend_num / den : dv->beta;  // beta keeps its value when tmp_den is 0
+  if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
+  const dfield<T> pv = D.p[v], lpv = D.lp[v];
+  dfield<T> lps[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
+  const fld_axpy<T> enew{ea.o, lpv.o, b};
+  dd acc[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
+  double mx = -DBL_MAX, mn = DBL_MAX;
+
+  __shared__ T pl[4][kPJ][kPK];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTK + tx;
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int nkt = (n2 + kTK - 1) / kTK, njt = (n1 + kTJ - 1) / kTJ, nch = (n0 + chunk - 1) / chunk;
+  const long long n_items = (long long)nkt * njt * nch;
+  constexpr int NQ = (kPJ * kPK + kRedThreads - 1) / kRedThreads;  // tile points per thread
+  auto slot = [](int i) { return i & 3; };  // planes i >= -2: i & 3 is i mod 4
+  for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int kt = int(item % nkt);
+    const long long rest = item / nkt;
+    const int jt = int(rest % njt), ch = int(rest / njt);
+    const int j = jt * kTJ + ty, k = kt * kTK + tx;
+    const int i0 = ch * chunk, i1 = min(i0 + chunk, n0);
+    const bool own = j < n1 && k < n2;
+    const bool colfast = j >= 2 && j <= n1 - 3 && k >= 2 && k <= n2 - 3;
+    // this thread's tile points (with halo) and their offsets within a plane
+    long long qo[NQ];
+    bool qin[NQ];
+#pragma unroll
+    for (int u = 0; u < NQ; ++u) {
+      const int q = tid + u * kRedThreads, pj = q / kPK, pk = q - pj * kPK;
+      const int jj = jt * kTJ - 2 + pj, kk = kt * kTK - 2 + pk;
+      qin[u] = q < kPJ * kPK && jj >= 0 && jj < n1 && kk >= 0 && kk < n2;
+      qo[u] = qin[u] ? off3(ea, 0, jj, kk) : 0;
+    }
+    // err and lap_p of the tile points of one plane, loaded a step before they are used
+    T xa[NQ], xb[NQ];
+    auto load = [&](int i) {
+      const long long io = (long long)i * ea.s0;
+#pragma unroll
+      for (int u = 0; u < NQ; ++u) {
+        const bool ok = qin[u] && i >= 0 && i < n0;
+        xa[u] = ok ? ea.o[io + qo[u]] : T(0);
+        xb[u] = ok ? lpv.o[io + qo[u]] : T(0);
+      }
+    };
+    auto store = [&](int i) {  // enew = err + beta lap_p (fld_axpy)
+      T *P = &pl[slot(i)][0][0];
+#pragma unroll
+      for (int u = 0; u < NQ; ++u) {
+        const int q = tid + u * kRedThreads;
+        if (q < kPJ * kPK) P[q] = xa[u] + b * xb[u];
+      }
+    };
+    __syncthreads();  // the previous item's reads are done
+    for (int i = i0 - 2; i <= i0 + 1; ++i) { load(i); store(i); }
+    load(i0 + 2);
+    __syncthreads();
+    T cm2 = pl[slot(i0 - 2)][ty + 2][tx + 2], cm1 = pl[slot(i0 - 1)][ty + 2][tx + 2];
+    // the own point's Phi, p and lap_p fields, also a step ahead
+    T fphi = T(0), fpv = T(0), flp[NV];
+    auto load_own = [&](int i) {
+      if (own && i < i1) {
+        fphi = phi(i, j, k);
+        fpv = pv(i, j, k);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) flp[l] = lps[l](i, j, k);
+      }
+    };
+    load_own(i0);
+    __syncthreads();  // cm2 is read before plane i0+2 replaces it
+    for (int i = i0; i < i1; ++i) {
+      store(i + 2);
+      load(i + 3);
+      const T cphi = fphi, cpv = fpv;
+      T clp[NV];
+#pragma unroll
+      for (int l = 0; l < NV; ++l) clp[l] = flp[l];
+      load_own(i + 1);
+      __syncthreads();
+      const T c0 = pl[slot(i)][ty + 2][tx + 2];
+      if (own) {
+        T le;
+        if (colfast && i >= 2 && i <= n0 - 3) {
+          const T(*P)[kPK] = pl[slot(i)];
+          const T nb[3][2] = {{pl[slot(i + 2)][ty + 2][tx + 2], cm2},
+                              {P[ty + 4][tx + 2], P[ty][tx + 2]},
+                              {P[ty + 2][tx + 4], P[ty + 2][tx]}};
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
+            const T gp = mpdx::qdiv<T>(nb[d][0] - c0, dx, rdx) * T(0.5);
+            const T gm = mpdx::qdiv<T>(c0 - nb[d][1], dx, rdx) * T(0.5);
+            const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
+            le = d == 0 ? term : le + term;
+          }
+        } else {
+          le = lap<T>(enew, ea, no_u{}, g, i, j, k);
+        }
+        phi(i, j, k) = cphi + b * cpv;
+        eb(i, j, k) = c0;
+        mx = fmax(mx, double(c0));
+        mn = fmin(mn, double(c0));
+        lap_err(i, j, k) = le;
+#pragma unroll
+        for (int l = 0; l < NV; ++l) acc[l] = dd_add(acc[l], dd{double(T(le * clp[l])), 0.0});
+      }
+      cm2 = cm1;
+      cm1 = c0;
+    }
+  }
+  if (grid_reduce<NV, true>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
+    const T amx = fabs(T(mx)), amn = fabs(T(mn));
+    const T error = amx < amn ? amn : amx;  // std::max(|max|, |min|)
+    dv->residual = double(error);
+    if (error <= err_tol) dv->converged = 1;
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const T dl = l == v ? den : dv->tmp_den[l];
+      if (dl != T(0)) dv->alpha[l] = -T(ddv(acc[l])) / dl;
+    }
+  }
+}
+
 // inner step v = NV - 1, second half: next search direction (mpdata_rhs_vip_prs_gcrk.hpp:66-92)
 template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk, dfield<T> err0, dfield<T> err1,
@@ -456,7 +600,8 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk
 template <class T, int NV>
 void launch_inner(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi, dfield<T> e0,
                   dfield<T> e1, dfield<T> le, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
-  k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part);
+  if (g.nd == 3) k_gcr_update3<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part, kGcrChunk);
+  else k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part);
   k_gcr_direction<T, NV><<<G, blk, 0, s>>>(g, kk, e0, e1, le, D, dv, part);
 }
 template <class T>
