@@ -399,14 +399,16 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
   }
 }
 
-// 3D form of k_gcr_update.  A block owns a tile of kTJ x kTK (j, k) columns and
-// marches along i over a chunk of planes.  The updated error of plane i+2, on the
-// tile plus a halo of 2, goes to a ring of 4 shared planes; the Laplacian at an
-// interior point then reads its j and k neighbours from the plane of i, its i+2
-// neighbour from the plane of i+2 and its i-2 neighbour from its own registers.
-// Points within 2 of a boundary take the general lap.  The arithmetic of every
-// point is k_gcr_update's (same operations in the same order).
-constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 16;
+// 3D form of k_gcr_update, in two phases within one launch (one reduction).
+// Interior: the points whose whole stencil lies inside the grid (every coordinate
+// in [2, n-3]).  A block owns a tile of kTJ x kTK (j, k) columns of the interior and
+// marches along i over a chunk of planes; the updated error of plane i+2, on the
+// tile plus a halo of 2, goes to a ring of 4 shared planes, so the Laplacian reads
+// its j and k neighbours from the plane of i, its i+2 neighbour from the plane of
+// i+2 and its i-2 neighbour from the thread's registers.  Shell: the remaining
+// points (within 2 of a face), with the general lap, one point per thread.  The
+// arithmetic of every point is k_gcr_update's (same operations in the same order).
+constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 32;
 static_assert(kTJ * kTK == kRedThreads, "one tile column per thread");
 template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_tol, dfield<T> phi, dfield<T> err0,
@@ -420,49 +422,67 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;  // beta keeps its value when tmp_den is 0
   if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
   const dfield<T> pv = D.p[v], lpv = D.lp[v];
-  dfield<T> lps[NV];
-#pragma unroll
-  for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
   const fld_axpy<T> enew{ea.o, lpv.o, b};
   dd acc[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
   double mx = -DBL_MAX, mn = DBL_MAX;
+  // every pressure-type field has the same layout: one linear offset addresses a
+  // point in all of them
+  T *const phio = phi.o, *const ebo = eb.o, *const leo = lap_err.o;
+  const T *const pvo = pv.o, *const eao = ea.o, *const lpvo = lpv.o;
+  const T *lpo[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) lpo[l] = D.lp[l].o;
+  const long long s0 = ea.s0;
+  // per-point outputs (mpdata_rhs_vip_prs_gcrk.hpp:43-64)
+  auto finish = [&](long long o, T e, T le, T cphi, T cpv, const T *clp) {
+    phio[o] = cphi + b * cpv;
+    ebo[o] = e;
+    mx = fmax(mx, double(e));
+    mn = fmin(mn, double(e));
+    leo[o] = le;
+#pragma unroll
+    for (int l = 0; l < NV; ++l) acc[l] = dd_add(acc[l], dd{double(T(le * clp[l])), 0.0});
+  };
 
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  // ---- interior: column march ----
   __shared__ T pl[4][kPJ][kPK];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTK + tx;
-  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
-  const int nkt = (n2 + kTK - 1) / kTK, njt = (n1 + kTJ - 1) / kTJ, nch = (n0 + chunk - 1) / chunk;
+  const int m0 = n0 - 4, m1 = n1 - 4, m2 = n2 - 4;  // interior extents
+  const int nkt = m2 > 0 ? (m2 + kTK - 1) / kTK : 0, njt = m1 > 0 ? (m1 + kTJ - 1) / kTJ : 0;
+  const int nch = m0 > 0 ? (m0 + chunk - 1) / chunk : 0;
   const long long n_items = (long long)nkt * njt * nch;
   constexpr int NQ = (kPJ * kPK + kRedThreads - 1) / kRedThreads;  // tile points per thread
-  auto slot = [](int i) { return i & 3; };  // planes i >= -2: i & 3 is i mod 4
+  auto slot = [](int i) { return i & 3; };  // i & 3 is i mod 4
   for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int kt = int(item % nkt);
     const long long rest = item / nkt;
     const int jt = int(rest % njt), ch = int(rest / njt);
-    const int j = jt * kTJ + ty, k = kt * kTK + tx;
-    const int i0 = ch * chunk, i1 = min(i0 + chunk, n0);
-    const bool own = j < n1 && k < n2;
-    const bool colfast = j >= 2 && j <= n1 - 3 && k >= 2 && k <= n2 - 3;
+    const int j = 2 + jt * kTJ + ty, k = 2 + kt * kTK + tx;
+    const int i0 = 2 + ch * chunk, i1 = min(i0 + chunk, n0 - 2);
+    const bool own = j < n1 - 2 && k < n2 - 2;
     // this thread's tile points (with halo) and their offsets within a plane
     long long qo[NQ];
     bool qin[NQ];
 #pragma unroll
     for (int u = 0; u < NQ; ++u) {
       const int q = tid + u * kRedThreads, pj = q / kPK, pk = q - pj * kPK;
-      const int jj = jt * kTJ - 2 + pj, kk = kt * kTK - 2 + pk;
-      qin[u] = q < kPJ * kPK && jj >= 0 && jj < n1 && kk >= 0 && kk < n2;
+      const int jj = jt * kTJ + pj, kk = kt * kTK + pk;  // = origin - 2 + offset, origin at 2
+      qin[u] = q < kPJ * kPK && jj < n1 && kk < n2;
       qo[u] = qin[u] ? off3(ea, 0, jj, kk) : 0;
     }
     // err and lap_p of the tile points of one plane, loaded a step before they are used
     T xa[NQ], xb[NQ];
     auto load = [&](int i) {
-      const long long io = (long long)i * ea.s0;
+      const long long io = (long long)i * s0;
+      const bool iok = i < n0;
 #pragma unroll
       for (int u = 0; u < NQ; ++u) {
-        const bool ok = qin[u] && i >= 0 && i < n0;
-        xa[u] = ok ? ea.o[io + qo[u]] : T(0);
-        xb[u] = ok ? lpv.o[io + qo[u]] : T(0);
+        const bool ok = qin[u] && iok;
+        xa[u] = ok ? eao[io + qo[u]] : T(0);
+        xb[u] = ok ? lpvo[io + qo[u]] : T(0);
       }
     };
     auto store = [&](int i) {  // enew = err + beta lap_p (fld_axpy)
@@ -478,14 +498,15 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
     load(i0 + 2);
     __syncthreads();
     T cm2 = pl[slot(i0 - 2)][ty + 2][tx + 2], cm1 = pl[slot(i0 - 1)][ty + 2][tx + 2];
-    // the own point's Phi, p and lap_p fields, also a step ahead
+    const long long colo = own ? off3(ea, 0, j, k) : 0;
     T fphi = T(0), fpv = T(0), flp[NV];
-    auto load_own = [&](int i) {
+    auto load_own = [&](int i) {  // the own point's Phi, p and lap_p, a step ahead
       if (own && i < i1) {
-        fphi = phi(i, j, k);
-        fpv = pv(i, j, k);
+        const long long o = colo + i * s0;
+        fphi = phio[o];
+        fpv = pvo[o];
 #pragma unroll
-        for (int l = 0; l < NV; ++l) flp[l] = lps[l](i, j, k);
+        for (int l = 0; l < NV; ++l) flp[l] = lpo[l][o];
       }
     };
     load_own(i0);
@@ -501,34 +522,50 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
       __syncthreads();
       const T c0 = pl[slot(i)][ty + 2][tx + 2];
       if (own) {
-        T le;
-        if (colfast && i >= 2 && i <= n0 - 3) {
-          const T(*P)[kPK] = pl[slot(i)];
-          const T nb[3][2] = {{pl[slot(i + 2)][ty + 2][tx + 2], cm2},
-                              {P[ty + 4][tx + 2], P[ty][tx + 2]},
-                              {P[ty + 2][tx + 4], P[ty + 2][tx]}};
+        const T(*P)[kPK] = pl[slot(i)];
+        const T nb[3][2] = {{pl[slot(i + 2)][ty + 2][tx + 2], cm2},
+                            {P[ty + 4][tx + 2], P[ty][tx + 2]},
+                            {P[ty + 2][tx + 4], P[ty + 2][tx]}};
+        T le = T(0);
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
-            const T gp = mpdx::qdiv<T>(nb[d][0] - c0, dx, rdx) * T(0.5);
-            const T gm = mpdx::qdiv<T>(c0 - nb[d][1], dx, rdx) * T(0.5);
-            const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
-            le = d == 0 ? term : le + term;
-          }
-        } else {
-          le = lap<T>(enew, ea, no_u{}, g, i, j, k);
+        for (int d = 0; d < 3; ++d) {  // lap: grad(c+1) - grad(c-1), each a centred difference
+          const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
+          const T gp = mpdx::qdiv<T>(nb[d][0] - c0, dx, rdx) * T(0.5);
+          const T gm = mpdx::qdiv<T>(c0 - nb[d][1], dx, rdx) * T(0.5);
+          const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
+          le = d == 0 ? term : le + term;
         }
-        phi(i, j, k) = cphi + b * cpv;
-        eb(i, j, k) = c0;
-        mx = fmax(mx, double(c0));
-        mn = fmin(mn, double(c0));
-        lap_err(i, j, k) = le;
-#pragma unroll
-        for (int l = 0; l < NV; ++l) acc[l] = dd_add(acc[l], dd{double(T(le * clp[l])), 0.0});
+        finish(colo + i * s0, c0, le, cphi, cpv, clp);
       }
       cm2 = cm1;
       cm1 = c0;
     }
+  }
+  // ---- shell: points within 2 of a face ----
+  // i-slabs {0, 1, n0-2, n0-1} x all (j, k); then j-slabs inside them; then k-slabs
+  const int ci0 = n0 < 4 ? n0 : 4, ii = n0 - ci0;                // i layers in the shell, interior i count
+  const int cj0 = n1 < 4 ? n1 : 4, jj = n1 - cj0, ck0 = n2 < 4 ? n2 : 4;
+  const long long sa = (long long)ci0 * n1 * n2, sb = (long long)ii * cj0 * n2, sc = (long long)ii * jj * ck0;
+  auto shell_coord = [](int q, int c, int n) { return q < c / 2 ? q : n - c + q; };  // q-th shell layer
+  const long long nthr = (long long)gridDim.x * kRedThreads;
+  for (long long q = (long long)blockIdx.x * kRedThreads + tid; q < sa + sb + sc; q += nthr) {
+    int i, j, k;
+    if (q < sa) {
+      k = int(q % n2); const long long r = q / n2; j = int(r % n1); i = shell_coord(int(r / n1), ci0, n0);
+    } else if (q < sa + sb) {
+      const long long w = q - sa;
+      k = int(w % n2); const long long r = w / n2; j = shell_coord(int(r % cj0), cj0, n1); i = 2 + int(r / cj0);
+    } else {
+      const long long w = q - sa - sb;
+      k = shell_coord(int(w % ck0), ck0, n2); const long long r = w / ck0; j = 2 + int(r % jj); i = 2 + int(r / jj);
+    }
+    const long long o = off3(ea, i, j, k);
+    const T e = enew(o);
+    const T le = lap<T>(enew, ea, no_u{}, g, i, j, k);
+    T clp[NV];
+#pragma unroll
+    for (int l = 0; l < NV; ++l) clp[l] = lpo[l][o];
+    finish(o, e, le, phio[o], pvo[o], clp);
   }
   if (grid_reduce<NV, true>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     const T amx = fabs(T(mx)), amn = fabs(T(mn));
