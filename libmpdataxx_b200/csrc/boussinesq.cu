@@ -595,28 +595,35 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk
   const bool restart = v == kk - 1;
   const dfield<T> pd = restart ? D.p[0] : D.p[NV < kGcrMaxK ? NV : 0], lpd = restart ? D.lp[0] : D.lp[NV < kGcrMaxK ? NV : 0];
   dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  // every pressure-type field has the same layout: one linear offset per point
+  const T *const eo = e.o, *const leo = lap_err.o;
+  T *const pdo = pd.o, *const lpdo = lpd.o;
+  const T *po[NV], *lpo[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) { po[l] = ps[l].o; lpo[l] = lps[l].o; }
   for_interior(g, [&](int i, int j, int k) {
-    const T ev = e(i, j, k);
+    const long long o = off3(e, i, j, k);
+    const T ev = eo[o];
     T pn, ln;
     if (!restart) {
       pn = ev;
-      ln = lap_err(i, j, k);
+      ln = leo[o];
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
-        pn = pn + a[l] * ps[l](i, j, k);
-        ln = ln + a[l] * lps[l](i, j, k);
+        pn = pn + a[l] * po[l][o];
+        ln = ln + a[l] * lpo[l][o];
       }
     } else {
-      pn = ev + a[0] * ps[0](i, j, k);
-      ln = lap_err(i, j, k) + a[0] * lps[0](i, j, k);
+      pn = ev + a[0] * po[0][o];
+      ln = leo[o] + a[0] * lpo[0][o];
 #pragma unroll
       for (int l = 1; l < NV; ++l) {
-        pn = pn + a[l] * ps[l](i, j, k);
-        ln = ln + a[l] * lps[l](i, j, k);
+        pn = pn + a[l] * po[l][o];
+        ln = ln + a[l] * lpo[l][o];
       }
     }
-    pd(i, j, k) = pn;
-    lpd(i, j, k) = ln;
+    pdo[o] = pn;
+    lpdo[o] = ln;
     acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
     acc[1] = dd_add(acc[1], dd{double(T(ev * ln)), 0.0});
   });
