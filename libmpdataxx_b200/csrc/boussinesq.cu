@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
 
 // inner step v = NV - 1, second half: next search direction (mpdata_rhs_vip_prs_gcrk.hpp:66-92)
 template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk, dfield<T> err0, dfield<T> err1,
+__global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk, dfield<T> err0, dfield<T> err1,
                                                                   dfield<T> lap_err, dirs<T> D, gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
   if (dv->done) return;
@@ -601,32 +601,56 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction(geom g, int kk
   const T *po[NV], *lpo[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) { po[l] = ps[l].o; lpo[l] = lps[l].o; }
-  for_interior(g, [&](int i, int j, int k) {
-    const long long o = off3(e, i, j, k);
-    const T ev = eo[o];
-    T pn, ln;
-    if (!restart) {
-      pn = ev;
-      ln = leo[o];
+  // U points per thread and pass, all loads issued before the arithmetic (memory-level parallelism)
+  constexpr int U = NV == 1 ? 4 : (NV <= 4 ? 2 : 1);
+  for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < g.nrows; row += gridDim.x * blockDim.y) {
+    int i = row, j = 0;
+    if (g.nd == 3) { i = row / g.n[1]; j = row - i * g.n[1]; }
+    for (int f0 = threadIdx.x; f0 < g.nf; f0 += U * blockDim.x) {
+      long long o[U];
+      bool ok[U];
+      T ev[U], le[U], pv[U][NV], lv[U][NV];
 #pragma unroll
-      for (int l = 0; l < NV; ++l) {
-        pn = pn + a[l] * po[l][o];
-        ln = ln + a[l] * lpo[l][o];
+      for (int u = 0; u < U; ++u) {
+        const int f = f0 + u * blockDim.x;
+        ok[u] = f < g.nf;
+        o[u] = ok[u] ? (g.nd == 3 ? off3(e, i, j, f) : off3(e, i, f, 0)) : 0;
+        ev[u] = ok[u] ? eo[o[u]] : T(0);
+        le[u] = ok[u] ? leo[o[u]] : T(0);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          pv[u][l] = ok[u] ? po[l][o[u]] : T(0);
+          lv[u][l] = ok[u] ? lpo[l][o[u]] : T(0);
+        }
       }
-    } else {
-      pn = ev + a[0] * po[0][o];
-      ln = leo[o] + a[0] * lpo[0][o];
 #pragma unroll
-      for (int l = 1; l < NV; ++l) {
-        pn = pn + a[l] * po[l][o];
-        ln = ln + a[l] * lpo[l][o];
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        T pn, ln;
+        if (!restart) {
+          pn = ev[u];
+          ln = le[u];
+#pragma unroll
+          for (int l = 0; l < NV; ++l) {
+            pn = pn + a[l] * pv[u][l];
+            ln = ln + a[l] * lv[u][l];
+          }
+        } else {
+          pn = ev[u] + a[0] * pv[u][0];
+          ln = le[u] + a[0] * lv[u][0];
+#pragma unroll
+          for (int l = 1; l < NV; ++l) {
+            pn = pn + a[l] * pv[u][l];
+            ln = ln + a[l] * lv[u][l];
+          }
+        }
+        pdo[o[u]] = pn;
+        lpdo[o[u]] = ln;
+        acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
+        acc[1] = dd_add(acc[1], dd{double(T(ev[u] * ln)), 0.0});
       }
     }
-    pdo[o] = pn;
-    lpdo[o] = ln;
-    acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
-    acc[1] = dd_add(acc[1], dd{double(T(ev * ln)), 0.0});
-  });
+  }
   double mx = 0, mn = 0;
   if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     dv->pend_den = T(ddv(acc[0]));
