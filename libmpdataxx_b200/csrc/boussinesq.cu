@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
 // i+2 and its i-2 neighbour from the thread's registers.  Shell: the remaining
 // points (within 2 of a face), with the general lap, one point per thread.  The
 // arithmetic of every point is k_gcr_update's (same operations in the same order).
-constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 32;
+constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 32, kSteps = 2;
 static_assert(kTJ * kTK == kRedThreads, "one tile column per thread");
 template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_tol, dfield<T> phi, dfield<T> err0,
@@ -448,14 +448,14 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
 
   const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
   // ---- interior: column march ----
-  __shared__ T pl[4][kPJ][kPK];
+  __shared__ T pl[8][kPJ][kPK];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTK + tx;
   const int m0 = n0 - 4, m1 = n1 - 4, m2 = n2 - 4;  // interior extents
   const int nkt = m2 > 0 ? (m2 + kTK - 1) / kTK : 0, njt = m1 > 0 ? (m1 + kTJ - 1) / kTJ : 0;
   const int nch = m0 > 0 ? (m0 + chunk - 1) / chunk : 0;
   const long long n_items = (long long)nkt * njt * nch;
   constexpr int NQ = (kPJ * kPK + kRedThreads - 1) / kRedThreads;  // tile points per thread
-  auto slot = [](int i) { return i & 3; };  // i & 3 is i mod 4
+  auto slot = [](int i) { return i & 7; };  // i & 7 is i mod 8
   for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int kt = int(item % nkt);
     const long long rest = item / nkt;
@@ -473,72 +473,86 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gcr_update3(geom g, T err_to
       qin[u] = q < kPJ * kPK && jj < n1 && kk < n2;
       qo[u] = qin[u] ? off3(ea, 0, jj, kk) : 0;
     }
-    // err and lap_p of the tile points of one plane, loaded a step before they are used
-    T xa[NQ], xb[NQ];
-    auto load = [&](int i) {
+    // err and lap_p of the tile points of kSteps planes, loaded a pass before they are used
+    T xa[kSteps][NQ], xb[kSteps][NQ];
+    auto load = [&](int i, int q0) {
       const long long io = (long long)i * s0;
       const bool iok = i < n0;
 #pragma unroll
       for (int u = 0; u < NQ; ++u) {
         const bool ok = qin[u] && iok;
-        xa[u] = ok ? eao[io + qo[u]] : T(0);
-        xb[u] = ok ? lpvo[io + qo[u]] : T(0);
+        xa[q0][u] = ok ? eao[io + qo[u]] : T(0);
+        xb[q0][u] = ok ? lpvo[io + qo[u]] : T(0);
       }
     };
-    auto store = [&](int i) {  // enew = err + beta lap_p (fld_axpy)
+    auto store = [&](int i, int q0) {  // enew = err + beta lap_p (fld_axpy)
       T *P = &pl[slot(i)][0][0];
 #pragma unroll
       for (int u = 0; u < NQ; ++u) {
         const int q = tid + u * kRedThreads;
-        if (q < kPJ * kPK) P[q] = xa[u] + b * xb[u];
+        if (q < kPJ * kPK) P[q] = xa[q0][u] + b * xb[q0][u];
       }
     };
     __syncthreads();  // the previous item's reads are done
-    for (int i = i0 - 2; i <= i0 + 1; ++i) { load(i); store(i); }
-    load(i0 + 2);
+    for (int i = i0 - 2; i <= i0 + 1; ++i) { load(i, 0); store(i, 0); }
+#pragma unroll
+    for (int q0 = 0; q0 < kSteps; ++q0) load(i0 + 2 + q0, q0);
     __syncthreads();
     T cm2 = pl[slot(i0 - 2)][ty + 2][tx + 2], cm1 = pl[slot(i0 - 1)][ty + 2][tx + 2];
     const long long colo = own ? off3(ea, 0, j, k) : 0;
-    T fphi = T(0), fpv = T(0), flp[NV];
-    auto load_own = [&](int i) {  // the own point's Phi, p and lap_p, a step ahead
+    T fphi[kSteps], fpv[kSteps], flp[kSteps][NV];
+    auto load_own = [&](int i, int q0) {  // the own point's Phi, p and lap_p, a pass ahead
       if (own && i < i1) {
         const long long o = colo + i * s0;
-        fphi = phio[o];
-        fpv = pvo[o];
+        fphi[q0] = phio[o];
+        fpv[q0] = pvo[o];
 #pragma unroll
-        for (int l = 0; l < NV; ++l) flp[l] = lpo[l][o];
+        for (int l = 0; l < NV; ++l) flp[q0][l] = lpo[l][o];
       }
     };
-    load_own(i0);
-    __syncthreads();  // cm2 is read before plane i0+2 replaces it
-    for (int i = i0; i < i1; ++i) {
-      store(i + 2);
-      load(i + 3);
-      const T cphi = fphi, cpv = fpv;
-      T clp[NV];
 #pragma unroll
-      for (int l = 0; l < NV; ++l) clp[l] = flp[l];
-      load_own(i + 1);
-      __syncthreads();
-      const T c0 = pl[slot(i)][ty + 2][tx + 2];
-      if (own) {
-        const T(*P)[kPK] = pl[slot(i)];
-        const T nb[3][2] = {{pl[slot(i + 2)][ty + 2][tx + 2], cm2},
-                            {P[ty + 4][tx + 2], P[ty][tx + 2]},
-                            {P[ty + 2][tx + 4], P[ty + 2][tx]}};
-        T le = T(0);
+    for (int q0 = 0; q0 < kSteps; ++q0) load_own(i0 + q0, q0);
+    // kSteps planes per barrier: the ring of 8 shared planes holds the 4 planes a pass
+    // reads (i .. i+kSteps+1) and the kSteps planes the next pass writes
+    for (int i = i0; i < i1; i += kSteps) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {  // lap: grad(c+1) - grad(c-1), each a centred difference
-          const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
-          const T gp = mpdx::qdiv<T>(nb[d][0] - c0, dx, rdx) * T(0.5);
-          const T gm = mpdx::qdiv<T>(c0 - nb[d][1], dx, rdx) * T(0.5);
-          const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
-          le = d == 0 ? term : le + term;
-        }
-        finish(colo + i * s0, c0, le, cphi, cpv, clp);
+      for (int q0 = 0; q0 < kSteps; ++q0) store(i + 2 + q0, q0);
+#pragma unroll
+      for (int q0 = 0; q0 < kSteps; ++q0) load(i + 2 + kSteps + q0, q0);
+      T cphi[kSteps], cpv[kSteps], clp[kSteps][NV];
+#pragma unroll
+      for (int q0 = 0; q0 < kSteps; ++q0) {
+        cphi[q0] = fphi[q0];
+        cpv[q0] = fpv[q0];
+#pragma unroll
+        for (int l = 0; l < NV; ++l) clp[q0][l] = flp[q0][l];
       }
-      cm2 = cm1;
-      cm1 = c0;
+#pragma unroll
+      for (int q0 = 0; q0 < kSteps; ++q0) load_own(i + kSteps + q0, q0);
+      __syncthreads();
+#pragma unroll
+      for (int q0 = 0; q0 < kSteps; ++q0) {
+        const int ip = i + q0;
+        const T c0 = pl[slot(ip)][ty + 2][tx + 2];
+        if (own && ip < i1) {
+          const T(*P)[kPK] = pl[slot(ip)];
+          const T nb[3][2] = {{pl[slot(ip + 2)][ty + 2][tx + 2], cm2},
+                              {P[ty + 4][tx + 2], P[ty][tx + 2]},
+                              {P[ty + 2][tx + 4], P[ty + 2][tx]}};
+          T le = T(0);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {  // lap: grad(c+1) - grad(c-1), each a centred difference
+            const T dx = g.dx<T>(d), rdx = g.rdx<T>(d);
+            const T gp = mpdx::qdiv<T>(nb[d][0] - c0, dx, rdx) * T(0.5);
+            const T gm = mpdx::qdiv<T>(c0 - nb[d][1], dx, rdx) * T(0.5);
+            const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
+            le = d == 0 ? term : le + term;
+          }
+          finish(colo + ip * s0, c0, le, cphi[q0], cpv[q0], clp[q0]);
+        }
+        cm2 = cm1;
+        cm1 = c0;
+      }
     }
   }
   // ---- shell: points within 2 of a face ----
