@@ -98,14 +98,44 @@ class ClockSampler:
 
 
 def dist_init():
+    """One process per GPU under torchrun (RANK/LOCAL_RANK/WORLD_SIZE from the
+    environment); NCCL between GPUs, gloo where there is no GPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        import torch
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return world, rank, local
+
+
+def max_over_ranks(x, world):
+    """The largest of the ranks' values of x (every rank gets it); x itself on one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(world, units_per_rank, steps, seconds):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank * steps / seconds
+
+
+def dist_done(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def build_run(w, dtype, torch):
@@ -313,7 +343,7 @@ def reference_arm(args, rank):
                              "sample": f"{n}^3 grid per step (bounded sample of the {args.n}^3 workload); CPU restatement of the reference "
                                        "(reference unbuildable here: Blitz++/Boost absent), -Ofast + OpenMP"},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -330,10 +360,11 @@ def main():
     ap.add_argument("--extra", choices=["rotation_2d", "batched_2d", "gcr"],
                     help="run only this one extra measurement on one GPU and print its JSON object")
     args = ap.parse_args()
-    world, rank, local = dist_init()
     if args.impl == "reference":
-        reference_arm(args, rank)
+        # CPU work on rank 0 alone: no process group (the other ranks exit at once)
+        reference_arm(args, int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_init()
 
     import torch
     torch.cuda.set_device(local)
@@ -373,14 +404,9 @@ def main():
     barrier()
     clocks = sampler.stop()
     per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    ms_total = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ev[0].elapsed_time(ev[-1]), world)
     ms_step = ms_total / args.steps
-    value = world * n_cells * args.steps / (ms_total / 1e3)
+    value = aggregate(world, n_cells, args.steps, ms_total / 1e3)
 
     # end-to-end through the public API: every step uploads its inputs from
     # pinned host memory, advances one step and reads the result back
@@ -400,15 +426,12 @@ def main():
         run.advance(1)
         run.L.mpdx_get_field(run.h, _lib.FIELD_ADVECTEE, 0, host_out.data_ptr(), None)
     run.sync()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * n_cells * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = aggregate(world, n_cells, e2e_steps, e2e_s)
 
     if rank != 0:
+        run.close()
+        dist_done(world)
         return
     hbm, src = peaks()
     avg_launch_ms = statistics.mean(per)
@@ -442,8 +465,9 @@ def main():
         line["rotation_2d"] = rotation_extra()
         line["batched_2d"] = batched_extra()
         line["gcr"] = gcr_extra()
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
     run.close()
+    dist_done(world)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,61 @@
+"""The multi-process plumbing of bench.py on CPU: two gloo ranks on 127.0.0.1.
+The timed value is the maximum over ranks, the aggregate counts every rank's
+work, and under torchrun the reference arm prints one JSON line from rank 0
+while the other rank exits 0 without work."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    import bench
+    w, r, _ = bench.dist_init()
+    t = bench.max_over_ranks(1.5 + rank, w)          # rank 1 is the slower one
+    v = bench.aggregate(w, 1000.0, 10, t)
+    out.put((r, w, t, v))
+    bench.dist_done(w)
+
+
+def test_max_over_ranks_and_aggregate_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for r, w, t, v in res:
+        assert w == 2 and t == 2.5
+        assert v == pytest.approx(2 * 1000.0 * 10 / 2.5)
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--n-ref", "24"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
