@@ -409,7 +409,9 @@ def main():
     value = aggregate(world, n_cells, args.steps, ms_total / 1e3)
 
     # end-to-end through the public API: every step uploads its inputs from
-    # pinned host memory, advances one step and reads the result back
+    # pinned host memory, advances one step and reads the result back, with the
+    # asynchronous transfer entry points (the upload of step k+1's advector
+    # overlaps the download of step k's advectee)
     host_in = [a.cpu().pin_memory() for a in w["advectee"] + w["advector"]]
     host_out = torch.empty_like(w["advectee"][0], device="cpu").pin_memory()
     itemsize = host_out.element_size()
@@ -420,11 +422,11 @@ def main():
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        run.set_field(_lib.FIELD_ADVECTEE, 0, host_in[0].numpy())
         for d in range(3):
-            run.set_field(_lib.FIELD_ADVECTOR, d, host_in[1 + d].numpy())
+            run.set_field_async(_lib.FIELD_ADVECTOR, d, host_in[1 + d].data_ptr())
+        run.set_field_async(_lib.FIELD_ADVECTEE, 0, host_in[0].data_ptr())
         run.advance(1)
-        run.L.mpdx_get_field(run.h, _lib.FIELD_ADVECTEE, 0, host_out.data_ptr(), None)
+        run.get_field_async(_lib.FIELD_ADVECTEE, 0, host_out.data_ptr())
     run.sync()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = aggregate(world, n_cells, e2e_steps, e2e_s)

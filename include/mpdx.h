@@ -123,12 +123,23 @@ mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const i
 mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev);
 mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev);
 
+/* Asynchronous transfers for pipelined host loops (no counterpart in the reference):
+ * `host` must be page-locked (pinned) and C-ordered, and must stay valid and
+ * unchanged until mpdx_sync(h) returns.  Uploads and downloads run on two
+ * transfer streams of the handle, each after all compute enqueued before the
+ * call and after the previous asynchronous transfer of the same field; later
+ * compute (mpdx_advance) and the synchronous entry points wait for them.  An
+ * upload of the advector can therefore overlap the download of the previous
+ * step's advectee. */
+mpdx_status mpdx_set_field_async(mpdx_handle h, int kind, int idx, const void *host);
+mpdx_status mpdx_get_field_async(mpdx_handle h, int kind, int idx, void *host);
+
 /* run.advance(nt)  (concurr_common.hpp:380-385 -> solver_common.hpp:270-358).
  * Asynchronous with respect to the host except on the first call (the
  * divergence check of hook_ante_loop reads one device scalar back). */
 mpdx_status mpdx_advance(mpdx_handle h, int64_t nt);
 
-/* Blocks until the handle's stream is idle. */
+/* Blocks until the handle's stream and its transfer streams are idle. */
 mpdx_status mpdx_sync(mpdx_handle h);
 
 /* run.min()/max()/timestep plus FP64 mass and pressure-solver counters

@@ -22,7 +22,7 @@ SCLR_THT_E = 0
 
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
-           "mpdx_get_field_device", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
+           "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
            "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc", "mpdx_batch_create", "mpdx_batch_advance",
            "mpdx_batch_get_info", "mpdx_batch_sync", "mpdx_batch_last_error", "mpdx_batch_destroy",
            "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
@@ -78,7 +78,7 @@ def lib():
     for f in ("mpdx_set_field", "mpdx_get_field"):
         getattr(L, f).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, i64p]
         getattr(L, f).restype = ctypes.c_int
-    for f in ("mpdx_set_field_device", "mpdx_get_field_device"):
+    for f in ("mpdx_set_field_device", "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async"):
         getattr(L, f).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
         getattr(L, f).restype = ctypes.c_int
     L.mpdx_advance.argtypes = [vp, ctypes.c_int64]

@@ -150,6 +150,17 @@ class cuda:
     def get_field_device(self, kind, idx, ptr):
         _check(self.L, self.h, self.L.mpdx_get_field_device(self.h, kind, idx, ctypes.c_void_p(ptr)))
 
+    def set_field_async(self, kind, idx, ptr):
+        """Upload from page-locked host memory at ptr (C order) without waiting;
+        the buffer must stay untouched until sync()."""
+        _check(self.L, self.h, self.L.mpdx_set_field_async(self.h, kind, idx, ctypes.c_void_p(ptr)))
+        self._mirrors.pop((kind, idx), None)
+        self._fresh.discard((kind, idx))
+
+    def get_field_async(self, kind, idx, ptr):
+        """Download into page-locked host memory at ptr (C order), complete after sync()."""
+        _check(self.L, self.h, self.L.mpdx_get_field_async(self.h, kind, idx, ctypes.c_void_p(ptr)))
+
     # -- time stepping ----------------------------------------------------------
     def advance(self, nt):
         self._flush()

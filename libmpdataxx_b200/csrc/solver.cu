@@ -5,6 +5,7 @@
 // through mpdx_set_field / mpdx_get_field / mpdx_stats.
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -34,16 +35,91 @@ __global__ void k_view_copy(dfield<T> f, T *buf, int e0, int e1, int e2, int o0,
   }
 }
 
+// device address and element strides of a field view (element (0, 0, 0) of the view)
+struct view_desc {
+  int nd, ex[3];
+  void *base;
+  long long st[3];
+};
+
+// Asynchronous pinned-memory transfers (mpdx_set_field_async / mpdx_get_field_async):
+// uploads run on their own stream, downloads on another, each after the compute
+// enqueued so far and after the last transfer of the same field; compute and the
+// synchronous entry points wait for every transfer issued before them (join).
+struct async_xfer {
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_compute = nullptr, ev_h2d = nullptr, ev_d2h = nullptr;
+  std::map<std::pair<int, int>, cudaEvent_t> last;
+  bool pending = false;
+  ~async_xfer() {
+    if (h2d) cudaStreamSynchronize(h2d);
+    if (d2h) cudaStreamSynchronize(d2h);
+    for (auto &kv : last) cudaEventDestroy(kv.second);
+    for (cudaEvent_t e : {ev_compute, ev_h2d, ev_d2h}) if (e) cudaEventDestroy(e);
+    if (h2d) cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamDestroy(d2h);
+  }
+  void ensure() {
+    if (h2d) return;
+    MPDX_CUDA(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+    MPDX_CUDA(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&ev_compute, &ev_h2d, &ev_d2h}) MPDX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  // one pitched copy between a C-ordered host array and the view
+  static void copy(const view_desc &v, void *host, int es, bool up, cudaStream_t s) {
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    size_t w = 0, rows = 1, planes = 1, dpitch = 0, dslice_rows = 1;
+    if (v.nd == 3) { w = v.ex[2]; rows = v.ex[1]; planes = v.ex[0]; dpitch = v.st[1]; dslice_rows = size_t(v.st[0] / v.st[1]); }
+    else if (v.nd == 2) { w = v.ex[1]; rows = v.ex[0]; dpitch = v.st[0]; dslice_rows = rows; }
+    else { w = v.ex[0]; dpitch = w; }
+    const cudaPitchedPtr dev = make_cudaPitchedPtr(v.base, dpitch * es, w, dslice_rows);
+    const cudaPitchedPtr hst = make_cudaPitchedPtr(host, w * es, w, rows);
+    p.srcPtr = up ? hst : dev;
+    p.dstPtr = up ? dev : hst;
+    p.extent = make_cudaExtent(w * es, rows, planes);
+    p.kind = up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    MPDX_CUDA(cudaMemcpy3DAsync(&p, s));
+  }
+  void transfer(cudaStream_t compute, int kind, int idx, const view_desc &v, void *host, int es, bool up) {
+    ensure();
+    cudaStream_t s = up ? h2d : d2h;
+    MPDX_CUDA(cudaEventRecord(ev_compute, compute));
+    MPDX_CUDA(cudaStreamWaitEvent(s, ev_compute, 0));
+    cudaEvent_t &e = last[{kind, idx}];
+    if (e) MPDX_CUDA(cudaStreamWaitEvent(s, e, 0));
+    else MPDX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    copy(v, host, es, up, s);
+    MPDX_CUDA(cudaEventRecord(e, s));
+    MPDX_CUDA(cudaEventRecord(up ? ev_h2d : ev_d2h, s));
+    pending = true;
+  }
+  void join(cudaStream_t compute) {
+    if (!pending) return;
+    MPDX_CUDA(cudaStreamWaitEvent(compute, ev_h2d, 0));
+    MPDX_CUDA(cudaStreamWaitEvent(compute, ev_d2h, 0));
+    pending = false;
+  }
+  void sync() {
+    if (h2d) MPDX_CUDA(cudaStreamSynchronize(h2d));
+    if (d2h) MPDX_CUDA(cudaStreamSynchronize(d2h));
+  }
+};
+
 struct solver_base {
   virtual ~solver_base() {
+    xfer_async.reset();
     if (stream) cudaStreamDestroy(stream);
   }
   cudaStream_t stream = nullptr;
   std::string err;
   int dtype = 8;
+  std::unique_ptr<async_xfer> xfer_async{new async_xfer};
   virtual void set_field(int kind, int idx, const void *src, bool device) = 0;
   virtual void get_field(int kind, int idx, void *dst, bool device) = 0;
   virtual void view_extent(int kind, int idx, int ex[3]) = 0;
+  virtual view_desc describe(int kind, int idx) = 0;
+  virtual void invalidate_fused() {}
   virtual void advance(long long nt) = 0;
   virtual void stats(mpdx_step_stats *out) = 0;
   // learned GCR preconditioner (Boussinesq solvers only)
@@ -145,6 +221,16 @@ struct mpdata_solver : solver_base {
   void view_extent(int kind, int idx, int ex[3]) override {
     int off[3]; field<T> *f; view(kind, idx, ex, off, f);
   }
+  view_desc describe(int kind, int idx) override {
+    view_desc d;
+    int off[3]; field<T> *f;
+    view(kind, idx, d.ex, off, f);
+    d.nd = st.nd;
+    d.base = &f->v(off[0], off[1], off[2]);
+    d.st[0] = f->v.s0; d.st[1] = f->v.s1; d.st[2] = f->v.s2;
+    return d;
+  }
+  void invalidate_fused() override { fus.invalidate(); }
   void set_field(int kind, int idx, const void *src, bool device) override {
     int ex[3], off[3]; field<T> *f;
     view(kind, idx, ex, off, f);
@@ -213,6 +299,15 @@ struct boussinesq_solver : solver_base {
   }
   void view_extent(int kind, int idx, int ex[3]) override {
     int off[3]; field<T> *f; view(kind, idx, ex, off, f);
+  }
+  view_desc describe(int kind, int idx) override {
+    view_desc d;
+    int off[3]; field<T> *f;
+    view(kind, idx, d.ex, off, f);
+    d.nd = b->st.nd;
+    d.base = &f->v(off[0], off[1], off[2]);
+    d.st[0] = f->v.s0; d.st[1] = f->v.s1; d.st[2] = f->v.s2;
+    return d;
   }
   void set_field(int kind, int idx, const void *src, bool device) override {
     int ex[3], off[3]; field<T> *f;
@@ -554,6 +649,7 @@ static void strided_pack(const void *src, void *dst, const int ex[3], const int6
 mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, const int64_t *strides) {
   return guarded(h, [&] {
     if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    h->impl->xfer_async->join(h->impl->stream);
     if (!strides) { h->impl->set_field(kind, idx, host, false); return; }
     int ex[3];
     h->impl->view_extent(kind, idx, ex);
@@ -567,6 +663,7 @@ mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, c
 mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const int64_t *strides) {
   return guarded(h, [&] {
     if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    h->impl->xfer_async->join(h->impl->stream);
     if (!strides) { h->impl->get_field(kind, idx, host, false); return; }
     int ex[3];
     h->impl->view_extent(kind, idx, ex);
@@ -580,6 +677,7 @@ mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const i
 mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev) {
   return guarded(h, [&] {
     if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    h->impl->xfer_async->join(h->impl->stream);
     h->impl->set_field(kind, idx, dev, true);
   });
 }
@@ -587,21 +685,46 @@ mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *
 mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev) {
   return guarded(h, [&] {
     if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    h->impl->xfer_async->join(h->impl->stream);
     h->impl->get_field(kind, idx, dev, true);
   });
 }
 
+mpdx_status mpdx_set_field_async(mpdx_handle h, int kind, int idx, const void *host) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    const auto v = h->impl->describe(kind, idx);
+    h->impl->xfer_async->transfer(h->impl->stream, kind, idx, v, const_cast<void *>(host), h->impl->dtype, true);
+    h->impl->invalidate_fused();
+  });
+}
+
+mpdx_status mpdx_get_field_async(mpdx_handle h, int kind, int idx, void *host) {
+  return guarded(h, [&] {
+    if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
+    const auto v = h->impl->describe(kind, idx);
+    h->impl->xfer_async->transfer(h->impl->stream, kind, idx, v, host, h->impl->dtype, false);
+  });
+}
+
 mpdx_status mpdx_advance(mpdx_handle h, int64_t nt) {
-  return guarded(h, [&] { h->impl->advance(nt); });
+  return guarded(h, [&] {
+    h->impl->xfer_async->join(h->impl->stream);
+    h->impl->advance(nt);
+  });
 }
 
 mpdx_status mpdx_sync(mpdx_handle h) {
-  return guarded(h, [&] { MPDX_CUDA(cudaStreamSynchronize(h->impl->stream)); });
+  return guarded(h, [&] {
+    MPDX_CUDA(cudaStreamSynchronize(h->impl->stream));
+    h->impl->xfer_async->sync();
+  });
 }
 
 mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
   return guarded(h, [&] {
     if (!out) throw mpdx::error(MPDX_E_ARG, "null output");
+    h->impl->xfer_async->join(h->impl->stream);
     h->impl->stats(out);
   });
 }
