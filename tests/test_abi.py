@@ -101,3 +101,23 @@ def test_null_arguments():
     assert L.mpdx_create(None, None) == _lib.MPDX_E_ARG
     assert L.mpdx_advance(None, 1) == _lib.MPDX_E_ARG
     assert L.mpdx_last_error(None) == b"invalid handle"
+
+
+def test_option_and_parameter_validation():
+    from libmpdataxx_b200 import opts as o
+    # nug is built for solvers::mpdata only
+    rc, msg = _create(_cfg(solver=_lib.SOLVER_BOUSSINESQ, n_dims=2, n_eqns=3, grid=(8, 8, 1), opts=o.nug | o.fct,
+                           dt=0.1, tht_ref=300.0))
+    assert rc == _lib.MPDX_E_UNSUPPORTED and "nug" in msg
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), upwind_filter_freq=-1))
+    assert rc == _lib.MPDX_E_ARG and "upwind_filter_freq" in msg
+    # unbuilt MPDATA variants are refused whatever else is set
+    for bad in (o.div_2nd, o.fot, o.div_3rd):
+        rc, msg = _create(_cfg(n_dims=3, grid=(8, 8, 8, ), opts=o.iga | bad))
+        assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+
+
+def test_async_transfer_arguments():
+    L = _lib.lib()
+    assert L.mpdx_set_field_async(None, 0, 0, None) == _lib.MPDX_E_ARG
+    assert L.mpdx_get_field_async(None, 0, 0, None) == _lib.MPDX_E_ARG
