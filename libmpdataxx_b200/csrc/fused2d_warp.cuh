@@ -143,9 +143,18 @@ __device__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
   Q eu4 = zero, ed4 = zero;            // betas2 row t-4
   Q gx5 = zero;                        // limited x flux of iteration 2, face t-5
 
+  // rows loaded one step ahead (psi^n t+2, Courant components t+1), reduced modulo
+  // the period by a compare per step
+  int xin = pmod(ts + 2, A.P0), xg = pmod(ts + 1, A.P0);
   for (int t = ts; t <= te; ++t) {
     const Q pnp = n_pn, gx0 = n_gx, gy0 = n_gy;  // psi^n row t+1, GC_x face t, GC_y row t
-    if (t < te) { n_pn = L(A.in, t + 2); n_gx = L(A.g0, t + 1); n_gy = L(A.g1, t + 1); }
+    if (t < te) {
+      n_pn = ldq(A.in, xin, jb, contig, jc);
+      n_gx = ldq(A.g0, xg, jb, contig, jc);
+      n_gy = ldq(A.g1, xg, jb, contig, jc);
+    }
+    if (++xin == A.P0) xin = 0;
+    if (++xg == A.P0) xg = 0;
 
     // ---- psi1(t) (donor-cell, donorcell_formulae.hpp:104-130) ----
     const Q fxp = qflux(pn0, pnp, gx0), fxm = qflux(pn1, pn0, gx1);

@@ -129,8 +129,7 @@ struct canvas {
 // asynchronous copy of one quad of field f (plane x, canvas row offset `ro`,
 // columns kb..kb+3) into shared memory at dst
 template <class T>
-__device__ __forceinline__ void gcopy(T *dst, const dfield<T> &f, int x, long long ro, int kb, bool contig, const int *kc) {
-  const T *p = f.o + (long long)x * f.s0 + ro;
+__device__ __forceinline__ void gcopy_row(T *dst, const T *p, int kb, bool contig, const int *kc) {
   if (contig) {
 #pragma unroll
     for (int h = 0; h < int(sizeof(T) * 4 / 16); ++h) {
@@ -142,6 +141,31 @@ __device__ __forceinline__ void gcopy(T *dst, const dfield<T> &f, int x, long lo
     for (int e = 0; e < 4; ++e) cp_async(dst + e, p + kc[e]);
   }
 }
+// the same for plane x of field f (x already reduced modulo the period)
+template <class T>
+__device__ __forceinline__ void gcopy(T *dst, const dfield<T> &f, int x, long long ro, int kb, bool contig, const int *kc) {
+  gcopy_row(dst, f.o + (long long)x * f.s0 + ro, kb, contig, kc);
+}
+
+// pointer to one row of successive planes of a periodic field, advanced a plane
+// at a time with the wrap done by a compare (no integer division in the loop)
+template <class T>
+struct plane_walker {
+  const T *p;
+  long long step, wrap;
+  int x, P;
+  __device__ void init(const dfield<T> &f, int x0, int P_, long long ro) {
+    P = P_;
+    x = pmod(x0, P);
+    step = f.s0;
+    wrap = (long long)P * f.s0;
+    p = f.o + (long long)x * f.s0 + ro;
+  }
+  __device__ __forceinline__ void next() {
+    p += step;
+    if (++x == P) { x = 0; p -= wrap; }
+  }
+};
 
 template <class T>
 __device__ __forceinline__ T elem(const q4<T> &v, int e) {
@@ -211,15 +235,22 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d(const args<T> A) {
   // Barriers per step: one before the step reads the planes of the previous
   // step, one after psi1(t+1) is stored, and (FCT) one after the y-face
   // pseudo-velocities are stored, so that each row reads the face below it.
+  // rows of the planes the steps prefetch: psi^n t+3, the Courant components t+2
+  plane_walker<T> w_in, w_g0, w_g1, w_g2;
+  w_in.init(A.in, ts + 3, A.P0, ro_in);
+  w_g0.init(A.g0, ts + 2, A.P0, ro_g0);
+  w_g1.init(A.g1, ts + 2, A.P0, ro_g1);
+  w_g2.init(A.g2, ts + 2, A.P0, ro_g2);
   for (int t = ts; t <= x1; ++t) {
     cp_wait_all();
     __syncthreads();
     T *const s0b = sm + C::S0 * N, *const g0b = sm + C::G0 * N, *const g1b = sm + C::G1 * N, *const g2b = sm + C::G2 * N;
-    cp_in(s0b + r_s0.at(4) * N, t + 3);
-    cp_g0(g0b + r_g0.at(3) * N, t + 2);
-    cp_g1(g1b + r_g1.at(2) * N, t + 2);
-    cp_g2(g2b + r_g1.at(2) * N, t + 2);
+    gcopy_row(s0b + r_s0.at(4) * N + me, w_in.p, kb, contig, kc);
+    gcopy_row(g0b + r_g0.at(3) * N + me, w_g0.p, kb, contig, kc);
+    gcopy_row(g1b + r_g1.at(2) * N + me, w_g1.p, kb, contig, kc);
+    gcopy_row(g2b + r_g1.at(2) * N + me, w_g2.p, kb, contig, kc);
     cp_commit();
+    w_in.next(); w_g0.next(); w_g1.next(); w_g2.next();
     const T *S0m = s0b + r_s0.at(0) * N, *S0c = s0b + r_s0.at(1) * N, *S0p = s0b + r_s0.at(2) * N;
     const T *S0pp = s0b + r_s0.at(3) * N;
     const T *G0m = g0b + r_g0.at(0) * N, *G0c = g0b + r_g0.at(1) * N, *G0p = g0b + r_g0.at(2) * N;
