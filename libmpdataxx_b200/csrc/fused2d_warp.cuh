@@ -109,9 +109,11 @@ __device__ __forceinline__ void minmax(const q4<T> &xm, const q4<T> &c, const q4
   mxq = qd::qmax(qd::qmax(qd::qmax(qd::qmax(yp, xm), c), xp), ym);
 }
 
-// one strip of one problem: columns [j0, j0 + WV), rows [x0, x1)
+// one strip of one problem: columns [j0, j0 + WV), rows [x0, x1).  Not inlined:
+// the single-problem and the batched kernels call the same compiled code, so
+// their FP32 results agree bit for bit (FMA contraction is decided once).
 template <class T, int NI, bool IGA, bool FCT>
-__device__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
+__device__ __noinline__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
   static_assert(NI == 2 || (NI == 3 && !IGA), "n_iters 3 is built without iga");
   using Q = q4<T>;
   using S = shape<NI>;
