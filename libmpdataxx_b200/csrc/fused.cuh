@@ -8,21 +8,60 @@
 // solver runs the reference-structured kernels (both paths are CUDA).
 #pragma once
 
+#include <vector>
+
+#include "fused2d.cuh"
 #include "state.cuh"
 
 namespace mpdx {
 
 // launchers (one translation unit per real type)
 template <class T> void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s);
-template <class T> void fused2d_launch(mpdata_state<T> &st, int e, cudaStream_t s);
+template <class T> struct fused2d_plan;
+template <class T> void fused2d_plan_init(const mpdata_state<T> &st, fused2d_plan<T> &p);
+template <class T> void fused2d_launch(const mpdata_state<T> &st, const fused2d_plan<T> &p, int e, cudaStream_t s);
 template <class T> bool fused_seams_consistent(mpdata_state<T> &st, double *scratch);
 template <class T> bool fused_configurable(const mpdata_state<T> &st);
+
+// 2D step descriptor of equation e whose input is time level tl
+template <class T>
+f2::prob<T> fused2d_prob(const mpdata_state<T> &st, int e, int tl) {
+  f2::prob<T> a;
+  a.in = st.psi[e][tl].v;
+  a.out = st.psi[e][tl ^ 1].v;
+  a.g0 = st.GC[0].v; a.g1 = st.GC[1].v;
+  a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1;
+  a.n0 = st.n[0]; a.n1 = st.n[1];
+  return a;
+}
+
+// Device-resident work plan of the 2D kernel for one solver.  The fields never
+// move after setup, so descriptors and work list are written once.
+template <class T>
+struct fused2d_plan {
+  f2::prob<T> *probs = nullptr;  // step descriptors, [equation][input time level]
+  f2::item *items = nullptr;     // strips x row chunks of the problem (problem index 0)
+  int *counter = nullptr;        // work counter and finished warps, re-armed by the kernel
+  int n_items = 0, grid = 0;
+
+  fused2d_plan() = default;
+  fused2d_plan(const fused2d_plan &) = delete;
+  fused2d_plan &operator=(const fused2d_plan &) = delete;
+  ~fused2d_plan() {
+    if (probs) cudaFree(probs);
+    if (items) cudaFree(items);
+    if (counter) cudaFree(counter);
+  }
+};
 
 template <class T>
 struct fused_engine {
   int known = -1;  // cached seam check: -1 unknown, 0 inconsistent, 1 consistent
+  fused2d_plan<T> plan2;
 
-  void init(const mpdata_state<T> &) {}
+  void init(const mpdata_state<T> &st) {
+    if (st.nd == 2) fused2d_plan_init(st, plan2);
+  }
 
   static bool configurable(const mpdata_state<T> &st) { return fused_configurable(st); }
 
@@ -35,7 +74,7 @@ struct fused_engine {
   void step(mpdata_state<T> &st) {
     for (int e = 0; e < st.n_eqns; ++e) {
       if (st.nd == 3) fused3d_launch(st, e, st.stream);
-      else fused2d_launch(st, e, st.stream);
+      else fused2d_launch(st, plan2, e, st.stream);
       st.tl[e] ^= 1;
     }
   }

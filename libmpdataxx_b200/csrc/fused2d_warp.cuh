@@ -109,11 +109,9 @@ __device__ __forceinline__ void minmax(const q4<T> &xm, const q4<T> &c, const q4
   mxq = qd::qmax(qd::qmax(qd::qmax(qd::qmax(yp, xm), c), xp), ym);
 }
 
-// one strip of one problem: columns [j0, j0 + WV), rows [x0, x1).  Not inlined:
-// the single-problem and the batched kernels call the same compiled code, so
-// their FP32 results agree bit for bit (FMA contraction is decided once).
+// one strip of one problem: columns [j0, j0 + WV), rows [x0, x1)
 template <class T, int NI, bool IGA, bool FCT>
-__device__ __noinline__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
+__device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int x1) {
   static_assert(NI == 2 || (NI == 3 && !IGA), "n_iters 3 is built without iga");
   using Q = q4<T>;
   using S = shape<NI>;
@@ -260,29 +258,33 @@ __device__ __noinline__ void march(const f2::prob<T> &A, int j0, int x0, int x1)
   }
 }
 
-// single problem: warp w takes strip w % n_strips of row chunk w / n_strips
+// The one 2D kernel, for the single-problem and the batched advance alike:
+// persistent warps take work items (problem, strip, rows) from counter[0] until
+// the list of n_items is exhausted (no warp waits on another).  One kernel with
+// one call site of march keeps the FP32 arithmetic of both advances the same
+// compiled code, so their results agree bit for bit (FMA contraction is decided
+// once).  The last warp to finish re-arms the counter (counter[1] counts the
+// finished warps), so consecutive launches on one stream need no reset.
 template <class T, int NI, bool IGA, bool FCT>
-__global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w(const f2::prob<T> A, int LX, int n_strips, int n_warps) {
-  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (w >= n_warps) return;
-  const int x0 = (w / n_strips) * LX;
-  march<T, NI, IGA, FCT>(A, (w % n_strips) * shape<NI>::WV, x0, min(x0 + LX, A.P0));
-}
-
-// batched: persistent warps take work items (problem, strip, rows) from a
-// counter in global memory until the list is exhausted (no warp waits on another)
-template <class T, int NI, bool IGA, bool FCT>
-__global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w_batched(const f2::prob<T> *probs, const f2::item *items, int n_items,
-                                                           int *counter) {
+__global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w(const f2::prob<T> *probs, const f2::item *items,
+                                                                   int n_items, int *counter) {
   const int lane = threadIdx.x & 31;
   for (;;) {
-    int w = 0;
-    if (lane == 0) w = atomicAdd(counter, 1);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    if (w >= n_items) break;
-    const f2::item it = items[w];
+    int q = 0;
+    if (lane == 0) q = atomicAdd(counter, 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= n_items) break;
+    const f2::item it = items[q];
     const f2::prob<T> A = probs[it.prob];
     march<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
+  }
+  if (lane == 0) {
+    __threadfence();  // this warp's last take from counter[0] precedes its count
+    const int n_warps = int(gridDim.x) * int(blockDim.x >> 5);
+    if (atomicAdd(counter + 1, 1) == n_warps - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
   }
 }
 

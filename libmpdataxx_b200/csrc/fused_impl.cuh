@@ -72,52 +72,43 @@ void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
   else launch3<T, false, false>(a, s, grid);
 }
 
-// 2D: one warp per strip of 128 columns (fused2d_warp.cuh); rows per warp chosen
-// so that small problems still spread over the GPU (the warm-up rows of every
-// chunk are recomputed, so chunks stay at 16 rows or more)
-template <class T, int NI, bool IGA, bool FCT>
-static void launch2(const f2::prob<T> &a, cudaStream_t s) {
-  using S = f2w::shape<NI>;
-  static int n_sm = 0;
-  if (!n_sm) {
-    int dev = 0;
-    MPDX_CUDA(cudaGetDevice(&dev));
-    MPDX_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-  }
-  const int n_strips = (a.P1 + S::WV - 1) / S::WV;
-  int LX = 64;
-  while (LX > 16 && (long long)n_strips * ((a.P0 + LX - 1) / LX) < 8LL * n_sm) LX /= 2;
-  const int n_warps = n_strips * ((a.P0 + LX - 1) / LX);
-  f2w::k_fused2d_w<T, NI, IGA, FCT><<<(n_warps + 3) / 4, 128, 0, s>>>(a, LX, n_strips, n_warps);
-  MPDX_LAUNCH_CHECK();
-}
-
+// 2D: one warp per item of one strip (128 columns) x LX rows; the rows per item
+// are chosen so that small problems still spread over the GPU (the warm-up rows
+// of every chunk are recomputed, so chunks stay at 16 rows or more)
 template <class T>
-void fused2d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
-  f2::prob<T> a;
-  a.in = st.psi[e][st.tl[e]].v;
-  a.out = st.psi[e][st.tl[e] ^ 1].v;
-  a.g0 = st.GC[0].v; a.g1 = st.GC[1].v;
-  a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1;
-  a.n0 = st.n[0]; a.n1 = st.n[1];
-  const bool iga = st.opts & o_iga, fct = st.opts & o_fct;
-  if (st.n_iters == 3) {
-    if (fct) launch2<T, 3, false, true>(a, s);
-    else launch2<T, 3, false, false>(a, s);
-  } else {
-    if (iga && fct) launch2<T, 2, true, true>(a, s);
-    else if (iga) launch2<T, 2, true, false>(a, s);
-    else if (fct) launch2<T, 2, false, true>(a, s);
-    else launch2<T, 2, false, false>(a, s);
-  }
+void fused2d_plan_init(const mpdata_state<T> &st, fused2d_plan<T> &p) {
+  int dev = 0, n_sm = 0;
+  MPDX_CUDA(cudaGetDevice(&dev));
+  MPDX_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  const int P0 = st.n[0] - 1, P1 = st.n[1] - 1;
+  const int WV = st.n_iters == 3 ? f2w::shape<3>::WV : f2w::shape<2>::WV;
+  const int n_strips = (P1 + WV - 1) / WV;
+  int LX = 64;
+  while (LX > 16 && (long long)n_strips * ((P0 + LX - 1) / LX) < 8LL * n_sm) LX /= 2;
+  std::vector<f2::item> items;
+  for (int x0 = 0; x0 < P0; x0 += LX)
+    for (int j0 = 0; j0 < P1; j0 += WV) items.push_back({0, j0, x0, std::min(x0 + LX, P0)});
+  std::vector<f2::prob<T>> pr(2 * st.n_eqns);
+  for (int e = 0; e < st.n_eqns; ++e)
+    for (int tl = 0; tl < 2; ++tl) pr[2 * e + tl] = fused2d_prob(st, e, tl);
+  MPDX_CUDA(cudaMalloc(&p.probs, pr.size() * sizeof(f2::prob<T>)));
+  MPDX_CUDA(cudaMalloc(&p.items, items.size() * sizeof(f2::item)));
+  MPDX_CUDA(cudaMalloc(&p.counter, 2 * sizeof(int)));
+  MPDX_CUDA(cudaMemcpy(p.probs, pr.data(), pr.size() * sizeof(f2::prob<T>), cudaMemcpyHostToDevice));
+  MPDX_CUDA(cudaMemcpy(p.items, items.data(), items.size() * sizeof(f2::item), cudaMemcpyHostToDevice));
+  MPDX_CUDA(cudaMemset(p.counter, 0, 2 * sizeof(int)));
+  MPDX_CUDA(cudaDeviceSynchronize());
+  p.n_items = int(items.size());
+  p.grid = (p.n_items + 3) / 4;  // one warp per item, blocks of 4 warps
 }
 
 // ---------------------------------------------------------------------------
-// batched persistent launch (fused2d_batch.cuh): blocks of 4 independent warps
+// the 2D kernel for given options: launch it (or, with occupancy_only, return
+// its resident CTAs per SM)
 template <class T, int NI, bool IGA, bool FCT>
-static int batched_do(const f2::prob<T> *probs, const f2::item *items, int n_items, int *counter, int grid,
-                      cudaStream_t s, bool occupancy_only) {
-  auto kern = f2w::k_fused2d_w_batched<T, NI, IGA, FCT>;
+static int launch2(const f2::prob<T> *probs, const f2::item *items, int n_items, int *counter, int grid,
+                   cudaStream_t s, bool occupancy_only) {
+  auto kern = f2w::k_fused2d_w<T, NI, IGA, FCT>;
   if (occupancy_only) {
     int occ = 0;
     MPDX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0));
@@ -129,17 +120,31 @@ static int batched_do(const f2::prob<T> *probs, const f2::item *items, int n_ite
 }
 
 template <class T>
+static int launch2_opts(int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
+                        int *counter, int grid, cudaStream_t s, bool occ) {
+  if (ni == 3) {
+    if (fct) return launch2<T, 3, false, true>(probs, items, n_items, counter, grid, s, occ);
+    return launch2<T, 3, false, false>(probs, items, n_items, counter, grid, s, occ);
+  }
+  if (iga && fct) return launch2<T, 2, true, true>(probs, items, n_items, counter, grid, s, occ);
+  if (iga) return launch2<T, 2, true, false>(probs, items, n_items, counter, grid, s, occ);
+  if (fct) return launch2<T, 2, false, true>(probs, items, n_items, counter, grid, s, occ);
+  return launch2<T, 2, false, false>(probs, items, n_items, counter, grid, s, occ);
+}
+
+template <class T>
+void fused2d_launch(const mpdata_state<T> &st, const fused2d_plan<T> &p, int e, cudaStream_t s) {
+  launch2_opts<T>(st.n_iters, st.opts & o_iga, st.opts & o_fct, p.probs + 2 * e + st.tl[e], p.items, p.n_items,
+                  p.counter, p.grid, s, false);
+}
+
+// batched persistent launch (fused2d_batch.cuh): the same kernel over the work
+// list of many problems
+template <class T>
 int fused2d_batched(int tile, int ni, bool iga, bool fct, const f2::prob<T> *probs, const f2::item *items, int n_items,
                     int *counter, int grid, cudaStream_t s, bool occ) {
   (void)tile;  // the rows per item are in the work list
-  if (ni == 3) {
-    if (fct) return batched_do<T, 3, false, true>(probs, items, n_items, counter, grid, s, occ);
-    return batched_do<T, 3, false, false>(probs, items, n_items, counter, grid, s, occ);
-  }
-  if (iga && fct) return batched_do<T, 2, true, true>(probs, items, n_items, counter, grid, s, occ);
-  if (iga) return batched_do<T, 2, true, false>(probs, items, n_items, counter, grid, s, occ);
-  if (fct) return batched_do<T, 2, false, true>(probs, items, n_items, counter, grid, s, occ);
-  return batched_do<T, 2, false, false>(probs, items, n_items, counter, grid, s, occ);
+  return launch2_opts<T>(ni, iga, fct, probs, items, n_items, counter, grid, s, occ);
 }
 
 // ---------------------------------------------------------------------------

@@ -371,7 +371,7 @@ struct batch_impl : batch_base {
   f2::prob<T> *probs_dev = nullptr;  // [2][n]: step parity 0 and 1
   f2::item *items_dev = nullptr;
   size_t items_cap = 0;
-  int *counter = nullptr;            // one per parity
+  int *counter = nullptr;            // work counter and finished warps, re-armed by the kernel
   cudaGraphExec_t graph = nullptr;   // two steps (parity 0, then 1)
   long long cells = 0;
 
@@ -396,6 +396,7 @@ struct batch_impl : batch_base {
     MPDX_CUDA(cudaEventCreate(&ev_b));
     MPDX_CUDA(cudaMalloc(&probs_dev, 2 * hs.size() * sizeof(f2::prob<T>)));
     MPDX_CUDA(cudaMalloc(&counter, 2 * sizeof(int)));
+    MPDX_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(int), stream));
     int dev = 0;
     MPDX_CUDA(cudaGetDevice(&dev));
     MPDX_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
@@ -431,9 +432,8 @@ struct batch_impl : batch_base {
     items_tile = t;
   }
   void one_step(int parity) {
-    MPDX_CUDA(cudaMemsetAsync(counter + parity, 0, sizeof(int), stream));
-    fused2d_batched<T>(items_tile, ni, iga, fct, probs_dev + parity * hs.size(), items_dev, n_items, counter + parity,
-                       grid, stream, false);
+    fused2d_batched<T>(items_tile, ni, iga, fct, probs_dev + parity * hs.size(), items_dev, n_items, counter, grid,
+                       stream, false);
   }
   void capture() {
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
@@ -466,13 +466,7 @@ struct batch_impl : batch_base {
     for (size_t p = 0; p < hs.size(); ++p) {
       auto &st = hs[p]->st;
       for (int par = 0; par < 2; ++par) {
-        f2::prob<T> a;
-        a.in = st.psi[0][st.tl[0] ^ par].v;
-        a.out = st.psi[0][st.tl[0] ^ par ^ 1].v;
-        a.g0 = st.GC[0].v; a.g1 = st.GC[1].v;
-        a.P0 = st.n[0] - 1; a.P1 = st.n[1] - 1;
-        a.n0 = st.n[0]; a.n1 = st.n[1];
-        pr[par * hs.size() + p] = a;
+        pr[par * hs.size() + p] = fused2d_prob(st, 0, st.tl[0] ^ par);
       }
     }
     MPDX_CUDA(cudaMemcpyAsync(probs_dev, pr.data(), pr.size() * sizeof(f2::prob<T>), cudaMemcpyHostToDevice, stream));
@@ -480,7 +474,7 @@ struct batch_impl : batch_base {
     if (mode == MPDX_BATCH_PER_PROBLEM) {
       for (; s < nt; ++s)
         for (auto *h : hs) {
-          fused2d_launch(h->st, 0, stream);
+          fused2d_launch(h->st, h->fus.plan2, 0, stream);
           h->st.tl[0] ^= 1;
         }
     } else {
