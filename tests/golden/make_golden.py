@@ -10,6 +10,11 @@ Outputs, next to this script:
                       (601 cells, 5 option sets, t=0 and t=1200, 2 equations)
   basic_example.npz   1D field dumps of tests/paper_2015_GMD/0_basic_example
                       (101 cells, every 20 steps up to t=100)
+  revolving_sphere_fields.npz
+                      the 3D psi fields of tests/paper_2015_GMD/4_revolving_sphere_3d
+                      after 556 steps (HDF5, float32, read by hdf5_read.py): three
+                      full planes through the sphere's centre and sums over 6^3-cell
+                      blocks of the whole 59^3 field (the full fields would be 4 MB)
 
 Usage:  python tests/golden/make_golden.py [path-to-libmpdataxx-checkout]
 """
@@ -92,6 +97,45 @@ def boussinesq_stats(path):
     return {"header": head, "rows": rows}
 
 
+SPHERE_BLOCK = 6
+
+
+def sphere_fields(gmd):
+    """Planes and block sums of the reference's 59^3 float32 output fields."""
+    sys.path.insert(0, HERE)
+    import hdf5_read
+    d = os.path.join(gmd, "4_revolving_sphere_3d", "refdata")
+    out = {}
+    g0 = hdf5_read.read_dataset(os.path.join(d, "common", "timestep0000000000.h5"), "psi").astype(np.float64)
+    # planes through the centre of the initial sphere (one revolution brings it back)
+    w = g0 / g0.sum()
+    idx = np.indices(g0.shape)
+    centre = [int(round(float((w * idx[a]).sum()))) for a in range(3)]
+    out["centre"] = np.array(centre)
+    out["block"] = np.array(SPHERE_BLOCK)
+    for case in ["upwind", "basic", "iga", "fct", "iga_fct"]:
+        g = hdf5_read.read_dataset(os.path.join(d, case, "timestep0000000556.h5"), "psi")
+        assert g.dtype == np.float32 and g.shape == (59, 59, 59)
+        out[case + "/plane0"] = g[centre[0], :, :]
+        out[case + "/plane1"] = g[:, centre[1], :]
+        out[case + "/plane2"] = g[:, :, centre[2]]
+        s, a = block_sums(g)
+        out[case + "/block_sum"] = s
+        out[case + "/block_abs"] = a
+    return out
+
+
+def block_sums(f):
+    """FP64 sums of f and |f| over blocks of SPHERE_BLOCK^3 cells (edge blocks smaller)."""
+    f = np.asarray(f, dtype=np.float64)
+    b = SPHERE_BLOCK
+    s = np.add.reduceat(np.add.reduceat(np.add.reduceat(f, np.arange(0, f.shape[0], b), 0),
+                                        np.arange(0, f.shape[1], b), 1), np.arange(0, f.shape[2], b), 2)
+    a = np.add.reduceat(np.add.reduceat(np.add.reduceat(np.abs(f), np.arange(0, f.shape[0], b), 0),
+                                        np.arange(0, f.shape[1], b), 1), np.arange(0, f.shape[2], b), 2)
+    return s, a
+
+
 def main(ref):
     gmd = os.path.join(ref, "tests", "paper_2015_GMD")
     golden = {"source": "libmpdata++ tests/paper_2015_GMD refdata"}
@@ -125,6 +169,7 @@ def main(ref):
     recs = [np.array([v[0] for v in ds])[::2] for p in plots for ds in p["data"]]
     np.savez_compressed(os.path.join(HERE, "basic_example.npz"), records=np.array(recs),
                         timesteps=np.arange(0, 101, 20))
+    np.savez_compressed(os.path.join(HERE, "revolving_sphere_fields.npz"), **sphere_fields(gmd))
     print("wrote", sorted(os.listdir(HERE)))
 
 

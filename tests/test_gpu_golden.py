@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from libmpdataxx_b200 import opts as o, setups
+from runners import check_sphere_fields
 from test_gpu_parity import make_run
 
 pytestmark = pytest.mark.gpu
@@ -66,7 +67,9 @@ def test_revolving_sphere_3d(case):
     opts, iters = setups.SPHERE_CASES[case]
     run = run_setup(s, opts, iters)
     run.advance(s["nt"])
-    st = setups.sphere_stats(s["advectee"][0], run.advectee(), s["nt"], s["dt"])
+    out = run.advectee()
+    st = setups.sphere_stats(s["advectee"][0], out, s["nt"], s["dt"])
     want = golden()["revolving_sphere_3d"][case]
     for k in ["max(solution)", "min(solution)", "Linf", "L2", "L1"]:
         assert abs(st[k] - want["tN:" + k]) <= 6e-9, (k, st[k], want["tN:" + k])
+    check_sphere_fields(case, out)

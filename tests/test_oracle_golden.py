@@ -11,7 +11,7 @@ import pytest
 from libmpdataxx_b200 import opts as o
 from libmpdataxx_b200 import setups
 from oracle import Oracle
-from runners import run_oracle
+from runners import check_sphere_fields, run_oracle
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -61,7 +61,8 @@ def test_rotating_cone_2d(case):
     _check_stats(st, golden()["rotating_cone_2d"][case], ["min(psi)", "max(psi)", "rms error"])
 
 
-# 4_revolving_sphere_3d: 59^3 open, 556 steps; stats with 8 decimals
+# 4_revolving_sphere_3d: 59^3 open, 556 steps; stats with 8 decimals, and the
+# float32 output fields (HDF5 refdata: planes through the sphere and block sums)
 @pytest.mark.parametrize("case", list(setups.SPHERE_CASES))
 def test_revolving_sphere_3d(case):
     s = setups.revolving_sphere()
@@ -69,6 +70,23 @@ def test_revolving_sphere_3d(case):
     out = run_oracle(s, opts, n_iters=iters)[0]
     st = setups.sphere_stats(s["advectee"][0], out, s["nt"], s["dt"])
     _check_stats(st, golden()["revolving_sphere_3d"][case], ["max(solution)", "min(solution)", "Linf", "L2", "L1"])
+    check_sphere_fields(case, out)
+
+
+def test_revolving_sphere_fields_fixture_catches_a_change():
+    """The field check is not vacuous: one cell of the sphere moved by 1e-6 fails it."""
+    s = setups.revolving_sphere()
+    opts, iters = setups.SPHERE_CASES["fct"]
+    out = run_oracle(s, opts, n_iters=iters)[0]
+    ref = np.load(os.path.join(GOLD, "revolving_sphere_fields.npz"))
+    c = ref["centre"]
+    out[c[0], c[1], c[2]] += 1e-6
+    with pytest.raises(AssertionError):
+        check_sphere_fields("fct", out)
+    out[c[0], c[1], c[2]] -= 1e-6
+    out[3, 50, 7] += 1e-5  # off every plane: caught by the block sums
+    with pytest.raises(AssertionError):
+        check_sphere_fields("fct", out)
 
 
 # tests/unit/cone_bugs: FP32 fct never undershoots the background (exact)
