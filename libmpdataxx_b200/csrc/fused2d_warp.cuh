@@ -258,6 +258,16 @@ __device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int 
   }
 }
 
+template <class T, int NI, bool IGA, bool FCT>
+__device__ __noinline__ void march_call(const f2::prob<T> &A, int j0, int x0, int x1) {
+  march<T, NI, IGA, FCT>(A, j0, x0, x1);
+}
+
+// resident CTAs of 4 warps per SM that the register budget is sized for
+// (FP64 quads take twice the registers of FP32 ones)
+template <class T, int NI>
+constexpr int kMinBlocks2 = sizeof(T) == 4 ? (NI == 3 ? 2 : 4) : (NI == 3 ? 1 : 2);
+
 // The one 2D kernel, for the single-problem and the batched advance alike:
 // persistent warps take work items (problem, strip, rows) from counter[0] until
 // the list of n_items is exhausted (no warp waits on another).  One kernel with
@@ -266,7 +276,7 @@ __device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int 
 // once).  The last warp to finish re-arms the counter (counter[1] counts the
 // finished warps), so consecutive launches on one stream need no reset.
 template <class T, int NI, bool IGA, bool FCT>
-__global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w(const f2::prob<T> *probs, const f2::item *items,
+__global__ void __launch_bounds__(128, kMinBlocks2<T, NI>) k_fused2d_w(const f2::prob<T> *probs, const f2::item *items,
                                                                    int n_items, int *counter) {
   const int lane = threadIdx.x & 31;
   for (;;) {
@@ -275,8 +285,15 @@ __global__ void __launch_bounds__(128, NI == 3 ? 2 : 4) k_fused2d_w(const f2::pr
     q = __shfl_sync(0xffffffffu, q, 0);
     if (q >= n_items) break;
     const f2::item it = items[q];
-    const f2::prob<T> A = probs[it.prob];
-    march<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
+    if constexpr (sizeof(T) == 4) {
+      const f2::prob<T> A = probs[it.prob];  // FP32: the descriptor in registers
+      march<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
+    } else {
+      // FP64: the quads fill the registers; the march runs as a called function
+      // (its own register allocation, the descriptor read from the stack)
+      const f2::prob<T> A = probs[it.prob];
+      march_call<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
+    }
   }
   if (lane == 0) {
     __threadfence();  // this warp's last take from counter[0] precedes its count
