@@ -223,14 +223,17 @@ def batched_extra(n_problems=256, steps=50):
     return out
 
 
-def rotation_extra(n=1024, steps=200):
+def rotation_extra(n=1024, steps=200, revolution=6283):
     """C2: 2D n^2 cyclic solid-body rotation of a cone, fct, n_iters=3, in FP32 and
     FP64 (fused 2D kernel; the FP32 fields, 12 MB, fit in L2): device time per step
-    on the solver's stream, FP32 - FP64 differences, minimum and mass drift."""
+    on the solver's stream over `steps` steps, then on to one full revolution:
+    FP32 - FP64 differences, the error against the initial cone, minimum, maximum
+    and mass drift."""
     import numpy as np
     import torch
     from libmpdataxx_b200 import _lib, bcond, concurr, opts, solvers, workloads
-    out = {"workload": f"2D {n}^2 cyclic solid-body rotation, cone h=4 r=0.15n, fct, n_iters=3", "steps": steps}
+    out = {"workload": f"2D {n}^2 cyclic solid-body rotation (offsets clipped at 0.48 (n-1)), cone h=4 r=0.15n, fct, "
+                       f"n_iters=3, one revolution", "steps": steps}
     fields = {}
     for dt in ("float32", "float64"):
         w = workloads.rotation_2d(n, dtype=dt)
@@ -258,14 +261,19 @@ def rotation_extra(n=1024, steps=200):
             e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        run.advance(revolution - 3 - steps)
         st = run.stats()
         fields[dt] = np.array(run.advectee(), dtype=np.float64)
+        err = fields[dt] - w["advectee"][0].double().cpu().numpy()
         out[dt] = {"ms_per_step": ms, "cell_updates_per_s": n * n / (ms * 1e-3),
                    "path": "fused" if st["path"] == _lib.PATH_FUSED else "general",
-                   "min": st["min"], "max": st["max"], "mass_rel_drift": (st["mass"] - m0) / m0}
+                   "after_steps": revolution, "min": st["min"], "max": st["max"],
+                   "mass_rel_drift": (st["mass"] - m0) / m0,
+                   "vs_initial_cone": {"max_abs": float(np.abs(err).max()), "l2": float(np.sqrt((err * err).mean()))}}
         run.close()
     d = fields["float32"] - fields["float64"]
-    out["fp32_vs_fp64"] = {"max_abs": float(np.abs(d).max()), "l2": float(np.sqrt((d * d).mean()))}
+    out["fp32_vs_fp64"] = {"after_steps": revolution, "max_abs": float(np.abs(d).max()),
+                           "l2": float(np.sqrt((d * d).mean()))}
     return out
 
 

@@ -38,6 +38,18 @@ ADVSCHEME_CASES = {"abs": o.abs, "iga": o.iga, "iga_tot": o.iga | o.tot, "iga_fc
                    "iga_tot_fct": o.iga | o.tot | o.fct}
 
 
+# --- plain 1D MPDATA on a periodic box (the CPU-runnable benchmark case) ------
+def box_1d(nx=2000, seed=1, courant=0.5):
+    """nx points cyclic (period nx - 1), constant Courant number 0.5, advectee
+    0.1 + U[0, 0.01) (seed) with 1 on cells 200..400, point nx - 1 = point 0;
+    run with opts 0, n_iters 2 for 1000 steps."""
+    rng = np.random.default_rng(seed)
+    psi = 0.1 + rng.uniform(0.0, 0.01, nx - 1)
+    psi[200:401] = 1.0
+    return {"grid": (nx,), "bcs": ["cyclic"] * 2, "advectee": [wrap_periodic(psi)],
+            "advector": [np.full((nx,), courant)], "nt": 1000, "opts": 0, "n_iters": 2}
+
+
 # --- tests/paper_2015_GMD/0_basic_example/basic_example.cpp:10-50 -------------
 def basic_example(nx=101, dx=0.1):
     i = np.arange(nx, dtype=np.float64)

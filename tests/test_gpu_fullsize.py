@@ -1,0 +1,175 @@
+"""The benchmark configurations at their full sizes, checked through properties
+that hold at any size (the oracle is too slow for most of them):
+
+  1D box, 2000 points, 1000 steps (plain MPDATA, FP64): the whole run against
+      the oracle, mass conservation, positivity, translation at the Courant speed;
+  2D 1024^2 solid-body rotation, fct, n_iters 3, one full revolution (6283
+      steps) in FP64 and FP32: FCT bounds (no value leaves [0, 4]), mass,
+      the cone's centroid back where it started, FP32 against FP64;
+  3D 512^3 deformational flow, fct|iga, 200 steps, FP32 and FP64: bounds, mass,
+      FP32 against FP64;
+  256 batched 2D problems (sides 64..1024), 500 steps: the persistent launch bit
+      for bit equal to one launch per problem, positivity and mass per problem;
+  3D Boussinesq 256 x 256 x 128 with the GCR pressure solve: every solve
+      reaches max|err| <= prs_tol / dt.
+
+Mass is the FP64 compensated sum over the unique cells (run.stats())."""
+import math
+
+import numpy as np
+import pytest
+
+from libmpdataxx_b200 import _lib, bcond, concurr, opts as o, setups, solvers, workloads
+from runners import run_oracle
+from test_gpu_parity import make_run
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_run(w, opts, n_iters, dtype, path="fused"):
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    nd = len(w["grid"])
+    ct.real_t = dtype
+    ct.n_dims = nd
+    ct.n_eqns = 1
+    ct.opts = opts
+    p = solvers.mpdata.rt_params_t(grid_size=list(w["grid"]), n_iters=n_iters, max_abs_div_eps=1e-6)
+    run = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * (2 * nd), p=p, path=path)
+    run.set_field_device(_lib.FIELD_ADVECTEE, 0, w["advectee"][0].data_ptr())
+    for d, a in enumerate(w["advector"]):
+        run.set_field_device(_lib.FIELD_ADVECTOR, d, a.data_ptr())
+    return run
+
+
+def _centroid_periodic(psi, period):
+    """Mass-weighted circular mean position along each axis (unique cells)."""
+    u = psi[tuple(slice(0, period) for _ in psi.shape)]
+    out = []
+    for ax in range(u.ndim):
+        ang = 2 * np.pi * np.arange(period) / period
+        w = u.sum(axis=tuple(a for a in range(u.ndim) if a != ax))
+        out.append((math.atan2(float((w * np.sin(ang)).sum()), float((w * np.cos(ang)).sum())) / (2 * np.pi) * period)
+                   % period)
+    return np.array(out)
+
+
+def test_box_1d_full():
+    s = setups.box_1d()
+    run = make_run(s["grid"], s["opts"], n_iters=s["n_iters"], bcs=s["bcs"], dtype=np.float64)
+    run.set_advectee(s["advectee"][0])
+    run.set_advector(s["advector"][0], 0)
+    m0 = run.stats()["mass"]
+    run.advance(s["nt"])
+    got = run.advectee()
+    st = run.stats()
+    ref = run_oracle(s, s["opts"], n_iters=s["n_iters"])[0]
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert abs(st["mass"] - m0) <= 1e-12 * abs(m0)
+    assert st["min"] >= 0.0
+    # the box (cells 200..400) moved by C nt = 500 cells
+    c0 = _centroid_periodic(np.where(s["advectee"][0] > 0.5, s["advectee"][0], 0.0), 1999)[0]
+    c1 = _centroid_periodic(np.maximum(got - 0.105, 0.0), 1999)[0]
+    assert abs(((c1 - c0) - 500.0 + 999.5) % 1999 - 999.5) <= 1.0, (c0, c1)
+
+
+def test_rotation_2d_full_revolution():
+    n, steps = 1024, 6283
+    fields = {}
+    for dt in ("float64", "float32"):
+        w = workloads.rotation_2d(n, dtype=dt)
+        run = _device_run(w, o.fct, 3, dt)
+        m0 = run.stats()["mass"]
+        run.advance(steps)
+        st = run.stats()
+        assert st["path"] == _lib.PATH_FUSED
+        assert st["min"] >= 0.0 and st["max"] <= 4.0, (dt, st["min"], st["max"])
+        tol = 1e-12 if dt == "float64" else 1e-5
+        assert abs(st["mass"] - m0) <= tol * m0, (dt, (st["mass"] - m0) / m0)
+        fields[dt] = np.array(run.advectee(), dtype=np.float64)
+        init = w["advectee"][0].double().cpu().numpy()
+        # one revolution brings the cone back: centroid within a quarter cell
+        d = _centroid_periodic(fields[dt], n - 1) - _centroid_periodic(init, n - 1)
+        assert np.abs(d).max() <= 0.25, (dt, d)
+        assert st["max"] >= 3.0, (dt, st["max"])  # the peak is smoothed, not lost
+        run.close()
+    diff = np.abs(fields["float32"] - fields["float64"]).max()
+    assert diff <= 1e-3, diff
+
+
+def test_advection_3d_full():
+    torch = pytest.importorskip("torch")
+    n, steps = 512, 200
+    out = {}
+    for dt in ("float32", "float64"):
+        w = workloads.advection_3d(n, dtype=dt)
+        mx0 = float(w["advectee"][0].max())
+        mn0 = float(w["advectee"][0].min())
+        run = _device_run(w, o.fct | o.iga, 2, dt)
+        m0 = run.stats()["mass"]
+        run.advance(steps)
+        st = run.stats()
+        assert st["path"] == _lib.PATH_FUSED
+        assert st["min"] >= mn0 and st["max"] <= mx0, (dt, st["min"], st["max"], mn0, mx0)
+        tol = 1e-12 if dt == "float64" else 1e-7
+        assert abs(st["mass"] - m0) <= tol * m0, (dt, (st["mass"] - m0) / m0)
+        out[dt] = torch.from_numpy(np.asarray(run.advectee())).to(torch.float64)
+        del w
+        run.close()
+    diff = float((out["float32"] - out["float64"]).abs().max())
+    assert diff <= 1e-3, diff
+
+
+def test_batched_full():
+    probs = setups.batched_problems(n=256)
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = np.float32
+    ct.n_dims = 2
+    ct.n_eqns = 1
+    ct.opts = o.fct
+    runs = {}
+    for mode in ("persistent", "per_problem"):
+        rs = []
+        for s in probs:
+            p = solvers.mpdata.rt_params_t(grid_size=list(s["grid"]), n_iters=2, max_abs_div_eps=1e-6)
+            r = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * 4, p=p, path="fused")
+            r.set_advectee(s["advectee"][0])
+            for d, a in enumerate(s["advector"]):
+                r.set_advector(a, d)
+            rs.append(r)
+        runs[mode] = (rs, concurr.batch(rs, mode=mode))
+    m0 = [r.stats()["mass"] for r in runs["persistent"][0]]
+    for mode in runs:
+        runs[mode][1].advance(10)
+        runs[mode][1].sync()
+    for a, b in zip(runs["persistent"][0], runs["per_problem"][0]):
+        np.testing.assert_array_equal(a.advectee(), b.advectee())
+    runs["persistent"][1].advance(490)
+    runs["persistent"][1].sync()
+    for p, r in enumerate(runs["persistent"][0]):
+        st = r.stats()
+        assert st["timestep"] == 500
+        assert st["min"] >= 0.0, (p, st["min"])
+        assert abs(st["mass"] - m0[p]) <= 1e-5 * m0[p], (p, (st["mass"] - m0[p]) / m0[p])
+    for rs, b in runs.values():
+        b.close()
+        for r in rs:
+            r.close()
+
+
+def test_boussinesq_3d_full():
+    s = setups.boussinesq_bubble_3d(256, 256, 128)
+    run = setups.boussinesq_run(s, dtype=np.float32, prs_fp64=True)
+    tol = s["prs_tol"] / s["dt"]
+    for _ in range(3):
+        run.advance(1)
+        st = run.stats()
+        assert 0 < st["gcr_iters"] < 10000
+        assert st["gcr_residual"] <= tol, (st["gcr_residual"], tol)
+    tht = np.asarray(run.advectee(3))
+    assert np.isfinite(tht).all()
+    run.close()
