@@ -1155,6 +1155,7 @@ void boussinesq<T, P>::pressure_solve() {
   for (;;) {
     long long batch = launched == 0 ? std::max(1LL, predicted) : std::max(4LL, predicted / 4);
     if (rec) batch = std::min(batch, 16LL);  // snapshots are taken between batches
+    if (pcnd) batch = std::min(batch, 4LL);  // the hand-over test below runs between batches
     for (long long b = 0; b < batch; ++b)
       for (int v = 0; v < k_iters; ++v) {
         if (!pcnd) {
@@ -1188,9 +1189,13 @@ void boussinesq<T, P>::pressure_solve() {
       MPDX_LAUNCH_CHECK();
       ++n_rec;
     }
-    if (pcnd && hdev->iters > std::max(20LL, 2 * last_plain_iters)) {
-      // the learned directions are not converging: continue from the current
-      // iterate with plain GCR (directions restart from the residual)
+    float elapsed = 0;
+    if (pcnd && last_plain_ms > 0) MPDX_CUDA(cudaEventElapsedTime(&elapsed, ev_solve[0], ev_solve[1]));
+    if (pcnd && (hdev->iters > std::max(20LL, 2 * last_plain_iters) || (last_plain_ms > 0 && elapsed > last_plain_ms))) {
+      // the learned directions are not converging, or the solve has already
+      // taken as long as a whole plain solve (so it can no longer be faster):
+      // continue from the current iterate with plain GCR (directions restart
+      // from the residual)
       bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
       MPDX_LAUNCH_CHECK();
       pcnd = false;
@@ -1205,7 +1210,7 @@ void boussinesq<T, P>::pressure_solve() {
   }
   iters = hdev->iters;
   iters_total += iters;
-  if (!(use_net && net)) last_plain_iters = iters;
+  if (!(use_net && net)) { last_plain_iters = iters; last_plain_ms = last_solve_ms; }
   last_residual = hdev->residual;
   predicted = std::max(1LL, iters);
   for (int q = 0; q < n_rec; ++q)  // corrections Phi_end - Phi_snapshot

@@ -65,6 +65,7 @@ struct boussinesq {
   double out_scale = 0;
   double *tr_loss = nullptr;
   long long last_plain_iters = 250, fallbacks = 0;
+  float last_plain_ms = 0;  // device time of the last plain solve (0: none yet)
   bool fell_back = false;
   long long max_pairs = 0, n_pairs = 0;
   int pc_channels[4] = {8, 16, 32, 64};
