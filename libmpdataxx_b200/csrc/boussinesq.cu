@@ -15,10 +15,12 @@
 // Pointwise stages that the reference runs as separate array statements are
 // fused into one kernel each (the per-point arithmetic and its order are
 // unchanged).  The GCR iteration runs as two kernels per inner step:
-//   k_gcr_update: Phi += beta p_v, err' = err + beta lap_p_v, lap_err = lap(err'),
-//                 max|err'| and the alpha sums;
-//   k_gcr_direction: new search direction and its lap, and the sums of the
-//                 next beta.
+//   k_gcr_update: err' = err + beta lap_p_v, lap_err = lap(err'), max|err'| and
+//                 the alpha sums;
+//   k_gcr_direction: Phi += beta p_v (deferred here from the reference's first
+//                 half because this kernel reads p_v anyway: same arithmetic,
+//                 8 bytes less per point), new search direction and its lap,
+//                 and the sums of the next beta.
 // lap() is evaluated straight from the interior values: a point outside the
 // interior takes the value its pressure halo fill would give it (cyclic copy,
 // or rigid one-sided extrapolation), and the gradient component vanishes on a
@@ -357,7 +359,7 @@ struct dirs {
 
 // inner step v = NV - 1, first half (mpdata_rhs_vip_prs_gcrk.hpp:43-64)
 template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol, dfield<T> phi, dfield<T> err0, dfield<T> err1,
+__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol, dfield<T> err0, dfield<T> err1,
                                                                dfield<T> lap_err, dirs<T> D, gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
   if (dv->done) return;
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
   const T den = dv->pend_den;
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;  // beta keeps its value when tmp_den is 0
   if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
-  const dfield<T> pv = D.p[v], lpv = D.lp[v];
+  const dfield<T> lpv = D.lp[v];
   dfield<T> lps[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
@@ -376,7 +378,6 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
   for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
   double mx = -DBL_MAX, mn = DBL_MAX;
   for_interior(g, [&](int i, int j, int k) {
-    phi(i, j, k) = phi(i, j, k) + b * pv(i, j, k);
     const T e = enew(off3(ea, i, j, k));
     eb(i, j, k) = e;
     mx = fmax(mx, double(e));
@@ -411,7 +412,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
 constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 32, kSteps = 2;
 static_assert(kTJ * kTK == kRedThreads, "one tile column per thread");
 template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(geom g, T err_tol, dfield<T> phi, dfield<T> err0,
+__global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(geom g, T err_tol, dfield<T> err0,
                                                                 dfield<T> err1, dfield<T> lap_err, dirs<T> D,
                                                                 gcr_dev<T> *dv, double *part, int chunk) {
   constexpr int v = NV - 1;
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
   const T den = dv->pend_den;
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;  // beta keeps its value when tmp_den is 0
   if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
-  const dfield<T> pv = D.p[v], lpv = D.lp[v];
+  const dfield<T> lpv = D.lp[v];
   const fld_axpy<T> enew{ea.o, lpv.o, b};
   dd acc[NV];
 #pragma unroll
@@ -429,15 +430,15 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
   double mx = -DBL_MAX, mn = DBL_MAX;
   // every pressure-type field has the same layout: one linear offset addresses a
   // point in all of them
-  T *const phio = phi.o, *const ebo = eb.o, *const leo = lap_err.o;
-  const T *const pvo = pv.o, *const eao = ea.o, *const lpvo = lpv.o;
+  T *const ebo = eb.o, *const leo = lap_err.o;
+  const T *const eao = ea.o, *const lpvo = lpv.o;
   const T *lpo[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) lpo[l] = D.lp[l].o;
   const long long s0 = ea.s0;
-  // per-point outputs (mpdata_rhs_vip_prs_gcrk.hpp:43-64)
-  auto finish = [&](long long o, T e, T le, T cphi, T cpv, const T *clp) {
-    phio[o] = cphi + b * cpv;
+  // per-point outputs (mpdata_rhs_vip_prs_gcrk.hpp:43-64); Phi += beta p_v is
+  // applied by k_gcr_direction, which reads p_v anyway
+  auto finish = [&](long long o, T e, T le, const T *clp) {
     ebo[o] = e;
     mx = fmax(mx, double(e));
     mn = fmin(mn, double(e));
@@ -500,12 +501,10 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
     __syncthreads();
     T cm2 = pl[slot(i0 - 2)][ty + 2][tx + 2], cm1 = pl[slot(i0 - 1)][ty + 2][tx + 2];
     const long long colo = own ? off3(ea, 0, j, k) : 0;
-    T fphi[kSteps], fpv[kSteps], flp[kSteps][NV];
-    auto load_own = [&](int i, int q0) {  // the own point's Phi, p and lap_p, a pass ahead
+    T flp[kSteps][NV];
+    auto load_own = [&](int i, int q0) {  // the own point's lap_p of every direction, a pass ahead
       if (own && i < i1) {
         const long long o = colo + i * s0;
-        fphi[q0] = phio[o];
-        fpv[q0] = pvo[o];
 #pragma unroll
         for (int l = 0; l < NV; ++l) flp[q0][l] = lpo[l][o];
       }
@@ -519,11 +518,9 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
       for (int q0 = 0; q0 < kSteps; ++q0) store(i + 2 + q0, q0);
 #pragma unroll
       for (int q0 = 0; q0 < kSteps; ++q0) load(i + 2 + kSteps + q0, q0);
-      T cphi[kSteps], cpv[kSteps], clp[kSteps][NV];
+      T clp[kSteps][NV];
 #pragma unroll
       for (int q0 = 0; q0 < kSteps; ++q0) {
-        cphi[q0] = fphi[q0];
-        cpv[q0] = fpv[q0];
 #pragma unroll
         for (int l = 0; l < NV; ++l) clp[q0][l] = flp[q0][l];
       }
@@ -548,7 +545,7 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
             const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
             le = d == 0 ? term : le + term;
           }
-          finish(colo + ip * s0, c0, le, cphi[q0], cpv[q0], clp[q0]);
+          finish(colo + ip * s0, c0, le, clp[q0]);
         }
         cm2 = cm1;
         cm1 = c0;
@@ -579,7 +576,7 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
     T clp[NV];
 #pragma unroll
     for (int l = 0; l < NV; ++l) clp[l] = lpo[l][o];
-    finish(o, e, le, phio[o], pvo[o], clp);
+    finish(o, e, le, clp);
   }
   if (grid_reduce<NV, true>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
     const T amx = fabs(T(mx)), amn = fabs(T(mn));
@@ -596,11 +593,13 @@ __global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(ge
 
 // inner step v = NV - 1, second half: next search direction (mpdata_rhs_vip_prs_gcrk.hpp:66-92)
 template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk, dfield<T> err0, dfield<T> err1,
-                                                                  dfield<T> lap_err, dirs<T> D, gcr_dev<T> *dv, double *part) {
+__global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk, dfield<T> phi, dfield<T> err0,
+                                                                  dfield<T> err1, dfield<T> lap_err, dirs<T> D,
+                                                                  gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
   if (dv->done) return;
   const int cur = dv->cur;
+  const T b = dv->beta;  // this inner step's beta, set by k_gcr_update
   const dfield<T> e = cur ? err0 : err1;  // the error written by k_gcr_update
   T a[NV];
   dfield<T> ps[NV], lps[NV];
@@ -611,7 +610,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
   dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
   // every pressure-type field has the same layout: one linear offset per point
   const T *const eo = e.o, *const leo = lap_err.o;
-  T *const pdo = pd.o, *const lpdo = lpd.o;
+  T *const pdo = pd.o, *const lpdo = lpd.o, *const phio = phi.o;
   const T *po[NV], *lpo[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) { po[l] = ps[l].o; lpo[l] = lps[l].o; }
@@ -623,7 +622,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
     for (int f0 = threadIdx.x; f0 < g.nf; f0 += U * blockDim.x) {
       long long o[U];
       bool ok[U];
-      T ev[U], le[U], pv[U][NV], lv[U][NV];
+      T ev[U], le[U], ph[U], pv[U][NV], lv[U][NV];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int f = f0 + u * blockDim.x;
@@ -631,6 +630,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
         o[u] = ok[u] ? (g.nd == 3 ? off3(e, i, j, f) : off3(e, i, f, 0)) : 0;
         ev[u] = ok[u] ? eo[o[u]] : T(0);
         le[u] = ok[u] ? leo[o[u]] : T(0);
+        ph[u] = ok[u] ? phio[o[u]] : T(0);
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           pv[u][l] = ok[u] ? po[l][o[u]] : T(0);
@@ -640,6 +640,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
+        phio[o[u]] = ph[u] + b * pv[u][v];  // Phi += beta p_v (mpdata_rhs_vip_prs_gcrk.hpp:51)
         T pn, ln;
         if (!restart) {
           pn = ev[u];
@@ -682,9 +683,9 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
 template <class T, int NV>
 void launch_inner(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi, dfield<T> e0,
                   dfield<T> e1, dfield<T> le, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
-  if (g.nd == 3) k_gcr_update3<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part, kGcrChunk);
-  else k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, e0, e1, le, D, dv, part);
-  k_gcr_direction<T, NV><<<G, blk, 0, s>>>(g, kk, e0, e1, le, D, dv, part);
+  if (g.nd == 3) k_gcr_update3<T, NV><<<G, blk, 0, s>>>(g, err_tol, e0, e1, le, D, dv, part, kGcrChunk);
+  else k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, e0, e1, le, D, dv, part);
+  k_gcr_direction<T, NV><<<G, blk, 0, s>>>(g, kk, phi, e0, e1, le, D, dv, part);
 }
 template <class T>
 void launch_inner(int v, unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi,
