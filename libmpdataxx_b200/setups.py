@@ -50,6 +50,41 @@ def box_1d(nx=2000, seed=1, courant=0.5):
             "advector": [np.full((nx,), courant)], "nt": 1000, "opts": 0, "n_iters": 2}
 
 
+# --- tests/paper_2015_GMD/2_convergence_1d/convergence_1d.cpp:59-160 ----------
+CONVERGENCE_SOLVERS = {"iters=1": (0, 1), "iters=2": (0, 2), "iters=3": (0, 3), "iters=3_tot": (o.tot, 3),
+                       "iters=i": (o.iga, 2), "iters=2_fct": (o.fct, 2), "iters=i_fct": (o.fct | o.iga, 2),
+                       "iters=i_fct_tot": (o.fct | o.iga | o.tot, 2)}
+CONVERGENCE_COURANTS = [.05, .1, .15, .2, .25, .3, .35, .4, .45, .5, .55, .6, .65, .7, .75, .8, .85, .9, .95]
+CONVERGENCE_DXS = [1.0 / 2 ** q for q in range(8)]
+
+
+def convergence_1d(dx, courant):
+    """A Gaussian (sigma 1.5) averaged over each cell, advected by one unit
+    (t_max 1, velocity 1) across a 440-unit domain with open boundaries;
+    returns the set-up and the cell-averaged exact solution at the end."""
+    t_max, x_max, sgma, velocity, A0 = 1.0, 440.0, 1.5, 1.0, 0.0
+    x0 = 0.5 * x_max
+    A = 1.0 / sgma / math.sqrt(2 * math.pi)
+
+    def gauss_int(a):
+        return A0 * dx + A * sgma * math.sqrt(math.pi / 2) * (
+            math.erf((a + dx / 2 - x0) / math.sqrt(2) / sgma) - math.erf((a - dx / 2 - x0) / math.sqrt(2) / sgma))
+
+    dt = courant * dx / velocity
+    cround = lambda v: int(math.floor(v + 0.5))  # C's round(): halves away from zero (v > 0)
+    nx = cround(x_max / dx)
+    nt = cround(t_max / dt)
+    psi = np.array([gauss_int(i * dx) / dx for i in range(nx)])
+    exact = np.array([gauss_int(i * dx - velocity * dt * nt) / dx for i in range(nx)])
+    return {"grid": (nx,), "bcs": ["open"] * 2, "advectee": [psi], "advector": [np.full((nx,), courant)],
+            "nt": nt, "dt": dt, "exact": exact}
+
+
+def convergence_error(psi, exact, nt, dt):
+    """sqrt(sum((psi - exact)^2) / nx) / (nt dt) (convergence_1d.cpp:152-153)"""
+    return math.sqrt(float(((psi - exact) ** 2).sum()) / psi.size) / (nt * dt)
+
+
 # --- tests/paper_2015_GMD/0_basic_example/basic_example.cpp:10-50 -------------
 def basic_example(nx=101, dx=0.1):
     i = np.arange(nx, dtype=np.float64)

@@ -5,7 +5,8 @@ gzip'd refdata files of its test suite as text); the GPU host never runs it.
 Outputs, next to this script:
 
   golden_stats.json   rotating-cone (2D) and revolving-sphere (3D) error stats,
-                      2D Boussinesq per-10-step stats (min/max theta, max |u|)
+                      2D Boussinesq per-10-step stats (min/max theta, max |u|),
+                      1D convergence errors (8 solvers x 8 grid steps x 19 Courant numbers)
   advscheme_opts.npz  1D field dumps of tests/paper_2015_GMD/1_advscheme_opts
                       (601 cells, 5 option sets, t=0 and t=1200, 2 equations)
   basic_example.npz   1D field dumps of tests/paper_2015_GMD/0_basic_example
@@ -151,6 +152,17 @@ def main(ref):
     golden["revolving_sphere_3d"] = sphere
 
     golden["boussinesq_2d"] = boussinesq_stats(os.path.join(gmd, "8_boussinesq_2d", "refdata", "stats.txt.gz"))
+
+    # 2_convergence_1d: rows "dx  courant  error" (4 significant digits) per solver key
+    conv = {}
+    for key in ["iters=1", "iters=2", "iters=3", "iters=3_tot", "iters=i", "iters=2_fct", "iters=i_fct",
+                "iters=i_fct_tot"]:
+        rows = []
+        for line in read_gz(os.path.join(gmd, "2_convergence_1d", "refdata", f"err_mpdata_{key}.txt.gz")).splitlines():
+            if line.strip():
+                rows.append([float(x) for x in line.split()])
+        conv[key] = rows
+    golden["convergence_1d"] = conv
 
     with open(os.path.join(HERE, "golden_stats.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)

@@ -73,3 +73,25 @@ def test_revolving_sphere_3d(case):
     for k in ["max(solution)", "min(solution)", "Linf", "L2", "L1"]:
         assert abs(st[k] - want["tN:" + k]) <= 6e-9, (k, st[k], want["tN:" + k])
     check_sphere_fields(case, out)
+
+
+# 2_convergence_1d: all 8 grid steps x 19 Courant numbers x 8 solvers, 4 significant digits
+def test_convergence_1d_all():
+    import math
+    conv = golden()["convergence_1d"]
+    want = {(k, dx, c): e for k, rows in conv.items() for dx, c, e in rows}
+    checked = 0
+    for dx in setups.CONVERGENCE_DXS:
+        for cour in setups.CONVERGENCE_COURANTS:
+            s = setups.convergence_1d(dx, cour)
+            for key, (opts, iters) in setups.CONVERGENCE_SOLVERS.items():
+                run = make_run(s["grid"], opts, n_iters=iters, bcs=s["bcs"])
+                run.set_advectee(s["advectee"][0])
+                run.set_advector(s["advector"][0], 0)
+                run.advance(s["nt"])
+                got = setups.convergence_error(run.advectee(), s["exact"], s["nt"], s["dt"])
+                w = want[(key, dx, cour)]
+                assert abs(got - w) <= 0.5e-4 * 10 ** math.floor(math.log10(abs(w))) * 1.01, (key, dx, cour, got, w)
+                run.close()
+                checked += 1
+    assert checked == 8 * 19 * 8

@@ -3,6 +3,7 @@ extracted from libmpdata++ tests/paper_2015_GMD/*/refdata by make_golden.py).
 The oracle is trusted as the parity checker for the CUDA path only because it
 reproduces these numbers."""
 import json
+import math
 import os
 
 import numpy as np
@@ -49,6 +50,28 @@ def test_basic_example_1d():
 def _check_stats(got, want, keys, atol=6e-9):
     for k in keys:
         assert abs(got[k] - want["tN:" + k]) <= atol, (k, got[k], want["tN:" + k])
+
+
+# 2_convergence_1d: error norms printed with 4 significant digits; the oracle runs
+# the four coarsest grid steps (every Courant number and solver), the GPU all eight
+def within_4_digits(got, want):
+    return abs(got - want) <= 0.5e-4 * 10 ** math.floor(math.log10(abs(want))) * 1.01
+
+
+@pytest.mark.parametrize("key", list(setups.CONVERGENCE_SOLVERS))
+def test_convergence_1d_coarse(key):
+    opts, iters = setups.CONVERGENCE_SOLVERS[key]
+    rows = golden()["convergence_1d"][key]
+    checked = 0
+    for dx, cour, want in rows:
+        if dx < 0.125:
+            continue
+        s = setups.convergence_1d(dx, cour)
+        out = run_oracle(s, opts, n_iters=iters)[0]
+        got = setups.convergence_error(out, s["exact"], s["nt"], s["dt"])
+        assert within_4_digits(got, want), (key, dx, cour, got, want)
+        checked += 1
+    assert checked == 4 * 19
 
 
 # 3_rotating_cone_2d: 101^2 open, 3768 steps; stats with 8 decimals
