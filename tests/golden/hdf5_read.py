@@ -7,17 +7,17 @@ or 1, version-1 object headers with continuation blocks, a root group held as a
 symbol table (version-1 group B-tree, symbol-table nodes, local heap), the
 dataspace (versions 1 and 2), datatype (fixed-point and floating-point), data
 layout (version 3: contiguous, chunked with a version-1 raw-data B-tree) and
-filter pipeline (versions 1 and 2; deflate only) messages.
+filter pipeline (versions 1 and 2; deflate only) messages, and scalar
+attributes (message version 1).
 
 Written from the HDF5 File Format Specification (The HDF Group, version 2.0 of
 the format document, sections II.A superblock, III.A.1 version-1 B-trees,
 III.B symbol table nodes, III.D local heaps, IV.A.1 version-1 object headers,
-IV.A.2 messages 0x0001, 0x0003, 0x0008, 0x000B, 0x0010).  No HDF5 library is
+IV.A.2 messages 0x0001, 0x0003, 0x0008, 0x000B, 0x000C, 0x0010).  No HDF5 library is
 available where this runs; Python's zlib decodes the deflate filter.
 
 Usage:  read_dataset(path, "psi") -> numpy array (C order, as stored)
 """
-import struct
 import zlib
 
 import numpy as np
@@ -238,6 +238,54 @@ class File:
             sl_in = tuple(slice(0, s.stop - s.start) for s in sl_out)
             out[sl_out] = block[sl_in]
         return out
+
+
+    # ---- attributes (message 0x000C, version 1) ----
+    def attributes(self, name):
+        """{attribute: value} of the root member `name` (scalar or 1-element attributes)."""
+        links = self.group_links(self.root)
+        out = {}
+        for t, d, size in self.object_header(links[name]["header"]):
+            if t != 0x000C:
+                continue
+            ver = self.b[d]
+            if ver != 1:
+                raise H5Error("attribute message version %d not supported" % ver)
+            ns, ts, ss = self.uint(d + 2, 2), self.uint(d + 4, 2), self.uint(d + 6, 2)
+            p = d + 8
+            nm = self.b[p:p + ns].split(b"\0")[0].decode()
+            p += (ns + 7) // 8 * 8
+            tp = p
+            p += (ts + 7) // 8 * 8
+            shape = self._dataspace(p, ss)
+            p += (ss + 7) // 8 * 8
+            count = int(np.prod(shape)) if shape else 1
+            if self.b[tp] & 0x0F == 3:  # string
+                n = self.uint(tp + 4, 4)
+                out[nm] = self.b[p:p + n].split(b"\0")[0].decode()
+            else:
+                dt = self._datatype(tp, ts)
+                v = np.frombuffer(self.b, dt, count, p)
+                out[nm] = v[0] if count == 1 else v.copy()
+        return out
+
+    def attribute_messages(self, name):
+        """{attribute: raw attribute message} of the root member `name`."""
+        links = self.group_links(self.root)
+        out = {}
+        for t, d, size in self.object_header(links[name]["header"]):
+            if t == 0x000C:
+                ns = self.uint(d + 2, 2)
+                out[self.b[d + 8:d + 8 + ns].split(b"\0")[0].decode()] = bytes(self.b[d:d + size])
+        return out
+
+    def message_bytes(self, name, mtype):
+        """Raw bytes of the first message of type mtype in the header of root member `name`."""
+        links = self.group_links(self.root)
+        for t, d, size in self.object_header(links[name]["header"]):
+            if t == mtype:
+                return bytes(self.b[d:d + size])
+        return None
 
 
 def read_dataset(path, name):

@@ -11,6 +11,9 @@ Outputs, next to this script:
                       (601 cells, 5 option sets, t=0 and t=1200, 2 equations)
   basic_example.npz   1D field dumps of tests/paper_2015_GMD/0_basic_example
                       (101 cells, every 20 steps up to t=100)
+  output_layout.json  the reference's output of the revolving-sphere fct run: its
+                      XDMF files, the raw HDF5 messages of const.h5 (datasets and
+                      attributes) and its coordinate samples
   revolving_sphere_fields.npz
                       the 3D psi fields of tests/paper_2015_GMD/4_revolving_sphere_3d
                       after 556 steps (HDF5, float32, read by hdf5_read.py): three
@@ -126,6 +129,32 @@ def sphere_fields(gmd):
     return out
 
 
+def output_layout(gmd):
+    """The reference's output files of the revolving-sphere fct run: XDMF texts,
+    the raw HDF5 messages of const.h5's datasets and attributes, coordinate samples."""
+    sys.path.insert(0, HERE)
+    import hdf5_read
+    d = os.path.join(gmd, "4_revolving_sphere_3d", "refdata", "fct")
+    out = {}
+    for name in ["timestep0000000000.xmf", "timestep0000000556.xmf", "temp.xmf"]:
+        with open(os.path.join(d, name)) as f:
+            out[name] = f.read()
+    c = hdf5_read.File(os.path.join(d, "const.h5"))
+    msgs = {}
+    for ds in ["T", "X", "Y", "Z"]:
+        for t in (0x0001, 0x0003, 0x0005):
+            msgs["%s/%d" % (ds, t)] = c.message_bytes(ds, t).hex()
+    psi = hdf5_read.File(os.path.join(d, "timestep0000000556.h5"))
+    msgs["psi/3"] = psi.message_bytes("psi", 0x0003).hex()
+    msgs["psi/1"] = psi.message_bytes("psi", 0x0001).hex()
+    out["messages"] = msgs
+    out["advection"] = {k: v.hex() for k, v in c.attribute_messages("advection").items()}
+    X, Y, Z = (c.dataset(a) for a in "XYZ")
+    out["coords"] = {"X": X[:, 0, 0].tolist(), "Y": Y[0, :, 0].tolist(), "Z": Z[0, 0, :].tolist(),
+                     "shape": list(X.shape), "T": c.dataset("T").tolist()}
+    return out
+
+
 def block_sums(f):
     """FP64 sums of f and |f| over blocks of SPHERE_BLOCK^3 cells (edge blocks smaller)."""
     f = np.asarray(f, dtype=np.float64)
@@ -182,6 +211,8 @@ def main(ref):
     np.savez_compressed(os.path.join(HERE, "basic_example.npz"), records=np.array(recs),
                         timesteps=np.arange(0, 101, 20))
     np.savez_compressed(os.path.join(HERE, "revolving_sphere_fields.npz"), **sphere_fields(gmd))
+    with open(os.path.join(HERE, "output_layout.json"), "w") as f:
+        json.dump(output_layout(gmd), f, indent=1, sort_keys=True)
     print("wrote", sorted(os.listdir(HERE)))
 
 

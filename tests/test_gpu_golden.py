@@ -95,3 +95,26 @@ def test_convergence_1d_all():
                 run.close()
                 checked += 1
     assert checked == 8 * 19 * 8
+
+
+# the output path on the same run: fields leave the GPU only at the output steps
+# (0 and 556) and are written in the reference's layout; the written psi passes
+# the field check and the XDMF files equal the reference's
+def test_revolving_sphere_output(tmp_path):
+    import sys
+    from libmpdataxx_b200 import output
+    sys.path.insert(0, GOLD)
+    import hdf5_read
+    with open(os.path.join(GOLD, "output_layout.json")) as f:
+        layout = json.load(f)
+    s = setups.revolving_sphere()
+    opts, iters = setups.SPHERE_CASES["fct"]
+    run = run_setup(s, opts, iters)
+    dx = 100.0 / (59 - 1)
+    w = output.hdf5_xdmf(str(tmp_path), s["grid"], s["dt"], (dx, dx, dx), {0: "psi"}, opts_str="fct", n_iters=iters)
+    w.run(run, s["nt"], s["nt"])
+    psi = hdf5_read.read_dataset(str(tmp_path / "timestep0000000556.h5"), "psi")
+    check_sphere_fields("fct", psi.astype(np.float64))
+    for name in ["timestep0000000000.xmf", "timestep0000000556.xmf", "temp.xmf"]:
+        with open(str(tmp_path / name)) as fh:
+            assert fh.read() == layout[name], name
