@@ -18,17 +18,20 @@
 // Hooks run on the host once per step (rank 0 only: there is one GPU).
 #pragma once
 
+#include <algorithm>
 #include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <mpdx.h>
 
 #include "../bcond/bcond.hpp"
 #include "../opts.hpp"
+#include "../output/hdf5_xdmf.hpp"
 #include "any.hpp"
 
 namespace libmpdataxx {
@@ -45,6 +48,11 @@ inline void check(mpdx_handle h, mpdx_status rc) {
     default: throw std::runtime_error(std::string("libmpdata++ (cuda backend): ") + (h ? mpdx_last_error(h) : mpdx_create_error()));
   }
 }
+// solver types wrapped in output::hdf5_xdmf carry has_output = true
+template <class S, class = void>
+struct has_output : std::false_type {};
+template <class S>
+struct has_output<S, std::void_t<decltype(S::has_output)>> : std::bool_constant<S::has_output> {};
 }  // namespace detail
 
 template <class solver_t, bcond::bcond_e bcxl, bcond::bcond_e bcxr, bcond::bcond_e bcyl = bcond::null,
@@ -106,20 +114,14 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
     return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_E);
   }
 
-  // run.advance(nt) (concurr_common.hpp:380-385); hooks, if set, run after every step
+  // run.advance(nt) (concurr_common.hpp:380-385); hooks, if set, run after every step;
+  // with output::hdf5_xdmf, records on the output steps (output_common.hpp:47-70, 150-165)
   void advance(int nt) override {
-    flush();
-    if (!hook_) {
-      detail::check(h_, mpdx_advance(h_, nt));
-      invalidate_state();
+    if constexpr (detail::has_output<solver_t>::value) {
+      advance_with_output(nt);
       return;
     }
-    for (int t = 0; t < nt && !panic_; ++t) {
-      detail::check(h_, mpdx_advance(h_, 1));
-      invalidate_state();
-      hook_(*this);
-      flush();
-    }
+    advance_steps(nt);
   }
 
   real_t min(int e = 0) override { return libmpdataxx::min(advectee(e)); }
@@ -138,6 +140,57 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   mpdx_handle handle() const { return h_; }
 
  private:
+  void advance_steps(int nt) {
+    flush();
+    if (!hook_) {
+      detail::check(h_, mpdx_advance(h_, nt));
+      invalidate_state();
+      return;
+    }
+    for (int t = 0; t < nt && !panic_; ++t) {
+      detail::check(h_, mpdx_advance(h_, 1));
+      invalidate_state();
+      hook_(*this);
+      flush();
+    }
+  }
+
+  // output steps: timestep % outfreq == 0 and timestep >= outstart; the fields
+  // leave the device only there
+  void advance_with_output(int nt) {
+    const long long t0 = stats().timestep, t1 = t0 + nt;
+    const long long f = std::max(1, int(p_.outfreq));
+    auto is_out = [&](long long t) { return t % f == 0 && t >= p_.outstart; };
+    if (!rec_) {
+      std::vector<int> grid(p_.grid_size.begin(), p_.grid_size.end());
+      std::vector<double> dijk{double(p_.di), double(p_.dj), double(p_.dk)};
+      dijk.resize(size_t(n_dims));
+      rec_.reset(new output::detail::xdmf_recorder(p_.outdir, grid, double(p_.dt), dijk,
+                                                     opts::opts_string(ct_params_t::opts), p_.n_iters));
+      std::vector<double> times;
+      for (long long t = t0; t <= t1; ++t)
+        if (is_out(t)) times.push_back(double(t) * double(p_.dt));
+      rec_->start(times);
+      if (is_out(t0)) record(t0);
+    }
+    long long t = t0;
+    while (t < t1) {
+      long long next = t + 1;
+      while (next < t1 && !is_out(next)) ++next;
+      advance_steps(int(next - t));
+      t = next;
+      if (is_out(t)) record(t);
+    }
+  }
+  void record(long long t) {
+    std::map<std::string, std::vector<float>> fields;
+    for (auto &v : p_.outvars) {
+      arr_t a = advectee(v.first);
+      fields[v.second.name] = std::vector<float>(a.data(), a.data() + a.size());
+    }
+    rec_->record(t, fields);
+  }
+
   struct mirror {
     std::vector<real_t> buf;
     bool fresh = false;
@@ -177,6 +230,7 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   std::map<std::pair<int, int>, mirror> mirrors_;
   std::function<void(cuda &)> hook_;
   bool panic_ = false;
+  std::unique_ptr<output::detail::xdmf_recorder> rec_;
 };
 
 }  // namespace concurr

@@ -35,9 +35,54 @@ def build(name):
     return exe
 
 
-@pytest.mark.parametrize("name", ["advscheme_opts", "revolving_sphere"])
+@pytest.mark.parametrize("name", ["advscheme_opts", "revolving_sphere", "output_layout", "revolving_sphere_output"])
 def test_cpp_programs_compile(name):
     assert os.path.exists(build(name))
+
+
+def _output_layout():
+    with open(os.path.join(ROOT, "tests", "golden", "output_layout.json")) as f:
+        return json.load(f)
+
+
+def test_cpp_output_writer_matches_reference_layout(tmp_path):
+    """The C++ writer's const.h5 messages, coordinates, times and XDMF files are the
+    reference's (the same checks as tests/test_output.py for the Python writer)."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import hdf5_read
+    subprocess.run([build("output_layout"), str(tmp_path)], check=True)
+    r = _output_layout()
+    f = hdf5_read.File(str(tmp_path / "const.h5"))
+    for key, hexbytes in r["messages"].items():
+        name, t = key.split("/")
+        if name != "psi":
+            assert f.message_bytes(name, int(t)).hex() == hexbytes, key
+    mine = f.attribute_messages("advection")
+    assert {k: v.hex() for k, v in mine.items()} == r["advection"]
+    np.testing.assert_array_equal(f.dataset("X")[:, 0, 0], np.float32(r["coords"]["X"]))
+    np.testing.assert_array_equal(f.dataset("Z")[0, 0, :], np.float32(r["coords"]["Z"]))
+    np.testing.assert_array_equal(f.dataset("T"), np.float32(r["coords"]["T"]))
+    for name in ["timestep0000000000.xmf", "timestep0000000556.xmf", "temp.xmf"]:
+        assert (tmp_path / name).read_text() == r[name], name
+    g = hdf5_read.File(str(tmp_path / "timestep0000000556.h5"))
+    assert g.message_bytes("psi", 3).hex() == r["messages"]["psi/3"]
+
+
+@pytest.mark.gpu
+def test_cpp_revolving_sphere_output_matches_golden(tmp_path):
+    """output::hdf5_xdmf<slv_t> on concurr::cuda: the written field passes the 3D
+    golden field check and the XDMF files are the reference's."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import hdf5_read
+    from runners import check_sphere_fields
+    subprocess.run([build("revolving_sphere_output"), str(tmp_path)], check=True)
+    psi = hdf5_read.read_dataset(str(tmp_path / "timestep0000000556.h5"), "psi")
+    check_sphere_fields("fct", psi.astype(np.float64))
+    r = _output_layout()
+    for name in ["timestep0000000000.xmf", "timestep0000000556.xmf", "temp.xmf"]:
+        assert (tmp_path / name).read_text() == r[name], name
 
 
 @pytest.mark.gpu
