@@ -276,3 +276,5 @@ class hdf5_xdmf:
                 run.advance(s - done)
                 done = s
             self.record(s, {name: run.advectee(e) for e, name in self.outvars.items()})
+        if nt > done:  # steps after the last output step
+            run.advance(nt - done)
