@@ -91,3 +91,29 @@ def test_records_and_xdmf_match_reference(tmp_path):
 def test_1d_output_rejected(tmp_path):
     with pytest.raises(ValueError, match="2D and 3D"):
         output.hdf5_xdmf(str(tmp_path), (10,), 1.0, (1.0,), {0: "psi"})
+
+
+def test_run_records_on_output_steps_and_advances_all_steps(tmp_path):
+    """run(): records at 0 and every outfreq steps, reads fields back only there, and
+    advances the steps after the last output step too."""
+    class FakeRun:
+        def __init__(self):
+            self.t, self.reads = 0, []
+
+        def advance(self, n):
+            self.t += n
+
+        def advectee(self, e):
+            self.reads.append(self.t)
+            return np.full((4, 5), float(self.t))
+
+    w = output.hdf5_xdmf(str(tmp_path), (4, 5), 0.5, (1.0, 2.0), {0: "psi"})
+    r = FakeRun()
+    w.run(r, 10, 3)
+    assert r.t == 10 and r.reads == [0, 3, 6, 9]
+    assert w.timesteps == ["timestep%010d.xmf" % t for t in (0, 3, 6, 9)]
+    f = hdf5_read.File(str(tmp_path / "timestep0000000006.h5"))
+    np.testing.assert_array_equal(f.dataset("psi"), np.full((4, 5), 6.0, np.float32))
+    c = hdf5_read.File(str(tmp_path / "const.h5"))
+    np.testing.assert_array_equal(c.dataset("T"), np.float32([0.0, 1.5, 3.0, 4.5]))
+    np.testing.assert_array_equal(c.dataset("Y")[0, :], np.float32(2.0 * np.arange(6)))
