@@ -9,10 +9,12 @@ Mirrors libmpdata++'s concurr::{serial,openmp,threads}<solver_t, bc...>
     run.advance(nt)
     run.advectee(e)                  # state after nt steps (downloaded on access)
 
-Host mirrors handed out by advectee()/advector()/sclr_array() are uploaded
-before the next advance() (the reference's views alias solver memory, so any
-write through them is seen by the next step); after advance() they are
-refreshed on the next access.  Fields otherwise stay on the device.
+Host mirrors handed out by advectee()/advector()/sclr_array() since the last
+advance() are uploaded before the next one (the reference's views alias solver
+memory, so a write through a view is seen by the next step); a mirror that was
+not handed out again is not uploaded again, so write through a view obtained
+after the last advance().  After advance() the advectee mirrors are refreshed
+on the next access.  Fields otherwise stay on the device.
 """
 import ctypes
 
@@ -71,6 +73,7 @@ class cuda:
         self.h = h
         self._mirrors = {}   # (kind, idx) -> ndarray
         self._fresh = set()  # mirrors known to equal the device copy
+        self._dirty = set()  # mirrors handed out since the last upload
 
     # -- lifetime --------------------------------------------------------
     def close(self):
@@ -99,6 +102,7 @@ class cuda:
         if key not in self._fresh:
             _check(self.L, self.h, self.L.mpdx_get_field(self.h, kind, idx, a.ctypes.data, None))
             self._fresh.add(key)
+        self._dirty.add(key)
         return a
 
     def advectee(self, e=0):
@@ -124,8 +128,9 @@ class cuda:
 
     def _flush(self):
         for (kind, idx), a in self._mirrors.items():
-            if (kind, idx) in self._fresh:
+            if (kind, idx) in self._fresh and (kind, idx) in self._dirty:
                 _check(self.L, self.h, self.L.mpdx_set_field(self.h, kind, idx, np.ascontiguousarray(a).ctypes.data, None))
+        self._dirty = set()
         # state fields change on the device; advectors, scalar arrays and G do not
         self._fresh = {k for k in self._fresh if k[0] in (_lib.FIELD_ADVECTOR, _lib.FIELD_SCLR_ARRAY, _lib.FIELD_G)}
 
@@ -135,6 +140,7 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_set_field(self.h, kind, idx, a.ctypes.data, None))
         self._mirrors.pop((kind, idx), None)
         self._fresh.discard((kind, idx))
+        self._dirty.discard((kind, idx))
 
     def set_advectee(self, a, e=0):
         self.set_field(_lib.FIELD_ADVECTEE, e, a)
@@ -146,6 +152,7 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_set_field_device(self.h, kind, idx, ctypes.c_void_p(ptr)))
         self._mirrors.pop((kind, idx), None)
         self._fresh.discard((kind, idx))
+        self._dirty.discard((kind, idx))
 
     def get_field_device(self, kind, idx, ptr):
         _check(self.L, self.h, self.L.mpdx_get_field_device(self.h, kind, idx, ctypes.c_void_p(ptr)))
@@ -156,6 +163,7 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_set_field_async(self.h, kind, idx, ctypes.c_void_p(ptr)))
         self._mirrors.pop((kind, idx), None)
         self._fresh.discard((kind, idx))
+        self._dirty.discard((kind, idx))
 
     def get_field_async(self, kind, idx, ptr):
         """Download into page-locked host memory at ptr (C order), complete after sync()."""
@@ -209,9 +217,16 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_precond_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
 
     def min(self, e=0):
+        """run.min(e): equation 0 from the device-side statistics (no field download)."""
+        if e == 0:
+            self._flush()
+            return float(self.stats()["min"])
         return float(self.advectee(e).min())
 
     def max(self, e=0):
+        if e == 0:
+            self._flush()
+            return float(self.stats()["max"])
         return float(self.advectee(e).max())
 
     def time(self):

@@ -17,6 +17,7 @@
 // that overlap on the GPU (concurrent streams) race on the array and must be
 // serialised by the caller.
 #include <cfloat>
+#include <climits>
 #include <cstring>
 #include <mutex>
 
@@ -139,8 +140,10 @@ extern "C" mpdx_status mpdx_field_stats_noalloc(const void *dev_field, int dtype
     set_err(err, errlen, "extent along axis 0 exceeds the no-allocation maximum of 8192 slices");
     return MPDX_E_ARG;
   }
-  if (n[1] * n[2] > (int64_t(1) << 31)) {
-    set_err(err, errlen, "slice size exceeds 2^31 points");
+  // the kernels index a slice with int: each extent, and a slice's point count,
+  // must stay below 2^31 (checked one extent at a time, so the product cannot overflow)
+  if (n[1] > INT_MAX || n[2] > INT_MAX || n[1] * n[2] >= (int64_t(1) << 31)) {
+    set_err(err, errlen, "slice size must stay below 2^31 points (n[1], n[2] and n[1]*n[2])");
     return MPDX_E_ARG;
   }
   int dev = 0;
@@ -162,16 +165,25 @@ extern "C" mpdx_status mpdx_field_stats_noalloc(const void *dev_field, int dtype
     }
     scratch = g_addr[dev];
   }
+  // launched through cudaLaunchKernel, whose return value is this launch's own
+  // status: an error left pending by an earlier, unrelated call of the caller is
+  // neither reported as this call's failure nor cleared
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int n1 = int(n[1]), n2 = int(n[2]), m0 = int(m[0]), m1 = int(m[1]), m2 = int(m[2]), ns = int(n[0]);
+  cudaError_t e = cudaSuccess;
   if (dtype == 8) {
     view<double> v{static_cast<const double *>(dev_field), strides[0], strides[1], strides[2]};
-    k_slices<double><<<unsigned(n[0]), kThreads, 0, s>>>(v, int(n[1]), int(n[2]), int(m[0]), int(m[1]), int(m[2]), scratch);
+    void *args[] = {&v, &n1, &n2, &m0, &m1, &m2, &scratch};
+    e = cudaLaunchKernel((const void *)k_slices<double>, dim3(unsigned(ns)), dim3(kThreads), args, 0, s);
   } else {
     view<float> v{static_cast<const float *>(dev_field), strides[0], strides[1], strides[2]};
-    k_slices<float><<<unsigned(n[0]), kThreads, 0, s>>>(v, int(n[1]), int(n[2]), int(m[0]), int(m[1]), int(m[2]), scratch);
+    void *args[] = {&v, &n1, &n2, &m0, &m1, &m2, &scratch};
+    e = cudaLaunchKernel((const void *)k_slices<float>, dim3(unsigned(ns)), dim3(kThreads), args, 0, s);
   }
-  k_total<<<1, 32, 0, s>>>(scratch, int(n[0]), dev_out);
-  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    void *args[] = {&scratch, &ns, &dev_out};
+    e = cudaLaunchKernel((const void *)k_total, dim3(1), dim3(32), args, 0, s);
+  }
   if (e != cudaSuccess) {
     set_err(err, errlen, cudaGetErrorString(e));
     return MPDX_E_CUDA;

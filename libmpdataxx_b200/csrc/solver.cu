@@ -451,6 +451,9 @@ struct batch_impl : batch_base {
     if (nt <= 0) return;
     for (size_t p = 0; p < hs.size(); ++p) {
       auto *h = hs[p];
+      // transfers issued with the asynchronous entry points on this member come
+      // first: the seam check and the batched kernel read the uploaded fields
+      h->xfer_async->join(h->stream);
       MPDX_CUDA(cudaStreamSynchronize(h->stream));
       try {
         if (h->st.timestep == 0) h->gen.ante_loop(h->scratch);

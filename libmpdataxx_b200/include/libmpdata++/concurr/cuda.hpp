@@ -12,9 +12,12 @@
 //
 // Fields live on the device.  advectee()/advector()/sclr_array() return
 // writable views of host mirrors: a mirror is downloaded when first handed
-// out after a step, and every mirror handed out is uploaded before the next
-// advance(), so writes through a view behave as writes into the reference's
-// Blitz++ views.  Data otherwise leaves the GPU only when a view is requested.
+// out after a step, and a mirror handed out since the last advance() is
+// uploaded before the next one, so writes through a view behave as writes
+// into the reference's Blitz++ views (write through a view obtained after the
+// last advance(): a mirror not handed out again is not uploaded again).
+// min(0)/max(0) come from the device-side statistics.  Data otherwise leaves
+// the GPU only when a view is requested.
 // Hooks run on the host once per step (rank 0 only: there is one GPU).
 #pragma once
 
@@ -124,8 +127,18 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
     advance_steps(nt);
   }
 
-  real_t min(int e = 0) override { return libmpdataxx::min(advectee(e)); }
-  real_t max(int e = 0) override { return libmpdataxx::max(advectee(e)); }
+  // run.min(e) / run.max(e) (concurr_common.hpp:392-402): equation 0 from the
+  // device-side statistics after pending uploads, other equations from their view
+  real_t min(int e = 0) override {
+    if (e != 0) return libmpdataxx::min(advectee(e));
+    flush();
+    return real_t(stats().min);
+  }
+  real_t max(int e = 0) override {
+    if (e != 0) return libmpdataxx::max(advectee(e));
+    flush();
+    return real_t(stats().max);
+  }
   real_t time() const override { return real_t(stats().timestep) * p_.dt; }
   bool *panic_ptr() override { return &panic_; }
 
@@ -156,7 +169,9 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   }
 
   // output steps: timestep % outfreq == 0 and timestep >= outstart; the fields
-  // leave the device only there
+  // leave the device only there.  As the reference's hook_ante_loop
+  // (output_common.hpp:47-64), every advance() call first rewrites const.h5 for
+  // its nt and records the state it starts from, output step or not.
   void advance_with_output(int nt) {
     const long long t0 = stats().timestep, t1 = t0 + nt;
     const long long f = std::max(1, int(p_.outfreq));
@@ -167,12 +182,17 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
       dijk.resize(size_t(n_dims));
       rec_.reset(new output::detail::xdmf_recorder(p_.outdir, grid, double(p_.dt), dijk,
                                                      opts::opts_string(ct_params_t::opts), p_.n_iters));
-      std::vector<double> times;
-      for (long long t = t0; t <= t1; ++t)
-        if (is_out(t)) times.push_back(double(t) * double(p_.dt));
-      rec_->start(times);
-      if (is_out(t0)) record(t0);
     }
+    // the T axis as hdf5.hpp:199-214 builds it from nt (outwindow 1): with
+    // outstart = 0 the times k outfreq dt for k = 0 .. nt / outfreq; with
+    // outstart > 0 t = 0 first, then outstart + k outfreq for k = 0 .. (nt - outstart) / outfreq
+    // (integer division truncating toward zero, as there)
+    std::vector<double> times;
+    const long long os = p_.outstart;
+    if (os > 0) times.push_back(0.0);
+    for (long long k = 0; k <= (nt - os) / f; ++k) times.push_back(double(os + k * f) * double(p_.dt));
+    rec_->start(times);
+    record(t0);
     long long t = t0;
     while (t < t1) {
       long long next = t + 1;
@@ -185,7 +205,7 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   void record(long long t) {
     std::map<std::string, std::vector<float>> fields;
     for (auto &v : p_.outvars) {
-      arr_t a = advectee(v.first);
+      arr_t a = view(MPDX_FIELD_ADVECTEE, v.first, false);  // read only: not re-uploaded
       fields[v.second.name] = std::vector<float>(a.data(), a.data() + a.size());
     }
     rec_->record(t, fields);
@@ -193,10 +213,11 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
 
   struct mirror {
     std::vector<real_t> buf;
-    bool fresh = false;
+    bool fresh = false;  // equals the device copy (downloaded after the last step)
+    bool dirty = false;  // handed out since the last upload
   };
 
-  arr_t view(int kind, int idx) {
+  arr_t view(int kind, int idx, bool hand_out = true) {
     std::array<int, n_dims> ext, lb;
     for (int d = 0; d < n_dims; ++d) {
       ext[d] = p_.grid_size[d];
@@ -214,15 +235,19 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
       detail::check(h_, mpdx_get_field(h_, kind, idx, m.buf.data(), nullptr));
       m.fresh = true;
     }
+    if (hand_out) m.dirty = true;
     return arr_t(m.buf.data(), lb, ext);
   }
   void flush() {
     for (auto &kv : mirrors_)
-      if (kv.second.fresh) detail::check(h_, mpdx_set_field(h_, kv.first.first, kv.first.second, kv.second.buf.data(), nullptr));
+      if (kv.second.fresh && kv.second.dirty) {
+        detail::check(h_, mpdx_set_field(h_, kv.first.first, kv.first.second, kv.second.buf.data(), nullptr));
+        kv.second.dirty = false;
+      }
   }
   void invalidate_state() {
     for (auto &kv : mirrors_)
-      if (kv.first.first == MPDX_FIELD_ADVECTEE) kv.second.fresh = false;
+      if (kv.first.first == MPDX_FIELD_ADVECTEE) kv.second.fresh = kv.second.dirty = false;
   }
 
   rt_params_t p_;

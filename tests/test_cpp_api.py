@@ -35,7 +35,8 @@ def build(name):
     return exe
 
 
-@pytest.mark.parametrize("name", ["advscheme_opts", "revolving_sphere", "output_layout", "revolving_sphere_output"])
+@pytest.mark.parametrize("name", ["advscheme_opts", "revolving_sphere", "output_layout", "revolving_sphere_output",
+                                  "output_outstart"])
 def test_cpp_programs_compile(name):
     assert os.path.exists(build(name))
 
@@ -83,6 +84,31 @@ def test_cpp_revolving_sphere_output_matches_golden(tmp_path):
     r = _output_layout()
     for name in ["timestep0000000000.xmf", "timestep0000000556.xmf", "temp.xmf"]:
         assert (tmp_path / name).read_text() == r[name], name
+
+
+@pytest.mark.gpu
+def test_cpp_output_outstart_records_start_state_and_t0(tmp_path):
+    """outstart > 0: the state at the start of every advance() call is recorded
+    (output_common.hpp hook_ante_loop) and T holds t = 0 before the output
+    times outstart, outstart + outfreq, ... (output/hdf5.hpp T axis)."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import hdf5_read
+    one, two = tmp_path / "one", tmp_path / "two"
+    subprocess.run([build("output_outstart"), str(one), "1"], check=True)
+    names = sorted(p.name for p in one.glob("timestep*.h5"))
+    assert names == ["timestep%010d.h5" % t for t in (0, 4, 6, 8, 10)], names
+    np.testing.assert_array_equal(hdf5_read.File(str(one / "const.h5")).dataset("T"),
+                                  np.float32([0.0, 2.0, 3.0, 4.0, 5.0]))
+    psi0 = hdf5_read.read_dataset(str(one / "timestep0000000000.h5"), "psi")
+    assert psi0.shape == (16, 12) and psi0.min() == 1.0 and psi0.max() == 2.0
+    subprocess.run([build("output_outstart"), str(two), "2"], check=True)
+    names = sorted(p.name for p in two.glob("timestep*.h5"))
+    assert names == ["timestep%010d.h5" % t for t in (0, 4, 6, 8, 10, 12)], names
+    # the second call's const.h5 is rewritten for its nt = 3: (3 - 4) / 2 truncates to 0,
+    # so T = [0, outstart dt] as the reference computes it
+    np.testing.assert_array_equal(hdf5_read.File(str(two / "const.h5")).dataset("T"), np.float32([0.0, 2.0]))
+    assert (two / "temp.xmf").read_text().count("timestep0000000010.xmf") == 2
 
 
 @pytest.mark.gpu

@@ -88,3 +88,33 @@ def test_batch_rejects_mixed_problems():
     r3 = make(probs[1], o.fct, 2, np.float64)
     with pytest.raises(RuntimeError, match="same dtype"):
         concurr.batch([r1, r3])
+
+
+@pytest.mark.parametrize("mode", ["persistent", "per_problem"])
+def test_batch_after_async_uploads_equals_synchronous_uploads(mode):
+    """Fields uploaded with the asynchronous entry points right before a batched
+    advance are in place when the batch reads them (the batch waits for every
+    member's pending transfers)."""
+    import torch
+    from libmpdataxx_b200 import _lib
+    probs = setups.batched_problems(n=5, seed=17, lo=200, hi=600)
+    want = [make(s, o.fct, 2, np.float32) for s in probs]
+    bw = concurr.batch(want, mode=mode)
+    bw.advance(3)
+    runs = [make(s, o.fct, 2, np.float32) for s in probs]
+    b = concurr.batch(runs, mode=mode)
+    b.advance(3)
+    b.sync()
+    # upload a new advectee (the synchronous twin gets the same one) and advance at once
+    rng = np.random.default_rng(3)
+    keep = []
+    for r, w, s in zip(runs, want, probs):
+        a = setups.wrap_periodic(rng.uniform(0.5, 2.0, size=tuple(g - 1 for g in s["grid"]))).astype(np.float32)
+        t = torch.from_numpy(a).pin_memory()
+        keep.append(t)
+        r.set_field_async(_lib.FIELD_ADVECTEE, 0, t.data_ptr())
+        w.set_advectee(a)
+    b.advance(4)
+    bw.advance(4)
+    for r, w in zip(runs, want):
+        np.testing.assert_array_equal(r.advectee(), w.advectee())

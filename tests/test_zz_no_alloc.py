@@ -70,3 +70,8 @@ def test_noalloc_rejects_oversized_fields():
     rc = _entry()(dev.data_ptr(), 8, _i64([8193, 1, 1]), _i64([1, 1, 1]), _i64([8193, 1, 1]), out.data_ptr(),
                   None, err, 256)
     assert rc == _lib.MPDX_E_ARG and "8192" in err.value.decode()
+    # slice extents that the int-indexed kernels cannot address: each one alone,
+    # and a product at 2^31 or beyond (no launch happens, nothing is read)
+    for n in ([1, 2 ** 31, 1], [1, 1, 2 ** 31], [1, 2 ** 16, 2 ** 15], [1, 2 ** 62, 2 ** 62]):
+        rc = _entry()(dev.data_ptr(), 8, _i64(n), _i64([1, 1, 1]), _i64([0, 0, 0]), out.data_ptr(), None, err, 256)
+        assert rc == _lib.MPDX_E_ARG and "2^31" in err.value.decode(), (n, err.value)
