@@ -157,27 +157,55 @@ def build_run(w, dtype, torch):
     return run
 
 
-def cpu_baseline(n=160, steps=3):
-    """Oracle (CPU restatement, -Ofast + OpenMP on all host threads) on a
-    bounded sample: n^3 of the same configuration, `steps` steps."""
+def cpu_port_time(host, steps, warmup):
+    """The oracle's -Ofast + OpenMP build (the CPU restatement of the reference's
+    path) on the whole 3D workload `host` (numpy advectee and advector views):
+    `warmup` untimed steps, then `steps` timed ones; returns (seconds, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
-    from libmpdataxx_b200 import opts, setups
+    from libmpdataxx_b200 import opts
     from oracle import Oracle
-    gx, gy, gz = setups.periodic_curl_3d(n, 3, cmax=0.4, dtype=np.float32)
-    rng = np.random.default_rng(4)
-    psi = setups.wrap_periodic(rng.uniform(0, 1, size=(n - 1,) * 3))
-    orc = Oracle((n,) * 3, opts.fct | opts.iga, n_iters=2, dtype=np.float32, fast=True, max_abs_div_eps=1e-6)
+    psi, gx, gy, gz = host
+    orc = Oracle(psi.shape, opts.fct | opts.iga, n_iters=2, dtype=psi.dtype.type, fast=True, max_abs_div_eps=1e-6)
     orc.set_advectee(psi)
     for d, a in enumerate((gx, gy, gz)):
         orc.set_advector(a, d)
-    orc.advance(1)  # ante-loop checks and first touch
+    orc.advance(max(1, warmup))  # ante-loop checks and first touch of every field
     t0 = time.perf_counter()
     orc.advance(steps)
     dt = time.perf_counter() - t0
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    del orc
+    import oracle as orc_mod
+    return dt, orc_mod.max_threads()
+
+
+def cpu_baseline(host, n, steps=5):
+    """Oracle (CPU restatement, -Ofast + OpenMP on all host threads) on the bench's
+    own n^3 workload (same flow and blobs), `steps` steps."""
+    dt, threads = cpu_port_time(host, steps, 1)
     return {"value": n ** 3 * steps / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{n}^3 fct|iga n_iters=2 FP32, {steps} steps, {dt:.1f} s, oracle -Ofast+OpenMP"}
+            "sample": f"the full {n}^3 fct|iga n_iters=2 FP32 workload of this line (same flow and blobs), "
+                      f"{steps} steps after 1 untimed, {dt:.1f} s; oracle -Ofast + OpenMP"}
+
+
+def fp64_error(w, fp32_state, steps, torch):
+    """Error of the FP32 headline run against an FP64 run of the same inputs: the
+    FP32 advectee and advector promoted to FP64, advanced `steps` steps by the
+    FP64 fused kernel (the FP64 path equals the FP64 CPU restatement of the
+    reference to <= 1e-12), compared with the FP32 state after as many steps."""
+    from libmpdataxx_b200 import _lib
+    w64 = {"grid": w["grid"], "advectee": [w["advectee"][0].double()], "advector": [a.double() for a in w["advector"]]}
+    run = build_run(w64, "float64", torch)
+    run.advance(steps)
+    out = torch.empty_like(w64["advectee"][0])
+    run.get_field_device(_lib.FIELD_ADVECTEE, 0, out.data_ptr())
+    run.sync()
+    run.close()
+    d = fp32_state.double() - out
+    n = w["grid"][0]
+    return {"vs": "FP64 run of the same (FP32-rounded) inputs through the FP64 fused kernel", "after_steps": steps,
+            "max_abs": float(d.abs().max()), "l2": float(d.square().mean().sqrt()),
+            "field_max": float(out.abs().max()), "cells": n ** 3}
 
 
 def batched_extra(n_problems=256, steps=50):
@@ -220,6 +248,62 @@ def batched_extra(n_problems=256, steps=50):
         for r in runs:
             r.close()
     out["speedup_vs_per_problem"] = out["persistent"]["cell_updates_per_s"] / out["per_problem"]["cell_updates_per_s"]
+    return out
+
+
+def box_1d_extra(steps=1000):
+    """C1: 1D plain MPDATA (opts 0, n_iters 2), 2000 cyclic points, FP64, 1000 steps:
+    device time on the solver's stream (the general path: one kernel per formula
+    and halo fill, launch-bound at this size), mass and minimum after the run, and
+    the CPU restatement on the same set-up (one thread and all threads)."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from libmpdataxx_b200 import bcond, concurr, setups, solvers
+    from oracle import Oracle
+    s = setups.box_1d()
+    nx = s["grid"][0]
+
+    class ct(solvers.ct_params_default_t):
+        pass
+
+    ct.real_t = np.float64
+    ct.n_dims = 1
+    ct.n_eqns = 1
+    ct.opts = s["opts"]
+    p = solvers.mpdata.rt_params_t(grid_size=[nx], n_iters=s["n_iters"])
+    run = concurr.cuda(solvers.mpdata(ct), *[bcond.cyclic] * 2, p=p)
+    run.set_advectee(s["advectee"][0])
+    run.set_advector(s["advector"][0], 0)
+    m0 = run.stats()["mass"]
+    run.advance(5)
+    run.sync()
+    stream = torch.cuda.ExternalStream(run.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        run.advance(steps - 5)
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / (steps - 5)
+    st = run.stats()
+    run.close()
+    out = {"workload": f"1D {nx} cyclic, opts 0, n_iters 2, FP64, box on 0.1 + noise, C = 0.5, {steps} steps",
+           "ms_per_step": ms, "cell_updates_per_s": nx / (ms * 1e-3), "after_steps": steps,
+           "mass_rel_drift": (st["mass"] - m0) / m0, "min": st["min"]}
+    import oracle as orc_mod
+    threads = orc_mod.max_threads()
+    for label, nthr in (("cpu_port_1_thread", 1), ("cpu_port_all_threads", threads)):
+        orc_mod.set_threads(nthr)
+        orc = Oracle(s["grid"], s["opts"], n_iters=s["n_iters"], bcs=s["bcs"], fast=True)
+        orc.set_advectee(s["advectee"][0])
+        orc.set_advector(s["advector"][0], 0)
+        orc.advance(5)
+        t0 = time.perf_counter()
+        orc.advance(steps - 5)
+        dt = (time.perf_counter() - t0) / (steps - 5)
+        out[label] = {"ms_per_step": dt * 1e3, "cell_updates_per_s": nx / dt, "threads": nthr}
+    orc_mod.set_threads(threads)
     return out
 
 
@@ -316,40 +400,29 @@ def gcr_extra(grid=(256, 256, 128), record=20, train=400, compare=5):
 
 
 def reference_arm(args, rank):
-    """Each step advances a bounded sample of the workload: the same
-    configuration on an n_ref^3 grid (default 256^3, 1/8 of the cells), so that
-    K steps of the CPU path finish within minutes; the metric is per cell."""
+    """The reference's CPU path (its CPU restatement: the reference itself needs
+    Blitz++ and Boost, absent here) on this host's cores, on the same workload as
+    the GPU arm: the 512^3 flow and blobs of workloads.advection_3d, generated on
+    the host; every step is one full-grid MPDATA step."""
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-    from libmpdataxx_b200 import opts, setups
-    from oracle import Oracle
-    n = args.n_ref
-    gx, gy, gz = setups.periodic_curl_3d(n, 3, cmax=0.4, dtype=np.float32)
-    rng = np.random.default_rng(4)
-    psi = setups.wrap_periodic(rng.uniform(0, 1, size=(n - 1,) * 3).astype(np.float32))
-    orc = Oracle((n,) * 3, opts.fct | opts.iga, n_iters=2, dtype=np.float32, fast=True, max_abs_div_eps=1e-6)
-    orc.set_advectee(psi)
-    for d, a in enumerate((gx, gy, gz)):
-        orc.set_advector(a, d)
-    for _ in range(args.warmup):
-        orc.advance(1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        orc.advance(1)
-    dt = time.perf_counter() - t0
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    from libmpdataxx_b200 import workloads
+    w = workloads.advection_3d(n=args.size, dtype=args.dtype, device="cpu")
+    host = [w["advectee"][0].numpy()] + [a.numpy() for a in w["advector"]]
+    del w
+    dt, threads = cpu_port_time(host, args.steps, args.warmup)
+    n = args.size
     value = n ** 3 * args.steps / dt
     line = {"impl": "reference", "metric": "cell-updates/s per MPDATA step", "value": value,
             "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"3D MPDATA {args.n}^3 cyclic fct|iga n_iters=2 float32 (FP64 mass sums)",
-                       "grid": [args.n] * 3, "sample_grid": [n] * 3},
+            "vs_baseline": None, "dtype": "f32" if args.dtype == "float32" else "f64", "data": "synthetic",
+            "config": {"workload": f"3D MPDATA {n}^3 cyclic fct|iga n_iters=2 {args.dtype} (FP64 mass sums)",
+                       "grid": [n] * 3, "opts": "fct|iga", "n_iters": 2, "same_config": True},
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                             "sample": f"{n}^3 grid per step (bounded sample of the {args.n}^3 workload); CPU restatement of the reference "
-                                       "(reference unbuildable here: Blitz++/Boost absent), -Ofast + OpenMP"},
+                             "sample": f"the full {n}^3 workload every step ({args.steps} timed steps after "
+                                       f"{args.warmup}); CPU restatement of the reference (reference unbuildable "
+                                       "here: Blitz++/Boost absent), -Ofast + OpenMP"},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -360,12 +433,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
-    ap.add_argument("--n", type=int, default=512)
-    ap.add_argument("--n-ref", type=int, default=256)
+    ap.add_argument("--size", type=int, default=512, help="grid points per axis of the 3D workload")
     ap.add_argument("--dtype", default="float32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the 2D rotation, batched-2D and Boussinesq/GCR measurements")
-    ap.add_argument("--extra", choices=["rotation_2d", "batched_2d", "gcr"],
+    ap.add_argument("--extra", choices=["box_1d", "rotation_2d", "batched_2d", "gcr"],
                     help="run only this one extra measurement on one GPU and print its JSON object")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -377,13 +449,13 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.extra:
-        fn = {"rotation_2d": rotation_extra, "batched_2d": batched_extra, "gcr": gcr_extra}[args.extra]
+        fn = {"box_1d": box_1d_extra, "rotation_2d": rotation_extra, "batched_2d": batched_extra, "gcr": gcr_extra}[args.extra]
         print(json.dumps({args.extra: fn()}))
         return
     from libmpdataxx_b200 import _lib, workloads
-    w = workloads.advection_3d(n=args.n, dtype=args.dtype)
+    w = workloads.advection_3d(n=args.size, dtype=args.dtype)
     run = build_run(w, args.dtype, torch)
-    n_cells = float(args.n) ** 3
+    n_cells = float(args.size) ** 3
     stream = torch.cuda.ExternalStream(run.stream)
 
     def barrier():
@@ -411,6 +483,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
+    steps_done = max(args.warmup, 3) + args.steps
+    state = torch.empty_like(w["advectee"][0])
+    run.get_field_device(_lib.FIELD_ADVECTEE, 0, state.data_ptr())
     per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     ms_total = max_over_ranks(ev[0].elapsed_time(ev[-1]), world)
     ms_step = ms_total / args.steps
@@ -446,32 +521,38 @@ def main():
     hbm, src = peaks()
     avg_launch_ms = statistics.mean(per)
     achieved = BYTES_PER_CELL * n_cells / (avg_launch_ms / 1e3) / 1e9
-    traffic = None
+    traffic, traffic_src = None, None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        key = f"fused3d_{args.dtype}_{args.n}"
+        key = f"fused3d_{args.dtype}_{args.size}"
         if key in tj:
             traffic = tj[key]
+            traffic_src = tj.get("_source", {}).get(key)
     line = {
         "metric": "cell-updates/s per MPDATA step", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.dtype == "float32" else "f64",
         "data": "synthetic",
-        "config": {"workload": f"3D MPDATA {args.n}^3 cyclic fct|iga n_iters=2 {args.dtype} (FP64 mass sums)",
-                   "grid": [args.n] * 3, "opts": "fct|iga", "n_iters": 2, "parallelism": f"replicas x{world}",
+        "config": {"workload": f"3D MPDATA {args.size}^3 cyclic fct|iga n_iters=2 {args.dtype} (FP64 mass sums)",
+                   "grid": [args.size] * 3, "opts": "fct|iga", "n_iters": 2, "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2 ({BYTES_PER_CELL * n_cells / 1e9:.2f} GB per step)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_source": src,
+                     "traffic": traffic, "traffic_source": traffic_src, "peak_source": src,
                      "bytes_per_launch": BYTES_PER_CELL * n_cells, "avg_launch_ms": avg_launch_ms},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps,
         "clocks": clocks,
     }
+    line["error"] = fp64_error(w, state, steps_done, torch)
+    del state
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        host = [t.cpu().numpy() for t in w["advectee"] + w["advector"]]
+        line["cpu_baseline"] = cpu_baseline(host, args.size)
+        del host
     if world == 1 and not args.no_extras:
+        line["box_1d"] = box_1d_extra()
         line["rotation_2d"] = rotation_extra()
         line["batched_2d"] = batched_extra()
         line["gcr"] = gcr_extra()

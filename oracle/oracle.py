@@ -54,8 +54,19 @@ def lib(fast=False):
     L.orc_last_iters.restype = ctypes.c_longlong
     L.orc_last_error.argtypes = [vp]
     L.orc_last_error.restype = ctypes.c_char_p
+    L.orc_set_threads.argtypes = [ctypes.c_int]
+    L.orc_max_threads.restype = ctypes.c_int
     _libs[name] = L
     return L
+
+
+def set_threads(n, fast=True):
+    """OpenMP threads of the oracle's parallel loops from now on."""
+    lib(fast).orc_set_threads(int(n))
+
+
+def max_threads(fast=True):
+    return lib(fast).orc_max_threads()
 
 
 def _dptr(a):

@@ -77,6 +77,8 @@ struct bq_wrap_t : wrap_t<boussinesq<T>, T> {
 
 }  // namespace
 
+#include <omp.h>
+
 extern "C" {
 
 void *orc_mpdata_create(int dtype, int nd, const int *n, int n_eqns, unsigned opts, int n_iters,
@@ -138,5 +140,10 @@ int orc_advance(void *h, long long nt) { ORC_TRY(static_cast<base_t *>(h)->advan
 long long orc_timestep(void *h) { return static_cast<base_t *>(h)->timestep(); }
 long long orc_last_iters(void *h) { return static_cast<base_t *>(h)->last_iters(); }
 const char *orc_last_error(void *h) { return static_cast<base_t *>(h)->err.c_str(); }
+
+// OpenMP threads of the parallel loops that follow (the timed CPU baseline runs
+// with one thread and with all host threads in one process)
+void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+int orc_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -52,7 +52,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--n-ref", "24"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--size", "24"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
