@@ -3,8 +3,11 @@
 // gets its own compiler flags.
 #pragma once
 
+#include <type_traits>
+
 #include "fused.cuh"
 #include "fused3d.cuh"
+#include "fused3d_f32.cuh"
 #include "fused2d_batch.cuh"
 
 namespace mpdx {
@@ -51,6 +54,19 @@ static void launch3(const f3::args<T> &a, cudaStream_t s, dim3 grid) {
   MPDX_LAUNCH_CHECK();
 }
 
+// the FP32 kernel with the regrouped single-precision arithmetic (iga variants)
+template <bool FCT>
+static void launch3s(const f3::args<float> &a, cudaStream_t s, dim3 grid) {
+  constexpr int CR = tiles<float>::CR;
+  using C = f3::canvas<CR>;
+  auto kern = f3s::k_fused3d_s<FCT, CR>;
+  const size_t bytes = size_t(C::total) * C::N * sizeof(float);
+  static bool attr = false;
+  if (!attr) { set_smem(kern, bytes); attr = true; }
+  kern<<<grid, C::NT, bytes, s>>>(a);
+  MPDX_LAUNCH_CHECK();
+}
+
 template <class T>
 void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
   using C = f3::canvas<tiles<T>::CR>;
@@ -66,6 +82,13 @@ void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
   const int tiles_y = (a.P1 + C::TY - 1) / C::TY;
   dim3 grid(tiles_y * a.tiles_z, (a.P0 + LX - 1) / LX);
   const bool iga = st.opts & o_iga, fct = st.opts & o_fct;
+  if constexpr (std::is_same<T, float>::value) {
+    if (iga) {
+      if (fct) launch3s<true>(a, s, grid);
+      else launch3s<false>(a, s, grid);
+      return;
+    }
+  }
   if (iga && fct) launch3<T, true, true>(a, s, grid);
   else if (iga) launch3<T, true, false>(a, s, grid);
   else if (fct) launch3<T, false, true>(a, s, grid);
