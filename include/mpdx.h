@@ -35,8 +35,13 @@ typedef enum {
   MPDX_E_ARG = 7          /* invalid argument (null pointer, index out of range, ...) */
 } mpdx_status;
 
-/* boundary kinds (libmpdata++/bcond/detail/bcond_common.hpp bcond_e) */
-enum { MPDX_BC_CYCLIC = 0, MPDX_BC_OPEN = 1, MPDX_BC_RIGID = 2 };
+/* boundary kinds (libmpdata++/bcond/detail/bcond_common.hpp bcond_e).  GNDSKY is the
+ * 3D ground / sky condition of bcond/gndsky_3d.hpp: the rigid condition on every
+ * field this backend fills (its own fills are for subgrid-scale fields only). */
+enum { MPDX_BC_CYCLIC = 0, MPDX_BC_OPEN = 1, MPDX_BC_RIGID = 2, MPDX_BC_GNDSKY = 3 };
+
+/* velocity absorber (ct_params_t::vip_vab, mpdata_rhs_vip_common.hpp:16-21) */
+enum { MPDX_VAB_NONE = 0, MPDX_VAB_EXPL = 1, MPDX_VAB_IMPL = 2 };
 
 /* solver families (solvers::mpdata, solvers::boussinesq) */
 enum { MPDX_SOLVER_MPDATA = 0, MPDX_SOLVER_BOUSSINESQ = 1 };
@@ -60,7 +65,10 @@ enum {
   MPDX_FIELD_PRESSURE = 3,   /* Boussinesq: Phi, interior */
   MPDX_FIELD_G = 4           /* g_factor() with the nug option: G, interior (sharedmem.hpp:373-380) */
 };
-enum { MPDX_SCLR_THT_E = 0 };
+/* scalar arrays: sclr_array("tht_e"), ("tht_abs"), ("hflux_frc") (boussinesq_common.hpp:20-60),
+ * vab_coefficient() and vab_relaxed_state(d) (concurr_common.hpp:415-433) as MPDX_SCLR_VAB_RELAX + d */
+enum { MPDX_SCLR_THT_E = 0, MPDX_SCLR_THT_ABS = 1, MPDX_SCLR_HFLUX_FRC = 2, MPDX_SCLR_VAB_COEFF = 3,
+       MPDX_SCLR_VAB_RELAX = 4 };
 
 /* Run-time and compile-time parameters of one solver (ct_params_t + rt_params_t,
  * libmpdata++/opts.hpp:81-100, solver_common.hpp:217-221, mpdata_common.hpp:74-78,
@@ -86,6 +94,8 @@ typedef struct {
   int precond;             /* MPDX_PRECOND_* */
   int prs_fp64;            /* 1: pressure fields in FP64 even when real_t is float */
   int upwind_filter_freq;  /* rt_params upwind_filter_freq (mpdata_common.hpp:77): every n-th step is upwind only; 0 = never */
+  int impl_tht;            /* ct_params_t::impl_tht: theta is the perturbation from tht_e, its coupling with w implicit (boussinesq_impl.hpp) */
+  int vip_vab;             /* ct_params_t::vip_vab: MPDX_VAB_* velocity absorber */
 } mpdx_config;
 
 typedef struct mpdx_solver *mpdx_handle;

@@ -12,13 +12,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SO_PATH = os.path.join(HERE, "libmpdx.so")
 
 MPDX_OK, MPDX_E_GRID, MPDX_E_DIVERGENT, MPDX_E_PRS_STUCK, MPDX_E_UNSUPPORTED, MPDX_E_CUDA, MPDX_E_TIMEOUT, MPDX_E_ARG = range(8)
-BC = {"cyclic": 0, "open": 1, "rigid": 2}
+BC = {"cyclic": 0, "open": 1, "rigid": 2, "gndsky": 3}
 SOLVER_MPDATA, SOLVER_BOUSSINESQ = 0, 1
 PRS_CR, PRS_GCRK = 0, 1
 PRECOND_IDENTITY, PRECOND_LEARNED = 0, 1
 PATH_AUTO, PATH_GENERAL, PATH_FUSED = 0, 1, 2
 FIELD_ADVECTEE, FIELD_ADVECTOR, FIELD_SCLR_ARRAY, FIELD_PRESSURE, FIELD_G = 0, 1, 2, 3, 4
 SCLR_THT_E = 0
+SCLR_THT_ABS = 1
+SCLR_HFLUX_FRC = 2
+SCLR_VAB_COEFF = 3
+SCLR_VAB_RELAX = 4  # + d
+VAB_NONE, VAB_EXPL, VAB_IMPL = 0, 1, 2
 
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
@@ -42,7 +47,8 @@ class Config(ctypes.Structure):
                 ("prs_k_iters", ctypes.c_int), ("prs_tol", ctypes.c_double), ("g", ctypes.c_double),
                 ("tht_ref", ctypes.c_double), ("ix_u", ctypes.c_int), ("ix_v", ctypes.c_int),
                 ("ix_w", ctypes.c_int), ("ix_tht", ctypes.c_int), ("precond", ctypes.c_int),
-                ("prs_fp64", ctypes.c_int), ("upwind_filter_freq", ctypes.c_int)]
+                ("prs_fp64", ctypes.c_int), ("upwind_filter_freq", ctypes.c_int),
+                ("impl_tht", ctypes.c_int), ("vip_vab", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):

@@ -12,3 +12,4 @@ class _bc:
 cyclic = _bc("cyclic")
 open = _bc("open")
 rigid = _bc("rigid")
+gndsky = _bc("gndsky")  # bcond/gndsky_3d.hpp: ground (left) and sky (right) of the vertical axis, rigid for iles

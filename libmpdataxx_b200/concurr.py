@@ -111,10 +111,21 @@ class cuda:
     def advector(self, d=0):
         return self._mirror(_lib.FIELD_ADVECTOR, d)
 
+    _SCLR = {"tht_e": _lib.SCLR_THT_E, "tht_abs": _lib.SCLR_THT_ABS, "hflux_frc": _lib.SCLR_HFLUX_FRC}
+
     def sclr_array(self, name, n=0):
-        if name != "tht_e":
+        """Named scalar arrays of the Boussinesq solver (boussinesq_common.hpp:20-60)."""
+        if name not in self._SCLR:
             raise KeyError(name)
-        return self._mirror(_lib.FIELD_SCLR_ARRAY, _lib.SCLR_THT_E)
+        return self._mirror(_lib.FIELD_SCLR_ARRAY, self._SCLR[name])
+
+    def vab_coefficient(self):
+        """vab_coefficient() (concurr_common.hpp:420-423): the velocity absorber's coefficient."""
+        return self._mirror(_lib.FIELD_SCLR_ARRAY, _lib.SCLR_VAB_COEFF)
+
+    def vab_relaxed_state(self, d=0):
+        """vab_relaxed_state(d) (concurr_common.hpp:425-428): the velocity the absorber relaxes to."""
+        return self._mirror(_lib.FIELD_SCLR_ARRAY, _lib.SCLR_VAB_RELAX + d)
 
     def g_factor(self):
         """G of the nug option (sharedmem.hpp:373-380): a writable mirror, uploaded before the next advance."""

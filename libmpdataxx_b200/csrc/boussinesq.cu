@@ -47,6 +47,11 @@ struct geom {
   double dxd[3], rdxd[3];   // spacing and RN(1/spacing), FP64
   float dxf[3], rdxf[3];    // the same in FP32
   long long cells;
+  // normalize_vip of the gradient inside lap() (mpdata_rhs_vip_prs_common.hpp:72-74):
+  // lap_tmp[d] /= den[d] at every point, den[d] a pressure-type field; norm = 0: none
+  int norm = 0;
+  const void *den[3] = {nullptr, nullptr, nullptr};
+  template <class T> __device__ __forceinline__ T dn(int d, long long q) const { return static_cast<const T *>(den[d])[q]; }
   template <class T> __device__ __forceinline__ T dx(int d) const { if constexpr (sizeof(T) == 4) return dxf[d]; else return dxd[d]; }
   template <class T> __device__ __forceinline__ T rdx(int d) const { if constexpr (sizeof(T) == 4) return rdxf[d]; else return rdxd[d]; }
 };
@@ -140,6 +145,7 @@ __device__ __forceinline__ T lt(const F &A, const U &u, const geom &g, int d, lo
   if (rigid_edge(g, d, q)) return T(0);
   T v = grad<T>(A, g, d, base, sd, q);
   if constexpr (is_vec<U>::value) v -= T(u.u[d].o[ubase + q * usd]);
+  if (g.norm) v = v / g.dn<T>(d, base + q * sd);
   return v;
 }
 // lap_tmp[d] at coordinate q in [-1, n] (its own pressure halo fill)
@@ -179,6 +185,10 @@ __device__ __forceinline__ T lap(const F &A, const dfield<T> &lay, const U &u, c
         const long long usd = stride(u.u[d], d), uo = off3(u.u[d], i, j, k);
         gp -= T(u.u[d].o[uo + usd]);
         gm -= T(u.u[d].o[uo - usd]);
+      }
+      if (g.norm) {
+        gp = gp / g.dn<T>(d, o + sd);
+        gm = gm / g.dn<T>(d, o - sd);
       }
       const T term = mpdx::qdiv<T>(gp - gm, dx, rdx) * T(0.5);
       r = d == 0 ? term : r + term;
@@ -683,7 +693,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
 template <class T, int NV>
 void launch_inner(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, T err_tol, dfield<T> phi, dfield<T> e0,
                   dfield<T> e1, dfield<T> le, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
-  if (g.nd == 3) k_gcr_update3<T, NV><<<G, blk, 0, s>>>(g, err_tol, e0, e1, le, D, dv, part, kGcrChunk);
+  if (g.nd == 3 && !g.norm) k_gcr_update3<T, NV><<<G, blk, 0, s>>>(g, err_tol, e0, e1, le, D, dv, part, kGcrChunk);
   else k_gcr_update<T, NV><<<G, blk, 0, s>>>(g, err_tol, e0, e1, le, D, dv, part);
   k_gcr_direction<T, NV><<<G, blk, 0, s>>>(g, kk, phi, e0, e1, le, D, dv, part);
 }
@@ -909,7 +919,8 @@ enum { APPLY_PROJECT = 0, APPLY_RHS = 1, APPLY_FINISH = 2 };
 
 // grad Phi applied to the velocities: pressure_solver_apply + set_edges
 // (PROJECT), vip_rhs -= grad Phi (RHS, hook_ante_loop), or pressure_solver_apply +
-// set_edges + vip_rhs = (vip_rhs + u) / (dt / 2) (FINISH, vip_rhs_impl_fnlz)
+// normalize_vip (with g.norm) + set_edges + vip_rhs = (vip_rhs + u) / (dt / 2)
+// (FINISH, vip_rhs_impl_fnlz)
 template <class T, class P>
 __global__ void __launch_bounds__(kRedThreads, 4) k_apply_grad(geom g, int mode, dfield<P> phi, vec_u<T> vel, vec_u<T> vr, T hdt) {
   for_interior(g, [&](int i, int j, int k) {
@@ -924,6 +935,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_apply_grad(geom g, int mode,
         continue;
       }
       T v = T(P(vel.u[d](i, j, k)) - gd);
+      if (mode == APPLY_FINISH && g.norm) v = v / T(g.dn<P>(d, off3(phi, i, j, k)));  // normalize_vip
       if (rigid_edge(g, d, c[d])) v = T(0);
       vel.u[d](i, j, k) = v;
       if (mode == APPLY_FINISH) {
@@ -964,11 +976,26 @@ __global__ void k_intrp(dfield<T> gc, dfield<T> src, int d, T c, int i0, int j0,
   }
 }
 
-// hook_ante_step: fill_stash, apply_rhs(dt / 2), vip_rhs_apply
+// fields and constants of the forcings: theta environment, absorber, heat flux
+// (boussinesq_common.hpp:20-60, boussinesq_impl.hpp), velocity absorber
+// (mpdata_rhs_vip_common.hpp:182-256)
 template <class T>
-__global__ void k_ante_step(geom g, int ne, eqns<T> E, const int *vip, vec_u<T> stash, vec_u<T> vr, T dt2, T hdt) {
+struct forcing {
+  dfield<T> the, tabs, hflx, dthe, vabc;
+  vec_u<T> relax;
+  int impl, vab;  // impl_tht; vip_vab (MPDX_VAB_*)
+  T grav, tref, dt;
+};
+
+// hook_ante_step: fill_stash, vip_rhs_expl_calc, apply_rhs(dt / 2), vip_rhs_apply
+template <class T>
+__global__ void k_ante_step(geom g, int ne, eqns<T> E, const int *vip, vec_u<T> stash, vec_u<T> vr, T dt2, T hdt,
+                            forcing<T> F) {
   for_interior(g, [&](int i, int j, int k) {
     _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) stash.u[d](i, j, k) = E.psi[vip[d]](i, j, k);
+    if (F.vab == MPDX_VAB_EXPL)  // factor 2: vip_rhs_apply multiplies by dt / 2
+      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd)
+        vr.u[d](i, j, k) += -2 * F.vabc(i, j, k) * (E.psi[vip[d]](i, j, k) - F.relax.u[d](i, j, k));
     _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
     _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
       E.psi[vip[d]](i, j, k) = E.psi[vip[d]](i, j, k) + hdt * vr.u[d](i, j, k);
@@ -977,20 +1004,95 @@ __global__ void k_ante_step(geom g, int ne, eqns<T> E, const int *vip, vec_u<T> 
     });
 }
 
-// update_rhs (rhs = 0; rhs[w] += g (tht - tht_e) / Tht_ref), then (post step)
-// apply_rhs(dt / 2) and vip_rhs = -u, or (ante loop) vip_rhs = 0
+// update_rhs (rhs = 0, then the buoyancy and theta forcings of boussinesq_expl.hpp:81-126
+// or boussinesq_impl.hpp:82-113 at `at` = 0 / 1), then (post step) apply_rhs(dt / 2),
+// vip_rhs = -u and add_relax, or (ante loop) vip_rhs_impl_init
 template <class T>
-__global__ void k_rhs(geom g, int ne, int post, eqns<T> E, const int *vip, int iw, int ith, dfield<T> the, T grav,
-                      T tref, T dt2, vec_u<T> vr) {
+__global__ void k_rhs(geom g, int ne, int post, eqns<T> E, const int *vip, int iw, int ith, forcing<T> F, T dt2,
+                      vec_u<T> vr) {
   for_interior(g, [&](int i, int j, int k) {
     _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.rhs[e](i, j, k) = T(0);
-    E.rhs[iw](i, j, k) = T(0) + grav * (E.psi[ith](i, j, k) - the(i, j, k)) / tref;
+    const T th = E.psi[ith](i, j, k), te = F.the(i, j, k), ta = F.tabs(i, j, k), hf = F.hflx(i, j, k);
+    const T hdt = T(0.5) * F.dt;
+    if (!F.impl) {
+      if (!post) {
+        E.rhs[ith](i, j, k) = T(0) + (hf - ta * (th - te));
+        E.rhs[iw](i, j, k) = T(0) + F.grav * (th - te) / F.tref;
+      } else {
+        const T x = (th + hdt * hf + hdt * ta * te) / (1 + hdt * ta);
+        E.rhs[ith](i, j, k) = T(0) + (hf - ta * (x - te));
+        E.rhs[iw](i, j, k) = T(0) + F.grav * (x - te) / F.tref;
+      }
+    } else if (!post) {
+      E.rhs[ith](i, j, k) = T(0) + (-E.psi[iw](i, j, k) * F.dthe(i, j, k) + hf - ta * th);
+      E.rhs[iw](i, j, k) = T(0) + F.grav * th / F.tref;
+    } else {
+      const T rt = T(0) + hf;
+      E.rhs[ith](i, j, k) = rt;
+      E.rhs[iw](i, j, k) = T(0) + F.grav * (th + hdt * rt) / (F.tref * (1 + hdt * ta));
+    }
     if (post) {
       _Pragma("unroll") for (int e = 0; e < 4; ++e) if (e < ne) E.psi[e](i, j, k) = E.psi[e](i, j, k) + dt2 * E.rhs[e](i, j, k);
-      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) vr.u[d](i, j, k) = -E.psi[vip[d]](i, j, k);
+      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
+        vr.u[d](i, j, k) = -E.psi[vip[d]](i, j, k);
+        if (F.vab == MPDX_VAB_IMPL)  // add_relax (mpdata_rhs_vip_common.hpp:247-254)
+          E.psi[vip[d]](i, j, k) += T(0.5) * F.dt * F.vabc(i, j, k) * F.relax.u[d](i, j, k);
+      }
     } else {
-      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) vr.u[d](i, j, k) = T(0);
+      _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) {
+        if (F.vab == MPDX_VAB_IMPL) vr.u[d](i, j, k) = -F.vabc(i, j, k) * (E.psi[vip[d]](i, j, k) - F.relax.u[d](i, j, k));
+        else vr.u[d](i, j, k) = T(0);
+      }
     }
+    });
+}
+
+// impl_tht end of step (boussinesq_impl.hpp:115-125): theta with the implicit
+// w dtht_e / dz term, and its tendency
+template <class T>
+__global__ void k_impl_fnlz(geom g, eqns<T> E, int iw, int ith, forcing<T> F) {
+  for_interior(g, [&](int i, int j, int k) {
+    const T w = E.psi[iw](i, j, k), dte = F.dthe(i, j, k), ta = F.tabs(i, j, k);
+    const T th = (E.psi[ith](i, j, k) - T(0.5) * F.dt * w * dte) / (1 + T(0.5) * F.dt * ta);
+    E.psi[ith](i, j, k) = th;
+    E.rhs[ith](i, j, k) += -w * dte - ta * th;
+    });
+}
+
+// dtht_e = d(tht_e)/dz after the scalar halo fill of tht_e (boussinesq_impl.hpp:38-50):
+// along the vertical axis v, cyclic neighbours wrap with period n-1, rigid ones
+// mirror (rigid_3d.hpp fill_halos_sclr: a(-1) = a(1), a(n) = a(n-2))
+template <class T>
+__global__ void k_dtht_e(geom g, dfield<T> te, dfield<T> out) {
+  const int v = g.nd - 1;
+  for_interior(g, [&](int i, int j, int k) {
+    const int c[3] = {i, j, k};
+    const int n = g.n[v];
+    auto at = [&](int q) {
+      if (q < 0) q = g.bc[v][0] == MPDX_BC_CYCLIC ? q + n - 1 : -q;
+      else if (q > n - 1) q = g.bc[v][1] == MPDX_BC_CYCLIC ? q - (n - 1) : 2 * (n - 1) - q;
+      int a[3] = {c[0], c[1], c[2]};
+      a[v] = q;
+      return te(a[0], a[1], a[2]);
+    };
+    out(i, j, k) = mpdx::qdiv<T>(at(c[v] + 1) - at(c[v] - 1), g.dx<T>(v), g.rdx<T>(v)) * T(0.5);
+    });
+}
+
+// denominators of normalize_vip (mpdata_rhs_vip_common.hpp:235-245, boussinesq_impl.hpp:61-80),
+// evaluated in real_t and kept in the pressure type
+template <class T, class P>
+__global__ void k_norm_den(geom g, forcing<T> F, dfield<P> d0, dfield<P> d1, dfield<P> d2) {
+  for_interior(g, [&](int i, int j, int k) {
+    const T hdt = T(0.5) * F.dt;
+    const T vh = F.vab == MPDX_VAB_IMPL ? 1 + hdt * F.vabc(i, j, k) : T(1);
+    T vv = vh;
+    if (F.impl) {
+      const T b = T(0.25) * F.dt * F.dt * F.grav / F.tref * F.dthe(i, j, k) / (1 + hdt * F.tabs(i, j, k));
+      vv = F.vab == MPDX_VAB_IMPL ? 1 + hdt * F.vabc(i, j, k) + b : 1 + b;
+    }
+    dfield<P> D[3] = {d0, d1, d2};
+    _Pragma("unroll") for (int d = 0; d < 3; ++d) if (d < g.nd) D[d](i, j, k) = P(d == g.nd - 1 ? vv : vh);
     });
 }
 
@@ -1057,7 +1159,7 @@ boussinesq<T, P>::boussinesq(const mpdx_config &c, cudaStream_t s) {
   if (c.dt <= 0) throw error(MPDX_E_ARG, "dt must be positive");
   if (c.tht_ref == 0) throw error(MPDX_E_ARG, "Tht_ref must be non-zero");
   for (int q = 0; q < 2 * c.n_dims; ++q)
-    if (c.bcs[q] != MPDX_BC_CYCLIC && c.bcs[q] != MPDX_BC_RIGID)
+    if (c.bcs[q] != MPDX_BC_CYCLIC && c.bcs[q] != MPDX_BC_RIGID && c.bcs[q] != MPDX_BC_GNDSKY)
       throw error(MPDX_E_UNSUPPORTED, "the Boussinesq solver supports cyclic and rigid boundaries");
   k_iters = c.prs_scheme == MPDX_PRS_CR ? 1 : c.prs_k_iters;  // cr is gcrk<1> (mpdata_rhs_vip_prs.hpp:55-64)
   if (k_iters < 1 || k_iters > kGcrMaxK) throw error(MPDX_E_ARG, "prs_k_iters must be in 1..8");
@@ -1082,7 +1184,13 @@ boussinesq<T, P>::boussinesq(const mpdx_config &c, cudaStream_t s) {
   }
   ix_w = c.ix_w; ix_tht = c.ix_tht;
   if (ix_tht < 0 || ix_tht >= st.n_eqns || seen[ix_tht]) throw error(MPDX_E_ARG, "invalid theta equation index");
-  for (int d = 0; d < st.nd; ++d) { st.alloc_sclr(stash[d]); st.alloc_sclr(vip_rhs[d]); }
+  impl_tht = c.impl_tht ? 1 : 0;
+  vab = c.vip_vab;
+  if (vab != MPDX_VAB_NONE && vab != MPDX_VAB_EXPL && vab != MPDX_VAB_IMPL) throw error(MPDX_E_ARG, "unknown velocity absorber");
+  for (int d = 0; d < st.nd; ++d) { st.alloc_sclr(stash[d]); st.alloc_sclr(vip_rhs[d]); st.alloc_sclr(vab_relax[d]); }
+  st.alloc_sclr(tht_abs); st.alloc_sclr(hflux_frc); st.alloc_sclr(vab_coeff); st.alloc_sclr(dtht_e);
+  if (normalizes())
+    for (int d = 0; d < st.nd; ++d) st.alloc_sclr(den[d]);
   for (int e = 0; e < st.n_eqns; ++e) st.alloc_sclr(rhs[e]);
   st.alloc_sclr(tht_e); st.alloc_sclr(Phi); st.alloc_sclr(err[0]); st.alloc_sclr(err[1]); st.alloc_sclr(lap_err);
   p_err.resize(k_iters); lap_p_err.resize(k_iters);
@@ -1115,8 +1223,8 @@ boussinesq<T, P>::~boussinesq() {
 // pressure_solver_update (mpdata_rhs_vip_prs_common.hpp:99-123) without the final
 // gradient, which the callers fuse into their own kernels
 template <class T, class P>
-void boussinesq<T, P>::pressure_solve() {
-  const auto gm = make_geom(st, dijk);
+void boussinesq<T, P>::pressure_solve(bool simple) {
+  const auto gm = simple ? make_geom(st, dijk) : norm_geom(make_geom(st, dijk));
   const unsigned G = red_grid(gm);
   cudaStream_t s = st.stream;
   bq::vec_u<T> u;
@@ -1335,9 +1443,14 @@ void boussinesq<T, P>::ante_loop() {
     const int dd = d < st.nd ? d : 0;
     u.u[d] = vips(dd).v; vr.u[d] = vip_rhs[dd].v;
   }
-  // initial projection (mpdata_rhs_vip_prs_common.hpp:130-146); save_edges is a no-op here
+  if (impl_tht) {  // calc_dtht_e (boussinesq_impl.hpp:57-61) comes first
+    bq::k_dtht_e<T><<<G, kBlk, 0, s>>>(gm, tht_e.v, dtht_e.v);
+    MPDX_LAUNCH_CHECK();
+  }
+  // initial projection (mpdata_rhs_vip_prs_common.hpp:130-146), with the simple
+  // Laplacian (no normalize_vip); save_edges is a no-op here
   MPDX_CUDA(cudaMemsetAsync(Phi.base, 0, Phi.bytes, s));
-  pressure_solve();
+  pressure_solve(true);
   bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(gm, bq::APPLY_PROJECT, Phi.v, u, vr, T(0));
   MPDX_LAUNCH_CHECK();
   // mpdata_rhs_vip_common.hpp:283-302: GC = 0, stash = 0, parent hooks, vip_rhs = 0
@@ -1352,9 +1465,9 @@ void boussinesq<T, P>::ante_loop() {
     E.psi[e] = st.psi[ee][st.tl[ee]].v;
     E.rhs[e] = rhs[ee].v;
   }
-  // update_rhs(dt / 2, at = 0); update_rhs's halo exchange of every equation is
-  // left out: the next read of any halo is preceded by its own exchange
-  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 0, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
+  // update_rhs(dt / 2, at = 0) and vip_rhs_impl_init; update_rhs's halo exchange of
+  // every equation is left out: the next read of any halo is preceded by its own exchange
+  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 0, E, vip_dev, ix_w, ix_tht, forcing(), dtT / 2, vr);
   // ini_pressure (mpdata_rhs_vip_prs_common.hpp:86-97), then vip_rhs -= grad Phi
   double npoints = 1;
   for (int d = 0; d < st.nd; ++d) npoints *= st.n[d];
@@ -1399,7 +1512,7 @@ void boussinesq<T, P>::step() {
     E.psi[e] = st.psi[ee][st.tl[ee]].v;
     E.rhs[e] = rhs[ee].v;
   }
-  bq::k_ante_step<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, E, vip_dev, sh, vr, dtT / 2, T(0.5) * dtT);
+  bq::k_ante_step<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, E, vip_dev, sh, vr, dtT / 2, T(0.5) * dtT, forcing());
   MPDX_LAUNCH_CHECK();
   // advection of every equation
   gen.step();
@@ -1408,17 +1521,43 @@ void boussinesq<T, P>::step() {
   // hook_post_step
   for (int d = 0; d < 3; ++d) u.u[d] = vips(d < st.nd ? d : 0).v;
   for (int e = 0; e < 4; ++e) E.psi[e] = st.psi[e < st.n_eqns ? e : 0][st.tl[e < st.n_eqns ? e : 0]].v;
-  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 1, E, vip_dev, ix_w, ix_tht, tht_e.v, g, tht_ref, dtT / 2, vr);
+  bq::k_rhs<T><<<G, kBlk, 0, s>>>(gm, st.n_eqns, 1, E, vip_dev, ix_w, ix_tht, forcing(), dtT / 2, vr);
   MPDX_LAUNCH_CHECK();
-  pressure_solve();
-  bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(gm, bq::APPLY_FINISH, Phi.v, u, vr, T(0.5) * dtT);
+  pressure_solve(false);
+  bq::k_apply_grad<T, P><<<G, kBlk, 0, s>>>(norm_geom(gm), bq::APPLY_FINISH, Phi.v, u, vr, T(0.5) * dtT);
+  if (impl_tht) bq::k_impl_fnlz<T><<<G, kBlk, 0, s>>>(gm, E, ix_w, ix_tht, forcing());
   MPDX_LAUNCH_CHECK();
+}
+
+template <class T, class P>
+bq::forcing<T> boussinesq<T, P>::forcing() {
+  bq::forcing<T> F;
+  F.the = tht_e.v; F.tabs = tht_abs.v; F.hflx = hflux_frc.v; F.dthe = dtht_e.v; F.vabc = vab_coeff.v;
+  for (int d = 0; d < 3; ++d) F.relax.u[d] = vab_relax[d < st.nd ? d : 0].v;
+  F.impl = impl_tht; F.vab = vab;
+  F.grav = g; F.tref = tht_ref; F.dt = dtT;
+  return F;
+}
+
+// the geometry with normalize_vip inside lap() and after the pressure gradient,
+// where the configuration normalises (velocity absorber impl, or impl_tht)
+template <class T, class P>
+bq::geom boussinesq<T, P>::norm_geom(bq::geom gm) const {
+  if (!normalizes()) return gm;
+  gm.norm = 1;
+  for (int d = 0; d < 3; ++d) gm.den[d] = den[d < st.nd ? d : 0].v.o;
+  return gm;
 }
 
 template <class T, class P>
 void boussinesq<T, P>::advance(long long nt) {
   if (nt <= 0) return;
   if (st.timestep == 0) ante_loop();
+  if (normalizes()) {  // from the absorber / theta fields as they are now
+    const auto gm = make_geom(st, dijk);
+    bq::k_norm_den<T, P><<<red_grid(gm), kBlk, 0, st.stream>>>(gm, forcing(), den[0].v, den[1].v, den[2].v);
+    MPDX_LAUNCH_CHECK();
+  }
   for (long long t = 0; t < nt; ++t) step();
 }
 

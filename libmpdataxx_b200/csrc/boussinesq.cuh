@@ -11,6 +11,11 @@
 
 namespace mpdx {
 
+namespace bq {
+struct geom;
+template <class T> struct forcing;
+}  // namespace bq
+
 constexpr int kGcrMaxK = 8;        // largest k of GCR(k) built
 constexpr int kRedBlocks = 1184;   // largest reduction grid: 8 x 148 SMs (a fixed shape per grid size => reproducible sums)
 constexpr int kRedThreads = 256;
@@ -38,7 +43,12 @@ struct boussinesq {
   mpdata_state<T> st;
   general<T> gen{&st};
   field<T> stash[3], vip_rhs[3], rhs[4], tht_e;
-  field<P> Phi, err[2], lap_err;
+  // theta absorber and heat flux (sclr_array "tht_abs", "hflux_frc"), velocity
+  // absorber (vab_coefficient(), vab_relaxed_state(d)), d(tht_e)/dz (impl_tht)
+  field<T> tht_abs, hflux_frc, vab_coeff, vab_relax[3], dtht_e;
+  int impl_tht = 0, vab = MPDX_VAB_NONE;
+  bool normalizes() const { return vab == MPDX_VAB_IMPL || impl_tht; }
+  field<P> Phi, err[2], lap_err, den[3];  // den: normalize_vip denominators per velocity component
   std::vector<field<P>> p_err, lap_p_err;
   double dt = 0;
   T dtT = 0, g = 0, tht_ref = 0;
@@ -86,7 +96,10 @@ struct boussinesq {
   field<T> &vips(int d) { return st.psi[vip[d]][st.tl[vip[d]]]; }
   void ante_loop();
   void step();
-  void pressure_solve();  // pressure_solver_update up to the final gradient
+  // pressure_solver_update up to the final gradient; simple: no normalize_vip in lap()
+  void pressure_solve(bool simple);
+  bq::forcing<T> forcing();
+  bq::geom norm_geom(bq::geom g) const;
 };
 
 extern template struct boussinesq<float, float>;

@@ -287,8 +287,15 @@ struct boussinesq_solver : solver_base {
       return;
     }
     if (kind == MPDX_FIELD_SCLR_ARRAY) {
-      if (idx != MPDX_SCLR_THT_E) throw error(MPDX_E_ARG, "unknown scalar array");
-      f = &b->tht_e;
+      if (idx == MPDX_SCLR_THT_E) f = &b->tht_e;
+      else if (idx == MPDX_SCLR_THT_ABS) f = &b->tht_abs;
+      else if (idx == MPDX_SCLR_HFLUX_FRC) f = &b->hflux_frc;
+      else if (idx == MPDX_SCLR_VAB_COEFF || (idx >= MPDX_SCLR_VAB_RELAX && idx < MPDX_SCLR_VAB_RELAX + st.nd)) {
+        // vab_coefficient() / vab_relaxed_state(d) throw without the option (sharedmem.hpp:471-494)
+        if (b->vab == MPDX_VAB_NONE)
+          throw error(MPDX_E_ARG, "libmpdata++: vab_coeff() called with option vip_vab unset?");
+        f = idx == MPDX_SCLR_VAB_COEFF ? &b->vab_coeff : &b->vab_relax[idx - MPDX_SCLR_VAB_RELAX];
+      } else throw error(MPDX_E_ARG, "unknown scalar array");
       return;
     }
     if (kind == MPDX_FIELD_PRESSURE) {
@@ -571,8 +578,12 @@ void validate(const mpdx_config &c) {
   if ((o & o_iga) && (o & o_abs)) throw error(MPDX_E_ARG, "abs & iga options are mutually exclusive");
   for (int q = 0; q < 2 * c.n_dims; ++q) {
     const int k = c.bcs[q];
-    if (k != MPDX_BC_CYCLIC && k != MPDX_BC_OPEN && k != MPDX_BC_RIGID) throw error(MPDX_E_ARG, "unknown boundary kind");
+    if (k != MPDX_BC_CYCLIC && k != MPDX_BC_OPEN && k != MPDX_BC_RIGID && k != MPDX_BC_GNDSKY) throw error(MPDX_E_ARG, "unknown boundary kind");
+    if (k == MPDX_BC_GNDSKY && c.n_dims != 3) throw error(MPDX_E_UNSUPPORTED, "gndsky is a 3D boundary condition (bcond/gndsky_3d.hpp)");
   }
+  if (c.solver != MPDX_SOLVER_BOUSSINESQ && (c.impl_tht || c.vip_vab))
+    throw error(MPDX_E_ARG, "impl_tht and vip_vab are options of the Boussinesq solver");
+  if (c.vip_vab < MPDX_VAB_NONE || c.vip_vab > MPDX_VAB_IMPL) throw error(MPDX_E_ARG, "unknown velocity absorber");
 }
 }  // namespace
 
@@ -607,6 +618,11 @@ mpdx_status mpdx_create(const mpdx_config *cfg, mpdx_handle *out) {
   *out = nullptr;
   try {
     validate(*cfg);
+    // gndsky (bcond/gndsky_3d.hpp) is the rigid condition for every field filled here
+    mpdx_config cc = *cfg;
+    for (int q = 0; q < 2 * cc.n_dims; ++q)
+      if (cc.bcs[q] == MPDX_BC_GNDSKY) cc.bcs[q] = MPDX_BC_RIGID;
+    cfg = &cc;
     auto h = std::make_unique<mpdx_solver>();
     if (cfg->solver == MPDX_SOLVER_BOUSSINESQ) {
       if (cfg->dtype == 8) h->impl.reset(new mpdx::boussinesq_solver<double, double>(*cfg));

@@ -5,12 +5,15 @@
 
 namespace libmpdataxx {
 namespace bcond {
-enum bcond_e { null, cyclic, open, rigid };
+// gndsky: the 3D ground / sky condition (bcond/gndsky_3d.hpp), rigid for every field
+// this backend fills
+enum bcond_e { null, cyclic, open, rigid, gndsky };
 inline int to_c(bcond_e b) {
   switch (b) {
     case cyclic: return MPDX_BC_CYCLIC;
     case open: return MPDX_BC_OPEN;
     case rigid: return MPDX_BC_RIGID;
+    case gndsky: return MPDX_BC_GNDSKY;
     default: return -1;
   }
 }

@@ -21,9 +21,9 @@ class any {
   virtual void advectee_global_set(const arr_t &a, int e = 0) = 0;
   virtual arr_t advector(int d = 0) = 0;
   virtual arr_t g_factor() = 0;
-  // velocity absorbers (vip_vab) are not built on this backend
-  virtual arr_t vab_coefficient() { throw std::runtime_error("libmpdata++: vab_coefficient() is not built on this backend"); }
-  virtual arr_t vab_relaxed_state(int = 0) { throw std::runtime_error("libmpdata++: vab_relaxed_state() is not built on this backend"); }
+  // velocity absorber fields (vip_vab); solvers without the option throw (sharedmem.hpp:471-494)
+  virtual arr_t vab_coefficient() { throw std::runtime_error("libmpdata++: vab_coeff() called with option vip_vab unset?"); }
+  virtual arr_t vab_relaxed_state(int = 0) { throw std::runtime_error("libmpdata++: vab_relaxed_state() called with option vip_vab unset?"); }
   virtual arr_t sclr_array(const std::string &name, int n = 0) = 0;
   virtual void advance(advance_arg_t nt) = 0;
   virtual real_t min(int e = 0) = 0;

@@ -112,10 +112,16 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
     arr_t v = advectee(e);
     std::copy(a.data(), a.data() + v.size(), v.data());
   }
+  // named scalar arrays of the Boussinesq solver (boussinesq_common.hpp:20-60)
   arr_t sclr_array(const std::string &name, int = 0) override {
-    if (name != "tht_e") throw std::out_of_range("libmpdata++: unknown scalar array " + name);
-    return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_E);
+    if (name == "tht_e") return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_E);
+    if (name == "tht_abs") return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_THT_ABS);
+    if (name == "hflux_frc") return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_HFLUX_FRC);
+    throw std::out_of_range("libmpdata++: unknown scalar array " + name);
   }
+  // velocity absorber (concurr_common.hpp:420-428); the library throws without vip_vab
+  arr_t vab_coefficient() override { return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_VAB_COEFF); }
+  arr_t vab_relaxed_state(int d = 0) override { return view(MPDX_FIELD_SCLR_ARRAY, MPDX_SCLR_VAB_RELAX + d); }
 
   // run.advance(nt) (concurr_common.hpp:380-385); hooks, if set, run after every step;
   // with output::hdf5_xdmf, records on the output steps (output_common.hpp:47-70, 150-165)

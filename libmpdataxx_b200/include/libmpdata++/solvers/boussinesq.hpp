@@ -1,7 +1,9 @@
 // solvers::boussinesq<ct_params_t> (libmpdata++/solvers/boussinesq.hpp:20-52)
-// with explicit buoyancy, trapezoidal right-hand-side coupling and the GCR
-// pressure solve.  ct_params_t::ix names the equation indices
-// (u, [v,] w, tht and vip_i/vip_j/[vip_k]).
+// with explicit buoyancy (boussinesq_expl.hpp) or, with ct_params_t::impl_tht,
+// the implicit theta-perturbation form (boussinesq_impl.hpp), the velocity
+// absorber ct_params_t::vip_vab (noab, expl, impl), trapezoidal right-hand-side
+// coupling and the GCR pressure solve.  ct_params_t::ix names the equation
+// indices (u, [v,] w, tht and vip_i/vip_j/[vip_k]).
 #pragma once
 
 #include "mpdata.hpp"
@@ -46,7 +48,10 @@ struct boussinesq {
     c.ix_tht = ix::tht;
     c.precond = p.precond;
     c.prs_fp64 = p.prs_fp64 ? 1 : 0;
+    c.impl_tht = ct_params_t::impl_tht ? 1 : 0;
+    c.vip_vab = int(ct_params_t::vip_vab);  // noab 0, expl 1, impl 2 as MPDX_VAB_*
   }
+  static constexpr bool has_vab = ct_params_t::vip_vab != 0;
 
  private:
   template <class I> static constexpr int vip_j_of() { return I::vip_j; }

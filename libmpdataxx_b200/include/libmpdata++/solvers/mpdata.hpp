@@ -15,6 +15,7 @@ namespace solvers {
 
 enum rhs_scheme_t { euler_a, euler_b, trapez, mixed };  // mpdata_rhs.hpp:19-25
 enum prs_scheme_t { mr, cr, pc, gcrk };                  // mpdata_rhs_vip_prs.hpp:17-30
+enum vip_vab_t { noab, expl, impl };                     // mpdata_rhs_vip_common.hpp:16-21
 
 template <class ct_params_t>
 struct mpdata {

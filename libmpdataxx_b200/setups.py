@@ -324,7 +324,9 @@ def batched_problems(n=256, seed=5, lo=64, hi=1024, dtype=np.float32, cmax=0.5):
 
 def boussinesq_run(setup, opts=None, n_iters=2, dtype=np.float64, prs_scheme=None, prs_fp64=False):
     """concurr::cuda<solvers::boussinesq<...>> loaded with a Boussinesq set-up
-    (equations (u, [v,] w, tht) as in the reference's tests, boussinesq_2d.cpp:27-30)."""
+    (equations (u, [v,] w, tht) as in the reference's tests, boussinesq_2d.cpp:27-30).
+    Optional set-up keys: "impl_tht" (bool), "vip_vab" (solvers.noab/expl/impl), and
+    the arrays "tht_abs", "hflux_frc", "vab_coeff", "vab_relax" (list per dimension)."""
     from . import bcond, concurr, solvers
     nd = len(setup["grid"])
 
@@ -339,6 +341,8 @@ def boussinesq_run(setup, opts=None, n_iters=2, dtype=np.float64, prs_scheme=Non
     k = setup.get("prs_k", 1)
     ct.prs_scheme = prs_scheme if prs_scheme is not None else (solvers.cr if k == 1 else solvers.gcrk)
     ct.prs_k_iters = k
+    ct.impl_tht = bool(setup.get("impl_tht", False))
+    ct.vip_vab = int(setup.get("vip_vab", solvers.noab))
 
     class ix:
         pass
@@ -354,6 +358,13 @@ def boussinesq_run(setup, opts=None, n_iters=2, dtype=np.float64, prs_scheme=Non
                                        prs_fp64=prs_fp64)
     run = concurr.cuda(solvers.boussinesq(ct), *[getattr(bcond, b) for b in setup["bcs"]], p=p)
     run.sclr_array("tht_e")[...] = setup["tht_e"]
+    for name in ("tht_abs", "hflux_frc"):
+        if name in setup:
+            run.sclr_array(name)[...] = setup[name]
+    if "vab_coeff" in setup:
+        run.vab_coefficient()[...] = setup["vab_coeff"]
+        for d, a in enumerate(setup["vab_relax"]):
+            run.vab_relaxed_state(d)[...] = a
     for e, a in enumerate(setup["advectee"]):
         run.advectee(e)[...] = a
     return run

@@ -23,6 +23,7 @@ class ct_params_default_t:
     prs_khn = False
     sgs_scheme = 0
     impl_tht = False
+    vip_vab = 0       # noab (mpdata_rhs_vip_common.hpp:16-21)
 
 
 class _rt_base:
@@ -50,14 +51,20 @@ class mpdata:
             raise NotImplementedError("var_dt is not built on this backend")
 
 
-# right-hand-side schemes (mpdata_rhs.hpp:19-25) and pressure schemes (mpdata_rhs_vip_prs.hpp:17-30)
+# right-hand-side schemes (mpdata_rhs.hpp:19-25), pressure schemes (mpdata_rhs_vip_prs.hpp:17-30)
+# and velocity absorbers (mpdata_rhs_vip_common.hpp:16-21)
 euler_a, euler_b, trapez, mixed = range(4)
 mr, cr, pc, gcrk = range(4)
+noab, expl, impl = range(3)
 
 
 class boussinesq:
-    """solvers::boussinesq<ct_params_t> (solvers/boussinesq.hpp:20-52) with the
-    explicit buoyancy, trapezoidal rhs coupling and GCR pressure solve."""
+    """solvers::boussinesq<ct_params_t> (solvers/boussinesq.hpp:20-52): explicit
+    buoyancy (boussinesq_expl.hpp) or, with ct.impl_tht, the implicit theta
+    perturbation form (boussinesq_impl.hpp); trapezoidal rhs coupling, GCR
+    pressure solve, velocity absorber ct.vip_vab (noab, expl or impl).  The
+    absorber coefficient and relaxed states are the scalar arrays "vab_coeff"
+    and "vab_relax0..2" (vab_coefficient(), vab_relaxed_state(d))."""
 
     class rt_params_t(_rt_base):
         def __init__(self, **kw):
@@ -90,3 +97,5 @@ class boussinesq:
         cfg.ix_tht = int(ix.tht)
         cfg.precond = _lib.PRECOND_LEARNED if p.precond == "learned" else _lib.PRECOND_IDENTITY
         cfg.prs_fp64 = 1 if p.prs_fp64 else 0
+        cfg.impl_tht = 1 if getattr(ct, "impl_tht", False) else 0
+        cfg.vip_vab = int(getattr(ct, "vip_vab", noab))

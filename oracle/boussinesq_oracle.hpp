@@ -1,7 +1,9 @@
 // ORACLE -- test infrastructure only.
 //
 // CPU restatement of libmpdata++'s Boussinesq solver (solvers::boussinesq with
-// the trapezoidal right-hand side, iles, explicit buoyancy) and of the GCR(k)
+// the trapezoidal right-hand side and iles; explicit buoyancy, boussinesq_expl.hpp,
+// or implicit theta perturbation, boussinesq_impl.hpp; no, explicit or implicit
+// velocity absorber, mpdata_rhs_vip_common.hpp vip_vab) and of the GCR(k)
 // pressure solve it calls every step, on top of the MPDATA restatement in
 // mpdata_oracle.hpp.  Only tests/ and the CPU-baseline legs of bench.py load
 // it, and only as the checker.
@@ -15,13 +17,17 @@
 //   hook_post_step   mpdata_rhs_vip_common.hpp:366-370, mpdata_rhs.hpp:195-214,
 //                    mpdata_rhs_vip_prs_common.hpp:162-181
 //   pressure solve   mpdata_rhs_vip_prs_common.hpp:47-128, mpdata_rhs_vip_prs_gcrk.hpp:39-97
-//   buoyancy         boussinesq_expl.hpp:48-126
+//   buoyancy         boussinesq_expl.hpp:48-126 (expl), boussinesq_impl.hpp:36-141 (impl_tht)
+//   absorbers        mpdata_rhs_vip_common.hpp:182-256 (vip_rhs_impl_init, vip_rhs_expl_calc,
+//                    add_relax, normalize_vip), mpdata_rhs_vip_prs_common.hpp:49-84 (lap
+//                    normalises the gradient unless simple), :162-181 (vip_rhs_impl_fnlz)
 //
-// Two deliberate restatements:
-//  * hflux_frc and tht_abs are identically zero in the reference's Boussinesq
-//    constructor (boussinesq_common.hpp:48-49) and nothing here sets them, so the
-//    theta tendency is zero and buoy_at_1 equals buoy_at_0 exactly; both are
-//    written in their reduced form.
+// hflux_frc and tht_abs start at zero (boussinesq_common.hpp:48-49) and are
+// set, as in the reference, through sclr_array("hflux_frc") / ("tht_abs");
+// vab_coefficient() and vab_relaxed_state(d) are sclr arrays "vab_coeff" and
+// "vab_relax0..2" here.  Expressions keep the reference's operand order.
+//
+// One deliberate restatement:
 //  * prs_sum() (sharedmem.hpp:115-190) is a plain per-slice Blitz++ sum in the
 //    reference (Kahan with prs_khn).  Here every such sum is a compensated
 //    double-double sum (TwoSum), whose value is the exact sum rounded except in
@@ -56,9 +62,11 @@ struct boussinesq : mpdata<T> {
 
   T dt = 1, dijk[3] = {1, 1, 1}, g = T(9.81), Tht_ref = 300, prs_tol = T(1e-7), err_tol = 0;
   int k_iters = 1, vip[3] = {0, 1, 2}, ix_w = 1, ix_tht = 2;
-  std::array<arr<T>, 3> stash, vip_rhs, tmp_uvw, lap_tmp;
+  int impl_tht = 0;  // ct_params_t::impl_tht
+  int vab = 0;       // ct_params_t::vip_vab: 0 noab, 1 expl, 2 impl (mpdata_rhs_vip_common.hpp:16-21)
+  std::array<arr<T>, 3> stash, vip_rhs, tmp_uvw, lap_tmp, vab_relax;
   std::vector<arr<T>> rhs, p_err, lap_p_err;
-  arr<T> tht_e, Phi, err, lap_err;
+  arr<T> tht_e, Phi, err, lap_err, tht_abs, hflux_frc, vab_coeff, dtht_e;
   T beta = T(.25);                      // persists between solves (mpdata_rhs_vip_prs_gcrk.hpp:110-112)
   std::vector<T> alpha, tmp_den;
   T dt_stash0 = 0;
@@ -83,7 +91,12 @@ struct boussinesq : mpdata<T> {
     for (int d = 0; d < nd; ++d) {
       this->alloc_sclr(stash[d]); this->alloc_sclr(vip_rhs[d]);
       this->alloc_sclr(tmp_uvw[d]); this->alloc_sclr(lap_tmp[d]);
+      this->alloc_sclr(vab_relax[d]);
     }
+    this->alloc_sclr(tht_abs); this->alloc_sclr(hflux_frc); this->alloc_sclr(vab_coeff); this->alloc_sclr(dtht_e);
+    // zero at construction (boussinesq_common.hpp:48-49 for hflux_frc and tht_abs)
+    for (arr<T> *a : {&tht_abs, &hflux_frc, &vab_coeff, &vab_relax[0], &vab_relax[1], &vab_relax[2]})
+      if (!a->v.empty()) std::fill(a->v.begin(), a->v.end(), T(0));
     rhs.resize(this->n_eqns);
     for (auto &a : rhs) this->alloc_sclr(a);
     this->alloc_sclr(tht_e); this->alloc_sclr(Phi); this->alloc_sclr(err); this->alloc_sclr(lap_err);
@@ -93,7 +106,12 @@ struct boussinesq : mpdata<T> {
   }
 
   arr<T> &sclr_array(const char *name) {
-    if (std::string(name) == "tht_e") return tht_e;
+    const std::string s(name);
+    if (s == "tht_e") return tht_e;
+    if (s == "tht_abs") return tht_abs;
+    if (s == "hflux_frc") return hflux_frc;
+    if (s == "vab_coeff") return vab_coeff;
+    if (s.size() == 10 && s.compare(0, 9, "vab_relax") == 0 && s[9] >= '0' && s[9] < char('0' + nd)) return vab_relax[s[9] - '0'];
     throw std::runtime_error("no such scalar array");
   }
   arr<T> &vips(int d) { return this->state(vip[d]); }
@@ -137,13 +155,39 @@ struct boussinesq : mpdata<T> {
       out(i, j, k) = r;
     });
   }
-  // lap() (mpdata_rhs_vip_prs_common.hpp:49-84), G = 1, no velocity absorber
-  void lap(arr<T> &out, arr<T> &A, bool err_init) {
+  // normalize_vip (mpdata_rhs_vip_common.hpp:235-245; boussinesq_impl.hpp:61-80 with impl_tht)
+  void normalize_vip(const std::array<arr<T> *, 3> &v) {
+    const T hdt = T(0.5) * dt;
+    if (vab == 2) {
+      const int nh = impl_tht ? nd - 1 : nd;
+      for (int d = 0; d < nh; ++d) {
+        arr<T> &a = *v[d];
+        interior([&](int i, int j, int k) { a(i, j, k) /= (1 + hdt * vab_coeff(i, j, k)); });
+      }
+      if (impl_tht) {
+        arr<T> &a = *v[nd - 1];
+        interior([&](int i, int j, int k) {
+          a(i, j, k) /= (1 + hdt * vab_coeff(i, j, k)
+                         + T(0.25) * dt * dt * g / Tht_ref * dtht_e(i, j, k) / (1 + hdt * tht_abs(i, j, k)));
+        });
+      }
+    } else if (impl_tht) {
+      arr<T> &a = *v[nd - 1];
+      interior([&](int i, int j, int k) {
+        a(i, j, k) /= (1 + T(0.25) * dt * dt * g / Tht_ref * dtht_e(i, j, k) / (1 + hdt * tht_abs(i, j, k)));
+      });
+    }
+  }
+  bool normalizes() const { return vab == 2 || impl_tht; }
+
+  // lap() (mpdata_rhs_vip_prs_common.hpp:49-84), G = 1; simple: no normalize_vip
+  void lap(arr<T> &out, arr<T> &A, bool err_init, bool simple) {
     this->xchng_pres(A, 0);
     calc_grad(lap_tmp, A);
     if (err_init)
       for (int d = 0; d < nd; ++d) { arr<T> &l = lap_tmp[d], &u = tmp_uvw[d]; interior([&](int i, int j, int k) { l(i, j, k) -= u(i, j, k); }); }
     this->set_edges(ptrs(lap_tmp));
+    if (!simple) normalize_vip(ptrs(lap_tmp));
     for (int d = 0; d < nd; ++d) this->xchng_pres(lap_tmp[d], 0);
     div(out, lap_tmp);
   }
@@ -157,10 +201,11 @@ struct boussinesq : mpdata<T> {
   }
 
   // GCR(k) (mpdata_rhs_vip_prs_gcrk.hpp:39-97)
+  bool simple = false;  // pressure_solver_update(simple) of the running solve
   void loop_init() {
     arr<T> &p0 = p_err[0];
     interior([&](int i, int j, int k) { p0(i, j, k) = err(i, j, k); });
-    lap(lap_p_err[0], p_err[0], false);
+    lap(lap_p_err[0], p_err[0], false, simple);
   }
   void loop_body() {
     for (int v = 0; v < k_iters; ++v) {
@@ -170,7 +215,7 @@ struct boussinesq : mpdata<T> {
         interior([&](int i, int j, int k) { Phi(i, j, k) += b * p(i, j, k); });
         interior([&](int i, int j, int k) { err(i, j, k) += b * lp(i, j, k); }); }
       if (max_abs(err) <= err_tol) converged = true;
-      lap(lap_err, err, false);
+      lap(lap_err, err, false, simple);
       for (int l = 0; l <= v; ++l)
         if (tmp_den[l] != 0) alpha[l] = -T(sum2(lap_err, lap_p_err[l])) / tmp_den[l];
       if (v < k_iters - 1) {
@@ -196,9 +241,10 @@ struct boussinesq : mpdata<T> {
   }
 
   // pressure_solver_update / _apply (mpdata_rhs_vip_prs_common.hpp:99-128)
-  void pressure_solver_update() {
+  void pressure_solver_update(bool simple_ = false) {
+    simple = simple_;
     for (int d = 0; d < nd; ++d) { arr<T> &u = tmp_uvw[d], &v = vips(d); interior([&](int i, int j, int k) { u(i, j, k) = v(i, j, k); }); }
-    lap(err, Phi, true);
+    lap(err, Phi, true, simple);
     iters = 0;
     converged = false;
     loop_init();
@@ -215,12 +261,52 @@ struct boussinesq : mpdata<T> {
     for (int d = 0; d < nd; ++d) { arr<T> &u = tmp_uvw[d], &v = vips(d); interior([&](int i, int j, int k) { v(i, j, k) -= u(i, j, k); }); }
   }
 
-  // update_rhs (mpdata_rhs.hpp:39-61 + boussinesq_expl.hpp:83-126)
-  void update_rhs() {
+  // update_rhs (mpdata_rhs.hpp:39-61) + boussinesq_expl.hpp:81-126 or boussinesq_impl.hpp:82-113;
+  // at = 0 before the first step, 1 after each step
+  void update_rhs(int at) {
     for (int e = 0; e < this->n_eqns; ++e) { arr<T> &r = rhs[e]; interior([&](int i, int j, int k) { r(i, j, k) = T(0); }); }
     for (int e = 0; e < this->n_eqns; ++e) this->xchng(e);
-    arr<T> &r = rhs[ix_w], &th = this->state(ix_tht);
-    interior([&](int i, int j, int k) { r(i, j, k) += g * (th(i, j, k) - tht_e(i, j, k)) / Tht_ref; });
+    arr<T> &rw = rhs[ix_w], &rt = rhs[ix_tht], &th = this->state(ix_tht), &w = vips(nd - 1);
+    const T hdt = T(0.5) * dt;
+    if (!impl_tht) {
+      if (at == 0) {
+        interior([&](int i, int j, int k) {
+          rt(i, j, k) += hflux_frc(i, j, k) - tht_abs(i, j, k) * (th(i, j, k) - tht_e(i, j, k));
+          rw(i, j, k) += g * (th(i, j, k) - tht_e(i, j, k)) / Tht_ref;
+        });
+      } else {
+        interior([&](int i, int j, int k) {
+          const T x = (th(i, j, k) + hdt * hflux_frc(i, j, k) + hdt * tht_abs(i, j, k) * tht_e(i, j, k)) / (1 + hdt * tht_abs(i, j, k));
+          rt(i, j, k) += hflux_frc(i, j, k) - tht_abs(i, j, k) * (x - tht_e(i, j, k));
+          rw(i, j, k) += g * (x - tht_e(i, j, k)) / Tht_ref;
+        });
+      }
+    } else if (at == 0) {
+      interior([&](int i, int j, int k) {
+        rt(i, j, k) += -w(i, j, k) * dtht_e(i, j, k) + hflux_frc(i, j, k) - tht_abs(i, j, k) * th(i, j, k);
+        rw(i, j, k) += g * th(i, j, k) / Tht_ref;
+      });
+    } else {
+      interior([&](int i, int j, int k) {
+        rt(i, j, k) += hflux_frc(i, j, k);
+        rw(i, j, k) += g * (th(i, j, k) + hdt * rt(i, j, k)) / (Tht_ref * (1 + hdt * tht_abs(i, j, k)));
+      });
+    }
+  }
+  // dtht_e = d(tht_e)/dz after tht_e's scalar halo fill (boussinesq_impl.hpp:38-50)
+  void calc_dtht_e() {
+    this->xchng_sclr(tht_e, 0);
+    const int d = nd - 1;
+    int pi, pj, pk; off(d, 1, pi, pj, pk);
+    const T dx = dijk[d];
+    interior([&](int i, int j, int k) { dtht_e(i, j, k) = (tht_e(i + pi, j + pj, k + pk) - tht_e(i - pi, j - pj, k - pk)) / dx / T(2); });
+  }
+  // add_relax (mpdata_rhs_vip_common.hpp:247-254)
+  void add_relax() {
+    for (int d = 0; d < nd; ++d) {
+      arr<T> &v = vips(d), &r = vab_relax[d];
+      interior([&](int i, int j, int k) { v(i, j, k) += T(0.5) * dt * vab_coeff(i, j, k) * r(i, j, k); });
+    }
   }
   void apply_rhs(T dt_arg) {  // mpdata_rhs.hpp:63-76
     for (int e = 0; e < this->n_eqns; ++e) {
@@ -230,10 +316,11 @@ struct boussinesq : mpdata<T> {
   }
 
   void bq_ante_loop() {
+    if (impl_tht) calc_dtht_e();  // boussinesq_impl.hpp:57-61
     // correct initial velocity (mpdata_rhs_vip_prs_common.hpp:130-146)
     interior([&](int i, int j, int k) { Phi(i, j, k) = T(0); });
     this->xchng_pres(Phi, 0);
-    pressure_solver_update();
+    pressure_solver_update(true);
     this->xchng_pres(Phi, 0);
     calc_grad(tmp_uvw, Phi);
     pressure_solver_apply();
@@ -242,8 +329,13 @@ struct boussinesq : mpdata<T> {
     for (int d = 0; d < nd; ++d) std::fill(GC[d].v.begin(), GC[d].v.end(), T(0));
     for (int d = 0; d < nd; ++d) { arr<T> &s = stash[d]; interior([&](int i, int j, int k) { s(i, j, k) = T(0); }); }
     B::ante_loop();
-    update_rhs();  // trapez: update_rhs(rhs, dt / 2, 0)
-    for (int d = 0; d < nd; ++d) { arr<T> &r = vip_rhs[d]; interior([&](int i, int j, int k) { r(i, j, k) = T(0); }); }
+    update_rhs(0);  // trapez: update_rhs(rhs, dt / 2, 0)
+    // vip_rhs_impl_init (mpdata_rhs_vip_common.hpp:182-196)
+    for (int d = 0; d < nd; ++d) {
+      arr<T> &r = vip_rhs[d], &v = vips(d), &rl = vab_relax[d];
+      if (vab == 2) interior([&](int i, int j, int k) { r(i, j, k) = -vab_coeff(i, j, k) * (v(i, j, k) - rl(i, j, k)); });
+      else interior([&](int i, int j, int k) { r(i, j, k) = T(0); });
+    }
     // ini_pressure (mpdata_rhs_vip_prs_common.hpp:86-97)
     interior([&](int i, int j, int k) { Phi(i, j, k) = T(0); });
     long long npoints = 1;
@@ -288,8 +380,13 @@ struct boussinesq : mpdata<T> {
 
   void step() {
     calc_gc();
-    // hook_ante_step: fill_stash, apply_rhs(dt / 2), vip_rhs_apply
+    // hook_ante_step: fill_stash, vip_rhs_expl_calc, apply_rhs(dt / 2), vip_rhs_apply
     for (int d = 0; d < nd; ++d) { arr<T> &s = stash[d], &v = vips(d); interior([&](int i, int j, int k) { s(i, j, k) = v(i, j, k); }); }
+    if (vab == 1)
+      for (int d = 0; d < nd; ++d) {
+        arr<T> &r = vip_rhs[d], &v = vips(d), &rl = vab_relax[d];
+        interior([&](int i, int j, int k) { r(i, j, k) += -2 * vab_coeff(i, j, k) * (v(i, j, k) - rl(i, j, k)); });
+      }
     apply_rhs(dt / 2);
     for (int d = 0; d < nd; ++d) {
       arr<T> &v = vips(d), &r = vip_rhs[d];
@@ -299,16 +396,26 @@ struct boussinesq : mpdata<T> {
     ++this->timestep;
     dt_stash0 = dt;
     // hook_post_step: update_rhs(at = 1), apply_rhs(dt / 2), vip_rhs_impl_fnlz
-    update_rhs();
+    // (mpdata_rhs_vip_prs_common.hpp:162-181, then boussinesq_impl.hpp:115-125)
+    update_rhs(1);
     apply_rhs(dt / 2);
     for (int d = 0; d < nd; ++d) { arr<T> &r = vip_rhs[d], &v = vips(d); interior([&](int i, int j, int k) { r(i, j, k) = -v(i, j, k); }); }
+    if (vab == 2) add_relax();
     pressure_solver_update();
     pressure_solver_apply();
+    normalize_vip(vips_ptrs());
     this->set_edges(vips_ptrs());
     const T hdt = T(0.5) * dt;
     for (int d = 0; d < nd; ++d) {
       arr<T> &r = vip_rhs[d], &v = vips(d);
       interior([&](int i, int j, int k) { r(i, j, k) += v(i, j, k); r(i, j, k) /= hdt; });
+    }
+    if (impl_tht) {
+      arr<T> &th = this->state(ix_tht), &rt = rhs[ix_tht], &w = vips(nd - 1);
+      interior([&](int i, int j, int k) {
+        th(i, j, k) = (th(i, j, k) - T(0.5) * dt * w(i, j, k) * dtht_e(i, j, k)) / (1 + T(0.5) * dt * tht_abs(i, j, k));
+        rt(i, j, k) += -w(i, j, k) * dtht_e(i, j, k) - tht_abs(i, j, k) * th(i, j, k);
+      });
     }
   }
 

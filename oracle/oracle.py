@@ -141,6 +141,11 @@ class Oracle:
         a = np.ascontiguousarray(np.broadcast_to(a, self.grid), dtype=np.float64)
         self._check(self.L.orc_set_sclr_array(self.h, name.encode(), _dptr(a)))
 
+    def set_param(self, name, value):
+        """A parameter the reference fixes at compile time or in rt_params (upwind_filter_freq;
+        impl_tht and vip_vab of the Boussinesq solver), set before the first advance."""
+        self._check(self.L.orc_set_param(self.h, name.encode(), float(value)))
+
     def set_g_factor(self, a):
         """g_factor() = a (nug option): G at the interior points."""
         self.set_sclr_array("G", a)

@@ -73,6 +73,12 @@ struct bq_wrap_t : wrap_t<boussinesq<T>, T> {
     for (int i = 0; i < this->s.n[0]; ++i) for (int j = 0; j < this->s.n[1]; ++j) for (int k = 0; k < this->s.n[2]; ++k) a(i, j, k) = T(src[q++]);
   }
   long long last_iters() const override { return this->s.iters; }
+  // compile-time options of the reference's ct_params_t, set before the first advance
+  void set_param(const char *name, double v) override {
+    if (std::strcmp(name, "impl_tht") == 0) this->s.impl_tht = int(v);
+    else if (std::strcmp(name, "vip_vab") == 0) this->s.vab = int(v);
+    else wrap_t<boussinesq<T>, T>::set_param(name, v);
+  }
 };
 
 }  // namespace

@@ -31,9 +31,19 @@ def bq_params(setup):
 def bq_oracle(setup, opts=None, n_iters=2, dtype=np.float64, fast=False):
     """The CPU oracle of solvers::boussinesq loaded with a Boussinesq set-up."""
     from libmpdataxx_b200 import opts as o
-    orc = Oracle(setup["grid"], o.iga | o.fct if opts is None else opts, n_iters=n_iters, bcs=setup["bcs"],
+    bcs = ["rigid" if b == "gndsky" else b for b in setup["bcs"]]  # gndsky_3d.hpp: rigid for these fields
+    orc = Oracle(setup["grid"], o.iga | o.fct if opts is None else opts, n_iters=n_iters, bcs=bcs,
                  dtype=dtype, fast=fast, boussinesq=bq_params(setup))
     orc.set_sclr_array("tht_e", setup["tht_e"])
+    if setup.get("impl_tht"):
+        orc.set_param("impl_tht", 1)
+    if setup.get("vip_vab"):
+        orc.set_param("vip_vab", int(setup["vip_vab"]))
+    for name in ("tht_abs", "hflux_frc", "vab_coeff"):
+        if name in setup:
+            orc.set_sclr_array(name, setup[name])
+    for d, a in enumerate(setup.get("vab_relax", [])):
+        orc.set_sclr_array("vab_relax%d" % d, a)
     for e, a in enumerate(setup["advectee"]):
         orc.set_advectee(a, e)
     return orc

@@ -141,3 +141,70 @@ def test_reciprocal_division_matches_cuda_division(tmp_path):
     out = subprocess.run([exe], capture_output=True, text=True)
     print(out.stdout)
     assert out.returncode == 0, out.stdout + out.stderr
+
+
+def forced_bq(grid, bcs, seed, impl_tht, vip_vab):
+    """random_bq plus the forcings of boussinesq_common.hpp / boussinesq_impl.hpp and
+    the velocity absorber of mpdata_rhs_vip_common.hpp, all non-zero: a theta
+    absorber and a velocity absorber in the upper third, a heat flux decaying with
+    height, non-zero relaxed velocities.  With impl_tht the advected theta is the
+    perturbation from tht_e (boussinesq_impl.hpp:8-10)."""
+    s = random_bq(grid, bcs, seed)
+    nd = len(grid)
+    rng = np.random.default_rng(seed + 100)
+    z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in grid], indexing="ij")[-1] / (grid[-1] - 1)
+    top = np.where(z >= 2.0 / 3.0, (z - 2.0 / 3.0) * 3.0, 0.0)
+    s["tht_abs"] = 0.05 * top
+    s["hflux_frc"] = 1e-3 * np.exp(-4 * z)
+    s["impl_tht"] = impl_tht
+    s["vip_vab"] = vip_vab
+    if vip_vab:
+        s["vab_coeff"] = 0.08 * top
+        s["vab_relax"] = [rng.uniform(-0.2, 0.2, size=grid) for _ in range(nd)]
+    if impl_tht:
+        s["advectee"][nd] = s["advectee"][nd] - s["tht_e"]
+    for d in range(nd):  # duplicated-endpoint convention along cyclic axes
+        if bcs[2 * d] == "cyclic":
+            for f in [s["tht_abs"], s["hflux_frc"]] + s.get("vab_relax", []) + ([s["vab_coeff"]] if vip_vab else []):
+                sl_last = [slice(None)] * nd
+                sl_first = [slice(None)] * nd
+                sl_last[d], sl_first[d] = -1, 0
+                f[tuple(sl_last)] = f[tuple(sl_first)]
+    return s
+
+
+FORCED = [
+    ((29, 25), ["cyclic", "cyclic", "rigid", "rigid"], True, solvers.noab, 1),
+    ((29, 25), ["cyclic", "cyclic", "rigid", "rigid"], False, solvers.expl, 1),
+    ((27, 23), ["cyclic", "cyclic", "rigid", "rigid"], False, solvers.impl, 1),
+    ((27, 23), ["cyclic", "cyclic", "rigid", "rigid"], True, solvers.impl, 3),
+    ((15, 13, 17), ["cyclic"] * 4 + ["gndsky"] * 2, True, solvers.impl, 1),
+    ((13, 15, 14), ["cyclic"] * 4 + ["gndsky"] * 2, False, solvers.expl, 2),
+]
+
+
+@pytest.mark.parametrize("grid,bcs,impl_tht,vab,prs_k", FORCED)
+def test_boussinesq_forcings_fp64_match_oracle(grid, bcs, impl_tht, vab, prs_k):
+    """impl_tht (boussinesq_impl.hpp), the velocity absorber in its explicit and
+    implicit forms (mpdata_rhs_vip_common.hpp:182-256, normalised Laplacian of
+    mpdata_rhs_vip_prs_common.hpp:49-84), the theta absorber and heat flux, and the
+    3D ground/sky boundary (gndsky_3d.hpp): FP64 against the oracle after every step
+    with identical GCR iteration counts."""
+    s = forced_bq(grid, bcs, seed=len(grid) * 7 + prs_k, impl_tht=impl_tht, vip_vab=vab)
+    s["prs_k"] = prs_k
+    orc = bq_oracle(s)
+    run = bq_run(s)
+    for step in range(5):
+        orc.advance(1)
+        run.advance(1)
+        st = run.stats()
+        assert st["gcr_iters"] == orc.last_iters, (step, st["gcr_iters"], orc.last_iters)
+        for e in range(len(grid) + 1):
+            assert rel_err(run.advectee(e), orc.advectee(e)) <= RTOL64, (step, e)
+
+
+def test_vab_accessors_need_the_option():
+    s = random_bq((17, 15), ["cyclic", "cyclic", "rigid", "rigid"], seed=3)
+    run = bq_run(s)
+    with pytest.raises(_lib.MpdxError, match="vip_vab unset"):
+        run.vab_coefficient()

@@ -168,3 +168,45 @@ def test_boussinesq_pressure_solver_stuck():
     orc = bq_oracle(s)
     with pytest.raises(RuntimeError, match="stuck in pressure solver"):
         orc.advance(1)
+
+
+def test_oracle_boussinesq_zero_forcings_equal_plain():
+    """With the velocity absorber's coefficient and the theta absorber at zero, the
+    implicit absorber (normalisation by 1 + 0, relaxation by 0) gives the plain
+    solver's fields bit for bit."""
+    from runners import bq_oracle
+    from test_gpu_boussinesq import random_bq
+    s = random_bq((19, 17), ["cyclic", "cyclic", "rigid", "rigid"], seed=9)
+    a = bq_oracle(s)
+    t = dict(s)
+    t["vip_vab"] = 2
+    t["vab_coeff"] = np.zeros(s["grid"])
+    t["vab_relax"] = [np.zeros(s["grid"]), np.zeros(s["grid"])]
+    b = bq_oracle(t)
+    a.advance(3)
+    b.advance(3)
+    for e in range(3):
+        np.testing.assert_array_equal(a.advectee(e), b.advectee(e))
+
+
+def test_oracle_impl_tht_close_to_expl_with_uniform_environment():
+    """With a uniform tht_e (dtht_e = 0) and no absorbers, the implicit form
+    (theta as the perturbation, boussinesq_impl.hpp) and the explicit form
+    (full theta, boussinesq_expl.hpp) describe the same flow.  They agree to the
+    pressure solver's tolerance: the upwind flux of the constant 300 K part of the
+    full theta cancels only where the discrete divergence of the Courant field,
+    which the solve drives below prs_tol / dt, is zero."""
+    from runners import bq_oracle
+    from test_gpu_boussinesq import random_bq
+    s = random_bq((19, 17), ["cyclic"] * 4, seed=4)
+    a = bq_oracle(s)
+    t = dict(s)
+    t["advectee"] = list(s["advectee"])
+    t["advectee"][2] = s["advectee"][2] - s["tht_e"]
+    t["impl_tht"] = True
+    b = bq_oracle(t)
+    a.advance(4)
+    b.advance(4)
+    for e in range(2):
+        np.testing.assert_allclose(b.advectee(e), a.advectee(e), rtol=0, atol=1e-5)
+    np.testing.assert_allclose(b.advectee(2) + s["tht_e"], a.advectee(2), rtol=0, atol=1e-4)
