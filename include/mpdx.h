@@ -96,6 +96,8 @@ typedef struct {
   int upwind_filter_freq;  /* rt_params upwind_filter_freq (mpdata_common.hpp:77): every n-th step is upwind only; 0 = never */
   int impl_tht;            /* ct_params_t::impl_tht: theta is the perturbation from tht_e, its coupling with w implicit (boussinesq_impl.hpp) */
   int vip_vab;             /* ct_params_t::vip_vab: MPDX_VAB_* velocity absorber */
+  int sptl_intrp;          /* ct_params_t::sptl_intrp (formulae_mpdata_common.hpp:21-26) of the div_3rd spatial
+                              terms: 0 exact, 1 aver2, 2 aver4 */
 } mpdx_config;
 
 typedef struct mpdx_solver *mpdx_handle;

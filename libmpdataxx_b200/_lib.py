@@ -48,7 +48,7 @@ class Config(ctypes.Structure):
                 ("tht_ref", ctypes.c_double), ("ix_u", ctypes.c_int), ("ix_v", ctypes.c_int),
                 ("ix_w", ctypes.c_int), ("ix_tht", ctypes.c_int), ("precond", ctypes.c_int),
                 ("prs_fp64", ctypes.c_int), ("upwind_filter_freq", ctypes.c_int),
-                ("impl_tht", ctypes.c_int), ("vip_vab", ctypes.c_int)]
+                ("impl_tht", ctypes.c_int), ("vip_vab", ctypes.c_int), ("sptl_intrp", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):

@@ -64,6 +64,7 @@ class cuda:
         eps = getattr(p, "max_abs_div_eps", None)
         cfg.max_abs_div_eps = -1.0 if eps is None else float(eps)
         cfg.upwind_filter_freq = int(getattr(p, "upwind_filter_freq", 0) or 0)
+        cfg.sptl_intrp = int(getattr(ct, "sptl_intrp", 0))
         cfg.path = {"auto": _lib.PATH_AUTO, "general": _lib.PATH_GENERAL, "fused": _lib.PATH_FUSED}[path]
         if isinstance(solver, _bq):
             solver.fill_config(cfg, p)

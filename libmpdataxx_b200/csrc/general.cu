@@ -234,6 +234,145 @@ struct op_antidiff {
   }
 };
 
+// divergence-form antidiffusive velocity: div_2nd + div_3rd / div_3rd_dt
+// (formulae_mpdata_{1,2,3}d.hpp, helpers of formulae_mpdata_fdiv_{1,2,3}d.hpp,
+// _psi_*, _gc_*, _g_*), in the reference's operand order.  psi is the current
+// iterate psi_np1, pn the other time level psi[e][n-1]; G0 = GC[dim], G1 =
+// GC[dim+1], G2 = GC[dim-1].  The advector of solvers::mpdata is constant in
+// time, so ndt_GC = ndtt_GC = 0 (mpdata_osc_{1,2,3}d.hpp hook_ante_loop) and the
+// temporal terms multiplying them are exact zeros, left out like TOT and DFL
+// above.  1D has no div_3rd_dt form in the reference (it adds nothing there).
+template <int ND, int D, class T>
+struct op_antidiff_div {
+  dfield<T> res, psi, pn, G0, G1, G2;
+  unsigned o;
+  dfield<T> Gf;
+  int sptl;  // exact 0, aver2 1, aver4 2 (formulae_mpdata_common.hpp:21-26)
+  __device__ T q(const dfield<T> &A, int x, int y, int z) const {
+    const T v = P<ND, D>(A, x, y, z);
+    return (o & o_abs) ? fabs(v) : v;
+  }
+  __device__ T G(const dfield<T> &A, int x, int y, int z) const { return P<ND, D>(A, x, y, z); }
+  __device__ T g(int x, int y, int z) const { return (o & o_nug) ? P<ND, D>(Gf, x, y, z) : T(1); }
+  __device__ T pbx(const dfield<T> &A, int x, int y, int z) const { return (q(A, x + 1, y, z) + q(A, x, y, z)) / T(2); }
+  __device__ T pby(const dfield<T> &A, int x, int y, int z) const { return (q(A, x, y, z) + q(A, x, y + 1, z)) / T(2); }
+  __device__ T pbz(const dfield<T> &A, int x, int y, int z) const { return (q(A, x, y, z) + q(A, x, y, z + 1)) / T(2); }
+  __device__ T pbxy(const dfield<T> &A, int x, int y, int z) const {
+    return (q(A, x + 1, y, z) + q(A, x, y, z) + q(A, x, y + 1, z) + q(A, x + 1, y + 1, z)) / T(4);
+  }
+  __device__ T pbxz(const dfield<T> &A, int x, int y, int z) const {
+    return (q(A, x + 1, y, z) + q(A, x, y, z) + q(A, x, y, z + 1) + q(A, x + 1, y, z + 1)) / T(4);
+  }
+  __device__ T pbxyz(int x, int y, int z) const {
+    return (q(psi, x, y, z) + q(psi, x + 1, y, z) + q(psi, x, y + 1, z) + q(psi, x, y, z + 1) + q(psi, x + 1, y + 1, z)
+            + q(psi, x + 1, y, z + 1) + q(psi, x, y + 1, z + 1) + q(psi, x + 1, y + 1, z + 1)) / T(8);
+  }
+  // Courant-number averages (face x+1/2 stored at x)
+  __device__ T g0bx(int x, int y, int z) const { return (G(G0, x, y, z) + G(G0, x - 1, y, z)) / T(2); }
+  __device__ T g1bx(int x, int y, int z) const { return (G(G1, x + 1, y, z) + G(G1, x, y, z)) / T(2); }
+  __device__ T g2bx(int x, int y, int z) const { return (G(G2, x + 1, y, z) + G(G2, x, y, z)) / T(2); }
+  __device__ T g0bxy(int x, int y, int z) const { return (G(G0, x, y, z) + G(G0, x - 1, y, z) + G(G0, x, y + 1, z) + G(G0, x - 1, y + 1, z)) / T(4); }
+  __device__ T g1bxy(int x, int y, int z) const { return (G(G1, x + 1, y, z) + G(G1, x, y, z) + G(G1, x + 1, y - 1, z) + G(G1, x, y - 1, z)) / T(4); }
+  __device__ T g2bxy(int x, int y, int z) const { return (G(G2, x + 1, y + 1, z) + G(G2, x, y + 1, z) + G(G2, x + 1, y, z) + G(G2, x, y, z)) / T(4); }
+  __device__ T g0bxz(int x, int y, int z) const { return (G(G0, x, y, z) + G(G0, x - 1, y, z) + G(G0, x, y, z + 1) + G(G0, x - 1, y, z + 1)) / T(4); }
+  __device__ T g1bxz(int x, int y, int z) const { return (G(G1, x + 1, y, z) + G(G1, x + 1, y, z + 1) + G(G1, x, y, z) + G(G1, x, y, z + 1)) / T(4); }
+  __device__ T g2bxz(int x, int y, int z) const { return (G(G2, x + 1, y, z) + G(G2, x, y, z) + G(G2, x + 1, y, z - 1) + G(G2, x, y, z - 1)) / T(4); }
+  // G averages (formulae_mpdata_g_{1,2,3}d.hpp), 1 without nug
+  __device__ T gbx(int x, int y, int z) const { return (o & o_nug) ? (g(x + 1, y, z) + g(x, y, z)) / T(2) : T(1); }
+  __device__ T gbxy(int x, int y, int z) const {
+    return (o & o_nug) ? (g(x, y, z) + g(x, y + 1, z) + g(x + 1, y, z) + g(x + 1, y + 1, z)) / T(4) : T(1);
+  }
+  __device__ T gbxz(int x, int y, int z) const {
+    return (o & o_nug) ? (g(x, y, z) + g(x, y, z + 1) + g(x + 1, y, z) + g(x + 1, y, z + 1)) / T(4) : T(1);
+  }
+  // flux divergence at the cell centre (fdiv_centre) and at the xy / xz edges (fdiv_corner_*)
+  __device__ T fc(int x, int y, int z) const {
+    T r = G(G0, x, y, z) * pbx(psi, x, y, z) - G(G0, x - 1, y, z) * pbx(psi, x - 1, y, z);
+    if (ND > 1) r = r + G(G1, x, y, z) * pby(psi, x, y, z) - G(G1, x, y - 1, z) * pby(psi, x, y - 1, z);
+    if (ND > 2) r = r + G(G2, x, y, z) * pbz(psi, x, y, z) - G(G2, x, y, z - 1) * pbz(psi, x, y, z - 1);
+    return r / g(x, y, z);
+  }
+  __device__ T fxy(int x, int y, int z) const {
+    T r = g0bxy(x + 1, y, z) * pby(psi, x + 1, y, z) - g0bxy(x, y, z) * pby(psi, x, y, z)
+        + g1bxy(x, y + 1, z) * pbx(psi, x, y + 1, z) - g1bxy(x, y, z) * pbx(psi, x, y, z);
+    if (ND > 2) r = r + g2bxy(x, y, z) * pbxyz(x, y, z) - g2bxy(x, y, z - 1) * pbxyz(x, y, z - 1);
+    return r / gbxy(x, y, z);
+  }
+  __device__ T fxz(int x, int y, int z) const {
+    return (g0bxz(x + 1, y, z) * pbz(psi, x + 1, y, z) - g0bxz(x, y, z) * pbz(psi, x, y, z)
+            + g1bxz(x, y, z) * pbxyz(x, y, z) - g1bxz(x, y - 1, z) * pbxyz(x, y - 1, z)
+            + g2bxz(x, y, z + 1) * pbx(psi, x, y, z + 1) - g2bxz(x, y, z) * pbx(psi, x, y, z)) / gbxz(x, y, z);
+  }
+  // sum of psi over the six (2D) / ten (3D) points of nfdiv's denominator, continuing from s
+  __device__ T s_nf(const dfield<T> &A, int a, int b, int c, T s, bool first) const {
+    T r = first ? q(A, a + 1, b, c) + q(A, a, b, c) : s + q(A, a + 1, b, c) + q(A, a, b, c);
+    if (ND == 1) return r;
+    r = r + q(A, a, b + 1, c) + q(A, a + 1, b + 1, c) + q(A, a, b - 1, c) + q(A, a + 1, b - 1, c);
+    if (ND == 3) r = r + q(A, a + 1, b, c + 1) + q(A, a + 1, b, c - 1) + q(A, a, b, c - 1) + q(A, a, b, c + 1);
+    return r;
+  }
+  __device__ void operator()(int a, int b, int c) const {
+    const bool iga = o & o_iga;
+    const T C = G(G0, a, b, c);
+    const T m1 = T(2 + 4 * (ND - 1)), m2 = T(4 + 4 * (ND - 1));
+    // nfdiv (formulae_mpdata_fdiv_*d.hpp)
+    T nn = g0bx(a + 1, b, c) * q(psi, a + 1, b, c) - g0bx(a, b, c) * q(psi, a, b, c);
+    if (ND > 1) nn = nn + g1bx(a, b, c) * pbxy(psi, a, b, c) - g1bx(a, b - 1, c) * pbxy(psi, a, b - 1, c);
+    if (ND > 2) nn = nn + g2bx(a, b, c) * pbxz(psi, a, b, c) - g2bx(a, b, c - 1) * pbxz(psi, a, b, c - 1);
+    const T nfdiv = iga ? nn / gbx(a, b, c) : m1 * frac(o, nn, gbx(a, b, c) * s_nf(psi, a, b, c, T(0), true));
+    const T ndxp = ndx<ND, D>(o, psi, a, b, c);
+    const T d2 = fabs(C) / 2 * ndxp - C / 2 * nfdiv;  // div_2nd
+    const bool dt = (o & o_div_3rd_dt) && ND > 1;
+    if (!(o & o_div_3rd) && !dt) { P<ND, D>(res, a, b, c) = d2; return; }
+    const T up = iga ? T(0) : fabs(d2) / 2 * ndxp;  // upwind-differencing correction
+    const T ndxx_gc = G(G0, a + 1, b, c) + G(G0, a - 1, b, c) - 2 * G(G0, a, b, c);
+    const T nxxg = iga ? ndxx_gc * pbx(psi, a, b, c) : ndxx_gc;
+    const T helper = sptl == 0 ? nxxg : (sptl == 1 ? 4 * nxxg : T(0));
+    const T xx = nd2(o, P<ND, D>(psi, a + 2, b, c), P<ND, D>(psi, a + 1, b, c), P<ND, D>(psi, a, b, c), P<ND, D>(psi, a - 1, b, c));
+    const T spatial = -T(1.0 / 24) * (4 * C * xx + 2 * ndxp * ((G(G0, a + 1, b, c) - G(G0, a - 1, b, c)) / 2) + helper);
+    T r;
+    if (!dt) {
+      // div_3rd: mixed (ndx_fdiv) and temporal (nfdiv_fdiv) terms
+      T s4 = q(psi, a + 2, b, c) + q(psi, a + 1, b, c) + q(psi, a, b, c) + q(psi, a - 1, b, c);
+      T sf = s4, sx = s4;
+      if (ND > 1) {
+        sf = sf + q(psi, a, b + 1, c) + q(psi, a, b - 1, c) + q(psi, a + 1, b + 1, c) + q(psi, a + 1, b - 1, c);
+        if (ND == 3) {  // ndx_fdiv's denominator takes the points in another order
+          sf = sf + q(psi, a, b, c + 1) + q(psi, a, b, c - 1) + q(psi, a + 1, b, c + 1) + q(psi, a + 1, b, c - 1);
+          sx = s4 + q(psi, a, b + 1, c) + q(psi, a, b - 1, c) + q(psi, a, b, c - 1) + q(psi, a, b, c + 1) + q(psi, a + 1, b + 1, c)
+             + q(psi, a + 1, b - 1, c) + q(psi, a + 1, b, c - 1) + q(psi, a + 1, b, c + 1);
+        } else {
+          sx = sf;
+        }
+      }
+      const T f1 = fc(a + 1, b, c), f0 = fc(a, b, c);
+      T nf = g0bx(a + 1, b, c) * f1 - g0bx(a, b, c) * f0;
+      if (ND > 1) nf = nf + g1bx(a, b, c) * fxy(a, b, c) - g1bx(a, b - 1, c) * fxy(a, b - 1, c);
+      if (ND > 2) nf = nf + g2bx(a, b, c) * fxz(a, b, c) - g2bx(a, b, c - 1) * fxz(a, b, c - 1);
+      const T ndx_fdiv = iga ? f1 - f0 : m2 * frac(o, f1 - f0, sx);
+      const T nfdiv_fdiv = iga ? nf / gbx(a, b, c) : m2 * frac(o, nf, gbx(a, b, c) * sf);
+      r = d2 + (up + spatial + T(0.5) * fabs(C) * ndx_fdiv + T(1.0 / 24) * (-8 * C * nfdiv_fdiv));
+    } else {
+      // div_3rd_dt (2D, 3D): mixed term from d(psi)/dt, temporal term nfdiv_dt
+      const T p1 = P<ND, D>(psi, a + 1, b, c), n1 = P<ND, D>(pn, a + 1, b, c), p0 = P<ND, D>(psi, a, b, c), n0 = P<ND, D>(pn, a, b, c);
+      T ndtx;
+      if (iga) ndtx = p1 - n1 - p0 + n0;
+      else if (o & o_abs) ndtx = 4 * frac(o, fabs(p1) - fabs(n1) - fabs(p0) + fabs(n0), fabs(p1) + fabs(n1) + fabs(p0) + fabs(n0));
+      else ndtx = 4 * frac(o, p1 - n1 - p0 + n0, p1 + n1 + p0 + n0);
+      T nt = g0bx(a + 1, b, c) * (q(psi, a + 1, b, c) - q(pn, a + 1, b, c)) - g0bx(a, b, c) * (q(psi, a, b, c) - q(pn, a, b, c))
+           + g1bx(a, b, c) * (pbxy(psi, a, b, c) - pbxy(pn, a, b, c)) - g1bx(a, b - 1, c) * (pbxy(psi, a, b - 1, c) - pbxy(pn, a, b - 1, c));
+      if (ND > 2)
+        nt = nt + g2bx(a, b, c) * (pbxz(psi, a, b, c) - pbxz(pn, a, b, c)) - g2bx(a, b, c - 1) * (pbxz(psi, a, b, c - 1) - pbxz(pn, a, b, c - 1));
+      const T m4 = T(ND == 2 ? 12 : 20);
+      T nfdiv_dt;
+      if (iga) nfdiv_dt = nt / gbx(a, b, c);
+      else nfdiv_dt = m4 * frac(o, nt, gbx(a, b, c) * s_nf(pn, a, b, c, s_nf(psi, a, b, c, T(0), true), false));
+      r = d2 + (up + spatial - T(0.5) * fabs(C) * ndtx + T(1.0 / 24) * (8 * C * nfdiv_dt));
+    }
+    P<ND, D>(res, a, b, c) = r;
+  }
+};
+
 // donor-cell flux (donorcell_formulae.hpp:25-79)
 template <int ND, int D, class T>
 struct op_flux {
@@ -695,6 +834,21 @@ void general<T>::antidiff_nd(field<T> *res, field<T> &psi, field<T> *G) {
   auto &S = *s;
   const unsigned o = S.opts;
   const rng *ir = S.ir, *im = S.im;
+  if (o & o_div_2nd) {  // divergence form (formulae_mpdata_{1,2,3}d.hpp antidiff with div_2nd)
+    const dfield<T> pn = S.psi[cur_e][S.tl[cur_e] ^ 1].v;  // psi[e][n-1]
+    const int sp = S.sptl_intrp;
+    if (ND == 1) {
+      launch_frame<1, 0>(S.stream, op_antidiff_div<1, 0, T>{res[0].v, psi.v, pn, G[0].v, G[0].v, G[0].v, o, S.G.v, sp}, im[0], {0, 0}, {0, 0});
+    } else if (ND == 2) {
+      launch_frame<2, 0>(S.stream, op_antidiff_div<2, 0, T>{res[0].v, psi.v, pn, G[0].v, G[1].v, G[1].v, o, S.G.v, sp}, im[0], ir[1], {0, 0});
+      launch_frame<2, 1>(S.stream, op_antidiff_div<2, 1, T>{res[1].v, psi.v, pn, G[1].v, G[0].v, G[0].v, o, S.G.v, sp}, im[1], ir[0], {0, 0});
+    } else {
+      launch_frame<3, 0>(S.stream, op_antidiff_div<3, 0, T>{res[0].v, psi.v, pn, G[0].v, G[1].v, G[2].v, o, S.G.v, sp}, im[0], ir[1], ir[2]);
+      launch_frame<3, 1>(S.stream, op_antidiff_div<3, 1, T>{res[1].v, psi.v, pn, G[1].v, G[2].v, G[0].v, o, S.G.v, sp}, im[1], ir[2], ir[0]);
+      launch_frame<3, 2>(S.stream, op_antidiff_div<3, 2, T>{res[2].v, psi.v, pn, G[2].v, G[0].v, G[1].v, o, S.G.v, sp}, im[2], ir[0], ir[1]);
+    }
+    return;
+  }
   if (ND == 1) {
     launch_frame<1, 0>(S.stream, op_antidiff<1, 0, T>{res[0].v, psi.v, G[0].v, G[0].v, G[0].v, o, S.G.v}, im[0], {0, 0}, {0, 0});
   } else if (ND == 2) {
@@ -767,6 +921,7 @@ void general<T>::advop_nd(int e) {
       S.tl[e] ^= 1;  // cycle(e)
       xchng_sclr(S.psi[e][S.tl[e]], S.H);
       field<T> *corr = GC_corr(iter);
+      cur_e = e;
       antidiff_nd<ND>(corr, S.psi[e][S.tl[e]], GC_unco(iter));
       if (!(S.opts & o_fct) && iter != S.n_iters - 1) {
         xchng_vctr_nrml(corr, 0);

@@ -37,6 +37,7 @@ struct general {
   bool any_rigid() const;
 
  private:
+  int cur_e = 0;  // equation whose advop is running (the divergence form reads its other time level)
   field<T> *GC_unco(int iter);
   field<T> *GC_corr(int iter);
   field<T> *GCit(int iter);

@@ -187,6 +187,7 @@ struct mpdata_solver : solver_base {
     st.setup(c.n_dims, c.grid, c.n_eqns, unsigned(c.opts), c.n_iters, c.bcs);
     st.max_abs_div_eps = c.max_abs_div_eps < 0 ? std::numeric_limits<T>::epsilon() : T(c.max_abs_div_eps);
     st.upwind_filter_freq = c.upwind_filter_freq;
+    st.sptl_intrp = c.sptl_intrp;
     gen.init_g();
     path = c.path;
     MPDX_CUDA(cudaMalloc(&scratch, 64));
@@ -569,9 +570,19 @@ void validate(const mpdx_config &c) {
   if (c.n_eqns < 1) throw error(MPDX_E_ARG, "n_eqns must be positive");
   if (c.n_iters < 1) throw error(MPDX_E_ARG, "n_iters must be positive");
   const unsigned o = unsigned(c.opts);
-  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl | o_nug | o_khn;
+  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl | o_nug | o_khn | o_div_2nd | o_div_3rd | o_div_3rd_dt;
   if (o & ~built)
-    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl nug khn)");
+    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl nug khn div_2nd div_3rd div_3rd_dt)");
+  // the divergence form (formulae_mpdata_{1,2,3}d.hpp): div_3rd / div_3rd_dt extend div_2nd,
+  // exclude each other and tot / dfl (static_asserts and enable_ifs there)
+  if (o & (o_div_2nd | o_div_3rd | o_div_3rd_dt)) {
+    if (!(o & o_div_2nd)) throw error(MPDX_E_ARG, "div_3rd and div_3rd_dt need div_2nd");
+    if ((o & o_div_3rd) && (o & o_div_3rd_dt)) throw error(MPDX_E_ARG, "div_3rd and div_3rd_dt are mutually exclusive");
+    if (o & (o_tot | o_dfl)) throw error(MPDX_E_ARG, "div_2nd & div_3rd options are incompatible with tot and dfl");
+    if (c.solver == MPDX_SOLVER_BOUSSINESQ)
+      throw error(MPDX_E_UNSUPPORTED, "the divergence-form options are built for solvers::mpdata (constant advector) only");
+  }
+  if (c.sptl_intrp < 0 || c.sptl_intrp > 2) throw error(MPDX_E_ARG, "sptl_intrp must be exact (0), aver2 (1) or aver4 (2)");
   if ((o & o_nug) && c.solver == MPDX_SOLVER_BOUSSINESQ)
     throw error(MPDX_E_UNSUPPORTED, "nug option is built for solvers::mpdata only on this backend");
   if (c.upwind_filter_freq < 0) throw error(MPDX_E_ARG, "upwind_filter_freq must be non-negative");

@@ -24,6 +24,7 @@ struct mpdata_state {
   field<T> psi_min, psi_max, beta_up, beta_dn;
   field<T> G;                  // G factor with the nug option (sharedmem G); unallocated otherwise
   int upwind_filter_freq = 0;  // rt_params (mpdata_common.hpp:77): upwind-only step every n-th step
+  int sptl_intrp = 0;          // ct_params_t::sptl_intrp of the div_3rd spatial terms: exact 0, aver2 1, aver4 2
   cudaStream_t stream = nullptr;
   long long timestep = 0;
 

@@ -73,8 +73,8 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   static_assert(bcxl != bcond::null && bcxr != bcond::null, "x boundary conditions are required");
   static_assert(n_dims < 2 || (bcyl != bcond::null && bcyr != bcond::null), "y boundary conditions are required");
   static_assert(n_dims < 3 || (bczl != bcond::null && bczr != bcond::null), "z boundary conditions are required");
-  static_assert(!opts::isset(ct_params_t::opts, opts::div_2nd | opts::div_3rd | opts::div_3rd_dt | opts::fot),
-                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl nug khn)");
+  static_assert(!opts::isset(ct_params_t::opts, opts::fot),
+                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl nug khn div_2nd div_3rd div_3rd_dt)");
 
   explicit cuda(const rt_params_t &p) : p_(p) {
     mpdx_config c;
@@ -93,6 +93,7 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
     c.dk = p.dk != 0 ? double(p.dk) : 1.0;
     c.max_abs_div_eps = double(p.max_abs_div_eps);
     c.upwind_filter_freq = p.upwind_filter_freq;
+    c.sptl_intrp = int(ct_params_t::sptl_intrp);
     solver_t::fill(c, p);
     detail::check(nullptr, mpdx_create(&c, &h_));
   }

@@ -24,6 +24,7 @@ class ct_params_default_t:
     sgs_scheme = 0
     impl_tht = False
     vip_vab = 0       # noab (mpdata_rhs_vip_common.hpp:16-21)
+    sptl_intrp = 0    # exact (formulae_mpdata_common.hpp:21-26): div_3rd spatial terms
 
 
 class _rt_base:

@@ -33,7 +33,7 @@ namespace mpdx_oracle {
 enum : unsigned {
   o_fct = 1u << 0, o_abs = 1u << 1, o_tot = 1u << 2, o_pfc = 1u << 3,
   o_npa = 1u << 4, o_iga = 1u << 5, o_nug = 1u << 6, o_dfl = 1u << 7,
-  o_khn = 1u << 8
+  o_khn = 1u << 8, o_div_2nd = 1u << 9, o_div_3rd = 1u << 10, o_div_3rd_dt = 1u << 11
 };
 enum { bc_cyclic = 0, bc_open = 1, bc_rigid = 2 };
 
@@ -148,7 +148,10 @@ struct mpdata {
   rng ir[3];  // interior ranges
   rng im[3];  // (i.first-1 .. i.last) -- mpdata_osc_*d.hpp ctor
 
-  static int mpdata_halo(unsigned o) { return (o & (o_tot | o_dfl)) ? 2 : 1; }  // formulae_mpdata_common.hpp:50-59
+  static int mpdata_halo(unsigned o) {  // formulae_mpdata_common.hpp:50-59
+    return (o & (o_tot | o_dfl | o_div_2nd | o_div_3rd | o_div_3rd_dt)) ? 2 : 1;
+  }
+  int sptl_intrp = 0;  // ct_params_t::sptl_intrp: exact, aver2, aver4 (formulae_mpdata_common.hpp:21-26)
 
   void setup(int nd_, const int *n_, int n_eqns_, unsigned opts_, int n_iters_, const int *bcs_) {
     nd = nd_; n_eqns = n_eqns_; opts = opts_; n_iters = n_iters_;
@@ -577,6 +580,159 @@ struct mpdata {
         });
   }
 
+  // ---- divergence-form antidiffusive velocity: div_2nd + div_3rd / div_3rd_dt
+  // (formulae_mpdata_{1,2,3}d.hpp, helpers of formulae_mpdata_fdiv_{1,2,3}d.hpp,
+  // _psi_*, _gc_*, _g_*).  p is the current iterate psi_np1 and pn the other
+  // time level psi_n (psi[e][n-1]); G0 = GC[dim], G1 = GC[dim+1], G2 = GC[dim-1]
+  // (= GC[dim+2] in 3D).  The advector of solvers::mpdata does not change in
+  // time, so its time derivatives ndt_GC and ndtt_GC are zero
+  // (mpdata_osc_{1,2,3}d.hpp hook_ante_loop) and the temporal terms that
+  // multiply them are exact zeros, left out as TOT and DFL are above.  In 1D the
+  // reference has no div_3rd_dt form: there it adds nothing to div_2nd.
+  template <int ND, int D>
+  T adiv(const arr<T> &p, const arr<T> &pn, const arr<T> &G0, const arr<T> &G1, const arr<T> &G2, int a, int b, int c) const {
+    const bool iga = opts & o_iga, ab = opts & o_abs;
+    auto q = [&](const arr<T> &A, int x, int y, int z) { const T v = P<ND, D>(A, x, y, z); return ab ? std::abs(v) : v; };
+    auto ps = [&](int x, int y, int z) { return q(p, x, y, z); };
+    auto g = [&](int x, int y, int z) { return Gc3<ND, D>(x, y, z); };
+    auto G = [&](const arr<T> &A, int x, int y, int z) { return P<ND, D>(A, x, y, z); };
+    // interpolated psi (psi_bar_*: abs of each value with the abs option)
+    auto pbx = [&](const arr<T> &A, int x, int y, int z) { return (q(A, x + 1, y, z) + q(A, x, y, z)) / T(2); };
+    auto pby = [&](const arr<T> &A, int x, int y, int z) { return (q(A, x, y, z) + q(A, x, y + 1, z)) / T(2); };
+    auto pbz = [&](const arr<T> &A, int x, int y, int z) { return (q(A, x, y, z) + q(A, x, y, z + 1)) / T(2); };
+    auto pbxy = [&](const arr<T> &A, int x, int y, int z) {
+      return (q(A, x + 1, y, z) + q(A, x, y, z) + q(A, x, y + 1, z) + q(A, x + 1, y + 1, z)) / T(4);
+    };
+    auto pbxz = [&](const arr<T> &A, int x, int y, int z) {
+      return (q(A, x + 1, y, z) + q(A, x, y, z) + q(A, x, y, z + 1) + q(A, x + 1, y, z + 1)) / T(4);
+    };
+    auto pbxyz = [&](const arr<T> &A, int x, int y, int z) {
+      return (q(A, x, y, z) + q(A, x + 1, y, z) + q(A, x, y + 1, z) + q(A, x, y, z + 1) + q(A, x + 1, y + 1, z)
+              + q(A, x + 1, y, z + 1) + q(A, x, y + 1, z + 1) + q(A, x + 1, y + 1, z + 1)) / T(8);
+    };
+    // Courant-number averages (GC0_bar_x ... GC2_bar_xz; face x+1/2 stored at x)
+    auto g0bx = [&](int x, int y, int z) { return (G(G0, x, y, z) + G(G0, x - 1, y, z)) / T(2); };
+    auto g1bx = [&](int x, int y, int z) { return (G(G1, x + 1, y, z) + G(G1, x, y, z)) / T(2); };
+    auto g2bx = [&](int x, int y, int z) { return (G(G2, x + 1, y, z) + G(G2, x, y, z)) / T(2); };
+    auto g0bxy = [&](int x, int y, int z) { return (G(G0, x, y, z) + G(G0, x - 1, y, z) + G(G0, x, y + 1, z) + G(G0, x - 1, y + 1, z)) / T(4); };
+    auto g1bxy = [&](int x, int y, int z) { return (G(G1, x + 1, y, z) + G(G1, x, y, z) + G(G1, x + 1, y - 1, z) + G(G1, x, y - 1, z)) / T(4); };
+    auto g2bxy = [&](int x, int y, int z) { return (G(G2, x + 1, y + 1, z) + G(G2, x, y + 1, z) + G(G2, x + 1, y, z) + G(G2, x, y, z)) / T(4); };
+    auto g0bxz = [&](int x, int y, int z) { return (G(G0, x, y, z) + G(G0, x - 1, y, z) + G(G0, x, y, z + 1) + G(G0, x - 1, y, z + 1)) / T(4); };
+    auto g1bxz = [&](int x, int y, int z) { return (G(G1, x + 1, y, z) + G(G1, x + 1, y, z + 1) + G(G1, x, y, z) + G(G1, x, y, z + 1)) / T(4); };
+    auto g2bxz = [&](int x, int y, int z) { return (G(G2, x + 1, y, z) + G(G2, x, y, z) + G(G2, x + 1, y, z - 1) + G(G2, x, y, z - 1)) / T(4); };
+    // G averages (formulae_mpdata_g_{1,2,3}d.hpp): 1 without nug
+    const bool nug = opts & o_nug;
+    auto gbx = [&](int x, int y, int z) { return nug ? (g(x + 1, y, z) + g(x, y, z)) / T(2) : T(1); };
+    auto gbxy = [&](int x, int y, int z) { return nug ? (g(x, y, z) + g(x, y + 1, z) + g(x + 1, y, z) + g(x + 1, y + 1, z)) / T(4) : T(1); };
+    auto gbxz = [&](int x, int y, int z) { return nug ? (g(x, y, z) + g(x, y, z + 1) + g(x + 1, y, z) + g(x + 1, y, z + 1)) / T(4) : T(1); };
+    // flux divergences at the cell centre and at the xy / xz edges
+    auto fc = [&](int x, int y, int z) {
+      T r = G(G0, x, y, z) * pbx(p, x, y, z) - G(G0, x - 1, y, z) * pbx(p, x - 1, y, z);
+      if (ND > 1) r = r + G(G1, x, y, z) * pby(p, x, y, z) - G(G1, x, y - 1, z) * pby(p, x, y - 1, z);
+      if (ND > 2) r = r + G(G2, x, y, z) * pbz(p, x, y, z) - G(G2, x, y, z - 1) * pbz(p, x, y, z - 1);
+      return r / g(x, y, z);
+    };
+    auto fxy = [&](int x, int y, int z) {
+      T r = g0bxy(x + 1, y, z) * pby(p, x + 1, y, z) - g0bxy(x, y, z) * pby(p, x, y, z)
+          + g1bxy(x, y + 1, z) * pbx(p, x, y + 1, z) - g1bxy(x, y, z) * pbx(p, x, y, z);
+      if (ND > 2) r = r + g2bxy(x, y, z) * pbxyz(p, x, y, z) - g2bxy(x, y, z - 1) * pbxyz(p, x, y, z - 1);
+      return r / gbxy(x, y, z);
+    };
+    auto fxz = [&](int x, int y, int z) {
+      return (g0bxz(x + 1, y, z) * pbz(p, x + 1, y, z) - g0bxz(x, y, z) * pbz(p, x, y, z)
+              + g1bxz(x, y, z) * pbxyz(p, x, y, z) - g1bxz(x, y - 1, z) * pbxyz(p, x, y - 1, z)
+              + g2bxz(x, y, z + 1) * pbx(p, x, y, z + 1) - g2bxz(x, y, z) * pbx(p, x, y, z)) / gbxz(x, y, z);
+    };
+    // numerator of the nondimensionalised flux divergence at (a+1/2) (nfdiv)
+    auto nfdiv_num = [&]() {
+      T r = g0bx(a + 1, b, c) * ps(a + 1, b, c) - g0bx(a, b, c) * ps(a, b, c);
+      if (ND > 1) r = r + g1bx(a, b, c) * pbxy(p, a, b, c) - g1bx(a, b - 1, c) * pbxy(p, a, b - 1, c);
+      if (ND > 2) r = r + g2bx(a, b, c) * pbxz(p, a, b, c) - g2bx(a, b, c - 1) * pbxz(p, a, b, c - 1);
+      return r;
+    };
+    // sums of psi in the denominators (their orders follow the reference)
+    auto s_nfdiv = [&](const arr<T> &A) {
+      if (ND == 1) return q(A, a + 1, b, c) + q(A, a, b, c);
+      if (ND == 2)
+        return q(A, a + 1, b, c) + q(A, a, b, c) + q(A, a, b + 1, c) + q(A, a + 1, b + 1, c) + q(A, a, b - 1, c) + q(A, a + 1, b - 1, c);
+      return q(A, a + 1, b, c) + q(A, a, b, c) + q(A, a, b + 1, c) + q(A, a + 1, b + 1, c) + q(A, a, b - 1, c)
+           + q(A, a + 1, b - 1, c) + q(A, a + 1, b, c + 1) + q(A, a + 1, b, c - 1) + q(A, a, b, c - 1) + q(A, a, b, c + 1);
+    };
+    auto s4 = [&]() { return ps(a + 2, b, c) + ps(a + 1, b, c) + ps(a, b, c) + ps(a - 1, b, c); };
+    auto s_nfdiv_fdiv = [&]() {
+      if (ND == 1) return s4();
+      if (ND == 2) return s4() + ps(a, b + 1, c) + ps(a, b - 1, c) + ps(a + 1, b + 1, c) + ps(a + 1, b - 1, c);
+      return s4() + ps(a, b + 1, c) + ps(a, b - 1, c) + ps(a + 1, b + 1, c) + ps(a + 1, b - 1, c) + ps(a, b, c + 1)
+           + ps(a, b, c - 1) + ps(a + 1, b, c + 1) + ps(a + 1, b, c - 1);
+    };
+    auto s_ndx_fdiv = [&]() {
+      if (ND < 3) return s_nfdiv_fdiv();
+      return s4() + ps(a, b + 1, c) + ps(a, b - 1, c) + ps(a, b, c - 1) + ps(a, b, c + 1) + ps(a + 1, b + 1, c)
+           + ps(a + 1, b - 1, c) + ps(a + 1, b, c - 1) + ps(a + 1, b, c + 1);
+    };
+    const T m1 = T(2 + 4 * (ND - 1)), m2 = T(4 + 4 * (ND - 1));
+    const T C = G(G0, a, b, c);
+    const T nfdiv = iga ? nfdiv_num() / gbx(a, b, c) : m1 * frac(opts, nfdiv_num(), gbx(a, b, c) * s_nfdiv(p));
+    const T ndxp = ndx<ND, D>(p, a, b, c);
+    const T d2 = std::abs(C) / 2 * ndxp - C / 2 * nfdiv;  // div_2nd
+    const bool dt = (opts & o_div_3rd_dt) && ND > 1;
+    if (!(opts & o_div_3rd) && !dt) return d2;
+    // div_3rd: upwind-differencing correction (none with iga), spatial, mixed and temporal terms
+    const T up = iga ? T(0) : std::abs(d2) / 2 * ndxp;
+    const T ndxx_gc = G(G0, a + 1, b, c) + G(G0, a - 1, b, c) - 2 * G(G0, a, b, c);
+    const T nxxg = iga ? ndxx_gc * pbx(p, a, b, c) : ndxx_gc;
+    const T helper = sptl_intrp == 0 ? nxxg : (sptl_intrp == 1 ? 4 * nxxg : T(0));
+    const T spatial = -T(1.0 / 24) * (4 * C * ndxx<ND, D>(p, a, b, c)
+                                      + 2 * ndxp * ((G(G0, a + 1, b, c) - G(G0, a - 1, b, c)) / 2) + helper);
+    if (!dt) {
+      auto nfdiv_fdiv_num = [&]() {
+        T r = g0bx(a + 1, b, c) * fc(a + 1, b, c) - g0bx(a, b, c) * fc(a, b, c);
+        if (ND > 1) r = r + g1bx(a, b, c) * fxy(a, b, c) - g1bx(a, b - 1, c) * fxy(a, b - 1, c);
+        if (ND > 2) r = r + g2bx(a, b, c) * fxz(a, b, c) - g2bx(a, b, c - 1) * fxz(a, b, c - 1);
+        return r;
+      };
+      const T dfc = fc(a + 1, b, c) - fc(a, b, c);
+      const T ndx_fdiv = iga ? dfc : m2 * frac(opts, dfc, s_ndx_fdiv());
+      const T nfdiv_fdiv = iga ? nfdiv_fdiv_num() / gbx(a, b, c) : m2 * frac(opts, nfdiv_fdiv_num(), gbx(a, b, c) * s_nfdiv_fdiv());
+      return d2 + (up + spatial + T(0.5) * std::abs(C) * ndx_fdiv + T(1.0 / 24) * (-8 * C * nfdiv_fdiv));
+    }
+    // div_3rd_dt (2D, 3D)
+    auto dq = [&](int x, int y, int z) { return q(p, x, y, z) - q(pn, x, y, z); };
+    T ndtx;
+    {
+      const T p1 = P<ND, D>(p, a + 1, b, c), n1 = P<ND, D>(pn, a + 1, b, c), p0 = P<ND, D>(p, a, b, c), n0 = P<ND, D>(pn, a, b, c);
+      if (iga) ndtx = p1 - n1 - p0 + n0;
+      else if (ab) ndtx = 4 * frac(opts, std::abs(p1) - std::abs(n1) - std::abs(p0) + std::abs(n0),
+                                   std::abs(p1) + std::abs(n1) + std::abs(p0) + std::abs(n0));
+      else ndtx = 4 * frac(opts, p1 - n1 - p0 + n0, p1 + n1 + p0 + n0);
+    }
+    T ndt_num = g0bx(a + 1, b, c) * dq(a + 1, b, c) - g0bx(a, b, c) * dq(a, b, c)
+              + g1bx(a, b, c) * (pbxy(p, a, b, c) - pbxy(pn, a, b, c)) - g1bx(a, b - 1, c) * (pbxy(p, a, b - 1, c) - pbxy(pn, a, b - 1, c));
+    if (ND > 2)
+      ndt_num = ndt_num + g2bx(a, b, c) * (pbxz(p, a, b, c) - pbxz(pn, a, b, c)) - g2bx(a, b, c - 1) * (pbxz(p, a, b, c - 1) - pbxz(pn, a, b, c - 1));
+    const T m4 = T(ND == 2 ? 12 : 20);
+    // the denominator sums the psi_np1 values, then the psi_n values, as one chain
+    T s_dt = s_nfdiv(p);
+    if (!iga) {
+      if (ND == 2)
+        s_dt = s_dt + q(pn, a + 1, b, c) + q(pn, a, b, c) + q(pn, a, b + 1, c) + q(pn, a + 1, b + 1, c) + q(pn, a, b - 1, c)
+             + q(pn, a + 1, b - 1, c);
+      else
+        s_dt = s_dt + q(pn, a + 1, b, c) + q(pn, a, b, c) + q(pn, a, b + 1, c) + q(pn, a + 1, b + 1, c) + q(pn, a, b - 1, c)
+             + q(pn, a + 1, b - 1, c) + q(pn, a + 1, b, c + 1) + q(pn, a + 1, b, c - 1) + q(pn, a, b, c - 1) + q(pn, a, b, c + 1);
+    }
+    const T nfdiv_dt = iga ? ndt_num / gbx(a, b, c) : m4 * frac(opts, ndt_num, gbx(a, b, c) * s_dt);
+    return d2 + (up + spatial - T(0.5) * std::abs(C) * ndtx + T(1.0 / 24) * (8 * C * nfdiv_dt));
+  }
+  // res over faces im along D x interior across (formulae_mpdata_{1,2,3}d.hpp antidiff, divergence form)
+  template <int ND, int D> void antidiff_div(arr<T> &res, const arr<T> &p, const arr<T> &pn, const vctr<T> &G) {
+    const arr<T> &G0 = G[D], &G1 = G[(D + 1) % ND], &G2 = G[(D + 2) % ND];
+    const rng ra = im[D], rb = ND > 1 ? ir[(D + 1) % ND] : rng{0, 0}, rc = ND > 2 ? ir[(D + 2) % ND] : rng{0, 0};
+    box<ND, D>(ra, rb, rc, [&](int a, int b, int c) { P<ND, D>(res, a, b, c) = adiv<ND, D>(p, pn, G0, G1, G2, a, b, c); });
+  }
+  // G at a frame point (formulae::G; 1 without nug)
+  template <int ND, int D> T Gc3(int a, int b, int c) const { return (opts & o_nug) ? P<ND, D>(Gf, a, b, c) : T(1); }
+
   // ---- donor-cell flux over faces ra (frame a) x rb x rc (make_flux, donorcell_formulae.hpp:36-79) ----
   template <int ND, int D> void make_flux(arr<T> &F, const arr<T> &p, const arr<T> &C, rng ra, rng rb, rng rc) {
     box<ND, D>(ra, rb, rc, [&](int a, int b, int c) {
@@ -731,7 +887,12 @@ struct mpdata {
         xchng(e);
         const arr<T> &p = psi[e][tl[e]];
         vctr<T> &corr = GC_corr(iter), &unco = GC_unco(iter);
-        if (nd == 1) antidiff1(corr[0], p, unco);
+        if (opts & o_div_2nd) {
+          const arr<T> &pn = psi[e][(tl[e] + 1) % 2];  // psi[e][n-1]
+          if (nd == 1) antidiff_div<1, 0>(corr[0], p, pn, unco);
+          else if (nd == 2) { antidiff_div<2, 0>(corr[0], p, pn, unco); antidiff_div<2, 1>(corr[1], p, pn, unco); }
+          else { antidiff_div<3, 0>(corr[0], p, pn, unco); antidiff_div<3, 1>(corr[1], p, pn, unco); antidiff_div<3, 2>(corr[2], p, pn, unco); }
+        } else if (nd == 1) antidiff1(corr[0], p, unco);
         else if (nd == 2) { antidiff2<0>(corr[0], p, unco); antidiff2<1>(corr[1], p, unco); }
         else { antidiff3<0>(corr[0], p, unco); antidiff3<1>(corr[1], p, unco); antidiff3<2>(corr[2], p, unco); }
         if (!(opts & o_fct) && iter != n_iters - 1) {

@@ -61,6 +61,7 @@ struct wrap_t : base_t {
   }
   void set_param(const char *name, double v) override {
     if (std::strcmp(name, "upwind_filter_freq") == 0) s.upwind_filter_freq = int(v);
+    else if (std::strcmp(name, "sptl_intrp") == 0) s.sptl_intrp = int(v);
     else throw std::runtime_error("no such parameter");
   }
 };

@@ -90,8 +90,12 @@ def test_bogus_grid_size():
 
 def test_unsupported_option_rejected():
     from libmpdataxx_b200 import opts as o
-    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.div_2nd))
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.fot))
     assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    # the divergence form's own rules (formulae_mpdata_{1,2,3}d.hpp enable_ifs / static_asserts)
+    for bad in (o.div_3rd, o.div_2nd | o.div_3rd | o.div_3rd_dt, o.div_2nd | o.tot, o.div_2nd | o.dfl):
+        rc, _ = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=bad))
+        assert rc == _lib.MPDX_E_ARG, bad
     rc, _ = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.iga | o.abs))
     assert rc == _lib.MPDX_E_ARG
 
@@ -111,10 +115,13 @@ def test_option_and_parameter_validation():
     assert rc == _lib.MPDX_E_UNSUPPORTED and "nug" in msg
     rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), upwind_filter_freq=-1))
     assert rc == _lib.MPDX_E_ARG and "upwind_filter_freq" in msg
-    # unbuilt MPDATA variants are refused whatever else is set
-    for bad in (o.div_2nd, o.fot, o.div_3rd):
-        rc, msg = _create(_cfg(n_dims=3, grid=(8, 8, 8, ), opts=o.iga | bad))
-        assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    # the unbuilt MPDATA variant (fot) is refused whatever else is set
+    rc, msg = _create(_cfg(n_dims=3, grid=(8, 8, 8, ), opts=o.iga | o.fot))
+    assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    # the divergence form is built for solvers::mpdata (its advector is constant in time)
+    rc, msg = _create(_cfg(solver=_lib.SOLVER_BOUSSINESQ, n_dims=2, n_eqns=3, grid=(8, 8, 1), opts=o.div_2nd,
+                           dt=0.1, tht_ref=300.0))
+    assert rc == _lib.MPDX_E_UNSUPPORTED and "solvers::mpdata" in msg
 
 
 def test_async_transfer_arguments():

@@ -17,12 +17,13 @@ RTOL64 = 1e-12
 
 
 def make_run(grid, opts, n_iters=2, n_eqns=1, bcs=None, dtype=np.float64, path="general", max_abs_div_eps=None,
-             upwind_filter_freq=0):
+             upwind_filter_freq=0, sptl_intrp=0):
     nd = len(grid)
 
     class ct(solvers.ct_params_default_t):
         pass
 
+    ct.sptl_intrp = sptl_intrp
     ct.real_t = dtype
     ct.n_dims = nd
     ct.n_eqns = n_eqns
@@ -135,10 +136,12 @@ def test_general_path_fp64_matches_oracle(nd, grid, bc, opts, iters):
     _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10)
 
 
-def _check_parity(s, grid, bcs, opts, iters, eps, uff=0):
+def _check_parity(s, grid, bcs, opts, iters, eps, uff=0, sptl=0):
     orc = Oracle(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps, upwind_filter_freq=uff)
+    if sptl:
+        orc.set_param("sptl_intrp", sptl)
     load(orc, s)
-    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps, upwind_filter_freq=uff)
+    run = make_run(grid, opts, n_iters=iters, bcs=bcs, max_abs_div_eps=eps, upwind_filter_freq=uff, sptl_intrp=sptl)
     run.set_advectee(s["advectee"][0])
     for d, a in enumerate(s["advector"]):
         run.set_advector(a, d)
@@ -210,3 +213,35 @@ def test_stats_mass_conserved():
     assert abs(st["mass"] - m0) <= 1e-12 * abs(m0)
     psi = run.advectee()
     assert st["min"] == psi.min() and st["max"] == psi.max()
+
+
+# divergence-form MPDATA: div_2nd, div_3rd, div_3rd_dt (formulae_mpdata_{1,2,3}d.hpp,
+# formulae_mpdata_fdiv_{1,2,3}d.hpp), with the gauges, FCT, nug and the spatial helpers
+DIV_CASES = []
+for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
+    for bc in ("cyclic", "open", "rigid"):
+        for opts, iters, sptl in [(o.div_2nd, 2, 0), (o.div_2nd | o.div_3rd, 2, 0), (o.iga | o.div_2nd | o.div_3rd, 2, 1),
+                                  (o.abs | o.div_2nd | o.div_3rd, 2, 2), (o.div_2nd | o.div_3rd_dt, 2, 0),
+                                  (o.iga | o.fct | o.div_2nd | o.div_3rd_dt, 2, 0), (o.fct | o.div_2nd | o.div_3rd, 3, 1),
+                                  (o.nug | o.div_2nd | o.div_3rd, 2, 0), (o.nug | o.iga | o.div_2nd | o.div_3rd_dt, 2, 1)]:
+            DIV_CASES.append((nd, grid, bc, opts, iters, sptl))
+
+
+@pytest.mark.parametrize("nd,grid,bc,opts,iters,sptl", DIV_CASES)
+def test_div_fp64_matches_oracle(nd, grid, bc, opts, iters, sptl):
+    bcs = [bc] * (2 * nd)
+    s = random_setup(grid, bcs, seed=nd * 100 + iters + 11, signed=bool(opts & (o.abs | o.iga)))
+    if opts & o.nug:
+        rng = np.random.default_rng(nd + iters + 1)
+        G = rng.uniform(0.7, 1.3, grid)
+        if bc == "cyclic":
+            G = setups.wrap_periodic(G[tuple(slice(0, g - 1) for g in grid)])
+        s["G"] = G
+    _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10, sptl=sptl)
+
+
+def test_div_options_validated():
+    from libmpdataxx_b200 import _lib
+    for opts in (o.div_3rd, o.div_2nd | o.div_3rd | o.div_3rd_dt, o.div_2nd | o.tot):
+        with pytest.raises(_lib.MpdxError):
+            make_run((9, 9), opts)

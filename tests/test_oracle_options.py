@@ -155,3 +155,72 @@ def test_upwind_filter_every_step_is_upwind():
         r.advance(1)
     np.testing.assert_array_equal(uf.advectee(), ref.advectee())
     assert np.abs(mp.advectee() - ref.advectee()).max() > 1e-6      # timestep 1 is full MPDATA
+
+
+# ---- divergence-form MPDATA (div_2nd, div_3rd, div_3rd_dt) ----
+# No golden data of the reference pins these options on a plain MPDATA set-up
+# (its mp3 tests run them with var_dt and the nug geometry of the sphere).  The
+# restatement of formulae_mpdata_{1,2,3}d.hpp / formulae_mpdata_fdiv_{1,2,3}d.hpp
+# is checked against two properties instead:
+#  * for a uniform flow the divergence form of the second-order antidiffusive
+#    velocity is the standard one: in 1D for every gauge, and in 2D / 3D with
+#    iga (where nfdiv's transverse psi averages are the ndy / ndz numerators);
+#  * the third-order corrections reduce the error of a smooth translated field
+#    several times against second order (third-order accuracy in space and time).
+from libmpdataxx_b200 import setups  # noqa: E402
+
+D2, D3, DT = o.div_2nd, o.div_3rd, o.div_3rd_dt
+
+
+def _div_run(grid, opts, adv, psi, nt, sptl=None):
+    orc = Oracle(grid, opts, n_iters=2, bcs=["cyclic"] * (2 * len(grid)), max_abs_div_eps=1e-6)
+    if sptl is not None:
+        orc.set_param("sptl_intrp", sptl)
+    orc.set_advectee(psi)
+    for d, a in enumerate(adv):
+        orc.set_advector(a, d)
+    orc.advance(nt)
+    return orc.advectee()
+
+
+@pytest.mark.parametrize("grid,base", [((41,), 0), ((41,), o.iga), ((41,), o.abs), ((23, 19), o.iga),
+                                       ((13, 12, 11), o.iga), ((23, 19), o.iga | o.fct)])
+def test_div_2nd_equals_standard_form_for_uniform_flow(grid, base):
+    rng = np.random.default_rng(len(grid))
+    psi = setups.wrap_periodic(rng.uniform(0.5, 2.0, size=tuple(g - 1 for g in grid)))
+    adv = []
+    for d in range(len(grid)):
+        shp = list(grid)
+        if d > 0:
+            shp[0] += 1
+        adv.append(np.full(shp, [0.3, -0.2, 0.15][d]))
+    a = _div_run(grid, base, adv, psi, 3)
+    b = _div_run(grid, base | D2, adv, psi, 3)
+    np.testing.assert_allclose(b, a, rtol=0, atol=4e-15)
+
+
+def _smooth_translation(n=65, nt=64, c=(0.25, 0.125)):
+    P = n - 1
+    X, Y = np.meshgrid(np.arange(P), np.arange(P), indexing="ij")
+
+    def blob(sx, sy):
+        d2 = np.minimum(np.abs(X - sx), P - np.abs(X - sx)) ** 2 + np.minimum(np.abs(Y - sy), P - np.abs(Y - sy)) ** 2
+        return 1 + np.exp(-d2 / (2 * 6.0 ** 2))
+
+    psi = setups.wrap_periodic(blob(20, 20))
+    exact = setups.wrap_periodic(blob(20 + c[0] * nt, 20 + c[1] * nt))
+    adv = [np.full((n, n), c[0]), np.full((n + 1, n), c[1])]
+    return (n, n), adv, psi, exact, nt
+
+
+@pytest.mark.parametrize("base", [0, o.iga])
+def test_div_3rd_is_more_accurate_than_second_order(base):
+    grid, adv, psi, exact, nt = _smooth_translation()
+    err = lambda r: float(np.sqrt(((r - exact) ** 2).mean()))
+    e2 = err(_div_run(grid, base | D2, adv, psi, nt))
+    e3 = err(_div_run(grid, base | D2 | D3, adv, psi, nt))
+    edt = err(_div_run(grid, base | D2 | DT, adv, psi, nt))
+    assert e3 < 0.35 * e2 and edt < 0.2 * e2, (e2, e3, edt)
+    # the spatial helper (exact, aver2, aver4) multiplies ndxx_GC0, zero in a uniform flow
+    for sp in (1, 2):
+        assert err(_div_run(grid, base | D2 | D3, adv, psi, nt, sptl=sp)) == e3
