@@ -220,11 +220,14 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
  *
  * No counterpart in the reference (its cr / gcrk solvers use no
  * preconditioner).  FP64 pressure solves only (dtype 8, or prs_fp64).
- * mpdx_precond_record keeps the (initial residual, correction Phi_end -
- * Phi_start) pair of each of the next max_pairs pressure solves on the device;
- * mpdx_precond_train runs `steps` Adam steps of the network on randomly drawn
- * pairs (each normalised by its residual's max-norm) and returns the mean loss
- * of the last tenth; mpdx_precond_enable switches GCR to the flexible form whose
+ * mpdx_precond_record keeps (residual, correction Phi_end - Phi) pairs of the
+ * next pressure solves on the device (the start and iterations 16, 32, 64 of
+ * each, up to max_pairs); mpdx_precond_train runs `steps` Adam steps (linear
+ * warm-up, cosine decay to 1 % of lr) on the energy-norm loss of
+ * mpdx_precond_loss_grad over randomly drawn pairs, the last fifth of the pairs
+ * held out, and keeps the weights with the lowest held-out loss seen (never
+ * worse than the weights it started from); *final_loss is that held-out loss
+ * (1 = no correction).  mpdx_precond_enable switches GCR to the flexible form whose
  * search directions start from the network's output instead of the residual.
  * The stopping test (max|err| <= prs_tol / dt) is unchanged: only the
  * iteration count changes.  Weights are exchanged in the mpdx_pcnet layout. */
@@ -235,6 +238,13 @@ int64_t mpdx_precond_pairs(mpdx_handle h);
 int64_t mpdx_precond_num_params(mpdx_handle h);
 mpdx_status mpdx_precond_get_params(mpdx_handle h, float *host);
 mpdx_status mpdx_precond_set_params(mpdx_handle h, const float *host);
+/* The training loss for one pair given by the caller (no counterpart in the
+ * reference): residual r and correction t (interior, C order, FP64 on the host;
+ * A t = -r for the solve's operator A), network output q = net(r) scaled by c:
+ * *loss = e^T (-A) e / (t^T (-A) t) with e = c q - t (1 for a zero output), and
+ * its gradient with respect to the network parameters into grad (host,
+ * mpdx_precond_num_params floats; NULL for the loss alone). */
+mpdx_status mpdx_precond_loss_grad(mpdx_handle h, const double *r, const double *t, double c, double *loss, float *grad);
 
 /* ---- Learned GCR preconditioner network on its own ----
  *

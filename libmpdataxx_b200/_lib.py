@@ -34,7 +34,7 @@ EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_fie
            "mpdx_pcnet_get_params", "mpdx_pcnet_forward", "mpdx_pcnet_backward", "mpdx_pcnet_train_step",
            "mpdx_pcnet_last_error", "mpdx_pcnet_destroy", "mpdx_precond_record", "mpdx_precond_train",
            "mpdx_precond_enable", "mpdx_precond_pairs", "mpdx_precond_num_params", "mpdx_precond_get_params",
-           "mpdx_precond_set_params"]
+           "mpdx_precond_set_params", "mpdx_precond_loss_grad"]
 BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 
 
@@ -145,6 +145,9 @@ def lib():
     L.mpdx_precond_get_params.restype = ctypes.c_int
     L.mpdx_precond_set_params.argtypes = [vp, fp]
     L.mpdx_precond_set_params.restype = ctypes.c_int
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.mpdx_precond_loss_grad.argtypes = [vp, dp, dp, ctypes.c_double, dp, fp]
+    L.mpdx_precond_loss_grad.restype = ctypes.c_int
     _lib = L
     return L
 

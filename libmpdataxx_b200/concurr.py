@@ -224,6 +224,20 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_precond_get_params(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
 
+    def precond_loss_grad(self, r, t, c, grad=True):
+        """Energy-norm training loss of the learned preconditioner for one pair
+        (residual r, correction t with A t = -r, interior arrays) at output scale
+        c, and its gradient with respect to the network parameters."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        loss = ctypes.c_double()
+        g = np.zeros(self.L.mpdx_precond_num_params(self.h), dtype=np.float32) if grad else None
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self.L, self.h, self.L.mpdx_precond_loss_grad(
+            self.h, r.ctypes.data_as(dp), t.ctypes.data_as(dp), float(c), ctypes.byref(loss),
+            g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if grad else None))
+        return loss.value, g
+
     def set_precond_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
         _check(self.L, self.h, self.L.mpdx_precond_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))

@@ -870,8 +870,7 @@ __global__ void k_absmax(const float *x, long long n, float *s) {
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned *>(s), __float_as_uint(m));  // non-negative floats order as their bits
 }
-// training in the operator's norm: d = q - t; z = lap(d) with loss += sum z^2 / n and
-// dz = (2 / n) z (scale_out); then dq = lap(dz) (lap is symmetric up to the rigid-wall rows)
+// e = c q - t of the training loss
 __global__ void k_sub(const float *a, float ca, const float *b, long long n, float *o) {  // o = ca * a - b
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) o[q] = ca * a[q] - b[q];
 }
@@ -903,6 +902,49 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_lap_compact(geom g, const fl
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
     if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0) atomicAdd(loss, sq / double(g.cells));
   }
+}
+// Adjoint of lap() on compact arrays.  lap() is a sum of one-dimensional
+// operators, one per axis, each acting along the lines of its axis; with rigid
+// walls they are not symmetric.  adj_tab holds, per axis, the rows of the
+// transposed one-dimensional matrix (kAdjW column/value pairs per point, column
+// -1 for an unused slot), built on the host from the same halo and wall rules.
+constexpr int kAdjW = 8;
+struct adj_tab {
+  const int *col[3];
+  const float *val[3];
+};
+__global__ void __launch_bounds__(kRedThreads, 4) k_lap_adj_compact(geom g, adj_tab A, const float *x, float *out) {
+  const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+  for_interior(g, [&](int i, int j, int k) {
+    const int c[3] = {i, j, k};
+    const long long st[3] = {g.nd == 3 ? s0 : (long long)g.n[1], g.nd == 3 ? s1 : 1, 1};
+    const long long o = g.nd == 3 ? i * s0 + j * s1 + k : (long long)i * g.n[1] + j;
+    float acc = 0.f;
+    for (int d = 0; d < g.nd; ++d) {
+      const int *cl = A.col[d] + (long long)c[d] * kAdjW;
+      const float *vl = A.val[d] + (long long)c[d] * kAdjW;
+      const long long base = o - (long long)c[d] * st[d];
+#pragma unroll
+      for (int w = 0; w < kAdjW; ++w)
+        if (cl[w] >= 0) acc += vl[w] * x[base + (long long)cl[w] * st[d]];
+    }
+    out[o] = acc;
+  });
+}
+__global__ void k_neg2(const double *a, double *b) { *b = -*a; }
+__global__ void k_dot(const float *a, const float *b, long long n, double *out) {
+  double sq = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    sq += double(a[q]) * double(b[q]);
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, sq);
+}
+// gradient of the energy loss E = e^T (-A) e / den, den = *dn (-t^T A t), with
+// respect to q for e = c q - t: dq = -c (A e + A^T e) / den
+__global__ void k_energy_dq(const float *ae, const float *ate, long long n, const double *dn, float c, float *dq) {
+  const float f = *dn > 0.0 ? float(-double(c) / *dn) : 0.f;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dq[q] = f * (ae[q] + ate[q]);
 }
 __global__ void k_scale2(const float *r, const float *t, long long n, const float *s, float *ro, float *to) {
   const float inv = *s > 0.f ? 1.f / *s : 1.f;
@@ -1215,7 +1257,8 @@ boussinesq<T, P>::~boussinesq() {
   if (part) cudaFree(part);
   if (scratch) cudaFree(scratch);
   if (vip_dev) cudaFree(vip_dev);
-  for (float *p : {pairs, tr_r, tr_t, tr_q, tr_z, tr_dq}) if (p) cudaFree(p);
+  for (float *p : {pairs, tr_r, tr_t, tr_q, tr_z, tr_dq, tr_a, tr_b}) if (p) cudaFree(p);
+  for (int d = 0; d < 3; ++d) { if (adj_col[d]) cudaFree(adj_col[d]); if (adj_val[d]) cudaFree(adj_val[d]); }
   if (tr_loss) cudaFree(tr_loss);
   for (cudaEvent_t e : ev_solve) if (e) cudaEventDestroy(e);
 }
@@ -1361,6 +1404,106 @@ void boussinesq<T, P>::precond_record(long long n) {
   }
 }
 
+// The one-dimensional matrix of lap() along an axis of n points (pressure halo
+// rules: cyclic period n - 1, rigid 2 x(edge) - x(mirror); the gradient is zero at
+// a rigid wall point), built by applying the rule to unit vectors, transposed and
+// stored as kAdjW (column, value) pairs per row.
+static void lap1d_adj_rows(int n, bool rlo, bool rhi, double dx, std::vector<int> &col, std::vector<float> &val) {
+  auto src = [&](int q, int &a, int &b) {
+    a = q; b = -1;
+    if (q >= 0 && q < n) return;
+    if (q < 0) { if (rlo) { a = 0; b = -q; } else a = q + n - 1; }
+    else { if (rhi) { a = n - 1; b = 2 * (n - 1) - q; } else a = q - (n - 1); }
+  };
+  std::vector<double> M(size_t(n) * n, 0.0), e(n, 0.0);
+  auto aval = [&](int q) { int a, b; src(q, a, b); return b < 0 ? e[a] : 2 * e[a] - e[b]; };
+  auto lt = [&](int q) { if ((q == 0 && rlo) || (q == n - 1 && rhi)) return 0.0; return (aval(q + 1) - aval(q - 1)) / dx / 2; };
+  auto LT = [&](int q) { int a, b; src(q, a, b); return b < 0 ? lt(a) : 2 * lt(a) - lt(b); };
+  for (int j = 0; j < n; ++j) {
+    e.assign(n, 0.0);
+    e[j] = 1.0;
+    for (int i = 0; i < n; ++i) M[size_t(i) * n + j] = (LT(i + 1) - LT(i - 1)) / dx / 2;
+  }
+  col.assign(size_t(n) * bq::kAdjW, -1);
+  val.assign(size_t(n) * bq::kAdjW, 0.f);
+  for (int i = 0; i < n; ++i) {  // row i of M^T = column i of M
+    int w = 0;
+    for (int j = 0; j < n; ++j) {
+      const double v = M[size_t(j) * n + i];
+      if (v == 0.0) continue;
+      if (w == bq::kAdjW) throw error(MPDX_E_UNSUPPORTED, "pressure operator row wider than the adjoint table");
+      col[size_t(i) * bq::kAdjW + w] = j;
+      val[size_t(i) * bq::kAdjW + w] = float(v);
+      ++w;
+    }
+  }
+}
+
+template <class T, class P>
+void boussinesq<T, P>::ensure_training() {
+  const long long vox = st.cells();
+  if (!tr_r) {
+    for (float **b : {&tr_r, &tr_t, &tr_q, &tr_z, &tr_dq, &tr_a, &tr_b}) MPDX_CUDA(cudaMalloc(b, vox * sizeof(float)));
+    MPDX_CUDA(cudaMalloc(&tr_loss, 4 * sizeof(double)));
+  }
+  if (!adj_col[0]) {
+    for (int d = 0; d < st.nd; ++d) {
+      std::vector<int> c;
+      std::vector<float> v;
+      lap1d_adj_rows(st.n[d], st.bcs[d][0] == MPDX_BC_RIGID, st.bcs[d][1] == MPDX_BC_RIGID, dijk[d], c, v);
+      MPDX_CUDA(cudaMalloc(&adj_col[d], c.size() * sizeof(int)));
+      MPDX_CUDA(cudaMalloc(&adj_val[d], v.size() * sizeof(float)));
+      MPDX_CUDA(cudaMemcpy(adj_col[d], c.data(), c.size() * sizeof(int), cudaMemcpyHostToDevice));
+      MPDX_CUDA(cudaMemcpy(adj_val[d], v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  }
+}
+
+// Energy-norm loss of one pair (r, t) held in tr_r / tr_t: q = net(r), e = c q - t,
+// E = e^T (-A) e / (t^T (-A) t) (1 for a zero output); with grad, the parameter
+// gradient goes to net->grad.  Returns E (read back from the device).
+template <class T, class P>
+double boussinesq<T, P>::pair_energy(float c, bool grad) {
+  const auto gm = make_geom(st, dijk);
+  const unsigned G = red_grid(gm);
+  cudaStream_t s = st.stream;
+  const long long vox = st.cells();
+  net->forward_compact(tr_r, tr_q);
+  bq::k_sub<<<1184, 256, 0, s>>>(tr_q, c, tr_t, vox, tr_z);                 // e
+  bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_z, tr_dq, nullptr, 1.f);       // A e
+  bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_t, tr_a, nullptr, 1.f);        // A t
+  MPDX_CUDA(cudaMemsetAsync(tr_loss, 0, 2 * sizeof(double), s));
+  bq::k_dot<<<296, 256, 0, s>>>(tr_z, tr_dq, vox, tr_loss);                  // e^T A e
+  bq::k_dot<<<296, 256, 0, s>>>(tr_t, tr_a, vox, tr_loss + 1);               // t^T A t
+  if (grad) {
+    bq::adj_tab A;
+    for (int d = 0; d < 3; ++d) { A.col[d] = adj_col[d < st.nd ? d : 0]; A.val[d] = adj_val[d < st.nd ? d : 0]; }
+    bq::k_lap_adj_compact<<<G, kBlk, 0, s>>>(gm, A, tr_z, tr_b);             // A^T e
+    bq::k_neg2<<<1, 1, 0, s>>>(tr_loss + 1, tr_loss + 2);                    // -t^T A t
+    bq::k_energy_dq<<<1184, 256, 0, s>>>(tr_dq, tr_b, vox, tr_loss + 2, c, tr_a);
+    MPDX_LAUNCH_CHECK();
+    net->backward(tr_r, tr_a, net->grad);
+  }
+  MPDX_LAUNCH_CHECK();
+  double h[2];
+  MPDX_CUDA(cudaMemcpyAsync(h, tr_loss, sizeof(h), cudaMemcpyDeviceToHost, s));
+  MPDX_CUDA(cudaStreamSynchronize(s));
+  return h[1] < 0.0 ? h[0] / h[1] : 1.0;  // (-e^T A e) / (-t^T A t)
+}
+
+// pair k of the recorded ones, divided by rms(r), into tr_r / tr_t (the loss does not
+// depend on the common scale of a pair: the network is linear)
+template <class T, class P>
+void boussinesq<T, P>::load_pair(long long k) {
+  cudaStream_t s = st.stream;
+  const long long vox = st.cells();
+  const float *r = pairs + size_t(k) * 2 * vox, *d = r + vox;
+  MPDX_CUDA(cudaMemsetAsync(tr_loss + 3, 0, sizeof(double), s));
+  bq::k_sumsq<<<296, 256, 0, s>>>(r, vox, tr_loss + 3);
+  bq::k_scale_rms<<<1184, 256, 0, s>>>(r, d, vox, tr_loss + 3, tr_r, tr_t);
+  MPDX_LAUNCH_CHECK();
+}
+
 template <class T, class P>
 double boussinesq<T, P>::precond_train(long long steps, double lr, unsigned long long seed) {
   if constexpr (!std::is_same<P, double>::value) {
@@ -1369,13 +1512,8 @@ double boussinesq<T, P>::precond_train(long long steps, double lr, unsigned long
   } else {
     if (n_pairs < 1) throw error(MPDX_E_ARG, "no recorded pressure solves to train on (call precond_record first)");
     ensure_net();
+    ensure_training();
     const long long vox = st.cells();
-    if (!tr_r) {
-      for (float **b : {&tr_r, &tr_t, &tr_q, &tr_z, &tr_dq}) MPDX_CUDA(cudaMalloc(b, vox * sizeof(float)));
-      MPDX_CUDA(cudaMalloc(&tr_loss, 4 * sizeof(double)));
-    }
-    const auto gm = make_geom(st, dijk);
-    const unsigned G = red_grid(gm);
     cudaStream_t s = st.stream;
     // output scale: A^-1 amplifies the residual by orders of magnitude, so the
     // network learns q with c * q ~ correction, c = rms(correction) / rms(residual)
@@ -1395,34 +1533,58 @@ double boussinesq<T, P>::precond_train(long long steps, double lr, unsigned long
       out_scale = rr > 0 ? std::sqrt(dd / rr) : 1.0;
     }
     const float c = float(out_scale);
-    // loss: mean((A (c net(r) - t))^2) = mean((c A net(r) + r)^2) for a pair (r, t),
-    // A t = -r, each pair divided by rms(r): the relative squared residual left by c net(r)
+    // the last fifth of the pairs (at least one) is held out: the validation loss
+    // chooses the weights returned; training draws from the rest (all of them when
+    // only one pair was recorded)
+    const long long n_val = std::max(1LL, n_pairs / 5), n_tr = n_pairs > 1 ? n_pairs - n_val : 1;
+    auto validate = [&]() {
+      double sum = 0;
+      for (long long k = n_pairs - n_val; k < n_pairs; ++k) { load_pair(k); sum += pair_energy(c, false); }
+      return sum / double(n_val);
+    };
+    std::vector<float> best(size_t(net->n_params));
+    net->get_params(best.data());  // the starting weights (the zero-output layer at first)
+    double best_val = validate();
+    const long long every = std::max(1LL, steps / 20), warm = std::max(1LL, steps / 20);
     unsigned long long x = seed * 6364136223846793005ull + 1442695040888963407ull;
-    double tail = 0;
-    long long tail_n = 0;
     for (long long it = 0; it < steps; ++it) {
       x = x * 6364136223846793005ull + 1442695040888963407ull;
-      const long long k = (long long)((x >> 33) % (unsigned long long)n_pairs);
-      const float *r = pairs + size_t(k) * 2 * vox, *d = r + vox;
-      MPDX_CUDA(cudaMemsetAsync(tr_loss, 0, 2 * sizeof(double), s));
-      bq::k_sumsq<<<296, 256, 0, s>>>(r, vox, tr_loss);
-      bq::k_scale_rms<<<1184, 256, 0, s>>>(r, d, vox, tr_loss, tr_r, tr_t);
-      net->forward_compact(tr_r, tr_q);
-      bq::k_sub<<<1184, 256, 0, s>>>(tr_q, c, tr_t, vox, tr_z);
-      bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_z, tr_dq, tr_loss + 1, float(2.0 / double(vox)) * c);
-      bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_dq, tr_z, nullptr, 1.f);
-      MPDX_LAUNCH_CHECK();
-      net->backward(tr_r, tr_z, net->grad);
-      net->adam_step(float(lr));
-      if (it >= steps - std::max(1LL, steps / 10)) {
-        double l = 0;
-        MPDX_CUDA(cudaMemcpyAsync(&l, tr_loss + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
-        MPDX_CUDA(cudaStreamSynchronize(s));
-        tail += l;
-        ++tail_n;
+      load_pair((long long)((x >> 33) % (unsigned long long)n_tr));
+      pair_energy(c, true);
+      // linear warm-up, then cosine decay to 1 % of lr
+      const double ph = it < warm ? double(it + 1) / double(warm)
+                                  : 0.01 + 0.99 * 0.5 * (1.0 + std::cos(3.14159265358979 * double(it - warm) / double(std::max(1LL, steps - warm))));
+      net->adam_step(float(lr * ph));
+      if ((it + 1) % every == 0 || it + 1 == steps) {
+        const double v = validate();
+        if (v < best_val) { best_val = v; net->get_params(best.data()); }
       }
     }
-    return tail_n ? tail / double(tail_n) : 0.0;
+    net->set_params(best.data());
+    last_train_loss = best_val;
+    return best_val;
+  }
+}
+
+template <class T, class P>
+double boussinesq<T, P>::precond_loss_grad(const double *r, const double *t, double c, float *grad_host) {
+  if constexpr (!std::is_same<P, double>::value) {
+    (void)r; (void)t; (void)c; (void)grad_host;
+    throw error(MPDX_E_UNSUPPORTED, "the learned preconditioner needs the FP64 pressure solve (dtype 8, or prs_fp64)");
+  } else {
+    ensure_net();
+    ensure_training();
+    const long long vox = st.cells();
+    std::vector<float> hr(vox), ht(vox);
+    for (long long q = 0; q < vox; ++q) { hr[q] = float(r[q]); ht[q] = float(t[q]); }
+    MPDX_CUDA(cudaMemcpyAsync(tr_r, hr.data(), vox * sizeof(float), cudaMemcpyHostToDevice, st.stream));
+    MPDX_CUDA(cudaMemcpyAsync(tr_t, ht.data(), vox * sizeof(float), cudaMemcpyHostToDevice, st.stream));
+    const double E = pair_energy(float(c), grad_host != nullptr);
+    if (grad_host) {
+      MPDX_CUDA(cudaMemcpyAsync(grad_host, net->grad, net->n_params * sizeof(float), cudaMemcpyDeviceToHost, st.stream));
+      MPDX_CUDA(cudaStreamSynchronize(st.stream));
+    }
+    return E;
   }
 }
 

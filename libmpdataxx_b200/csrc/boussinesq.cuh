@@ -72,8 +72,11 @@ struct boussinesq {
   static constexpr int kSnaps = 3;  // recorded pairs per solve beyond the initial one (iterations 16, 32, 64)
   field<P> q_f, lq_f, snap[1 + kSnaps];
   float *pairs = nullptr, *tr_r = nullptr, *tr_t = nullptr, *tr_q = nullptr, *tr_z = nullptr, *tr_dq = nullptr;
-  double out_scale = 0;
+  float *tr_a = nullptr, *tr_b = nullptr;
+  double out_scale = 0, last_train_loss = -1;
   double *tr_loss = nullptr;
+  int *adj_col[3] = {nullptr, nullptr, nullptr};  // adjoint of the pressure operator, per axis
+  float *adj_val[3] = {nullptr, nullptr, nullptr};
   long long last_plain_iters = 250, fallbacks = 0;
   float last_plain_ms = 0;  // device time of the last plain solve (0: none yet)
   bool fell_back = false;
@@ -81,7 +84,12 @@ struct boussinesq {
   int pc_channels[4] = {8, 16, 32, 64};
 
   void precond_record(long long max_pairs);
+  // Adam on the energy-norm loss with a cosine learning-rate schedule; returns the
+  // held-out loss of the weights kept (the best seen, never worse than the start)
   double precond_train(long long steps, double lr, unsigned long long seed);
+  // energy-norm loss (and its parameter gradient, if grad_host) of one pair given by
+  // the caller (interior, C order), with output scale c
+  double precond_loss_grad(const double *r, const double *t, double c, float *grad_host);
   void precond_enable(bool on);
   void ensure_net();
 
@@ -98,6 +106,9 @@ struct boussinesq {
   void step();
   // pressure_solver_update up to the final gradient; simple: no normalize_vip in lap()
   void pressure_solve(bool simple);
+  void ensure_training();
+  double pair_energy(float c, bool grad);
+  void load_pair(long long k);
   bq::forcing<T> forcing();
   bq::geom norm_geom(bq::geom g) const;
 };

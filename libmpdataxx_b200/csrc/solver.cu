@@ -129,6 +129,9 @@ struct solver_base {
   virtual long long precond_pairs() { return 0; }
   virtual long long precond_num_params() { return 0; }
   virtual void precond_params(float *, const float *) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
+  virtual double precond_loss_grad(const double *, const double *, double, float *) {
+    throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver");
+  }
 };
 
 // common transfer machinery for solvers built on mpdata_state<T>
@@ -335,6 +338,9 @@ struct boussinesq_solver : solver_base {
   long long precond_num_params() override {
     b->ensure_net();
     return b->net->n_params;
+  }
+  double precond_loss_grad(const double *r, const double *t, double c, float *g) override {
+    return b->precond_loss_grad(r, t, c, g);
   }
   void precond_params(float *get, const float *set) override {
     b->ensure_net();
@@ -858,6 +864,13 @@ mpdx_status mpdx_precond_get_params(mpdx_handle h, float *host) {
   return guarded(h, [&] {
     if (!host) throw mpdx::error(MPDX_E_ARG, "null buffer");
     h->impl->precond_params(host, nullptr);
+  });
+}
+
+mpdx_status mpdx_precond_loss_grad(mpdx_handle h, const double *r, const double *t, double c, double *loss, float *grad) {
+  return guarded(h, [&] {
+    if (!r || !t || !loss) throw mpdx::error(MPDX_E_ARG, "null buffer");
+    *loss = h->impl->precond_loss_grad(r, t, c, grad);
   });
 }
 

@@ -190,3 +190,76 @@ def backward(dq, c, P, grid, wrap):
     de0 += pool_adj(dp1, sh[0])
     G["r"] = lin("e0", de0, c["r"])[0]
     return G
+
+
+# ---- the training loss, operator included ----
+# The pressure operator A = lap() of the GCR solve (mpdata_rhs_vip_prs_common.hpp:
+# 49-84, no normalisation): along every axis d, lap_tmp = grad (centred, 2 dx) with
+# the pressure halo rule (cyclic: period n - 1; rigid: 2 x(edge) - x(mirror)),
+# zero at a rigid wall point (set_edges), its own pressure halo rule, then the
+# centred divergence.  It is a sum of one-dimensional operators, each acting along
+# the lines of its axis; with rigid walls it is not symmetric, so its adjoint is
+# built from the transposed one-dimensional matrices.
+
+def _pres_src(q, n, rigid_lo, rigid_hi):
+    """(qa, qb): the point q takes x[qa] (qb < 0) or 2 x[qa] - x[qb]."""
+    if 0 <= q < n:
+        return q, -1
+    if q < 0:
+        return (0, -q) if rigid_lo else (q + n - 1, -1)
+    return (n - 1, 2 * (n - 1) - q) if rigid_hi else (q - (n - 1), -1)
+
+
+def lap1d_matrix(n, rigid_lo, rigid_hi, dx):
+    """Matrix of the one-dimensional part of lap() on a line of n points."""
+    M = np.zeros((n, n))
+
+    def aval(x, q):
+        a, b = _pres_src(q, n, rigid_lo, rigid_hi)
+        return x[a] if b < 0 else 2 * x[a] - x[b]
+
+    def lt(x, q):
+        if (q == 0 and rigid_lo) or (q == n - 1 and rigid_hi):
+            return 0.0
+        return (aval(x, q + 1) - aval(x, q - 1)) / dx / 2
+
+    def LT(x, q):
+        a, b = _pres_src(q, n, rigid_lo, rigid_hi)
+        return lt(x, a) if b < 0 else 2 * lt(x, a) - lt(x, b)
+
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        M[:, j] = [(LT(e, i + 1) - LT(e, i - 1)) / dx / 2 for i in range(n)]
+    return M
+
+
+def _apply_axes(x, mats):
+    out = np.zeros_like(x)
+    for ax, M in enumerate(mats):
+        out += np.moveaxis(np.tensordot(M, np.moveaxis(x, ax, 0), axes=(1, 0)), 0, ax)
+    return out
+
+
+def pressure_lap(x, bcs, dx):
+    """lap(x) of the pressure solve; bcs[d] = (rigid_lo, rigid_hi), dx[d] spacings."""
+    return _apply_axes(x, [lap1d_matrix(n, lo, hi, h) for n, (lo, hi), h in zip(x.shape, bcs, dx)])
+
+
+def pressure_lap_adj(x, bcs, dx):
+    """The adjoint (transpose) of pressure_lap."""
+    return _apply_axes(x, [lap1d_matrix(n, lo, hi, h).T for n, (lo, hi), h in zip(x.shape, bcs, dx)])
+
+
+def energy_loss(P, r, t, c, grid, wrap, bcs, dx, ch=(8, 16, 32, 64)):
+    """Training loss of the preconditioner for a pair (residual r, correction t,
+    A t = -r): the energy of the error e = c net(r) - t in the operator's norm
+    relative to that of t, E = e^T (-A) e / (t^T (-A) t); 1 for a zero output.
+    Returns (E, gradient dict of the parameters)."""
+    q, cache = forward(r, P, grid, wrap, ch)
+    e = c * q - t
+    Ae = pressure_lap(e, bcs, dx)
+    den = -float((t * pressure_lap(t, bcs, dx)).sum())
+    E = -float((e * Ae).sum()) / den
+    dq = -c * (Ae + pressure_lap_adj(e, bcs, dx)) / den
+    return E, backward(dq, cache, P, grid, wrap)

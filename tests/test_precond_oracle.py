@@ -51,3 +51,41 @@ def test_network_is_linear_and_shapes():
     assert q1.shape == grid
     assert np.allclose(q2, 3.0 * q1)  # zero biases at initialisation
     assert po.level_shapes(grid) == [(12, 9, 5), (6, 5, 3), (3, 3, 2), (2, 2, 1)]
+
+
+@pytest.mark.parametrize("grid,rigid", [((9, 7, 8), ((0, 0), (0, 0), (1, 1))), ((10, 9), ((0, 0), (1, 1)))])
+def test_training_loss_gradient_matches_finite_differences(grid, rigid):
+    """The whole training loss, the pressure operator with its rigid-wall rows
+    included: the energy-norm loss and its gradient (through the exact adjoint of
+    the operator) against central differences."""
+    nd = len(grid)
+    ch = (2, 3, 4, 5)
+    dx = (10.0, 10.0, 10.0)[:nd]
+    wrap3 = tuple(not r[0] for r in rigid) + (False,) * (3 - nd)
+    P = po.init_params(nd, ch, seed=3)
+    rng = np.random.default_rng(4)
+    r = rng.normal(size=grid)
+    t = rng.normal(size=grid)
+    c = 0.7
+    E, G = po.energy_loss(P, r, t, c, grid, wrap3, rigid, dx, ch)
+    eps = 1e-6
+    for name in ["W_e0", "W_m3", "W_d1", "W_q"]:
+        flat = P[name].reshape(-1)
+        for idx in rng.choice(flat.size, size=3, replace=False):
+            Pp = {k: v.copy() for k, v in P.items()}
+            Pm = {k: v.copy() for k, v in P.items()}
+            Pp[name].reshape(-1)[idx] += eps
+            Pm[name].reshape(-1)[idx] -= eps
+            fd = (po.energy_loss(Pp, r, t, c, grid, wrap3, rigid, dx, ch)[0]
+                  - po.energy_loss(Pm, r, t, c, grid, wrap3, rigid, dx, ch)[0]) / (2 * eps)
+            assert abs(fd - G[name].reshape(-1)[idx]) <= 1e-6 * max(1.0, abs(fd)), (name, idx, fd, G[name].reshape(-1)[idx])
+
+
+def test_pressure_operator_rigid_rows_are_not_symmetric():
+    """With a rigid wall the one-dimensional operator differs from its transpose
+    in the rows next to the wall (the reason the training gradient needs the adjoint)."""
+    M = po.lap1d_matrix(12, True, True, 1.0)
+    assert not np.allclose(M, M.T)
+    assert np.allclose(M[4:-4, 4:-4], M.T[4:-4, 4:-4])
+    C = po.lap1d_matrix(12, False, False, 1.0)
+    assert np.allclose((C @ np.ones(12)), 0.0)  # constants are in the kernel on a cyclic line
