@@ -225,7 +225,7 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
  * each, up to max_pairs); mpdx_precond_train runs `steps` Adam steps (linear
  * warm-up, cosine decay to 1 % of lr) on the energy-norm loss of
  * mpdx_precond_loss_grad over randomly drawn pairs, the last fifth of the pairs
- * held out, and keeps the weights with the lowest held-out loss seen (never
+ * (at most 8) held out, and keeps the weights with the lowest held-out loss seen (never
  * worse than the weights it started from); *final_loss is that held-out loss
  * (1 = no correction).  mpdx_precond_enable switches GCR to the flexible form whose
  * search directions start from the network's output instead of the residual.

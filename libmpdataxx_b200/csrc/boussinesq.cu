@@ -1536,7 +1536,7 @@ double boussinesq<T, P>::precond_train(long long steps, double lr, unsigned long
     // the last fifth of the pairs (at least one) is held out: the validation loss
     // chooses the weights returned; training draws from the rest (all of them when
     // only one pair was recorded)
-    const long long n_val = std::max(1LL, n_pairs / 5), n_tr = n_pairs > 1 ? n_pairs - n_val : 1;
+    const long long n_val = std::min(8LL, std::max(1LL, n_pairs / 5)), n_tr = n_pairs > 1 ? n_pairs - n_val : 1;
     auto validate = [&]() {
       double sum = 0;
       for (long long k = n_pairs - n_val; k < n_pairs; ++k) { load_pair(k); sum += pair_energy(c, false); }
