@@ -131,7 +131,11 @@ mpdx_status mpdx_create(const mpdx_config *cfg, mpdx_handle *out);
 mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, const int64_t *strides);
 mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const int64_t *strides);
 
-/* Same with device pointers (C order), for callers that keep data on the GPU. */
+/* Same with device pointers (C order), for callers that keep data on the GPU.
+ * The copy is ordered after all work already issued to the legacy default
+ * stream (where a producer that uses no streams of its own writes the buffer);
+ * a buffer written on any other stream must be complete (synchronised by the
+ * caller) before the call.  Both calls return after the copy. */
 mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev);
 mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev);
 

@@ -704,9 +704,20 @@ mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const i
   });
 }
 
+// the handle's stream waits for the work issued so far to the legacy default stream
+static void after_legacy_stream(cudaStream_t s) {
+  cudaEvent_t e;
+  MPDX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  MPDX_CUDA(cudaEventRecord(e, cudaStreamLegacy));
+  const cudaError_t w = cudaStreamWaitEvent(s, e, 0);
+  cudaEventDestroy(e);
+  MPDX_CUDA(w);
+}
+
 mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *dev) {
   return guarded(h, [&] {
     if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    after_legacy_stream(h->impl->stream);
     h->impl->xfer_async->join(h->impl->stream);
     h->impl->set_field(kind, idx, dev, true);
   });
@@ -715,6 +726,7 @@ mpdx_status mpdx_set_field_device(mpdx_handle h, int kind, int idx, const void *
 mpdx_status mpdx_get_field_device(mpdx_handle h, int kind, int idx, void *dev) {
   return guarded(h, [&] {
     if (!dev) throw mpdx::error(MPDX_E_ARG, "null device buffer");
+    after_legacy_stream(h->impl->stream);  // the buffer may still be in use there
     h->impl->xfer_async->join(h->impl->stream);
     h->impl->get_field(kind, idx, dev, true);
   });

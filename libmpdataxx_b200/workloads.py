@@ -85,6 +85,8 @@ def advection_3d(n=512, seed_flow=3, seed_blobs=4, cmax=0.4, n_modes=8, dtype="f
     psi = psi.to(dt)
     full = torch.arange(n, device=device) % P
     psi = psi[full][:, full][:, :, full].contiguous()
+    if device != "cpu":
+        torch.cuda.synchronize()  # the fields are complete when handed to another stream
     return {"grid": (n, n, n), "advectee": [psi], "advector": [gx, gy, gz],
             "desc": f"3D {n}^3 cyclic, fct|iga, n_iters=2, {dtype}; curl flow max|C|={cmax} (seed {seed_flow}), "
                     f"5 Gaussian blobs (seed {seed_blobs})"}
@@ -122,5 +124,8 @@ def rotation_2d(n=1024, dtype="float64", device="cuda"):
     I, J = torch.meshgrid(i % P, i % P, indexing="ij")
     d = torch.sqrt((I - x0) ** 2 + (J - y0) ** 2)
     psi = torch.clamp(4 * (1 - d / r), min=0)
-    return {"grid": (n, n), "advectee": [psi.to(dt).contiguous()], "advector": [gx.to(dt), gy.to(dt)],
+    out = [psi.to(dt).contiguous(), gx.to(dt), gy.to(dt)]
+    if device != "cpu":
+        torch.cuda.synchronize()
+    return {"grid": (n, n), "advectee": [out[0]], "advector": out[1:],
             "desc": f"2D {n}^2 cyclic rotation, cone r=0.15 nx h=4, {dtype}"}
