@@ -411,6 +411,112 @@ struct op_donorcell {
   }
 };
 
+// ---------------------------------------------------------------------------
+// One-dimensional problems in one block: every step of an advance() call in a
+// single launch, the fields held in shared memory, the same per-point functors
+// (so the same arithmetic, bit for bit) in the order the multi-kernel path
+// launches them, __syncthreads() where that path has a kernel boundary.  For
+// cyclic 1D problems without FCT, dfl and nug (the 1D box of a few thousand
+// points runs launch-bound otherwise).
+template <class T>
+struct blk1d_args {
+  T *psi[2];    // global time levels (element 0 of each), halo H on both sides
+  const T *gc;  // advector component 0 (element 0), valid over [-H, n-2+H]
+  int n, H, n_iters, tl, uff;
+  unsigned o;
+  long long t0, nt;
+};
+template <class T>
+__global__ void __launch_bounds__(1024, 1) k_block1d(blk1d_args<T> A) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  const int n = A.n, H = A.H, L = n + 2 * H + 2, base = H + 1;  // array index 0 sits at slot base
+  T *sm = reinterpret_cast<T *>(raw);
+  auto arr = [&](int k) { return dfield<T>{sm + (long long)k * L + base, 1, 0, 0}; };
+  dfield<T> P[2] = {arr(0), arr(1)}, GC = arr(2), T0 = arr(3), T1 = arr(4), FL = arr(5);
+  const int tid = threadIdx.x, nt_ = blockDim.x;
+  for (int i = -H + tid; i <= n - 1 + H; i += nt_) {
+    P[0](i, 0, 0) = A.psi[0][i];
+    P[1](i, 0, 0) = A.psi[1][i];
+  }
+  for (int i = -H + tid; i <= n - 2 + H; i += nt_) GC(i, 0, 0) = A.gc[i];
+  __syncthreads();
+  int tl = A.tl;
+  auto fill = [&](const dfield<T> &p) {  // cyclic halo: [-H, -1] <- [n-1-H, n-2], [n, n+H-1] <- [1, H]
+    for (int q = tid; q < 2 * H; q += nt_) {
+      if (q < H) p(-H + q, 0, 0) = p(n - 1 - H + q, 0, 0);
+      else p(n + q - H, 0, 0) = p(1 + q - H, 0, 0);
+    }
+  };
+  const dfield<T> none{};
+  for (long long s = 0; s < A.nt; ++s) {
+    fill(P[tl]);  // solve_loop_body: xchng(e)
+    __syncthreads();
+    for (int iter = 0; iter < A.n_iters; ++iter) {
+      const dfield<T> corr = iter % 2 ? T0 : T1, unco = iter == 1 ? GC : (iter % 2 ? T1 : T0);
+      if (iter != 0) {
+        tl ^= 1;
+        fill(P[tl]);
+        __syncthreads();
+        const op_antidiff<1, 0, T> ad{corr, P[tl], unco, unco, unco, A.o, none};
+        for (int a = -1 + tid; a <= n - 1; a += nt_) ad(a, 0, 0);
+        __syncthreads();
+      }
+      const dfield<T> git = iter == 0 ? GC : corr;
+      dfield<T> flx = git;
+      if (!(A.o & o_iga) || iter == 0) {
+        const op_flux<1, 0, T> fx{FL, P[tl], git, A.o};
+        for (int a = -1 + tid; a <= n - 1; a += nt_) fx(a, 0, 0);
+        flx = FL;
+        __syncthreads();
+      }
+      const op_donorcell<1, T> dc{P[tl ^ 1], P[tl], flx, flx, flx, A.o, none};
+      for (int i = tid; i <= n - 1; i += nt_) dc(i, 0, 0);
+      __syncthreads();
+      if (A.uff > 0 && (A.t0 + s) % A.uff == 0) break;  // upwind-only step (mpdata_osc_1d.hpp)
+    }
+    tl ^= 1;  // cycle(e)
+  }
+  for (int i = -H + tid; i <= n - 1 + H; i += nt_) {
+    A.psi[0][i] = P[0](i, 0, 0);
+    A.psi[1][i] = P[1](i, 0, 0);
+  }
+}
+
+template <class T>
+bool general<T>::block1d_ok() const {
+  const auto &S = *s;
+  if (S.nd != 1 || S.n_eqns != 1) return false;
+  if (S.bcs[0][0] != MPDX_BC_CYCLIC || S.bcs[0][1] != MPDX_BC_CYCLIC) return false;
+  if (S.opts & (o_fct | o_dfl | o_nug | o_div_2nd | o_div_3rd | o_div_3rd_dt)) return false;
+  const size_t bytes = size_t(6) * (S.n[0] + 2 * S.H + 2) * sizeof(T);
+  return S.n[0] >= 2 * S.H + 1 && bytes <= size_t(200) * 1024;
+}
+
+template <class T>
+void general<T>::block1d(long long nt) {
+  auto &S = *s;
+  const size_t bytes = size_t(6) * (S.n[0] + 2 * S.H + 2) * sizeof(T);
+  static bool attr = false;
+  if (!attr) {
+    MPDX_CUDA(cudaFuncSetAttribute(k_block1d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(200 * 1024)));
+    attr = true;
+  }
+  const long long kChunk = 1 << 16;  // steps per launch
+  for (long long s0 = 0; s0 < nt; s0 += kChunk) {
+    blk1d_args<T> a;
+    a.psi[0] = &S.psi[0][0].v(0, 0, 0);
+    a.psi[1] = &S.psi[0][1].v(0, 0, 0);
+    a.gc = &S.GC[0].v(0, 0, 0);
+    a.n = S.n[0]; a.H = S.H; a.n_iters = S.n_iters; a.tl = S.tl[0]; a.uff = S.upwind_filter_freq;
+    a.o = S.opts;
+    a.t0 = S.timestep + s0;
+    a.nt = std::min(kChunk, nt - s0);
+    k_block1d<T><<<1, 1024, bytes, S.stream>>>(a);
+    MPDX_LAUNCH_CHECK();
+    if (a.nt & 1) S.tl[0] ^= 1;
+  }
+}
+
 // fct_init (mpdata_fct_{1,2,3}d.hpp:31-55)
 template <int ND, class T>
 struct op_fct_init {

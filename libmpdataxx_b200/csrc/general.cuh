@@ -19,6 +19,10 @@ struct general {
   void init_g();
   // one time step of every equation (solver_common.hpp:127-136, 321-331)
   void step();
+  // nt steps of a small cyclic 1D problem (one equation; no fct, dfl, nug or
+  // divergence form) in one launch of one block, with step()'s arithmetic
+  bool block1d_ok() const;
+  void block1d(long long nt);
 
   // halo exchanges (solver_{1,2,3}d.hpp)
   void xchng_sclr(field<T> &A, int ex, bool deriv = false);

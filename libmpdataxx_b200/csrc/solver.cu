@@ -249,6 +249,12 @@ struct mpdata_solver : solver_base {
   void advance(long long nt) override {
     if (nt <= 0) return;
     if (st.timestep == 0) gen.ante_loop(scratch);
+    if (path != MPDX_PATH_GENERAL && gen.block1d_ok()) {
+      gen.block1d(nt);
+      st.timestep += nt;
+      last_path = MPDX_PATH_FUSED;
+      return;
+    }
     bool use_fused = false;
     if (path != MPDX_PATH_GENERAL && fus.configurable(st)) {
       use_fused = fus.seams_consistent(st, scratch);

@@ -245,3 +245,32 @@ def test_div_options_validated():
     for opts in (o.div_3rd, o.div_2nd | o.div_3rd | o.div_3rd_dt, o.div_2nd | o.tot):
         with pytest.raises(_lib.MpdxError):
             make_run((9, 9), opts)
+
+
+@pytest.mark.parametrize("opts,iters,uff", [(0, 2, 0), (o.iga, 2, 0), (0, 3, 0), (o.abs, 2, 0), (o.tot, 2, 0),
+                                            (o.iga | o.tot, 3, 0), (o.npa | o.pfc, 2, 0), (o.khn, 2, 0), (0, 2, 3)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_block1d_equals_general_path(opts, iters, uff, dtype):
+    """Cyclic 1D problems advance in one launch of one block (all steps of an
+    advance() call, fields in shared memory) with the per-point arithmetic of the
+    multi-kernel path: equal to it bit for bit, and to the oracle in FP64."""
+    grid = (2000,)
+    s = setups.box_1d()
+    s["advectee"][0] = s["advectee"][0].astype(dtype)
+    runs = {}
+    for path in ("general", "auto"):
+        r = make_run(grid, opts, n_iters=iters, dtype=dtype, path=path, upwind_filter_freq=uff)
+        r.set_advectee(s["advectee"][0])
+        r.set_advector(s["advector"][0].astype(dtype), 0)
+        runs[path] = r
+    for chunk in (13, 7):
+        for r in runs.values():
+            r.advance(chunk)
+        np.testing.assert_array_equal(runs["auto"].advectee(), runs["general"].advectee())
+    from libmpdataxx_b200 import _lib
+    assert runs["auto"].stats()["path"] == _lib.PATH_FUSED and runs["general"].stats()["path"] == _lib.PATH_GENERAL
+    if dtype == np.float64:
+        orc = Oracle(grid, opts, n_iters=iters, bcs=["cyclic"] * 2, upwind_filter_freq=uff)
+        load(orc, s)
+        orc.advance(20)
+        assert rel_err(runs["auto"].advectee(), orc.advectee()) <= RTOL64
