@@ -593,6 +593,12 @@ void validate(const mpdx_config &c) {
     if (o & (o_tot | o_dfl)) throw error(MPDX_E_ARG, "div_2nd & div_3rd options are incompatible with tot and dfl");
     if (c.solver == MPDX_SOLVER_BOUSSINESQ)
       throw error(MPDX_E_UNSUPPORTED, "the divergence-form options are built for solvers::mpdata (constant advector) only");
+    // a third pass reads its base velocity GC_unco(2) = GC_corr(1) (mpdata_common.hpp:40-60) at halo
+    // faces that no exchange of the second pass fills (mpdata_osc_2d.hpp:112-121 fills only the
+    // normal halos over the interior; the fdiv and ndx terms reach two faces along and the corners),
+    // so the reference's result there depends on uninitialised memory
+    if (c.n_iters > 2)
+      throw error(MPDX_E_UNSUPPORTED, "the divergence-form options are built for n_iters <= 2 (a third pass reads halo faces the reference never fills)");
   }
   if (c.sptl_intrp < 0 || c.sptl_intrp > 2) throw error(MPDX_E_ARG, "sptl_intrp must be exact (0), aver2 (1) or aver4 (2)");
   if ((o & o_nug) && c.solver == MPDX_SOLVER_BOUSSINESQ)

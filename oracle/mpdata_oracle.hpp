@@ -156,6 +156,10 @@ struct mpdata {
   void setup(int nd_, const int *n_, int n_eqns_, unsigned opts_, int n_iters_, const int *bcs_) {
     nd = nd_; n_eqns = n_eqns_; opts = opts_; n_iters = n_iters_;
     if (n_iters < 1) throw std::runtime_error("n_iters must be positive");
+    // divergence form with a third pass: its antidiffusive velocities read faces of GC_corr(1)
+    // that no exchange fills (mpdata_osc_2d.hpp:112-121), so the reference's result is not defined
+    if ((opts & (o_div_2nd | o_div_3rd | o_div_3rd_dt)) && n_iters > 2)
+      throw std::runtime_error("oracle: divergence-form options need n_iters <= 2");
     for (int d = 0; d < 3; ++d) n[d] = d < nd ? n_[d] : 1;
     for (int d = 0; d < nd; ++d) if (n[d] < 1) throw std::runtime_error("libmpdata++: bogus grid size");
     for (int d = 0; d < nd; ++d) for (int s = 0; s < 2; ++s) bcs[d][s] = bcs_[2 * d + s];

@@ -122,6 +122,9 @@ def test_option_and_parameter_validation():
     rc, msg = _create(_cfg(solver=_lib.SOLVER_BOUSSINESQ, n_dims=2, n_eqns=3, grid=(8, 8, 1), opts=o.div_2nd,
                            dt=0.1, tht_ref=300.0))
     assert rc == _lib.MPDX_E_UNSUPPORTED and "solvers::mpdata" in msg
+    # ... and for at most two passes (a third reads halo faces the reference never fills)
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.div_2nd | o.div_3rd, n_iters=3))
+    assert rc == _lib.MPDX_E_UNSUPPORTED and "n_iters" in msg
 
 
 def test_async_transfer_arguments():

@@ -222,7 +222,7 @@ for nd, grid in [(1, (37,)), (2, (19, 23)), (3, (13, 13, 13))]:
     for bc in ("cyclic", "open", "rigid"):
         for opts, iters, sptl in [(o.div_2nd, 2, 0), (o.div_2nd | o.div_3rd, 2, 0), (o.iga | o.div_2nd | o.div_3rd, 2, 1),
                                   (o.abs | o.div_2nd | o.div_3rd, 2, 2), (o.div_2nd | o.div_3rd_dt, 2, 0),
-                                  (o.iga | o.fct | o.div_2nd | o.div_3rd_dt, 2, 0), (o.fct | o.div_2nd | o.div_3rd, 3, 1),
+                                  (o.iga | o.fct | o.div_2nd | o.div_3rd_dt, 2, 0), (o.fct | o.div_2nd | o.div_3rd, 2, 1),
                                   (o.nug | o.div_2nd | o.div_3rd, 2, 0), (o.nug | o.iga | o.div_2nd | o.div_3rd_dt, 2, 1)]:
             DIV_CASES.append((nd, grid, bc, opts, iters, sptl))
 
@@ -245,6 +245,11 @@ def test_div_options_validated():
     for opts in (o.div_3rd, o.div_2nd | o.div_3rd | o.div_3rd_dt, o.div_2nd | o.tot):
         with pytest.raises(_lib.MpdxError):
             make_run((9, 9), opts)
+    # a third pass would read halo faces of the second pass's velocities that the reference
+    # never fills (its result there depends on uninitialised memory)
+    for opts in (o.div_2nd, o.fct | o.div_2nd | o.div_3rd):
+        with pytest.raises(_lib.MpdxError):
+            make_run((9, 9), opts, n_iters=3)
 
 
 @pytest.mark.parametrize("opts,iters,uff", [(0, 2, 0), (o.iga, 2, 0), (0, 3, 0), (o.abs, 2, 0), (o.tot, 2, 0),

@@ -224,3 +224,12 @@ def test_div_3rd_is_more_accurate_than_second_order(base):
     # the spatial helper (exact, aver2, aver4) multiplies ndxx_GC0, zero in a uniform flow
     for sp in (1, 2):
         assert err(_div_run(grid, base | D2 | D3, adv, psi, nt, sptl=sp)) == e3
+
+
+def test_div_third_pass_refused():
+    """With n_iters = 3 the third pass of the divergence form reads faces of the second
+    pass's velocities GC_corr(1) that no exchange fills (mpdata_osc_2d.hpp:112-121), so
+    the reference's result would depend on uninitialised memory: the oracle refuses."""
+    for opts in (D2, D2 | D3, o.fct | D2 | DT):
+        with pytest.raises(RuntimeError, match="n_iters"):
+            Oracle((9, 9), opts, n_iters=3, bcs=["cyclic"] * 4)
