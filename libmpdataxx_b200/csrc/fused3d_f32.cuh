@@ -19,7 +19,15 @@
 //     and the factors 1/4 * 1/4 * 1/2 are folded into one constant;
 //   * arithmetic on aligned quads uses the paired FP32 instructions of sm_100
 //     (two lanes per instruction: add/sub/mul/fma.rn.f32x2); expressions with a
-//     k-shifted operand stay elementwise.
+//     k-shifted operand stay elementwise;
+//   * the march is unrolled by the period (4) of its rings of shared planes,
+//     so every plane slot is a compile-time offset of one of three per-thread
+//     shared addresses (own quad, row above, row below) and the carried
+//     x-history is renamed rather than moved; C~ of the y-face and the betas
+//     of the previous plane are read back from shared memory instead of being
+//     carried, which keeps the kernel within the 128 registers that 512
+//     threads per SM allow;
+//   * the FCT quotients use the approximate-reciprocal division (qdiv).
 //
 // The result equals the reference's formulae up to FP32 rounding (the order of
 // additions differs from formulae_mpdata_3d.hpp:254-295); the properties that
@@ -36,7 +44,6 @@ namespace mpdx {
 namespace f3s {
 
 using Q = qd::q4<float>;
-using f3::canvas;
 
 // ---- paired (aligned) arithmetic: two FP32 lanes per instruction ----
 __device__ __forceinline__ float2 m2(float a, float b) { return make_float2(a, b); }
@@ -66,6 +73,20 @@ __device__ __forceinline__ Q ssub(const Q &x, const Q &y) {
 // C * (C > 0 ? l : r)  (donorcell_formulae.hpp:25-34; one product is zero)
 __device__ __forceinline__ Q flux(const Q &l, const Q &r, const Q &C) { return pmul(C, qd::sel_pos(C, l, r)); }
 
+// the FCT quotients (hi - psi) / (sum + eps): the approximate-reciprocal quotient
+// of __fdividef (within 2 ulp for these denominators, which lie in
+// [FLT_EPSILON, 2^126)); MPDX_F3S_IEEE_DIV=1 selects the correctly rounded one
+#ifndef MPDX_F3S_IEEE_DIV
+#define MPDX_F3S_IEEE_DIV 0
+#endif
+__device__ __forceinline__ Q qdiv(const Q &a, const Q &b) {
+#if MPDX_F3S_IEEE_DIV
+  return a / b;
+#else
+  return qd::mk(__fdividef(a.a.x, b.a.x), __fdividef(a.a.y, b.a.y), __fdividef(a.b.x, b.b.x), __fdividef(a.b.y, b.b.y));
+#endif
+}
+
 // antidiffusive velocity through one face from the two-point sums:
 //   |C|/2 (1 - |C|) nx - C (S1 D1 + S2 D2) / 32
 // (formulae_mpdata_3d.hpp:254-295 with G = 1 and iga: ndx = nx, the transverse
@@ -77,19 +98,72 @@ __device__ __forceinline__ Q adiff(const Q &C, const Q &nx, const Q &S1, const Q
   return pfma(pmuls(C, -1.f / 32.f), v, pmul(h, nx));
 }
 
+// shared planes of the single-precision kernel, in units of N elements.  Every
+// ring of planes along x has 4 slots (the 2-slot rings divide 4), so that with
+// the march unrolled by 4 every slot is a compile-time constant: plane x lives
+// in slot (x - ts) & 3 of its ring, ts being the first step of the CTA.
+//   S0: psi^n planes t-1, t, t+1, t+2; with FCT the prefetch of plane t+3
+//       into the slot of t-1 is issued once the limiter has read t-1 (each
+//       thread reads and refills only its own quad of that slot);
+//   G0: GC_x planes t-1, t, t+1, prefetch t+2;  G1, G2: t, t+1, prefetch t+2;
+//   S1: psi1 planes t-1, t, t+1;  CY, BU, BD: planes t-1, t
+template <int CR>
+struct canvas_s {
+  static constexpr int CC = 64, N = CR * CC, TY = CR - 6, TZ = 56, NT = CR * 16;
+  static constexpr int S0 = 0, G0 = 4, G1 = 8, G2 = 12, S1 = 16, CY = 20, BU = 22, BD = 24, total = 26;
+};
+
+template <int V> struct phase { static constexpr int value = V; };
+
+// shared-memory access at a 32-bit shared address plus a compile-time byte
+// offset (the plane slot), so that each access is one instruction with an
+// immediate offset and no per-slot address is kept in a register
+template <int OFF>
+__device__ __forceinline__ Q ldq(unsigned a) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a), "n"(OFF));
+  return qd::mk(v.x, v.y, v.z, v.w);
+}
+template <int OFF>
+__device__ __forceinline__ void stq(unsigned a, const Q &v) {
+  asm volatile("st.shared.v4.f32 [%0+%1], {%2, %3, %4, %5};" ::"r"(a), "n"(OFF), "f"(v.a.x), "f"(v.a.y), "f"(v.b.x), "f"(v.b.y)
+               : "memory");
+}
+// asynchronous copy of the own quad of one plane row: row points at column kb;
+// where the quad crosses the period, column kb + e is read at kb + e + m_e P2,
+// the four multiples packed as the bytes m_e + 1 of `wk`
+template <int OFF>
+__device__ __forceinline__ void cpq(unsigned a, const float *row, bool contig, unsigned wk, int P2) {
+  if (contig) {
+    asm volatile("cp.async.cg.shared.global [%0+%1], [%2], 16;\n" ::"r"(a), "n"(OFF), "l"(row) : "memory");
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int m = int((wk >> (8 * e)) & 0xffu) - 1;
+      const float *g = row + e + m * P2;
+      if (e == 0) asm volatile("cp.async.ca.shared.global [%0+%1], [%2], 4;\n" ::"r"(a), "n"(OFF), "l"(g) : "memory");
+      if (e == 1) asm volatile("cp.async.ca.shared.global [%0+%1], [%2], 4;\n" ::"r"(a), "n"(OFF + 4), "l"(g) : "memory");
+      if (e == 2) asm volatile("cp.async.ca.shared.global [%0+%1], [%2], 4;\n" ::"r"(a), "n"(OFF + 8), "l"(g) : "memory");
+      if (e == 3) asm volatile("cp.async.ca.shared.global [%0+%1], [%2], 4;\n" ::"r"(a), "n"(OFF + 12), "l"(g) : "memory");
+    }
+  }
+}
+
 template <bool FCT, int CR>
 __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> A) {
-  using C = canvas<CR>;
+  using C = canvas_s<CR>;
   constexpr int N = C::N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float *sm = reinterpret_cast<float *>(smem_raw);
+  float *const sm = reinterpret_cast<float *>(smem_raw);
 
   const int tid = threadIdx.x, lane = tid & 31;
   const int r = 2 * (tid >> 5) + (lane >> 4);   // canvas row
   const int q = lane & 15;                      // quad within the row
   const int me = r * C::CC + 4 * q;             // canvas offset of the own quad
-  auto R = [&](int d) { const int rr = r + d; return rr >= 0 && rr < CR ? me + d * C::CC : me; };
-  const int up = R(1), dn = R(-1);
+  const int up = r + 1 < CR ? me + C::CC : me, dn = r > 0 ? me - C::CC : me;
+  // shared addresses of the own quad and of the quads of the rows above / below
+  const unsigned s_base = unsigned(__cvta_generic_to_shared(sm));
+  const unsigned a_me = s_base + 4u * me, a_up = s_base + 4u * up, a_dn = s_base + 4u * dn;
 
   const int tile = blockIdx.x;
   const int j0 = (tile / A.tiles_z) * C::TY, k0 = (tile % A.tiles_z) * C::TZ;
@@ -101,155 +175,167 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
   int kc[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) kc[e] = f3::pmod(kb + e, A.P2);
-  const long long ro_in = (long long)jg * A.in.s1, ro_g0 = (long long)jg * A.g0.s1;
-  const long long ro_g1 = (long long)jg * A.g1.s1, ro_g2 = (long long)jg * A.g2.s1;
-
-  auto plane = [&](int base, int nslots, int x) { return sm + (base + ((x % nslots) + nslots) % nslots) * N; };
-  auto cp = [&](float *dst, const dfield<float> &f, long long ro, int x) {
-    f3::gcopy(dst + me, f, f3::pmod(x, A.P0), ro, kb, contig, kc);
+  // a quad crossing the period: column kb + e is kc[e] = kb + e + m_e P2 with
+  // -1 <= m_e <= 64 / P2 (the canvas spans 64 columns from k0 - 4 >= -4),
+  // packed as bytes m_e + 1
+  unsigned wk = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) wk |= unsigned((kc[e] - (kb + e)) / A.P2 + 1) << (8 * e);
+  // row offsets of the four inputs in elements (plane offsets are added per
+  // step; a row offset is below 2^31 for any field that fits in HBM)
+  const int o_in = jg * int(A.in.s1) + kb, o_g0 = jg * int(A.g0.s1) + kb;
+  const int o_g1 = jg * int(A.g1.s1) + kb, o_g2 = jg * int(A.g2.s1) + kb;
+  const int ts = x0 - 3;
+  auto slot = [&](int base, int x) { return sm + (base + ((x - ts) & 3)) * N + me; };
+  auto cp = [&](float *dst, const dfield<float> &f, int x) {
+    f3::gcopy_row(dst, f.o + (long long)f3::pmod(x, A.P0) * f.s0 + (long long)jg * f.s1, kb, contig, kc);
   };
 
   for (int p = tid; p < C::total * N; p += C::NT) sm[p] = 0.f;
   __syncthreads();
 
-  const int ts = x0 - 3;
-  for (int x = ts - 1; x <= ts + 2; ++x) cp(plane(C::S0, C::NS0, x), A.in, ro_in, x);
-  for (int x = ts - 1; x <= ts + 1; ++x) cp(plane(C::G0, C::NG0, x), A.g0, ro_g0, x);
-  for (int x = ts; x <= ts + 1; ++x) { cp(plane(C::G1, C::NG1, x), A.g1, ro_g1, x); cp(plane(C::G2, C::NG1, x), A.g2, ro_g2, x); }
+  for (int x = ts - 1; x <= ts + 2; ++x) cp(slot(C::S0, x), A.in, x);
+  for (int x = ts - 1; x <= ts + 1; ++x) cp(slot(C::G0, x), A.g0, x);
+  for (int x = ts; x <= ts + 1; ++x) { cp(slot(C::G1, x), A.g1, x); cp(slot(C::G2, x), A.g2, x); }
   f3::cp_commit();
-
+  f3::cp_wait_all();
+  __syncthreads();
   const Q zero = qd::bc<float>(0.f);
   // carried along the march (own quad): psi1 at t-1, t; the upwind x-flux
-  // through face t+1/2; the k-difference of psi1 at t and the k-sum of GC_z at
-  // t; the antidiffusive / limited quantities of plane t-1
-  Q p_m = zero, p_c = zero, fxa = zero, dzc = zero, szc = zero;
-  Q cx_m = zero, cy_m = zero, cz_m = zero, bu_m = zero, bd_m = zero, fx_prev = zero;
-  auto slot0 = [](int x, int n) { return ((x % n) + n) % n; };
-  f3::ring<C::NS0> r_s0{slot0(ts - 1, C::NS0)};
-  f3::ring<C::NG0> r_g0{slot0(ts - 1, C::NG0)};
-  f3::ring<C::NG1> r_g1{slot0(ts, C::NG1)};
-  f3::ring<3> r_s1{slot0(ts - 1, 3)};
-  f3::ring<2> r_2{slot0(ts - 1, 2)};
+  // through face t+1/2; the k-difference of psi1 at t and the k-sum of GC_z
+  // at t; C~ of the x- and z-faces of plane t-1 and the limited x-flux into it
+  // (C~ of its y-face and its betas are read back from shared memory)
+  Q p_m = zero, p_c = zero, fxa = flux(qd::lds(slot(C::S0, ts)), qd::lds(slot(C::S0, ts + 1)), qd::lds(slot(C::G0, ts)));
+  Q dzc = zero, szc = zero;
+  Q cx_m = zero, cz_m = zero, fx_prev = zero;
+  // plane indices (modulo the period) of the next prefetches
+  int xi = f3::pmod(ts + 3, A.P0), xg = f3::pmod(ts + 2, A.P0);
+  const int jrow = j0 - 3 + r;
+  const bool out_row = r >= 3 && r < CR - 3 && jrow < A.P1 && q >= 1 && q < 15;
 
-  f3::plane_walker<float> w_in, w_g0, w_g1, w_g2;
-  w_in.init(A.in, ts + 3, A.P0, ro_in);
-  w_g0.init(A.g0, ts + 2, A.P0, ro_g0);
-  w_g1.init(A.g1, ts + 2, A.P0, ro_g1);
-  w_g2.init(A.g2, ts + 2, A.P0, ro_g2);
-  for (int t = ts; t <= x1; ++t) {
+  auto step = [&](int t, auto ph) {
+    constexpr int PH = decltype(ph)::value;   // (t - ts) & 3
+    constexpr int M = (PH + 3) & 3, T0 = PH, T1 = (PH + 1) & 3, T2 = (PH + 2) & 3, T3 = (PH + 3) & 3;
+    constexpr int C2 = PH & 1, M2 = (PH + 1) & 1;
+    // byte offsets of the plane slots
+    constexpr int S0m = (C::S0 + M) * N * 4, S0c = (C::S0 + T0) * N * 4, S0p = (C::S0 + T1) * N * 4;
+    constexpr int S0pp = (C::S0 + T2) * N * 4, S0n = (C::S0 + T3) * N * 4;
+    constexpr int G0m = (C::G0 + M) * N * 4, G0c = (C::G0 + T0) * N * 4, G0p = (C::G0 + T1) * N * 4;
+    constexpr int G0n = (C::G0 + T2) * N * 4;
+    constexpr int G1c = (C::G1 + T0) * N * 4, G1p = (C::G1 + T1) * N * 4, G1n = (C::G1 + T2) * N * 4;
+    constexpr int G2c = (C::G2 + T0) * N * 4, G2p = (C::G2 + T1) * N * 4, G2n = (C::G2 + T2) * N * 4;
+    constexpr int S1m = (C::S1 + M) * N * 4, S1c = (C::S1 + T0) * N * 4, S1p = (C::S1 + T1) * N * 4;
+    constexpr int CYc = (C::CY + C2) * N * 4, BUc = (C::BU + C2) * N * 4, BDc = (C::BD + C2) * N * 4;
+    constexpr int CYm = (C::CY + M2) * N * 4, BUm = (C::BU + M2) * N * 4, BDm = (C::BD + M2) * N * 4;
     f3::cp_wait_all();
     __syncthreads();
-    float *const s0b = sm + C::S0 * N, *const g0b = sm + C::G0 * N, *const g1b = sm + C::G1 * N, *const g2b = sm + C::G2 * N;
-    f3::gcopy_row(s0b + r_s0.at(4) * N + me, w_in.p, kb, contig, kc);
-    f3::gcopy_row(g0b + r_g0.at(3) * N + me, w_g0.p, kb, contig, kc);
-    f3::gcopy_row(g1b + r_g1.at(2) * N + me, w_g1.p, kb, contig, kc);
-    f3::gcopy_row(g2b + r_g1.at(2) * N + me, w_g2.p, kb, contig, kc);
+    // prefetch: the advector planes t+2 and (without FCT) psi^n plane t+3
+    if (!FCT) cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
+    cpq<G0n>(a_me, A.g0.o + ((long long)xg * A.g0.s0 + o_g0), contig, wk, A.P2);
+    cpq<G1n>(a_me, A.g1.o + ((long long)xg * A.g1.s0 + o_g1), contig, wk, A.P2);
+    cpq<G2n>(a_me, A.g2.o + ((long long)xg * A.g2.s0 + o_g2), contig, wk, A.P2);
     f3::cp_commit();
-    w_in.next(); w_g0.next(); w_g1.next(); w_g2.next();
-    const float *S0m = s0b + r_s0.at(0) * N, *S0c = s0b + r_s0.at(1) * N, *S0p = s0b + r_s0.at(2) * N;
-    const float *S0pp = s0b + r_s0.at(3) * N;
-    const float *G0m = g0b + r_g0.at(0) * N, *G0c = g0b + r_g0.at(1) * N, *G0p = g0b + r_g0.at(2) * N;
-    const float *G1c = g1b + r_g1.at(0) * N, *G1p = g1b + r_g1.at(1) * N;
-    const float *G2c = g2b + r_g1.at(0) * N, *G2p = g2b + r_g1.at(1) * N;
-    float *const s1b = sm + C::S1 * N;
-    const float *S1m = s1b + r_s1.at(0) * N, *S1c = s1b + r_s1.at(1) * N;
-    float *S1p = s1b + r_s1.at(2) * N;
-    const int sc = r_2.at(1) * N, sm1 = r_2.at(0) * N;
-    float *CYc = sm + C::CY * N + sc, *BUc = sm + C::BU * N + sc, *BDc = sm + C::BD * N + sc;
-    const float *CYm = sm + C::CY * N + sm1, *BUm = sm + C::BU * N + sm1, *BDm = sm + C::BD * N + sm1;
-    r_s0.next(); r_g0.next(); r_g1.next(); r_s1.next(); r_2.next();
+    xg = xg + 1 == A.P0 ? 0 : xg + 1;
 
     // ---- A: psi1 at plane t+1 (mpdata_osc_3d.hpp:181-197) ----
-    const Q c = qd::lds(S0p + me);
-    const Q g1p = qd::lds(G1p + me), g1p_dn = qd::lds(G1p + dn), g2p = qd::lds(G2p + me);
-    // the x-flux through face t+1/2 comes from the previous step, except on the first
-    if (t == ts) fxa = flux(qd::lds(S0c + me), c, qd::lds(G0c + me));
-    const Q fxb = flux(c, qd::lds(S0pp + me), qd::lds(G0p + me));   // face t+3/2
-    const Q fyp = flux(c, qd::lds(S0p + up), g1p);
-    const Q fym = flux(qd::lds(S0p + dn), c, g1p_dn);
+    const Q c = ldq<S0p>(a_me);
+    const Q g1p = ldq<G1p>(a_me), g1p_dn = ldq<G1p>(a_dn), g2p = ldq<G2p>(a_me);
+    const Q fxb = flux(c, ldq<S0pp>(a_me), ldq<G0p>(a_me));   // face t+3/2
+    const Q fyp = flux(c, ldq<S0p>(a_up), g1p);
+    const Q fym = flux(ldq<S0p>(a_dn), c, g1p_dn);
     const Q fzp = flux(c, qd::kp1(c), g2p);
     const Q p_p = psub(c, padd(padd(psub(fxb, fxa), psub(fyp, fym)), ssub(fzp, qd::km1(fzp))));
     fxa = fxb;
-    qd::sts(S1p + me, p_p);
+    stq<S1p>(a_me, p_p);
     __syncthreads();
-    const Q pp_up = qd::lds(S1p + up), pp_dn = qd::lds(S1p + dn);
+    const Q pp_up = ldq<S1p>(a_up), pp_dn = ldq<S1p>(a_dn);
 
     // ---- B: C~ on the own x-face t+1/2, y-face j+1/2 and z-face k+1/2 of plane t ----
-    const Q pc_up = qd::lds(S1c + up), pc_dn = qd::lds(S1c + dn);
-    const Q g0c = qd::lds(G0c + me), g0m = qd::lds(G0m + me);
-    const Q g1c = qd::lds(G1c + me), g1c_dn = qd::lds(G1c + dn);
-    const Q g2c = qd::lds(G2c + me);
-    // two-point terms
-    const Q dxo = psub(p_p, p_m);                                 // psi1 x+1 - x-1, own row
-    const Q dyc = psub(pc_up, pc_dn);                             // psi1 j+1 - j-1 at t
-    const Q dyp = psub(pp_up, pp_dn);                             // the same at t+1
-    const Q kp_p = qd::kp1(p_p), km_p = qd::km1(p_p);
-    const Q dzp = ssub(kp_p, km_p);                               // psi1 k+1 - k-1 at t+1
-    const Q sxc = padd(g0c, g0m);                                 // GC_x faces t+-1/2
-    const Q syc = padd(g1c, g1c_dn), syp = padd(g1p, g1p_dn);     // GC_y faces j+-1/2
-    const Q szp = sadd(g2p, qd::km1(g2p));                        // GC_z faces k+-1/2 at t+1
-    Q cx_c, cy_c, cz_c;
-    // x-face t+1/2: transverse y (psi and GC_y), z (psi and GC_z)
-    cx_c = adiff(g0c, psub(p_p, p_c), padd(syp, syc), padd(dyp, dyc), padd(szp, szc), padd(dzp, dzc));
-    // y-face j+1/2 of plane t: transverse z, x
+    // (computed on every canvas row, as are the limiter and the output below:
+    // leaving the rows that do not need them to idle warps measured slower,
+    // through the registers the extra control flow holds)
+    Q kp_c, dzp, szp, cx_c, cy_c, cz_c;
+    const Q pc_up = ldq<S1c>(a_up), pc_dn = ldq<S1c>(a_dn);
     {
-      const Q g2c_up = qd::lds(G2c + up);
-      const Q dz_up = ssub(qd::kp1(pc_up), qd::km1(pc_up));
-      const Q sz_up = sadd(g2c_up, qd::km1(g2c_up));
-      const Q dx_up = psub(pp_up, qd::lds(S1m + up));
-      const Q sx_up = padd(qd::lds(G0c + up), qd::lds(G0m + up));
-      cy_c = adiff(g1c, psub(pc_up, p_c), padd(sz_up, szc), padd(dz_up, dzc), padd(sx_up, sxc), padd(dx_up, dxo));
-      qd::sts(CYc + me, cy_c);
+      const Q g0c = ldq<G0c>(a_me), g0m = ldq<G0m>(a_me);
+      const Q g1c = ldq<G1c>(a_me), g1c_dn = ldq<G1c>(a_dn);
+      const Q g2c = ldq<G2c>(a_me);
+      // two-point terms
+      const Q dxo = psub(p_p, p_m);                                 // psi1 x+1 - x-1, own row
+      const Q dyc = psub(pc_up, pc_dn);                             // psi1 j+1 - j-1 at t
+      const Q dyp = psub(pp_up, pp_dn);                             // the same at t+1
+      dzp = ssub(qd::kp1(p_p), qd::km1(p_p));                       // psi1 k+1 - k-1 at t+1
+      const Q sxc = padd(g0c, g0m);                                 // GC_x faces t+-1/2
+      const Q syc = padd(g1c, g1c_dn), syp = padd(g1p, g1p_dn);     // GC_y faces j+-1/2
+      szp = sadd(g2p, qd::km1(g2p));                                // GC_z faces k+-1/2 at t+1
+      // x-face t+1/2: transverse y (psi and GC_y), z (psi and GC_z)
+      cx_c = adiff(g0c, psub(p_p, p_c), padd(syp, syc), padd(dyp, dyc), padd(szp, szc), padd(dzp, dzc));
+      // y-face j+1/2 of plane t: transverse z, x
+      {
+        const Q g2c_up = ldq<G2c>(a_up);
+        const Q dz_up = ssub(qd::kp1(pc_up), qd::km1(pc_up));
+        const Q sz_up = sadd(g2c_up, qd::km1(g2c_up));
+        const Q dx_up = psub(pp_up, ldq<S1m>(a_up));
+        const Q sx_up = padd(ldq<G0c>(a_up), ldq<G0m>(a_up));
+        cy_c = adiff(g1c, psub(pc_up, p_c), padd(sz_up, szc), padd(dz_up, dzc), padd(sx_up, sxc), padd(dx_up, dxo));
+        stq<CYc>(a_me, cy_c);
+      }
+      // z-face k+1/2 of plane t: transverse x, y
+      kp_c = qd::kp1(p_c);
+      cz_c = adiff(g2c, ssub(kp_c, p_c), sadd(qd::kp1(sxc), sxc), sadd(qd::kp1(dxo), dxo), sadd(qd::kp1(syc), syc),
+                   sadd(qd::kp1(dyc), dyc));
     }
-    // z-face k+1/2 of plane t: transverse x, y
-    const Q kp_c = qd::kp1(p_c);
-    cz_c = adiff(g2c, ssub(kp_c, p_c), sadd(qd::kp1(sxc), sxc), sadd(qd::kp1(dxo), dxo), sadd(qd::kp1(syc), syc),
-                 sadd(qd::kp1(dyc), dyc));
 
     // ---- C: betas at plane t (formulae_mpdata_fct_3d.hpp:48-143) ----
     Q bu_c = zero, bd_c = zero;
     if (FCT) {
       __syncthreads();
-      const Q cy_dn = qd::lds(CYc + dn);
-      Q mnq, mxq;
       {
-        const Q s0c = qd::lds(S0c + me), s0p = qd::lds(S0p + me), s0m = qd::lds(S0m + me);
-        const Q yp = qd::lds(S0c + up), ym = qd::lds(S0c + dn), zp = qd::kp1(s0c), zm = qd::km1(s0c);
-        mnq = qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(s0c, s0p), s0m), yp), ym), zp), zm);
-        mxq = qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(s0c, s0p), s0m), yp), ym), zp), zm);
+        const Q cy_dn = ldq<CYc>(a_dn);
+        Q mnq, mxq;
+        {
+          const Q s0_c = ldq<S0c>(a_me), s0_m = ldq<S0m>(a_me);
+          const Q yp = ldq<S0c>(a_up), ym = ldq<S0c>(a_dn), zp = qd::kp1(s0_c), zm = qd::km1(s0_c);
+          mnq = qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(qd::qmin(s0_c, c), s0_m), yp), ym), zp), zm);
+          mxq = qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(qd::qmax(s0_c, c), s0_m), yp), ym), zp), zm);
+        }
+        const Q xp = p_p, xm = p_m, yp = pc_up, ym = pc_dn, zp = kp_c, zm = qd::km1(p_c);
+        const Q fxm = cx_m, fxp = cx_c, fym = cy_dn, fyp = cy_c, fzm = qd::km1(cz_c), fzp = cz_c;
+        const Q hi = qd::qmax(mxq, qd::qmax(p_c, qd::qmax(xp, qd::qmax(xm, qd::qmax(yp, qd::qmax(ym, qd::qmax(zp, zm)))))));
+        const Q lo = qd::qmin(mnq, qd::qmin(yp, qd::qmin(xm, qd::qmin(p_c, qd::qmin(xp, qd::qmin(zp, qd::qmin(zm, ym)))))));
+        const Q du = padd(padd(psub(qd::pos(fxm), qd::neg(fxp)), psub(qd::pos(fym), qd::neg(fyp))),
+                          psub(qd::pos(fzm), qd::neg(fzp)));
+        const Q dd = padd(padd(psub(qd::pos(fxp), qd::neg(fxm)), psub(qd::pos(fyp), qd::neg(fym))),
+                          psub(qd::pos(fzp), qd::neg(fzm)));
+        const Q e = qd::bc<float>(FLT_EPSILON);
+        bu_c = qdiv(psub(hi, p_c), padd(du, e));
+        bd_c = qdiv(psub(p_c, lo), padd(dd, e));
+        stq<BUc>(a_me, bu_c);
+        stq<BDc>(a_me, bd_c);
       }
-      const Q xp = p_p, xm = p_m, yp = pc_up, ym = pc_dn, zp = kp_c, zm = qd::km1(p_c);
-      const Q fxm = cx_m, fxp = cx_c, fym = cy_dn, fyp = cy_c, fzm = qd::km1(cz_c), fzp = cz_c;
-      const Q hi = qd::qmax(mxq, qd::qmax(p_c, qd::qmax(xp, qd::qmax(xm, qd::qmax(yp, qd::qmax(ym, qd::qmax(zp, zm)))))));
-      const Q lo = qd::qmin(mnq, qd::qmin(yp, qd::qmin(xm, qd::qmin(p_c, qd::qmin(xp, qd::qmin(zp, qd::qmin(zm, ym)))))));
-      const Q du = padd(padd(psub(qd::pos(fxm), qd::neg(fxp)), psub(qd::pos(fym), qd::neg(fyp))),
-                        psub(qd::pos(fzm), qd::neg(fzp)));
-      const Q dd = padd(padd(psub(qd::pos(fxp), qd::neg(fxm)), psub(qd::pos(fyp), qd::neg(fym))),
-                        psub(qd::pos(fzp), qd::neg(fzm)));
-      const Q e = qd::bc<float>(FLT_EPSILON);
-      bu_c = psub(hi, p_c) / padd(du, e);
-      bd_c = psub(p_c, lo) / padd(dd, e);
-      qd::sts(BUc + me, bu_c);
-      qd::sts(BDc + me, bd_c);
+      // psi^n plane t+3 into the slot of t-1, now read
+      cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
+      f3::cp_commit();
     }
+    xi = xi + 1 == A.P0 ? 0 : xi + 1;
 
-    // ---- D: limited fluxes at plane t-1 (formulae_mpdata_fct_3d.hpp:148-250) ----
-    Q fxx = cx_m, fyu = cy_m, fyd = qd::lds(CYm + dn), fzz = cz_m;
-    if (FCT) {
-      const Q bu_dn = qd::lds(BUm + dn), bd_dn = qd::lds(BDm + dn);
-      fxx = pmul(fxx, qd::qlim(fxx, bd_m, bu_c, bu_m, bd_c));
-      fyu = pmul(fyu, qd::qlim(fyu, bd_m, qd::lds(BUm + up), bu_m, qd::lds(BDm + up)));
-      fyd = pmul(fyd, qd::qlim(fyd, bd_dn, bu_m, bu_dn, bd_m));
-      fzz = pmul(fzz, qd::qlim(fzz, bd_m, qd::kp1(bu_m), bu_m, qd::kp1(bd_m)));
-    }
-
-    // ---- E: psi^{n+1} at plane t-1 ----
     {
+      // ---- D: limited fluxes at plane t-1 (formulae_mpdata_fct_3d.hpp:148-250) ----
+      Q fxx = cx_m, fyu = ldq<CYm>(a_me), fyd = ldq<CYm>(a_dn), fzz = cz_m;
+      if (FCT) {
+        const Q bu_m = ldq<BUm>(a_me), bd_m = ldq<BDm>(a_me);
+        const Q bu_dn = ldq<BUm>(a_dn), bd_dn = ldq<BDm>(a_dn);
+        fxx = pmul(fxx, qd::qlim(fxx, bd_m, bu_c, bu_m, bd_c));
+        fyu = pmul(fyu, qd::qlim(fyu, bd_m, ldq<BUm>(a_up), bu_m, ldq<BDm>(a_up)));
+        fyd = pmul(fyd, qd::qlim(fyd, bd_dn, bu_m, bu_dn, bd_m));
+        fzz = pmul(fzz, qd::qlim(fzz, bd_m, qd::kp1(bu_m), bu_m, qd::kp1(bd_m)));
+      }
+
+      // ---- E: psi^{n+1} at plane t-1 ----
       const int x = t - 1;
       const Q v = psub(p_m, padd(padd(psub(fxx, fx_prev), psub(fyu, fyd)), ssub(fzz, qd::km1(fzz))));
       fx_prev = fxx;
-      const int jrow = j0 - 3 + r;
-      if (x >= x0 && x < x1 && r >= 3 && r < CR - 3 && jrow < A.P1 && q >= 1 && q < 15) {
+      if (out_row && x >= x0 && x < x1) {
         float *o = A.out.o + (long long)x * A.out.s0 + (long long)jrow * A.out.s1;
         if (contig) {
           qd::sts(o + kb, v);
@@ -282,8 +368,17 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
     // shift the x-history
     p_m = p_c; p_c = p_p;
     dzc = dzp; szc = szp;
-    cx_m = cx_c; cy_m = cy_c; cz_m = cz_c;
-    bu_m = bu_c; bd_m = bd_c;
+    cx_m = cx_c; cz_m = cz_c;
+  };
+
+  // steps ts .. x1 (the last chunk rounds up to a whole unrolled group: the
+  // extra steps read wrapped planes and store nothing)
+  const int nsteps = (x1 - ts + 1 + 3) & ~3;
+  for (int u = 0; u < nsteps; u += 4) {
+    step(ts + u, phase<0>{});
+    step(ts + u + 1, phase<1>{});
+    step(ts + u + 2, phase<2>{});
+    step(ts + u + 3, phase<3>{});
   }
   f3::cp_wait_all();
 }

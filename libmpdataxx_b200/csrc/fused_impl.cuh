@@ -58,7 +58,7 @@ static void launch3(const f3::args<T> &a, cudaStream_t s, dim3 grid) {
 template <bool FCT>
 static void launch3s(const f3::args<float> &a, cudaStream_t s, dim3 grid) {
   constexpr int CR = tiles<float>::CR;
-  using C = f3::canvas<CR>;
+  using C = f3s::canvas_s<CR>;
   auto kern = f3s::k_fused3d_s<FCT, CR>;
   const size_t bytes = size_t(C::total) * C::N * sizeof(float);
   static bool attr = false;
