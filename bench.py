@@ -555,10 +555,13 @@ def main():
         line["cpu_baseline"] = cpu_baseline(host, args.size)
         del host
     if world == 1 and not args.no_extras:
-        line["box_1d"] = box_1d_extra()
-        line["rotation_2d"] = rotation_extra()
-        line["batched_2d"] = batched_extra()
-        line["gcr"] = gcr_extra()
+        # a failing extra measurement is reported in its own key; the headline stands
+        for name, fn in (("box_1d", box_1d_extra), ("rotation_2d", rotation_extra),
+                         ("batched_2d", batched_extra), ("gcr", gcr_extra)):
+            try:
+                line[name] = fn()
+            except Exception as e:  # noqa: BLE001
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     run.close()
     dist_done(world)

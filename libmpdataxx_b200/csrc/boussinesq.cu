@@ -332,8 +332,11 @@ __device__ __forceinline__ double ddv(dd a) { return a.s + a.c; }
 
 template <class T>
 __global__ void k_gcr_reset(gcr_dev<T> *dv) {
-  dv->converged = 0; dv->done = 0; dv->stuck = 0; dv->cur = 0; dv->iters = 0; dv->arrive = 0u;
+  dv->converged = 0; dv->done = 0; dv->stuck = 0; dv->cur = 0; dv->iters = 0; dv->arrive = 0u; dv->bad = 0;
 }
+// the learned directions are given up: plain GCR continues from the current iterate
+template <class T>
+__global__ void k_gcr_clear_bad(gcr_dev<T> *dv) { dv->bad = 0; }
 
 // err = lap(Phi) with err_init (u = the velocity being projected)
 template <class P, class T>
@@ -741,9 +744,16 @@ template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_tol, dfield<T> phi, dfield<T> err,
                                                                   dirs<T> D, gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
-  if (dv->done) return;
+  if (dv->done || dv->bad) return;
   const T den = dv->pend_den;
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;
+  // a direction from the network whose sums are not finite (an overflowing or NaN
+  // output) must not touch Phi or err: every block sees the same sums and returns,
+  // and the host continues with plain GCR from the iterate as it stands
+  if (!isfinite(double(den)) || !isfinite(double(b))) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) dv->bad = 1;
+    return;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) { dv->tmp_den[v] = den; dv->beta = b; }
   const dfield<T> pv = D.p[v], lpv = D.lp[v];
   dd acc[1] = {{0.0, 0.0}};
@@ -767,7 +777,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_
 template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_lapq(geom g, dfield<T> q, dfield<T> lq, dirs<T> D, gcr_dev<T> *dv,
                                                              double *part) {
-  if (dv->done) return;
+  if (dv->done || dv->bad) return;
   dfield<T> lps[NV];
 #pragma unroll
   for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
@@ -795,7 +805,7 @@ template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction_pc(geom g, int kk, dfield<T> err, dfield<T> q, dfield<T> lq,
                                                                      dirs<T> D, gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
-  if (dv->done) return;
+  if (dv->done || dv->bad) return;
   T a[NV];
   dfield<T> ps[NV], lps[NV];
 #pragma unroll
@@ -1267,6 +1277,7 @@ boussinesq<T, P>::~boussinesq() {
 // gradient, which the callers fuse into their own kernels
 template <class T, class P>
 void boussinesq<T, P>::pressure_solve(bool simple) {
+  const trace_range tr(use_net && net ? "gcr_solve_learned" : "gcr_solve");
   const auto gm = simple ? make_geom(st, dijk) : norm_geom(make_geom(st, dijk));
   const unsigned G = red_grid(gm);
   cudaStream_t s = st.stream;
@@ -1343,11 +1354,13 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
     }
     float elapsed = 0;
     if (pcnd && last_plain_ms > 0) MPDX_CUDA(cudaEventElapsedTime(&elapsed, ev_solve[0], ev_solve[1]));
-    if (pcnd && (hdev->iters > std::max(20LL, 2 * last_plain_iters) || (last_plain_ms > 0 && elapsed > last_plain_ms))) {
-      // the learned directions are not converging, or the solve has already
-      // taken as long as a whole plain solve (so it can no longer be faster):
-      // continue from the current iterate with plain GCR (directions restart
-      // from the residual)
+    if (pcnd && (hdev->bad || hdev->iters > std::max(20LL, 2 * last_plain_iters) ||
+                 (last_plain_ms > 0 && elapsed > last_plain_ms))) {
+      // a learned direction was not finite, the learned directions are not
+      // converging, or the solve has already taken as long as a whole plain
+      // solve (so it can no longer be faster): continue from the current iterate
+      // with plain GCR (directions restart from the residual)
+      bq::k_gcr_clear_bad<P><<<1, 1, 0, s>>>(dev);
       bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
       MPDX_LAUNCH_CHECK();
       pcnd = false;

@@ -32,6 +32,7 @@ struct gcr_dev {
   T mean;                // ini_pressure: mean of Phi
   double residual;       // max|err| at the last convergence check
   int converged, done, stuck, cur;
+  int bad;               // a learned direction gave non-finite sums: nothing was updated with it
   long long iters;
   unsigned int arrive;   // last-block ticket of the running reduction
 };

@@ -513,7 +513,15 @@ void general<T>::block1d(long long nt) {
     a.nt = std::min(kChunk, nt - s0);
     k_block1d<T><<<1, 1024, bytes, S.stream>>>(a);
     MPDX_LAUNCH_CHECK();
-    if (a.nt & 1) S.tl[0] ^= 1;
+    // every pass of a step flips the time level once (the cycle before each
+    // corrective pass and the one ending the step): n_iters flips per step,
+    // one on the upwind-only steps (timestep % upwind_filter_freq == 0)
+    long long flips = a.nt * S.n_iters;
+    if (a.uff > 0) {
+      const long long u = a.uff, b = a.t0 + a.nt;
+      flips -= ((b + u - 1) / u - (a.t0 + u - 1) / u) * (S.n_iters - 1);
+    }
+    if (flips & 1) S.tl[0] ^= 1;
   }
 }
 

@@ -7,9 +7,22 @@
 #include <stdexcept>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mpdx.h"
 
 namespace mpdx {
+
+// Named range on the NVTX timeline (the tracing of this library: Nsight Systems
+// and Nsight Compute show each entry point and solver phase by name).  NVTX is
+// header-only: without a tool attached a range costs one check of a function
+// pointer.
+struct trace_range {
+  explicit trace_range(const char *name) { nvtxRangePushA(name); }
+  ~trace_range() { nvtxRangePop(); }
+  trace_range(const trace_range &) = delete;
+  trace_range &operator=(const trace_range &) = delete;
+};
 
 // option bits (libmpdata++/opts.hpp:34-49)
 enum : unsigned {

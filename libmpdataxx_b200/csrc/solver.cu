@@ -689,6 +689,7 @@ static void strided_pack(const void *src, void *dst, const int ex[3], const int6
 }
 
 mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, const int64_t *strides) {
+  const mpdx::trace_range tr("mpdx_set_field");
   return guarded(h, [&] {
     if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
     h->impl->xfer_async->join(h->impl->stream);
@@ -703,6 +704,7 @@ mpdx_status mpdx_set_field(mpdx_handle h, int kind, int idx, const void *host, c
 }
 
 mpdx_status mpdx_get_field(mpdx_handle h, int kind, int idx, void *host, const int64_t *strides) {
+  const mpdx::trace_range tr("mpdx_get_field");
   return guarded(h, [&] {
     if (!host) throw mpdx::error(MPDX_E_ARG, "null host buffer");
     h->impl->xfer_async->join(h->impl->stream);
@@ -762,6 +764,7 @@ mpdx_status mpdx_get_field_async(mpdx_handle h, int kind, int idx, void *host) {
 }
 
 mpdx_status mpdx_advance(mpdx_handle h, int64_t nt) {
+  const mpdx::trace_range tr("mpdx_advance");
   return guarded(h, [&] {
     h->impl->xfer_async->join(h->impl->stream);
     h->impl->advance(nt);
@@ -776,6 +779,7 @@ mpdx_status mpdx_sync(mpdx_handle h) {
 }
 
 mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
+  const mpdx::trace_range tr("mpdx_stats");
   return guarded(h, [&] {
     if (!out) throw mpdx::error(MPDX_E_ARG, "null output");
     h->impl->xfer_async->join(h->impl->stream);
@@ -844,6 +848,7 @@ static mpdx_status batch_guarded(mpdx_batch_handle b, const std::function<void()
 }
 
 mpdx_status mpdx_batch_advance(mpdx_batch_handle b, int64_t nt) {
+  const mpdx::trace_range tr("mpdx_batch_advance");
   return batch_guarded(b, [&] { b->impl->advance(nt); });
 }
 
@@ -867,6 +872,7 @@ mpdx_status mpdx_precond_record(mpdx_handle h, int64_t max_pairs) {
 }
 
 mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t seed, double *final_loss) {
+  const mpdx::trace_range tr("mpdx_precond_train");
   return guarded(h, [&] {
     const double l = h->impl->precond_train(steps, lr, seed);
     if (final_loss) *final_loss = l;
