@@ -382,22 +382,28 @@ def gcr_extra(grid=(256, 256, 128), record=200, train=400, compare=1000):
     loss = learn.precond_train(train, lr=1e-3)
     t_train = time.perf_counter() - t0
     learn.precond_enable(True)
-    it_p, ms_p, it_l, ms_l, fb = [], [], [], [], 0
+    it_p, ms_p, it_l, ms_l, fb, nls = [], [], [], [], 0, {}
     for _ in range(compare):
         plain.advance(1)
         learn.advance(1)
         sp, sl = plain.stats(), learn.stats()
         it_p.append(sp["gcr_iters"]); ms_p.append(sp["gcr_ms"])
         it_l.append(sl["gcr_iters"]); ms_l.append(sl["gcr_ms"])
-        fb += int(sl["gcr_fallback"])
+        fb += int(sl["gcr_fallback"] == 2)
+        nl = learn.precond_directions()
+        nls[nl] = nls.get(nl, 0) + 1
     plain.close()
     learn.close()
     return {"workload": f"3D Boussinesq {grid[0]}x{grid[1]}x{grid[2]}, x/y cyclic, z rigid, FP32 advection, FP64 GCR (cr), "
                         f"prs_tol 1e-7; {record} recorded plain solves, then {compare} solves each, plain and learned",
             "plain": {"iters_per_solve": statistics.mean(it_p), "ms_per_solve": statistics.mean(ms_p)},
             "learned": {"iters_per_solve": statistics.mean(it_l), "ms_per_solve": statistics.mean(ms_l),
-                        "solves_handed_over_to_plain": fb},
+                        "solves_redone_with_plain_gcr": fb,
+                        "learned_directions_per_solve": {str(k): v for k, v in sorted(nls.items())},
+                        "last_500": {"iters_per_solve": statistics.mean(it_l[-500:]),
+                                     "ms_per_solve": statistics.mean(ms_l[-500:])}},
             "time_to_tol_speedup": statistics.mean(ms_p) / statistics.mean(ms_l),
+            "time_to_tol_speedup_last_500": statistics.mean(ms_p[-500:]) / statistics.mean(ms_l[-500:]),
             "training": {"pairs": n_pairs, "adam_steps": train,
                          "heldout_loss_relative_energy": loss, "seconds": t_train}}
 

@@ -113,7 +113,8 @@ typedef struct {
   double gcr_residual;     /* max|err| at the end of the last pressure solve */
   int path;                /* path used by the last advance (MPDX_PATH_GENERAL/FUSED) */
   double gcr_ms;           /* device time of the last pressure solve, start to max|err| <= prs_tol / dt */
-  int gcr_fallback;        /* 1 if the last solve left the learned preconditioner for plain GCR */
+  int gcr_fallback;        /* 1 if the last solve left the learned preconditioner for plain GCR,
+                              2 if it was redone from its start with plain GCR alone */
 } mpdx_step_stats;
 
 /* Fill *cfg with the reference defaults (opts = iga|fct, n_iters = 2, ...). */
@@ -231,13 +232,20 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
  * mpdx_precond_loss_grad over randomly drawn pairs, the last fifth of the pairs
  * (at most 8) held out, and keeps the weights with the lowest held-out loss seen (never
  * worse than the weights it started from); *final_loss is that held-out loss
- * (1 = no correction).  mpdx_precond_enable switches GCR to the flexible form whose
- * search directions start from the network's output instead of the residual.
- * The stopping test (max|err| <= prs_tol / dt) is unchanged: only the
- * iteration count changes.  Weights are exchanged in the mpdx_pcnet layout. */
+ * (1 = no correction).  With mpdx_precond_enable every pressure solve starts
+ * with nl learned corrections, Phi += beta q along q = net(err) with the step
+ * beta = -<err, q> / <q, lap q> that minimises the error in the operator's energy
+ * norm (the training norm), and continues with plain GCR from the iterate they
+ * reach; nl in {1, 2, 4, 0} is chosen by the measured device times of earlier
+ * solves (each tried twice, then the fastest, one re-measured every 64 solves).
+ * The stopping test (max|err| <= prs_tol / dt) is unchanged: only the iteration
+ * count and time change.  mpdx_precond_directions gives the nl of the last
+ * learned solve (-1 before the first).  Weights are exchanged in the mpdx_pcnet
+ * layout. */
 mpdx_status mpdx_precond_record(mpdx_handle h, int64_t max_pairs);
 mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t seed, double *final_loss);
 mpdx_status mpdx_precond_enable(mpdx_handle h, int on);
+int64_t mpdx_precond_directions(mpdx_handle h);
 int64_t mpdx_precond_pairs(mpdx_handle h);
 int64_t mpdx_precond_num_params(mpdx_handle h);
 mpdx_status mpdx_precond_get_params(mpdx_handle h, float *host);

@@ -203,6 +203,10 @@ class cuda:
         """Keep the (initial residual, correction) pair of each of the next max_pairs pressure solves."""
         _check(self.L, self.h, self.L.mpdx_precond_record(self.h, int(max_pairs)))
 
+    def precond_directions(self):
+        """Learned search directions at the start of the last learned solve (-1: none yet)."""
+        return int(self.L.mpdx_precond_directions(self.h))
+
     def precond_pairs(self):
         return int(self.L.mpdx_precond_pairs(self.h))
 

@@ -334,9 +334,11 @@ template <class T>
 __global__ void k_gcr_reset(gcr_dev<T> *dv) {
   dv->converged = 0; dv->done = 0; dv->stuck = 0; dv->cur = 0; dv->iters = 0; dv->arrive = 0u; dv->bad = 0;
 }
-// the learned directions are given up: plain GCR continues from the current iterate
+// after the learned corrections: plain GCR continues from the current iterate
 template <class T>
 __global__ void k_gcr_clear_bad(gcr_dev<T> *dv) { dv->bad = 0; }
+template <class T>
+__global__ void k_gcr_reset_conv(gcr_dev<T> *dv) { dv->converged = 0; }
 
 // err = lap(Phi) with err_init (u = the velocity being projected)
 template <class P, class T>
@@ -716,21 +718,26 @@ void launch_inner(int v, unsigned G, dim3 blk, cudaStream_t s, const geom &g, in
 }
 
 // ---------------------------------------------------------------------------
-// GCR(k) with a preconditioner M (the learned network): directions start from
-// q = M(err) instead of err (flexible GCR); err is updated with the exact
-// lap of each direction, so the stopping test is the reference's.  The
-// error is updated in place (no stencil reads it in the same kernel).
+// Learned corrections before plain GCR: q = M(err) from the network, a step along
+// q, and err updated with the exact lap of q, so the stopping test of the plain
+// iterations that follow is the reference's.  The error is updated in place (no
+// stencil reads it in the same kernel).
 
-// loop_init: p_0 = M(err) (already written by the network), lap_p_0 = lap(p_0); first beta sums
+// A learned correction: q = M(err) (written into p0 by the network), lap_q =
+// lap(q), and the sums of the step length that minimises the error in the energy
+// norm of the operator (the norm the network is trained in):
+// beta = -<err, q> / <q, lap q>  (err = lap(Phi) - rhs = lap(Phi - Phi*))
 template <class T>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_init_pc(geom g, dfield<T> err, dfield<T> p0, dfield<T> lp0,
                                                                 gcr_dev<T> *dv, double *part) {
+  if (dv->done || dv->bad || dv->converged) return;
   dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
   for_interior(g, [&](int i, int j, int k) {
+    const T q = p0(i, j, k);
     const T l = lap<T>(fld<T>{p0.o}, p0, no_u{}, g, i, j, k);
     lp0(i, j, k) = l;
-    acc[0] = dd_add(acc[0], dd{double(T(l * l)), 0.0});
-    acc[1] = dd_add(acc[1], dd{double(T(err(i, j, k) * l)), 0.0});
+    acc[0] = dd_add(acc[0], dd{double(T(q * l)), 0.0});
+    acc[1] = dd_add(acc[1], dd{double(T(err(i, j, k) * q)), 0.0});
   });
   double mx = 0, mn = 0;
   if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
@@ -744,7 +751,7 @@ template <class T, int NV>
 __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_tol, dfield<T> phi, dfield<T> err,
                                                                   dirs<T> D, gcr_dev<T> *dv, double *part) {
   constexpr int v = NV - 1;
-  if (dv->done || dv->bad) return;
+  if (dv->done || dv->bad || dv->converged) return;
   const T den = dv->pend_den;
   const T b = den != T(0) ? -dv->pend_num / den : dv->beta;
   // a direction from the network whose sums are not finite (an overflowing or NaN
@@ -773,80 +780,10 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_
   }
 }
 
-// lq = lap(q), alpha_l = -<lq, lap_p_l> / tmp_den[l]
-template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_lapq(geom g, dfield<T> q, dfield<T> lq, dirs<T> D, gcr_dev<T> *dv,
-                                                             double *part) {
-  if (dv->done || dv->bad) return;
-  dfield<T> lps[NV];
-#pragma unroll
-  for (int l = 0; l < NV; ++l) lps[l] = D.lp[l];
-  dd acc[NV];
-#pragma unroll
-  for (int l = 0; l < NV; ++l) acc[l] = dd{0.0, 0.0};
-  for_interior(g, [&](int i, int j, int k) {
-    const T l = lap<T>(fld<T>{q.o}, q, no_u{}, g, i, j, k);
-    lq(i, j, k) = l;
-#pragma unroll
-    for (int m = 0; m < NV; ++m) acc[m] = dd_add(acc[m], dd{double(T(l * lps[m](i, j, k))), 0.0});
-  });
-  double mx = 0, mn = 0;
-  if (grid_reduce<NV, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
-#pragma unroll
-    for (int l = 0; l < NV; ++l) {
-      const T dl = dv->tmp_den[l];
-      if (dl != T(0)) dv->alpha[l] = -T(ddv(acc[l])) / dl;
-    }
-  }
-}
-
-// next direction from q and lq; beta sums with the current error
-template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, 4) k_gcr_direction_pc(geom g, int kk, dfield<T> err, dfield<T> q, dfield<T> lq,
-                                                                     dirs<T> D, gcr_dev<T> *dv, double *part) {
-  constexpr int v = NV - 1;
-  if (dv->done || dv->bad) return;
-  T a[NV];
-  dfield<T> ps[NV], lps[NV];
-#pragma unroll
-  for (int l = 0; l < NV; ++l) { a[l] = dv->alpha[l]; ps[l] = D.p[l]; lps[l] = D.lp[l]; }
-  const bool restart = v == kk - 1;
-  const dfield<T> pd = restart ? D.p[0] : D.p[NV < kGcrMaxK ? NV : 0], lpd = restart ? D.lp[0] : D.lp[NV < kGcrMaxK ? NV : 0];
-  dd acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
-  for_interior(g, [&](int i, int j, int k) {
-    T pn = q(i, j, k), ln = lq(i, j, k);
-#pragma unroll
-    for (int l = 0; l < NV; ++l) {
-      pn = pn + a[l] * ps[l](i, j, k);
-      ln = ln + a[l] * lps[l](i, j, k);
-    }
-    pd(i, j, k) = pn;
-    lpd(i, j, k) = ln;
-    acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
-    acc[1] = dd_add(acc[1], dd{double(T(err(i, j, k) * ln)), 0.0});
-  });
-  double mx = 0, mn = 0;
-  if (grid_reduce<2, false>(acc, mx, mn, part, &dv->arrive) && threadIdx.x == 0 && threadIdx.y == 0) {
-    dv->pend_den = T(ddv(acc[0]));
-    dv->pend_num = T(ddv(acc[1]));
-    if (restart) {
-      dv->iters += 1;
-      if (dv->converged) dv->done = 1;
-      if (dv->iters > 10000) { dv->stuck = 1; dv->done = 1; }
-    }
-  }
-}
-
 template <class T, int NV>
 void launch_pc_update(unsigned G, dim3 blk, cudaStream_t s, const geom &g, T err_tol, dfield<T> phi, dfield<T> err,
                       const dirs<T> &D, gcr_dev<T> *dv, double *part) {
   k_gcr_update_pc<T, NV><<<G, blk, 0, s>>>(g, err_tol, phi, err, D, dv, part);
-}
-template <class T, int NV>
-void launch_pc_direction(unsigned G, dim3 blk, cudaStream_t s, const geom &g, int kk, dfield<T> err, dfield<T> q,
-                         dfield<T> lq, const dirs<T> &D, gcr_dev<T> *dv, double *part) {
-  k_gcr_lapq<T, NV><<<G, blk, 0, s>>>(g, q, lq, D, dv, part);
-  k_gcr_direction_pc<T, NV><<<G, blk, 0, s>>>(g, kk, err, q, lq, D, dv, part);
 }
 #define MPDX_NV_SWITCH(v, CALL)                     \
   switch ((v) + 1) {                                \
@@ -1302,46 +1239,67 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
   bq::k_gcr_reset<P><<<1, 1, 0, s>>>(dev);
   bq::k_err_init<P, T><<<G, kBlk, 0, s>>>(gm, Phi.v, u, err[0].v);
   if (rec) bq::k_to_compact<P><<<G, kBlk, 0, s>>>(gm, err[0].v, dfield<P>{}, pairs + size_t(rec_slots[0]) * 2 * gm.cells);
-  bool pcnd = use_net && net;
+  const bool learned = use_net && net;
+  const int nl_idx = learned ? pick_nl() : -1;
+  const long long nl = learned ? nl_cand[nl_idx] : 0;
+  bool pcnd = learned && nl > 0;
   fell_back = false;
+  restarted = false;
+  long long discarded = 0;  // iterations of a learned attempt that was given up
+  if (learned) bq::k_copy_field<P><<<G, kBlk, 0, s>>>(gm, Phi.v, phi_start.v);
+  long long learned_steps = 0;
   if (pcnd) {
+    // the learned corrections: nl steps Phi += beta q, err += beta lap(q) along
+    // q = M(err), each with the energy-optimal beta, before plain GCR starts
     if constexpr (std::is_same<P, double>::value) {
-      const auto &e = err[0].v;
-      net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, p_err[0].v.o, nullptr);
+      for (long long l = 0; l < nl; ++l) {
+        const auto &e = err[0].v;
+        net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, p_err[0].v.o, &dev->converged);
+        bq::k_gcr_init_pc<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+        bq::launch_pc_update<P, 1>(G, kBlk, s, gm, err_tol, Phi.v, err[0].v, D, dev, part);
+      }
     }
-    bq::k_gcr_init_pc<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
-  } else {
-    bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+    MPDX_LAUNCH_CHECK();
+    learned_steps = nl;
+    fell_back = true;  // the solve continues with plain directions
+    pcnd = false;
+    MPDX_CUDA(cudaMemcpyAsync(hdev, dev, sizeof(gcr_dev<P>), cudaMemcpyDeviceToHost, s));
+    MPDX_CUDA(cudaStreamSynchronize(s));
+    // a correction with non-finite sums changed nothing; the residual test of the
+    // reference runs in the plain iterations that follow
+    bq::k_gcr_clear_bad<P><<<1, 1, 0, s>>>(dev);
+    bq::k_gcr_reset_conv<P><<<1, 1, 0, s>>>(dev);
   }
+  bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
   MPDX_LAUNCH_CHECK();
   long long launched = 0;
   for (;;) {
     long long batch = launched == 0 ? std::max(1LL, predicted) : std::max(4LL, predicted / 4);
     if (rec) batch = std::min(batch, 16LL);  // snapshots are taken between batches
-    if (pcnd) batch = std::min(batch, 4LL);  // the hand-over test below runs between batches
     for (long long b = 0; b < batch; ++b)
-      for (int v = 0; v < k_iters; ++v) {
-        if (!pcnd) {
-          bq::launch_inner<P>(v, G, kBlk, s, gm, k_iters, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
-          continue;
-        }
-        // preconditioned step: update, q = M(err) (skipped once converged), lap(q), new direction
-#define MPDX_PC_UPD(NV) bq::launch_pc_update<P, NV>(G, kBlk, s, gm, err_tol, Phi.v, err[0].v, D, dev, part)
-#define MPDX_PC_DIR(NV) bq::launch_pc_direction<P, NV>(G, kBlk, s, gm, k_iters, err[0].v, q_f.v, lq_f.v, D, dev, part)
-        MPDX_NV_SWITCH(v, MPDX_PC_UPD)
-        if constexpr (std::is_same<P, double>::value) {
-          const auto &e = err[0].v;
-          net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, q_f.v.o, &dev->done);
-        }
-        MPDX_NV_SWITCH(v, MPDX_PC_DIR)
-#undef MPDX_PC_UPD
-#undef MPDX_PC_DIR
-      }
+      for (int v = 0; v < k_iters; ++v)
+        bq::launch_inner<P>(v, G, kBlk, s, gm, k_iters, err_tol, Phi.v, err[0].v, err[1].v, lap_err.v, D, dev, part);
     MPDX_LAUNCH_CHECK();
     launched += batch;
     MPDX_CUDA(cudaEventRecord(ev_solve[1], s));
     MPDX_CUDA(cudaMemcpyAsync(hdev, dev, sizeof(gcr_dev<P>), cudaMemcpyDeviceToHost, s));
     MPDX_CUDA(cudaStreamSynchronize(s));
+    // a learned solve that, after handing over, still runs far past a plain solve's
+    // iteration count is redone from its start with plain GCR alone, so the learned
+    // form never gives a worse result than the method without it
+    if (learned && !restarted && (hdev->stuck || (!pcnd && hdev->iters > 4 * last_plain_iters + 200))) {
+      discarded = hdev->iters;
+      bq::k_copy_field<P><<<G, kBlk, 0, s>>>(gm, phi_start.v, Phi.v);
+      bq::k_gcr_reset<P><<<1, 1, 0, s>>>(dev);
+      bq::k_err_init<P, T><<<G, kBlk, 0, s>>>(gm, Phi.v, u, err[0].v);
+      bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
+      MPDX_LAUNCH_CHECK();
+      pcnd = false;
+      fell_back = true;
+      restarted = true;
+      launched = 0;
+      continue;
+    }
     if (hdev->stuck) throw error(MPDX_E_PRS_STUCK, "libmpdata++: stuck in pressure solver");
     if (hdev->done) break;
     if (rec && n_rec < 1 + kSnaps && n_pairs < max_pairs && hdev->iters >= 16LL << (n_rec - 1)) {
@@ -1352,29 +1310,20 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
       MPDX_LAUNCH_CHECK();
       ++n_rec;
     }
-    float elapsed = 0;
-    if (pcnd && last_plain_ms > 0) MPDX_CUDA(cudaEventElapsedTime(&elapsed, ev_solve[0], ev_solve[1]));
-    if (pcnd && (hdev->bad || hdev->iters > std::max(20LL, 2 * last_plain_iters) ||
-                 (last_plain_ms > 0 && elapsed > last_plain_ms))) {
-      // a learned direction was not finite, the learned directions are not
-      // converging, or the solve has already taken as long as a whole plain
-      // solve (so it can no longer be faster): continue from the current iterate
-      // with plain GCR (directions restart from the residual)
-      bq::k_gcr_clear_bad<P><<<1, 1, 0, s>>>(dev);
-      bq::k_gcr_init<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
-      MPDX_LAUNCH_CHECK();
-      pcnd = false;
-      fell_back = true;
-      ++fallbacks;
-    }
   }
   {
     float ms = 0;
     MPDX_CUDA(cudaEventElapsedTime(&ms, ev_solve[0], ev_solve[1]));
     last_solve_ms = ms;
   }
-  iters = hdev->iters;
+  iters = hdev->iters + learned_steps + discarded;
   iters_total += iters;
+  if (learned) {
+    nl_ms[nl_idx] = nl_tries[nl_idx] == 0 ? last_solve_ms : 0.5 * (nl_ms[nl_idx] + last_solve_ms);
+    ++nl_tries[nl_idx];
+    nl_last = nl_idx;
+    ++n_learned;
+  }
   if (!(use_net && net)) { last_plain_iters = iters; last_plain_ms = last_solve_ms; }
   last_residual = hdev->residual;
   predicted = std::max(1LL, iters);
@@ -1394,8 +1343,7 @@ void boussinesq<T, P>::ensure_net() {
       wrap[d] = d < st.nd ? (st.bcs[d][0] == MPDX_BC_CYCLIC ? 1 : 0) : 1;
     }
     net.reset(new pc::net(st.nd, grid, wrap, pc_channels, 12345, st.stream));
-    st.alloc_sclr(q_f);
-    st.alloc_sclr(lq_f);
+    st.alloc_sclr(phi_start);
   }
 }
 
@@ -1599,6 +1547,20 @@ double boussinesq<T, P>::precond_loss_grad(const double *r, const double *t, dou
     }
     return E;
   }
+}
+
+// the number of learned directions at the start of the next learned solve: every
+// candidate is tried twice (in order), then the one with the shortest mean solve
+// time is taken, and every 64th learned solve re-measures one candidate in turn
+template <class T, class P>
+int boussinesq<T, P>::pick_nl() {
+  for (int c = 0; c < kNlCand; ++c)
+    if (nl_tries[c] < 2) return c;
+  if (n_learned % 64 == 63) return int((n_learned / 64) % kNlCand);
+  int best = 0;
+  for (int c = 1; c < kNlCand; ++c)
+    if (nl_ms[c] < nl_ms[best]) best = c;
+  return best;
 }
 
 template <class T, class P>

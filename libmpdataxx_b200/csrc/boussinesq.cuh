@@ -71,16 +71,26 @@ struct boussinesq {
   std::unique_ptr<pc::net> net;
   bool use_net = false;
   static constexpr int kSnaps = 3;  // recorded pairs per solve beyond the initial one (iterations 16, 32, 64)
-  field<P> q_f, lq_f, snap[1 + kSnaps];
+  field<P> snap[1 + kSnaps], phi_start;  // phi_start: Phi when a learned solve began
   float *pairs = nullptr, *tr_r = nullptr, *tr_t = nullptr, *tr_q = nullptr, *tr_z = nullptr, *tr_dq = nullptr;
   float *tr_a = nullptr, *tr_b = nullptr;
   double out_scale = 0, last_train_loss = -1;
   double *tr_loss = nullptr;
   int *adj_col[3] = {nullptr, nullptr, nullptr};  // adjoint of the pressure operator, per axis
   float *adj_val[3] = {nullptr, nullptr, nullptr};
-  long long last_plain_iters = 250, fallbacks = 0;
+  long long last_plain_iters = 250;
   float last_plain_ms = 0;  // device time of the last plain solve (0: none yet)
   bool fell_back = false;
+  bool restarted = false;   // the last learned solve was redone from its start with plain GCR
+  // learned solves: the first nl search directions come from the network, the rest
+  // are plain GCR's; nl is chosen among the candidates by the measured solve times
+  static constexpr int kNlCand = 4;
+  int nl_cand[kNlCand] = {1, 2, 4, 0};
+  double nl_ms[kNlCand] = {0, 0, 0, 0};
+  int nl_tries[kNlCand] = {0, 0, 0, 0};
+  int nl_last = -1;          // candidate index of the last learned solve
+  long long n_learned = 0;   // learned solves so far
+  int pick_nl();
   long long max_pairs = 0, n_pairs = 0;
   int pc_channels[4] = {8, 16, 32, 64};
 

@@ -81,6 +81,13 @@ template <int ND> struct tile;
 template <> struct tile<3> { static constexpr int T0 = 2, T1 = 4, T2 = 16; };
 template <> struct tile<2> { static constexpr int T0 = 8, T1 = 16, T2 = 1; };
 
+// the convolution's tile: R rows of 16 points per warp (8 warps); R = 4 on the fine
+// 3D levels, where every weight fragment then serves four MMAs
+template <int ND, int R> struct ctile;
+template <> struct ctile<3, 1> { static constexpr int T0 = 2, T1 = 4, T2 = 16; };
+template <> struct ctile<3, 4> { static constexpr int T0 = 4, T1 = 8, T2 = 16; };
+template <> struct ctile<2, 1> { static constexpr int T0 = 8, T1 = 16, T2 = 1; };
+
 template <int CIN>
 struct sv {  // bytes per point in the shared tile (padded against bank conflicts)
   static constexpr int v = CIN >= 16 ? CIN * 2 + 16 : 16;
@@ -102,12 +109,14 @@ struct conv_out {
   const uint16_t *skip; // BF16 tensor added to the output (or null)
 };
 
-// X: [vox][CIN] BF16 on grid g; Wf: fragments [chunk][COUT/8][32] x uint2
-template <int CIN, int COUT, int ND>
-__global__ void __launch_bounds__(256) k_conv_tc(grid3 g, const uint16_t *__restrict__ X, const uint2 *__restrict__ Wf,
+// X: [vox][CIN] BF16 on grid g; Wf: fragments [chunk][COUT/8][32] x uint2.
+// UP: X lives on the coarse grid cg and the input is its nearest up-sampling,
+// X(p) = X_coarse(floor(p / 2)) (k_up), read straight into the halo tile
+template <int CIN, int COUT, int ND, bool UP, int R>
+__global__ void __launch_bounds__(256) k_conv_tc(grid3 g, grid3 cg, const uint16_t *__restrict__ X, const uint2 *__restrict__ Wf,
                                                  conv_out o, const int *skip_flag) {
   if (skip_flag && *skip_flag) return;
-  using TL = tile<ND>;
+  using TL = ctile<ND, R>;
   constexpr int T0 = TL::T0, T1 = TL::T1, T2 = TL::T2;
   constexpr int H0 = T0 + 2, H1 = T1 + 2, H2 = ND == 3 ? T2 + 2 : 1;
   constexpr int CB = CIN / 8, SV = sv<CIN>::v, NTAPS = ND == 3 ? 27 : 9;
@@ -121,54 +130,81 @@ __global__ void __launch_bounds__(256) k_conv_tc(grid3 g, const uint16_t *__rest
   for (int q = threadIdx.x; q < H0 * H1 * H2 * CB; q += blockDim.x) {
     const int hv = q / CB, cb = q % CB;
     const int hk = hv % H2, hj = (hv / H2) % H1, hi = hv / (H2 * H1);
-    const long long v = nbr(g, i0 - 1 + hi, j0 - 1 + hj, ND == 3 ? k0 - 1 + hk : 0, 0, 0, 0);
-    uint4 val = make_uint4(0, 0, 0, 0);
-    if (v >= 0) val = *reinterpret_cast<const uint4 *>(X + v * CIN + cb * 8);
-    *reinterpret_cast<uint4 *>(sm + hv * SV + cb * 16) = val;
+    long long v;
+    if constexpr (UP) {
+      const int x = padx(i0 - 1 + hi, g.n[0], g.wrap[0]), y = padx(j0 - 1 + hj, g.n[1], g.wrap[1]);
+      const int z = ND == 3 ? padx(k0 - 1 + hk, g.n[2], g.wrap[2]) : 0;
+      v = (x < 0 || y < 0 || z < 0) ? -1
+                                    : vindex(cg, min(x / 2, cg.n[0] - 1), min(y / 2, cg.n[1] - 1), min(z / 2, cg.n[2] - 1));
+    } else {
+      v = nbr(g, i0 - 1 + hi, j0 - 1 + hj, ND == 3 ? k0 - 1 + hk : 0, 0, 0, 0);
+    }
+    // asynchronous 16-byte copy; a padding point copies no bytes and is zero-filled
+    const uint16_t *src = v >= 0 ? X + v * CIN + cb * 8 : X;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(sm + hv * SV + cb * 16)), "l"(src),
+                 "r"(v >= 0 ? 16 : 0)
+                 : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int ti = ND == 3 ? w / 4 : w, tj = ND == 3 ? w % 4 : 0;  // warp's row of the tile
+  // the warp's rows of the tile (ND = 3: rows (ti, tj) of 16 points along k; ND = 2: row ti along j)
+  int ti[R], tj[R];
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+    const int row = w * R + rr;
+    ti[rr] = ND == 3 ? row / T1 : row;
+    tj[rr] = ND == 3 ? row % T1 : 0;
+  }
   // ldmatrix row of this lane: point m, group slot gs (0: k 0-7, 1: k 8-15)
   const int lm = (lane & 7) + ((lane >> 3) & 1) * 8, gs = lane >> 4;
-  float acc[NT][4];
+  float acc[R][NT][4];
 #pragma unroll
-  for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+  for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+    for (int n = 0; n < NT; ++n) acc[rr][n][0] = acc[rr][n][1] = acc[rr][n][2] = acc[rr][n][3] = 0.f;
   const unsigned sbase = smem_u32(sm);
-#pragma unroll 2
+  // fully unrolled: every chunk's taps and channel groups are constants (a lane's
+  // group slot gs selects between two of them)
+#pragma unroll
   for (int ch = 0; ch < NCH; ++ch) {
     int gidx = 2 * ch + gs;
     if (gidx >= NG) gidx = 2 * ch;  // zero weights pair with any valid address
     const int tap = gidx / CB, cb = gidx % CB;
     int a, b, c;
     tap_off<ND>(tap, a, b, c);
-    int hv;
-    if (ND == 3) hv = ((ti + 1 + a) * H1 + (tj + 1 + b)) * H2 + (lm + 1 + c);
-    else hv = (ti + 1 + a) * H1 + (lm + 1 + b);
-    unsigned af[4];
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(af[0]), "=r"(af[1]), "=r"(af[2]), "=r"(af[3])
-                 : "r"(sbase + hv * SV + cb * 16));
+    uint2 bw[NT];
 #pragma unroll
-    for (int n = 0; n < NT; ++n) {
-      const uint2 bw = __ldg(Wf + (size_t(ch) * NT + n) * 32 + lane);
-      mma16816(acc[n], af, bw.x, bw.y);
+    for (int n = 0; n < NT; ++n) bw[n] = __ldg(Wf + (size_t(ch) * NT + n) * 32 + lane);
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      int hv;
+      if (ND == 3) hv = ((ti[rr] + 1 + a) * H1 + (tj[rr] + 1 + b)) * H2 + (lm + 1 + c);
+      else hv = (ti[rr] + 1 + a) * H1 + (lm + 1 + b);
+      unsigned af[4];
+      asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                   : "=r"(af[0]), "=r"(af[1]), "=r"(af[2]), "=r"(af[3])
+                   : "r"(sbase + hv * SV + cb * 16));
+#pragma unroll
+      for (int n = 0; n < NT; ++n) mma16816(acc[rr][n], af, bw[n].x, bw[n].y);
     }
   }
   // epilogue: rows lane/4 and lane/4 + 8, columns 2 (lane % 4) + {0, 1} of each 8-channel tile
 #pragma unroll
+  for (int rr = 0; rr < R; ++rr)
+#pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int m = lane / 4 + 8 * h;
     int gi, gj, gk;
-    if (ND == 3) { gi = i0 + ti; gj = j0 + tj; gk = k0 + m; }
-    else { gi = i0 + ti; gj = j0 + m; gk = 0; }
+    if (ND == 3) { gi = i0 + ti[rr]; gj = j0 + tj[rr]; gk = k0 + m; }
+    else { gi = i0 + ti[rr]; gj = j0 + m; gk = 0; }
     if (gi >= g.n[0] || gj >= g.n[1] || gk >= g.n[2]) continue;
     const long long v = vindex(g, gi, gj, gk);
 #pragma unroll
     for (int n = 0; n < NT; ++n) {
       const int co = n * 8 + 2 * (lane % 4);
-      float y0 = acc[n][2 * h], y1 = acc[n][2 * h + 1];
+      float y0 = acc[rr][n][2 * h], y1 = acc[rr][n][2 * h + 1];
       if (o.bias) { y0 += o.bias[co]; y1 += o.bias[co + 1]; }
       if (o.skip) {
         const unsigned s2 = *reinterpret_cast<const unsigned *>(o.skip + v * COUT + co);
@@ -308,62 +344,213 @@ __global__ void k_db_reduce(const float *part, int nblk, int C, float *grad_b) {
 // ---------------------------------------------------------------------------
 // end layers (per-point loops)
 
-// e0[p][co] = b[co] + sum_t W[co][t] r(p + tap_t); r from an FP64 halo'ed field or a compact FP32 array
-template <int C0, int ND, bool FIELD>
-__global__ void k_conv_in(grid3 g, const double *rf, long long s0, long long s1, long long s2, const float *rc,
-                          const float *W, const float *b, uint16_t *e0, const int *skip_flag) {
+// Tiles of the per-point end layers: 512 points, 128 threads, each thread a column
+// of four points along i (ND = 3: 4 x 8 x 16; ND = 2: 4 x 128), even sizes at even
+// origins so that every 2^d block of the pooling lies inside one tile.  A thread
+// reads the six halo values of its column once per (j, k) tap offset and uses
+// them for the three i offsets of all four points.
+template <int ND> struct etile;
+template <> struct etile<3> { static constexpr int T0 = 4, T1 = 8, T2 = 16, H0 = 6, H1 = 10, H2 = 18; };
+template <> struct etile<2> { static constexpr int T0 = 4, T1 = 128, T2 = 1, H0 = 6, H1 = 130, H2 = 1; };
+constexpr int kEndThreads = 128;
+
+template <int ND>
+__device__ __forceinline__ void etile_origin(const grid3 &g, int b, int &i0, int &j0, int &k0) {
+  using E = etile<ND>;
+  const int n1 = (g.n[1] + E::T1 - 1) / E::T1, n2 = (g.n[2] + E::T2 - 1) / E::T2;
+  i0 = (b / (n1 * n2)) * E::T0; j0 = ((b / n2) % n1) * E::T1; k0 = (b % n2) * E::T2;
+}
+template <int ND>
+inline long long etile_count(const grid3 &g) {
+  using E = etile<ND>;
+  return (long long)((g.n[0] + E::T0 - 1) / E::T0) * ((g.n[1] + E::T1 - 1) / E::T1) * ((g.n[2] + E::T2 - 1) / E::T2);
+}
+// tap index of offsets (ta, tb, tc) in tap_off's order
+template <int ND>
+__device__ __forceinline__ constexpr int tap_of(int ta, int tb, int tc) {
+  return ND == 3 ? (ta + 1) * 9 + (tb + 1) * 3 + (tc + 1) : (ta + 1) * 3 + (tb + 1);
+}
+
+// e0[p][co] = b[co] + sum_t W[co][t] r(p + tap_t), r from an FP64 halo'ed field or a
+// compact FP32 array, staged with its halo in shared memory; with POOL the CTA also
+// writes the pooled level-1 input p1 = pool(e0) of its tile (k_pool's average of the
+// BF16 values, in k_pool's order)
+template <int C0, int ND, bool FIELD, bool POOL>
+__global__ void __launch_bounds__(kEndThreads) k_conv_in(grid3 g, grid3 cg, const double *rf, long long s0, long long s1,
+                                                         long long s2, const float *rc, const float *W, const float *b,
+                                                         uint16_t *e0, uint16_t *p1, const int *skip_flag) {
   if (skip_flag && *skip_flag) return;
-  constexpr int NTAPS = ND == 3 ? 27 : 9;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.vox; p += (long long)gridDim.x * blockDim.x) {
-    const int k = int(p % g.n[2]), j = int((p / g.n[2]) % g.n[1]), i = int(p / ((long long)g.n[2] * g.n[1]));
-    float acc[C0];
+  using E = etile<ND>;
+  constexpr int NTAPS = ND == 3 ? 27 : 9, NH = E::H0 * E::H1 * E::H2, NP = E::T0 * E::T1 * E::T2;
+  constexpr int TC = ND == 3 ? 1 : 0;  // k offsets -TC..TC
+  __shared__ float rs[NH];
+  __shared__ __align__(16) float ws[NTAPS * C0];  // tap-major: ws[t][co]
+  __shared__ float bs[C0];
+  __shared__ float es[POOL ? NP * C0 : 1];
+  int i0, j0, k0;
+  etile_origin<ND>(g, blockIdx.x, i0, j0, k0);
+  for (int q = threadIdx.x; q < C0 * NTAPS; q += blockDim.x) ws[(q % NTAPS) * C0 + q / NTAPS] = W[q];
+  if (threadIdx.x < C0) bs[threadIdx.x] = b[threadIdx.x];
+  for (int q = threadIdx.x; q < NH; q += blockDim.x) {
+    const int hk = q % E::H2, hj = (q / E::H2) % E::H1, hi = q / (E::H2 * E::H1);
+    const int x = padx(i0 - 1 + hi, g.n[0], g.wrap[0]), y = padx(j0 - 1 + hj, g.n[1], g.wrap[1]);
+    const int z = ND == 3 ? padx(k0 - 1 + hk, g.n[2], g.wrap[2]) : 0;
+    float r = 0.f;
+    if (x >= 0 && y >= 0 && z >= 0) r = FIELD ? float(rf[x * s0 + y * s1 + z * s2]) : rc[vindex(g, x, y, z)];
+    rs[q] = r;
+  }
+  __syncthreads();
+  const int c = threadIdx.x % E::T2, bb = threadIdx.x / E::T2;
+  float acc[4][C0];
 #pragma unroll
-    for (int c = 0; c < C0; ++c) acc[c] = b[c];
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int t = 0; t < NTAPS; ++t) {
-      int a, bb, c;
-      tap_off<ND>(t, a, bb, c);
-      const int x = padx(i + a, g.n[0], g.wrap[0]), y = padx(j + bb, g.n[1], g.wrap[1]), z = padx(k + c, g.n[2], g.wrap[2]);
-      if (x < 0 || y < 0 || z < 0) continue;
-      const float r = FIELD ? float(rf[x * s0 + y * s1 + z * s2]) : rc[vindex(g, x, y, z)];
+    for (int co = 0; co < C0; ++co) acc[a][co] = bs[co];
 #pragma unroll
-      for (int co = 0; co < C0; ++co) acc[co] = fmaf(W[co * NTAPS + t], r, acc[co]);
+  for (int tb = -1; tb <= 1; ++tb)
+#pragma unroll
+    for (int tc = -TC; tc <= TC; ++tc) {
+      float col[6];
+#pragma unroll
+      for (int h = 0; h < 6; ++h) col[h] = rs[(h * E::H1 + (bb + 1 + tb)) * E::H2 + (ND == 3 ? c + 1 + tc : 0)];
+#pragma unroll
+      for (int ta = -1; ta <= 1; ++ta) {
+        const int t = tap_of<ND>(ta, tb, tc);
+        float w[C0];
+#pragma unroll
+        for (int q = 0; q < C0 / 4; ++q) {
+          const float4 v = reinterpret_cast<const float4 *>(ws + t * C0)[q];
+          w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int co = 0; co < C0; ++co) acc[a][co] = fmaf(w[co], col[a + 1 + ta], acc[a][co]);
+      }
     }
 #pragma unroll
-    for (int c = 0; c < C0; c += 2)
-      *reinterpret_cast<unsigned *>(e0 + p * C0 + c) = unsigned(f2bf(acc[c])) | (unsigned(f2bf(acc[c + 1])) << 16);
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + a, j = j0 + bb, k = k0 + c;
+    unsigned pk[C0 / 2];
+#pragma unroll
+    for (int co = 0; co < C0; co += 2) pk[co / 2] = unsigned(f2bf(acc[a][co])) | (unsigned(f2bf(acc[a][co + 1])) << 16);
+    if (i < g.n[0] && j < g.n[1] && k < g.n[2]) {
+      uint4 *dst = reinterpret_cast<uint4 *>(e0 + vindex(g, i, j, k) * C0);
+#pragma unroll
+      for (int h = 0; h < C0 / 8; ++h) dst[h] = make_uint4(pk[4 * h], pk[4 * h + 1], pk[4 * h + 2], pk[4 * h + 3]);
+    }
+    if constexpr (POOL) {
+      const int lin = (a * E::T1 + bb) * E::T2 + c;
+#pragma unroll
+      for (int co = 0; co < C0; co += 2) {
+        es[lin * C0 + co] = bf2f(uint16_t(pk[co / 2] & 0xffffu));
+        es[lin * C0 + co + 1] = bf2f(uint16_t(pk[co / 2] >> 16));
+      }
+    }
+  }
+  if constexpr (POOL) {
+    __syncthreads();
+    constexpr int Q0 = E::T0 / 2, Q1 = E::T1 / 2, Q2 = ND == 3 ? E::T2 / 2 : 1;
+    for (int q = threadIdx.x; q < Q0 * Q1 * Q2 * C0; q += blockDim.x) {
+      const int co = q % C0, V = q / C0;
+      const int K = V % Q2, J = (V / Q2) % Q1, I = V / (Q2 * Q1);
+      const int gI = i0 / 2 + I, gJ = j0 / 2 + J, gK = ND == 3 ? k0 / 2 + K : 0;
+      if (gI >= cg.n[0] || gJ >= cg.n[1] || gK >= cg.n[2]) continue;
+      float sum = 0.f;
+      int cnt = 0;
+      const int l0 = ((2 * gI - i0) * E::T1 + (2 * gJ - j0)) * E::T2 + (ND == 3 ? 2 * gK - k0 : 0);
+      const bool full = 2 * gI + 1 < g.n[0] && 2 * gJ + 1 < g.n[1] && (ND == 2 || 2 * gK + 1 < g.n[2]);
+      if (full) {  // the whole 2^d block exists: k_pool's order without the checks
+        constexpr int DK = ND == 3 ? 1 : 0;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+            for (int d = 0; d <= DK; ++d) sum += es[(l0 + (a * E::T1 + bb) * E::T2 + d) * C0 + co];
+        cnt = ND == 3 ? 8 : 4;
+      } else {
+        for (int a = 0; a < 2; ++a)
+          for (int bb = 0; bb < 2; ++bb)
+            for (int d = 0; d < 2; ++d) {
+              const int i = 2 * gI + a, j = 2 * gJ + bb, k = 2 * gK + d;
+              if (i >= g.n[0] || j >= g.n[1] || k >= g.n[2]) continue;
+              if ((g.n[0] == 1 && a) || (g.n[1] == 1 && bb) || (g.n[2] == 1 && d)) continue;
+              const int lin = ((i - i0) * E::T1 + (j - j0)) * E::T2 + (ND == 3 ? k - k0 : 0);
+              sum += es[lin * C0 + co];
+              ++cnt;
+            }
+      }
+      p1[vindex(cg, gI, gJ, gK) * C0 + co] = f2bf(sum / float(cnt));
+    }
   }
 }
 
-// q(p) = b + sum_t sum_ci W[t][ci] d0[p + tap_t][ci]; to an FP64 halo'ed field or a compact FP32 array
+// q(p) = b + sum_t sum_ci W[t][ci] d0[p + tap_t][ci], to an FP64 halo'ed field or a
+// compact FP32 array; d0 (BF16) is staged with its halo in shared memory
 template <int C0, int ND, bool FIELD>
-__global__ void k_conv_outl(grid3 g, const uint16_t *d0, const float *W, const float *b, double *qf, long long s0,
-                            long long s1, long long s2, float *qc, const int *skip_flag) {
+__global__ void __launch_bounds__(kEndThreads) k_conv_outl(grid3 g, const uint16_t *d0, const float *W, const float *b,
+                                                           double *qf, long long s0, long long s1, long long s2, float *qc,
+                                                           const int *skip_flag) {
   if (skip_flag && *skip_flag) return;
-  constexpr int NTAPS = ND == 3 ? 27 : 9;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.vox; p += (long long)gridDim.x * blockDim.x) {
-    const int k = int(p % g.n[2]), j = int((p / g.n[2]) % g.n[1]), i = int(p / ((long long)g.n[2] * g.n[1]));
-    float acc = b[0];
+  using E = etile<ND>;
+  constexpr int NTAPS = ND == 3 ? 27 : 9, NH = E::H0 * E::H1 * E::H2, CB = C0 / 8;
+  constexpr int TC = ND == 3 ? 1 : 0;
+  __shared__ uint4 ds[NH * CB];
+  __shared__ __align__(16) float ws[NTAPS * C0];  // W[t][ci]
+  __shared__ float b0;
+  int i0, j0, k0;
+  etile_origin<ND>(g, blockIdx.x, i0, j0, k0);
+  for (int q = threadIdx.x; q < NTAPS * C0; q += blockDim.x) ws[q] = W[q];
+  if (threadIdx.x == 0) b0 = b[0];
+  for (int q = threadIdx.x; q < NH * CB; q += blockDim.x) {
+    const int hv = q / CB, cb = q % CB;
+    const int hk = hv % E::H2, hj = (hv / E::H2) % E::H1, hi = hv / (E::H2 * E::H1);
+    const int x = padx(i0 - 1 + hi, g.n[0], g.wrap[0]), y = padx(j0 - 1 + hj, g.n[1], g.wrap[1]);
+    const int z = ND == 3 ? padx(k0 - 1 + hk, g.n[2], g.wrap[2]) : 0;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (x >= 0 && y >= 0 && z >= 0) v = *reinterpret_cast<const uint4 *>(d0 + vindex(g, x, y, z) * C0 + cb * 8);
+    ds[q] = v;
+  }
+  __syncthreads();
+  const int c = threadIdx.x % E::T2, bb = threadIdx.x / E::T2;
+  float acc[4] = {b0, b0, b0, b0};
 #pragma unroll
-    for (int t = 0; t < NTAPS; ++t) {
-      int a, bb, c;
-      tap_off<ND>(t, a, bb, c);
-      const long long v = nbr(g, i, j, k, a, bb, c);
-      if (v < 0) continue;
-      const uint16_t *src = d0 + v * C0;
+  for (int tb = -1; tb <= 1; ++tb)
 #pragma unroll
-      for (int ci = 0; ci < C0; ci += 8) {
-        const uint4 u = *reinterpret_cast<const uint4 *>(src + ci);
-        const unsigned w4[4] = {u.x, u.y, u.z, u.w};
+    for (int tc = -TC; tc <= TC; ++tc)
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          acc = fmaf(W[t * C0 + ci + 2 * h], bf2f(uint16_t(w4[h] & 0xffffu)), acc);
-          acc = fmaf(W[t * C0 + ci + 2 * h + 1], bf2f(uint16_t(w4[h] >> 16)), acc);
+      for (int cb = 0; cb < CB; ++cb) {
+        float col[6][8];
+#pragma unroll
+        for (int h = 0; h < 6; ++h) {
+          const uint4 u = ds[((h * E::H1 + (bb + 1 + tb)) * E::H2 + (ND == 3 ? c + 1 + tc : 0)) * CB + cb];
+          const unsigned w4[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            col[h][2 * e] = bf2f(uint16_t(w4[e] & 0xffffu));
+            col[h][2 * e + 1] = bf2f(uint16_t(w4[e] >> 16));
+          }
+        }
+#pragma unroll
+        for (int ta = -1; ta <= 1; ++ta) {
+          const int t = tap_of<ND>(ta, tb, tc);
+          const float4 wa = reinterpret_cast<const float4 *>(ws + t * C0 + cb * 8)[0];
+          const float4 wb = reinterpret_cast<const float4 *>(ws + t * C0 + cb * 8)[1];
+          const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int e = 0; e < 8; ++e) acc[a] = fmaf(w[e], col[a + 1 + ta][e], acc[a]);
         }
       }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + a, j = j0 + bb, k = k0 + c;
+    if (i < g.n[0] && j < g.n[1] && k < g.n[2]) {
+      if (FIELD) qf[i * s0 + j * s1 + k * s2] = double(acc[a]);
+      else qc[vindex(g, i, j, k)] = acc[a];
     }
-    if (FIELD) qf[i * s0 + j * s1 + k * s2] = double(acc);
-    else qc[p] = acc;
   }
 }
 
@@ -443,14 +630,16 @@ __global__ void k_endl_reduce(const float *part, int nblk, int ntaps, int cy, in
 // ---------------------------------------------------------------------------
 // pooling / up-sampling and their adjoints, conversions
 
-// coarse[P][c] = mean over fine p with floor(p/2) = P
+// coarse[P][c] = mean over fine p with floor(p/2) = P; a thread per coarse point and
+// group of 8 channels (16-byte loads and stores; C is a multiple of 8)
 __global__ void k_pool(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y, const int *skip_flag) {
   if (skip_flag && *skip_flag) return;
-  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < cg.vox * C; P += (long long)gridDim.x * blockDim.x) {
-    const int c = int(P % C);
-    const long long V = P / C;
+  const int CB = C / 8;
+  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < cg.vox * CB; P += (long long)gridDim.x * blockDim.x) {
+    const int cb = int(P % CB);
+    const long long V = P / CB;
     const int K = int(V % cg.n[2]), J = int((V / cg.n[2]) % cg.n[1]), I = int(V / ((long long)cg.n[2] * cg.n[1]));
-    float s = 0.f;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int cnt = 0;
     for (int a = 0; a < 2; ++a)
       for (int b = 0; b < 2; ++b)
@@ -458,10 +647,20 @@ __global__ void k_pool(grid3 f, grid3 cg, int C, const uint16_t *x, uint16_t *y,
           const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + d;
           if (i >= f.n[0] || j >= f.n[1] || k >= f.n[2]) continue;
           if ((f.n[0] == 1 && a) || (f.n[1] == 1 && b) || (f.n[2] == 1 && d)) continue;
-          s += bf2f(x[vindex(f, i, j, k) * C + c]);
+          const uint4 u = *reinterpret_cast<const uint4 *>(x + vindex(f, i, j, k) * C + cb * 8);
+          const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
+            s[2 * h] += bf2f(uint16_t(w[h] & 0xffffu));
+            s[2 * h + 1] += bf2f(uint16_t(w[h] >> 16));
+          }
           ++cnt;
         }
-    y[P] = f2bf(s / float(cnt));
+    unsigned o[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+      o[h] = unsigned(f2bf(s[2 * h] / float(cnt))) | (unsigned(f2bf(s[2 * h + 1] / float(cnt))) << 16);
+    *reinterpret_cast<uint4 *>(y + V * C + cb * 8) = make_uint4(o[0], o[1], o[2], o[3]);
   }
 }
 // fine[p][c] = coarse[floor(p/2)][c]
@@ -693,17 +892,41 @@ grid3 g3(const lvl &l, const int *wrap) {
   return g;
 }
 
-template <int CIN, int COUT, int ND>
-void conv_tc_launch(const grid3 &g, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip, cudaStream_t s) {
-  using TL = tile<ND>;
+template <int ND, int R>
+long long ctile_count(const grid3 &g) {
+  using TL = ctile<ND, R>;
+  return (long long)((g.n[0] + TL::T0 - 1) / TL::T0) * ((g.n[1] + TL::T1 - 1) / TL::T1) * ((g.n[2] + TL::T2 - 1) / TL::T2);
+}
+template <int CIN, int COUT, int ND, bool UP, int R>
+void conv_tc_launch_r(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
+                      cudaStream_t s) {
+  using TL = ctile<ND, R>;
   constexpr int H2 = ND == 3 ? TL::T2 + 2 : 1;
   const size_t smem = size_t(TL::T0 + 2) * (TL::T1 + 2) * H2 * sv<CIN>::v;
-  auto kern = k_conv_tc<CIN, COUT, ND>;
+  auto kern = k_conv_tc<CIN, COUT, ND, UP, R>;
   static bool attr = false;
   if (!attr) { MPDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); attr = true; }
-  const long long nb = (long long)((g.n[0] + TL::T0 - 1) / TL::T0) * ((g.n[1] + TL::T1 - 1) / TL::T1) * ((g.n[2] + TL::T2 - 1) / TL::T2);
-  kern<<<unsigned(nb), 256, smem, s>>>(g, X, reinterpret_cast<const uint2 *>(Wf), o, skip);
+  kern<<<unsigned(ctile_count<ND, R>(g)), 256, smem, s>>>(g, cg, X, reinterpret_cast<const uint2 *>(Wf), o, skip);
   MPDX_LAUNCH_CHECK();
+}
+// four rows per warp where the grid still gives every SM four or more tiles (and
+// the tile fits shared memory comfortably), one row per warp otherwise
+template <int CIN, int COUT, int ND, bool UP>
+void conv_tc_launch2(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
+                     cudaStream_t s) {
+  if constexpr (ND == 3 && CIN <= 32) {
+    if (ctile_count<3, 4>(g) >= 4 * 148) return conv_tc_launch_r<CIN, COUT, ND, UP, 4>(g, cg, X, Wf, o, skip, s);
+  }
+  conv_tc_launch_r<CIN, COUT, ND, UP, 1>(g, cg, X, Wf, o, skip, s);
+}
+template <int CIN, int COUT, int ND>
+void conv_tc_launch(const grid3 &g, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip, cudaStream_t s) {
+  conv_tc_launch2<CIN, COUT, ND, false>(g, g, X, Wf, o, skip, s);
+}
+template <int CIN, int COUT, int ND>
+void conv_tc_up_launch(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
+                       cudaStream_t s) {
+  conv_tc_launch2<CIN, COUT, ND, true>(g, cg, X, Wf, o, skip, s);
 }
 template <int CIN, int COUT, int ND>
 int conv_dw_launch(const grid3 &g, const uint16_t *dY, const uint16_t *X, float *part, size_t part_floats, cudaStream_t s) {
@@ -732,6 +955,16 @@ void conv_tc(int cin, int cout, const grid3 &g, const uint16_t *X, const uint16_
 #undef MPDX_PC_TC
   throw error(MPDX_E_ARG, "unsupported channel pair");
 }
+// the decoder's convolutions of the nearest up-sampling of a coarse tensor (C_in > C_out)
+template <int ND>
+void conv_tc_up(int cin, int cout, const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o,
+                const int *skip, cudaStream_t s) {
+#define MPDX_PC_TCU(A, B) if (cin == A && cout == B) return conv_tc_up_launch<A, B, ND>(g, cg, X, Wf, o, skip, s);
+  MPDX_PC_TCU(16, 8) MPDX_PC_TCU(32, 16) MPDX_PC_TCU(64, 32) MPDX_PC_TCU(64, 64) MPDX_PC_TCU(32, 32) MPDX_PC_TCU(16, 16)
+  MPDX_PC_TCU(32, 8) MPDX_PC_TCU(64, 16) MPDX_PC_TCU(64, 8) MPDX_PC_TCU(8, 8)
+#undef MPDX_PC_TCU
+  throw error(MPDX_E_ARG, "unsupported channel pair");
+}
 template <int ND>
 int conv_dw(int cin, int cout, const grid3 &g, const uint16_t *dY, const uint16_t *X, float *part, size_t pf, cudaStream_t s) {
 #define MPDX_PC_DW(A, B) if (cin == A && cout == B) return conv_dw_launch<A, B, ND>(g, dY, X, part, pf, s);
@@ -753,19 +986,20 @@ static void forward_impl(net &N, const double *rf, long long s0, long long s1, l
   for (int l = 0; l < 4; ++l) G[l] = g3(N.L[l], N.wrap);
   const float *P = N.params;
   const int c0 = N.ch[0];
-  // e0
+  // e0, and the level-1 input pool(e0) in the same pass
   const float *W0 = P + N.w_off[0], *B0 = P + N.b_off[0];
+  const unsigned EB = unsigned(etile_count<ND>(G[0]));
   if (c0 == 8) {
-    if (rf) k_conv_in<8, ND, true><<<gsz(G[0].vox), 256, 0, s>>>(G[0], rf, s0, s1, s2, nullptr, W0, B0, a_e[0], skip);
-    else k_conv_in<8, ND, false><<<gsz(G[0].vox), 256, 0, s>>>(G[0], nullptr, 0, 0, 0, rc, W0, B0, a_e[0], skip);
+    if (rf) k_conv_in<8, ND, true, true><<<EB, kEndThreads, 0, s>>>(G[0], G[1], rf, s0, s1, s2, nullptr, W0, B0, a_e[0], a_p[1], skip);
+    else k_conv_in<8, ND, false, true><<<EB, kEndThreads, 0, s>>>(G[0], G[1], nullptr, 0, 0, 0, rc, W0, B0, a_e[0], a_p[1], skip);
   } else if (c0 == 16) {
-    if (rf) k_conv_in<16, ND, true><<<gsz(G[0].vox), 256, 0, s>>>(G[0], rf, s0, s1, s2, nullptr, W0, B0, a_e[0], skip);
-    else k_conv_in<16, ND, false><<<gsz(G[0].vox), 256, 0, s>>>(G[0], nullptr, 0, 0, 0, rc, W0, B0, a_e[0], skip);
+    if (rf) k_conv_in<16, ND, true, true><<<EB, kEndThreads, 0, s>>>(G[0], G[1], rf, s0, s1, s2, nullptr, W0, B0, a_e[0], a_p[1], skip);
+    else k_conv_in<16, ND, false, true><<<EB, kEndThreads, 0, s>>>(G[0], G[1], nullptr, 0, 0, 0, rc, W0, B0, a_e[0], a_p[1], skip);
   } else throw error(MPDX_E_ARG, "level-0 channels must be 8 or 16");
   MPDX_LAUNCH_CHECK();
   // encoder
   for (int l = 1; l < 4; ++l) {
-    k_pool<<<gsz(G[l].vox * N.ch[l - 1]), 256, 0, s>>>(G[l - 1], G[l], N.ch[l - 1], a_e[l - 1], a_p[l], skip);
+    if (l > 1) k_pool<<<gsz(G[l].vox * N.ch[l - 1] / 8), 256, 0, s>>>(G[l - 1], G[l], N.ch[l - 1], a_e[l - 1], a_p[l], skip);
     conv_tc<ND>(N.cin[l], N.cout[l], G[l], a_p[l], wf[l], conv_out{a_e[l], nullptr, P + N.b_off[l], nullptr}, skip, s);
   }
   conv_tc<ND>(N.cin[4], N.cout[4], G[3], a_e[3], wf[4], conv_out{a_m3, nullptr, P + N.b_off[4], nullptr}, skip, s);
@@ -773,18 +1007,18 @@ static void forward_impl(net &N, const double *rf, long long s0, long long s1, l
   const uint16_t *coarse = a_m3;
   for (int q = 5; q <= 7; ++q) {
     const int l = N.level[q];
-    k_up<<<gsz(G[l].vox * N.cin[q]), 256, 0, s>>>(G[l], G[l + 1], N.cin[q], coarse, a_u[l], skip);
-    conv_tc<ND>(N.cin[q], N.cout[q], G[l], a_u[l], wf[q], conv_out{a_d[l], nullptr, P + N.b_off[q], a_e[l]}, skip, s);
+    // up-sampling read by the convolution's tile load (not written out)
+    conv_tc_up<ND>(N.cin[q], N.cout[q], G[l], G[l + 1], coarse, wf[q], conv_out{a_d[l], nullptr, P + N.b_off[q], a_e[l]}, skip, s);
     coarse = a_d[l];
   }
   MPDX_LAUNCH_CHECK();
   const float *W8 = P + N.w_off[8], *B8 = P + N.b_off[8];
   if (c0 == 8) {
-    if (qf) k_conv_outl<8, ND, true><<<gsz(G[0].vox), 256, 0, s>>>(G[0], a_d[0], W8, B8, qf, s0, s1, s2, nullptr, skip);
-    else k_conv_outl<8, ND, false><<<gsz(G[0].vox), 256, 0, s>>>(G[0], a_d[0], W8, B8, nullptr, 0, 0, 0, qc, skip);
+    if (qf) k_conv_outl<8, ND, true><<<EB, kEndThreads, 0, s>>>(G[0], a_d[0], W8, B8, qf, s0, s1, s2, nullptr, skip);
+    else k_conv_outl<8, ND, false><<<EB, kEndThreads, 0, s>>>(G[0], a_d[0], W8, B8, nullptr, 0, 0, 0, qc, skip);
   } else {
-    if (qf) k_conv_outl<16, ND, true><<<gsz(G[0].vox), 256, 0, s>>>(G[0], a_d[0], W8, B8, qf, s0, s1, s2, nullptr, skip);
-    else k_conv_outl<16, ND, false><<<gsz(G[0].vox), 256, 0, s>>>(G[0], a_d[0], W8, B8, nullptr, 0, 0, 0, qc, skip);
+    if (qf) k_conv_outl<16, ND, true><<<EB, kEndThreads, 0, s>>>(G[0], a_d[0], W8, B8, qf, s0, s1, s2, nullptr, skip);
+    else k_conv_outl<16, ND, false><<<EB, kEndThreads, 0, s>>>(G[0], a_d[0], W8, B8, nullptr, 0, 0, 0, qc, skip);
   }
   MPDX_LAUNCH_CHECK();
 }
@@ -828,6 +1062,9 @@ static void backward_impl(net &N, const float *r, const float *dq, float *gr, ui
   // ---- decoder: layers 7 (level 0), 6 (1), 5 (2); dE[l] holds d(d_l) on entry ----
   for (int q = 7; q >= 5; --q) {
     const int l = N.level[q], ci = N.cin[q], co = N.cout[q];
+    // the forward pass reads the up-sampled input inside its convolution; the weight
+    // gradient needs it written out
+    k_up<<<gsz(G[l].vox * ci), 256, 0, s>>>(G[l], G[l + 1], ci, l == 2 ? a_m3 : a_d[l + 1], a_u[l], nullptr);
     k_to_bf16<<<gsz(G[l].vox * co), 256, 0, s>>>(dE[l], g_h, G[l].vox * co);
     const int gx = conv_dw<ND>(ci, co, G[l], g_h, a_u[l], part, pf, s);
     k_dw_reduce<<<64, 256, 0, s>>>(part, gx, nt, co, ci, gr + N.w_off[q]);

@@ -127,6 +127,7 @@ struct solver_base {
   virtual double precond_train(long long, double, unsigned long long) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual void precond_enable(bool) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual long long precond_pairs() { return 0; }
+  virtual long long precond_directions() { return -1; }
   virtual long long precond_num_params() { return 0; }
   virtual void precond_params(float *, const float *) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual double precond_loss_grad(const double *, const double *, double, float *) {
@@ -340,6 +341,7 @@ struct boussinesq_solver : solver_base {
   void precond_record(long long n) override { b->precond_record(n); }
   double precond_train(long long steps, double lr, unsigned long long seed) override { return b->precond_train(steps, lr, seed); }
   void precond_enable(bool on) override { b->precond_enable(on); }
+  long long precond_directions() override { return b->nl_last < 0 ? -1 : b->nl_cand[b->nl_last]; }
   long long precond_pairs() override { return b->n_pairs; }
   long long precond_num_params() override {
     b->ensure_net();
@@ -363,7 +365,7 @@ struct boussinesq_solver : solver_base {
     out->gcr_iters_total = b->iters_total;
     out->gcr_residual = b->last_residual;
     out->gcr_ms = b->last_solve_ms;
-    out->gcr_fallback = b->fell_back ? 1 : 0;
+    out->gcr_fallback = b->restarted ? 2 : (b->fell_back ? 1 : 0);
     out->path = MPDX_PATH_GENERAL;
   }
 };
@@ -877,6 +879,10 @@ mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t
     const double l = h->impl->precond_train(steps, lr, seed);
     if (final_loss) *final_loss = l;
   });
+}
+
+int64_t mpdx_precond_directions(mpdx_handle h) {
+  return (h && h->impl) ? h->impl->precond_directions() : -1;
 }
 
 mpdx_status mpdx_precond_enable(mpdx_handle h, int on) {
