@@ -366,8 +366,10 @@ def gcr_extra(grid=(256, 256, 128), record=200, train=400, compare=1000):
     Two identical runs advance `record` steps; one records the (residual,
     correction) pairs of its solves (their start and iterations 16/32/64), which
     train the learned preconditioner.  Then both advance `compare` more steps, one
-    with plain GCR and one with the learned preconditioner: iterations and device
-    time per solve, averaged over the solves."""
+    with plain GCR and one with the learned preconditioner (one learned
+    correction at the start of each solve, then plain GCR): iterations (the
+    learned correction included) and device time per solve, averaged over the
+    solves."""
     import numpy as np
     from libmpdataxx_b200 import setups
     s = setups.boussinesq_bubble_3d(*grid)

@@ -228,7 +228,7 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
  * mpdx_precond_record keeps (residual, correction Phi_end - Phi) pairs of the
  * next pressure solves on the device (the start and iterations 16, 32, 64 of
  * each, up to max_pairs); mpdx_precond_train runs `steps` Adam steps (linear
- * warm-up, cosine decay to 1 % of lr) on the energy-norm loss of
+ * warm-up, cosine decay to 1 % of lr) on the energy loss of
  * mpdx_precond_loss_grad over randomly drawn pairs, the last fifth of the pairs
  * (at most 8) held out, and keeps the weights with the lowest held-out loss seen (never
  * worse than the weights it started from); *final_loss is that held-out loss
@@ -236,8 +236,11 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
  * with nl learned corrections, Phi += beta q along q = net(err) with the step
  * beta = -<err, q> / <q, lap q> that minimises the error in the operator's energy
  * norm (the training norm), and continues with plain GCR from the iterate they
- * reach; nl in {1, 2, 4, 0} is chosen by the measured device times of earlier
- * solves (each tried twice, then the fastest, one re-measured every 64 solves).
+ * reach.  nl = 1 unless mpdx_precond_set_directions sets another count (0..64)
+ * or -1, which chooses nl in {1, 2, 4, 0} by the measured device times of
+ * earlier solves (each tried twice, then the fastest, one re-measured every 64
+ * solves; a choice by single solves, which does not see that the learned
+ * corrections also make the next solves start closer to their solution).
  * The stopping test (max|err| <= prs_tol / dt) is unchanged: only the iteration
  * count and time change.  mpdx_precond_directions gives the nl of the last
  * learned solve (-1 before the first).  Weights are exchanged in the mpdx_pcnet
@@ -245,6 +248,7 @@ void mpdx_batch_destroy(mpdx_batch_handle b);
 mpdx_status mpdx_precond_record(mpdx_handle h, int64_t max_pairs);
 mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t seed, double *final_loss);
 mpdx_status mpdx_precond_enable(mpdx_handle h, int on);
+mpdx_status mpdx_precond_set_directions(mpdx_handle h, int64_t nl);
 int64_t mpdx_precond_directions(mpdx_handle h);
 int64_t mpdx_precond_pairs(mpdx_handle h);
 int64_t mpdx_precond_num_params(mpdx_handle h);
@@ -253,9 +257,13 @@ mpdx_status mpdx_precond_set_params(mpdx_handle h, const float *host);
 /* The training loss for one pair given by the caller (no counterpart in the
  * reference): residual r and correction t (interior, C order, FP64 on the host;
  * A t = -r for the solve's operator A), network output q = net(r) scaled by c:
- * *loss = e^T (-A) e / (t^T (-A) t) with e = c q - t (1 for a zero output), and
- * its gradient with respect to the network parameters into grad (host,
- * mpdx_precond_num_params floats; NULL for the loss alone). */
+ * *loss = sum_d |G_d e| ^2 / sum_d |G_d t|^2 with e = c q - t and G_d the pressure
+ * solve's centred gradient along axis d (pressure halo rules, zero on a rigid
+ * wall): the error's energy, which for cyclic axes is e^T (-A) e, and which with
+ * rigid walls (where -A is not symmetric and its quadratic form can be negative)
+ * stays non-negative; 1 for a zero output.  Its gradient with respect to the
+ * network parameters goes into grad (host, mpdx_precond_num_params floats; NULL
+ * for the loss alone). */
 mpdx_status mpdx_precond_loss_grad(mpdx_handle h, const double *r, const double *t, double c, double *loss, float *grad);
 
 /* ---- Learned GCR preconditioner network on its own ----

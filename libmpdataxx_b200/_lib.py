@@ -33,7 +33,7 @@ EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_fie
            "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
            "mpdx_pcnet_get_params", "mpdx_pcnet_forward", "mpdx_pcnet_backward", "mpdx_pcnet_train_step",
            "mpdx_pcnet_last_error", "mpdx_pcnet_destroy", "mpdx_precond_record", "mpdx_precond_train",
-           "mpdx_precond_enable", "mpdx_precond_directions", "mpdx_precond_pairs", "mpdx_precond_num_params", "mpdx_precond_get_params",
+           "mpdx_precond_enable", "mpdx_precond_directions", "mpdx_precond_set_directions", "mpdx_precond_pairs", "mpdx_precond_num_params", "mpdx_precond_get_params",
            "mpdx_precond_set_params", "mpdx_precond_loss_grad"]
 BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 
@@ -137,6 +137,8 @@ def lib():
     L.mpdx_precond_train.restype = ctypes.c_int
     L.mpdx_precond_enable.argtypes = [vp, ctypes.c_int]
     L.mpdx_precond_enable.restype = ctypes.c_int
+    L.mpdx_precond_set_directions.argtypes = [vp, ctypes.c_int64]
+    L.mpdx_precond_set_directions.restype = ctypes.c_int
     L.mpdx_precond_directions.argtypes = [vp]
     L.mpdx_precond_directions.restype = ctypes.c_int64
     L.mpdx_precond_pairs.argtypes = [vp]

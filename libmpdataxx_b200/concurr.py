@@ -203,6 +203,10 @@ class cuda:
         """Keep the (initial residual, correction) pair of each of the next max_pairs pressure solves."""
         _check(self.L, self.h, self.L.mpdx_precond_record(self.h, int(max_pairs)))
 
+    def precond_set_directions(self, nl):
+        """Learned corrections at the start of every learned solve: 0..64 (1 by default), or -1 to tune them by solve time."""
+        _check(self.L, self.h, self.L.mpdx_precond_set_directions(self.h, int(nl)))
+
     def precond_directions(self):
         """Learned search directions at the start of the last learned solve (-1: none yet)."""
         return int(self.L.mpdx_precond_directions(self.h))

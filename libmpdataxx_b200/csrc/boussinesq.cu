@@ -723,6 +723,20 @@ void launch_inner(int v, unsigned G, dim3 blk, cudaStream_t s, const geom &g, in
 // iterations that follow is the reference's.  The error is updated in place (no
 // stencil reads it in the same kernel).
 
+// q(n-1) = q(0) along every cyclic axis (in axis order, as a halo fill would):
+// the network pads a cyclic axis with period n, while point n-1 of the
+// reference's cyclic convention duplicates point 0; a correction without the
+// duplicate would make Phi, and the projected velocity, differ across the seam
+template <class T>
+__global__ void k_seam_dup(geom g, dfield<T> q, int d) {
+  for_interior(g, [&](int i, int j, int k) {
+    const int c[3] = {i, j, k};
+    if (c[d] != g.n[d] - 1) return;
+    const long long o = off3(q, i, j, k);
+    q.o[o] = q.o[o - (long long)(g.n[d] - 1) * stride(q, d)];
+  });
+}
+
 // A learned correction: q = M(err) (written into p0 by the network), lap_q =
 // lap(q), and the sums of the step length that minimises the error in the energy
 // norm of the operator (the norm the network is trained in):
@@ -757,7 +771,9 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update_pc(geom g, T err_
   // a direction from the network whose sums are not finite (an overflowing or NaN
   // output) must not touch Phi or err: every block sees the same sums and returns,
   // and the host continues with plain GCR from the iterate as it stands
-  if (!isfinite(double(den)) || !isfinite(double(b))) {
+  // (a correction along q needs <q, lap q> < 0: lap is negative on every direction
+  // it does not annihilate)
+  if (!isfinite(double(den)) || !isfinite(double(b)) || !(den < T(0))) {
     if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) dv->bad = 1;
     return;
   }
@@ -809,14 +825,6 @@ template <class T>
 __global__ void k_copy_field(geom g, dfield<T> src, dfield<T> dst) {
   for_interior(g, [&](int i, int j, int k) { dst(i, j, k) = src(i, j, k); });
 }
-// pair normalisation: s = max|r|, then r / s and t / s
-__global__ void k_absmax(const float *x, long long n, float *s) {
-  float m = 0.f;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    m = fmaxf(m, fabsf(x[q]));
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned *>(s), __float_as_uint(m));  // non-negative floats order as their bits
-}
 // e = c q - t of the training loss
 __global__ void k_sub(const float *a, float ca, const float *b, long long n, float *o) {  // o = ca * a - b
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) o[q] = ca * a[q] - b[q];
@@ -837,69 +845,67 @@ __global__ void k_scale_rms(const float *r, const float *t, long long n, const d
     to[q] = t[q] * inv;
   }
 }
-__global__ void __launch_bounds__(kRedThreads, 4) k_lap_compact(geom g, const float *x, float *out, double *loss, float scale_out) {
-  const dfield<float> lay{const_cast<float *>(x), (long long)g.n[1] * g.n[2], g.n[2], g.nd == 3 ? 1 : 0};
-  double sq = 0.0;
-  for_interior(g, [&](int i, int j, int k) {
-    const float z = lap<float>(fld<float>{x}, lay, no_u{}, g, i, j, k);
-    out[off3(lay, i, j, k)] = scale_out * z;
-    sq += double(z) * double(z);
-  });
-  if (loss) {
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-    if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0) atomicAdd(loss, sq / double(g.cells));
-  }
+
+// centred gradient of a compact FP32 array along axis d at point c (the pressure
+// solve's lap_tmp: (x(c+1) - x(c-1)) / 2 dx, neighbours under the halo rule, zero
+// on a rigid wall)
+__device__ __forceinline__ float grad_c(const geom &g, const dfield<float> &lay, const float *x, int d, const int *c) {
+  if (rigid_edge(g, d, c[d])) return 0.f;
+  const long long o = off3(lay, c[0], c[1], c[2]), sd = stride(lay, d), base = o - c[d] * sd;
+  const fld<float> A{x};
+  return (aval<float>(A, g, d, base, sd, c[d] + 1) - aval<float>(A, g, d, base, sd, c[d] - 1)) * (0.5f * g.rdxf[d]);
 }
-// Adjoint of lap() on compact arrays.  lap() is a sum of one-dimensional
-// operators, one per axis, each acting along the lines of its axis; with rigid
-// walls they are not symmetric.  adj_tab holds, per axis, the rows of the
-// transposed one-dimensional matrix (kAdjW column/value pairs per point, column
-// -1 for an unused slot), built on the host from the same halo and wall rules.
-constexpr int kAdjW = 8;
-struct adj_tab {
-  const int *col[3];
-  const float *val[3];
-};
-__global__ void __launch_bounds__(kRedThreads, 4) k_lap_adj_compact(geom g, adj_tab A, const float *x, float *out) {
-  const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+// gd[d] = G_d x for each axis (where gd[d] is not null), *sum += sum_d |G_d x|^2
+__global__ void __launch_bounds__(kRedThreads, 4) k_grad_sq(geom g, const float *x, float *g0, float *g1, float *g2,
+                                                           double *sum) {
+  const dfield<float> lay{const_cast<float *>(x), (long long)g.n[1] * g.n[2], g.n[2], g.nd == 3 ? 1 : 0};
+  float *gd[3] = {g0, g1, g2};
+  double sq = 0.0;
   for_interior(g, [&](int i, int j, int k) {
     const int c[3] = {i, j, k};
-    const long long st[3] = {g.nd == 3 ? s0 : (long long)g.n[1], g.nd == 3 ? s1 : 1, 1};
-    const long long o = g.nd == 3 ? i * s0 + j * s1 + k : (long long)i * g.n[1] + j;
+    const long long o = off3(lay, i, j, k);
+    for (int d = 0; d < g.nd; ++d) {
+      const float v = grad_c(g, lay, x, d, c);
+      if (gd[d]) gd[d][o] = v;
+      sq += double(v) * double(v);
+    }
+  });
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0) atomicAdd(sum, sq);
+}
+// out = f * sum_d G_d^T y_d, f = 2 c / (*den): the gradient of sum_d |G_d e|^2 / den
+// with respect to q for e = c q - t.  G_d^T gathers the rows that read point m:
+// cyclic (period n - 1): y(m-1) [m >= 1] + y(n-1) [m = 1] - y(m+1) [m <= n-2] - y(0) [m = n-2];
+// rigid (rows 0 and n-1 zero): y(m-1) [1 <= m-1 <= n-2] - y(m+1) [1 <= m+1 <= n-2]
+__global__ void __launch_bounds__(kRedThreads, 4) k_grad_adj(geom g, const float *y0, const float *y1, const float *y2,
+                                                            const double *den, float c, float *out) {
+  const dfield<float> lay{out, (long long)g.n[1] * g.n[2], g.n[2], g.nd == 3 ? 1 : 0};
+  const float *yd[3] = {y0, y1, y2};
+  const float f = *den > 0.0 ? float(2.0 * double(c) / *den) : 0.f;
+  for_interior(g, [&](int i, int j, int k) {
+    const int c3[3] = {i, j, k};
+    const long long o = off3(lay, i, j, k);
     float acc = 0.f;
     for (int d = 0; d < g.nd; ++d) {
-      const int *cl = A.col[d] + (long long)c[d] * kAdjW;
-      const float *vl = A.val[d] + (long long)c[d] * kAdjW;
-      const long long base = o - (long long)c[d] * st[d];
-#pragma unroll
-      for (int w = 0; w < kAdjW; ++w)
-        if (cl[w] >= 0) acc += vl[w] * x[base + (long long)cl[w] * st[d]];
+      const int m = c3[d], n = g.n[d];
+      const long long sd = stride(lay, d), base = o - m * sd;
+      const float *y = yd[d];
+      float v = 0.f;
+      if (g.bc[d][0] == MPDX_BC_CYCLIC) {
+        if (m >= 1) v += y[base + (m - 1) * sd];
+        if (m == 1) v += y[base + (n - 1) * sd];
+        if (m <= n - 2) v -= y[base + (m + 1) * sd];
+        if (m == n - 2) v -= y[base];
+      } else {
+        if (m - 1 >= 1 && m - 1 <= n - 2) v += y[base + (m - 1) * sd];
+        if (m + 1 >= 1 && m + 1 <= n - 2) v -= y[base + (m + 1) * sd];
+      }
+      acc += v * (0.5f * g.rdxf[d]);
     }
-    out[o] = acc;
+    out[o] = f * acc;
   });
 }
-__global__ void k_neg2(const double *a, double *b) { *b = -*a; }
-__global__ void k_dot(const float *a, const float *b, long long n, double *out) {
-  double sq = 0.0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    sq += double(a[q]) * double(b[q]);
-  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, sq);
-}
-// gradient of the energy loss E = e^T (-A) e / den, den = *dn (-t^T A t), with
-// respect to q for e = c q - t: dq = -c (A e + A^T e) / den
-__global__ void k_energy_dq(const float *ae, const float *ate, long long n, const double *dn, float c, float *dq) {
-  const float f = *dn > 0.0 ? float(-double(c) / *dn) : 0.f;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    dq[q] = f * (ae[q] + ate[q]);
-}
-__global__ void k_scale2(const float *r, const float *t, long long n, const float *s, float *ro, float *to) {
-  const float inv = *s > 0.f ? 1.f / *s : 1.f;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    ro[q] = r[q] * inv;
-    to[q] = t[q] * inv;
-  }
-}
+
 
 // ---------------------------------------------------------------------------
 // pointwise stages
@@ -1205,7 +1211,6 @@ boussinesq<T, P>::~boussinesq() {
   if (scratch) cudaFree(scratch);
   if (vip_dev) cudaFree(vip_dev);
   for (float *p : {pairs, tr_r, tr_t, tr_q, tr_z, tr_dq, tr_a, tr_b}) if (p) cudaFree(p);
-  for (int d = 0; d < 3; ++d) { if (adj_col[d]) cudaFree(adj_col[d]); if (adj_val[d]) cudaFree(adj_val[d]); }
   if (tr_loss) cudaFree(tr_loss);
   for (cudaEvent_t e : ev_solve) if (e) cudaEventDestroy(e);
 }
@@ -1240,8 +1245,8 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
   bq::k_err_init<P, T><<<G, kBlk, 0, s>>>(gm, Phi.v, u, err[0].v);
   if (rec) bq::k_to_compact<P><<<G, kBlk, 0, s>>>(gm, err[0].v, dfield<P>{}, pairs + size_t(rec_slots[0]) * 2 * gm.cells);
   const bool learned = use_net && net;
-  const int nl_idx = learned ? pick_nl() : -1;
-  const long long nl = learned ? nl_cand[nl_idx] : 0;
+  const int nl_idx = learned && nl_fixed < 0 ? pick_nl() : -1;
+  const long long nl = !learned ? 0 : (nl_fixed >= 0 ? nl_fixed : nl_cand[nl_idx]);
   bool pcnd = learned && nl > 0;
   fell_back = false;
   restarted = false;
@@ -1255,6 +1260,8 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
       for (long long l = 0; l < nl; ++l) {
         const auto &e = err[0].v;
         net->forward_field(e.o, e.s0, e.s1, e.s2, nullptr, p_err[0].v.o, &dev->converged);
+        for (int d = 0; d < st.nd; ++d)
+          if (gm.bc[d][0] == MPDX_BC_CYCLIC) bq::k_seam_dup<P><<<G, kBlk, 0, s>>>(gm, p_err[0].v, d);
         bq::k_gcr_init_pc<P><<<G, kBlk, 0, s>>>(gm, err[0].v, p_err[0].v, lap_p_err[0].v, dev, part);
         bq::launch_pc_update<P, 1>(G, kBlk, s, gm, err_tol, Phi.v, err[0].v, D, dev, part);
       }
@@ -1319,9 +1326,11 @@ void boussinesq<T, P>::pressure_solve(bool simple) {
   iters = hdev->iters + learned_steps + discarded;
   iters_total += iters;
   if (learned) {
-    nl_ms[nl_idx] = nl_tries[nl_idx] == 0 ? last_solve_ms : 0.5 * (nl_ms[nl_idx] + last_solve_ms);
-    ++nl_tries[nl_idx];
-    nl_last = nl_idx;
+    if (nl_idx >= 0) {
+      nl_ms[nl_idx] = nl_tries[nl_idx] == 0 ? last_solve_ms : 0.5 * (nl_ms[nl_idx] + last_solve_ms);
+      ++nl_tries[nl_idx];
+    }
+    nl_used = nl;
     ++n_learned;
   }
   if (!(use_net && net)) { last_plain_iters = iters; last_plain_ms = last_solve_ms; }
@@ -1365,40 +1374,6 @@ void boussinesq<T, P>::precond_record(long long n) {
   }
 }
 
-// The one-dimensional matrix of lap() along an axis of n points (pressure halo
-// rules: cyclic period n - 1, rigid 2 x(edge) - x(mirror); the gradient is zero at
-// a rigid wall point), built by applying the rule to unit vectors, transposed and
-// stored as kAdjW (column, value) pairs per row.
-static void lap1d_adj_rows(int n, bool rlo, bool rhi, double dx, std::vector<int> &col, std::vector<float> &val) {
-  auto src = [&](int q, int &a, int &b) {
-    a = q; b = -1;
-    if (q >= 0 && q < n) return;
-    if (q < 0) { if (rlo) { a = 0; b = -q; } else a = q + n - 1; }
-    else { if (rhi) { a = n - 1; b = 2 * (n - 1) - q; } else a = q - (n - 1); }
-  };
-  std::vector<double> M(size_t(n) * n, 0.0), e(n, 0.0);
-  auto aval = [&](int q) { int a, b; src(q, a, b); return b < 0 ? e[a] : 2 * e[a] - e[b]; };
-  auto lt = [&](int q) { if ((q == 0 && rlo) || (q == n - 1 && rhi)) return 0.0; return (aval(q + 1) - aval(q - 1)) / dx / 2; };
-  auto LT = [&](int q) { int a, b; src(q, a, b); return b < 0 ? lt(a) : 2 * lt(a) - lt(b); };
-  for (int j = 0; j < n; ++j) {
-    e.assign(n, 0.0);
-    e[j] = 1.0;
-    for (int i = 0; i < n; ++i) M[size_t(i) * n + j] = (LT(i + 1) - LT(i - 1)) / dx / 2;
-  }
-  col.assign(size_t(n) * bq::kAdjW, -1);
-  val.assign(size_t(n) * bq::kAdjW, 0.f);
-  for (int i = 0; i < n; ++i) {  // row i of M^T = column i of M
-    int w = 0;
-    for (int j = 0; j < n; ++j) {
-      const double v = M[size_t(j) * n + i];
-      if (v == 0.0) continue;
-      if (w == bq::kAdjW) throw error(MPDX_E_UNSUPPORTED, "pressure operator row wider than the adjoint table");
-      col[size_t(i) * bq::kAdjW + w] = j;
-      val[size_t(i) * bq::kAdjW + w] = float(v);
-      ++w;
-    }
-  }
-}
 
 template <class T, class P>
 void boussinesq<T, P>::ensure_training() {
@@ -1407,17 +1382,7 @@ void boussinesq<T, P>::ensure_training() {
     for (float **b : {&tr_r, &tr_t, &tr_q, &tr_z, &tr_dq, &tr_a, &tr_b}) MPDX_CUDA(cudaMalloc(b, vox * sizeof(float)));
     MPDX_CUDA(cudaMalloc(&tr_loss, 4 * sizeof(double)));
   }
-  if (!adj_col[0]) {
-    for (int d = 0; d < st.nd; ++d) {
-      std::vector<int> c;
-      std::vector<float> v;
-      lap1d_adj_rows(st.n[d], st.bcs[d][0] == MPDX_BC_RIGID, st.bcs[d][1] == MPDX_BC_RIGID, dijk[d], c, v);
-      MPDX_CUDA(cudaMalloc(&adj_col[d], c.size() * sizeof(int)));
-      MPDX_CUDA(cudaMalloc(&adj_val[d], v.size() * sizeof(float)));
-      MPDX_CUDA(cudaMemcpy(adj_col[d], c.data(), c.size() * sizeof(int), cudaMemcpyHostToDevice));
-      MPDX_CUDA(cudaMemcpy(adj_val[d], v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
-  }
+
 }
 
 // Energy-norm loss of one pair (r, t) held in tr_r / tr_t: q = net(r), e = c q - t,
@@ -1430,26 +1395,21 @@ double boussinesq<T, P>::pair_energy(float c, bool grad) {
   cudaStream_t s = st.stream;
   const long long vox = st.cells();
   net->forward_compact(tr_r, tr_q);
-  bq::k_sub<<<1184, 256, 0, s>>>(tr_q, c, tr_t, vox, tr_z);                 // e
-  bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_z, tr_dq, nullptr, 1.f);       // A e
-  bq::k_lap_compact<<<G, kBlk, 0, s>>>(gm, tr_t, tr_a, nullptr, 1.f);        // A t
+  bq::k_sub<<<1184, 256, 0, s>>>(tr_q, c, tr_t, vox, tr_z);                 // e = c q - t
   MPDX_CUDA(cudaMemsetAsync(tr_loss, 0, 2 * sizeof(double), s));
-  bq::k_dot<<<296, 256, 0, s>>>(tr_z, tr_dq, vox, tr_loss);                  // e^T A e
-  bq::k_dot<<<296, 256, 0, s>>>(tr_t, tr_a, vox, tr_loss + 1);               // t^T A t
+  // |grad e|^2 and |grad t|^2 (the gradients of e kept for the adjoint)
+  bq::k_grad_sq<<<G, kBlk, 0, s>>>(gm, tr_z, tr_dq, st.nd > 1 ? tr_a : nullptr, st.nd > 2 ? tr_b : nullptr, tr_loss);
+  bq::k_grad_sq<<<G, kBlk, 0, s>>>(gm, tr_t, nullptr, nullptr, nullptr, tr_loss + 1);
   if (grad) {
-    bq::adj_tab A;
-    for (int d = 0; d < 3; ++d) { A.col[d] = adj_col[d < st.nd ? d : 0]; A.val[d] = adj_val[d < st.nd ? d : 0]; }
-    bq::k_lap_adj_compact<<<G, kBlk, 0, s>>>(gm, A, tr_z, tr_b);             // A^T e
-    bq::k_neg2<<<1, 1, 0, s>>>(tr_loss + 1, tr_loss + 2);                    // -t^T A t
-    bq::k_energy_dq<<<1184, 256, 0, s>>>(tr_dq, tr_b, vox, tr_loss + 2, c, tr_a);
+    bq::k_grad_adj<<<G, kBlk, 0, s>>>(gm, tr_dq, tr_a, tr_b, tr_loss + 1, c, tr_q);  // dL/dq
     MPDX_LAUNCH_CHECK();
-    net->backward(tr_r, tr_a, net->grad);
+    net->backward(tr_r, tr_q, net->grad);
   }
   MPDX_LAUNCH_CHECK();
   double h[2];
   MPDX_CUDA(cudaMemcpyAsync(h, tr_loss, sizeof(h), cudaMemcpyDeviceToHost, s));
   MPDX_CUDA(cudaStreamSynchronize(s));
-  return h[1] < 0.0 ? h[0] / h[1] : 1.0;  // (-e^T A e) / (-t^T A t)
+  return h[1] > 0.0 ? h[0] / h[1] : 1.0;  // |grad e|^2 / |grad t|^2
 }
 
 // pair k of the recorded ones, divided by rms(r), into tr_r / tr_t (the loss does not

@@ -76,8 +76,6 @@ struct boussinesq {
   float *tr_a = nullptr, *tr_b = nullptr;
   double out_scale = 0, last_train_loss = -1;
   double *tr_loss = nullptr;
-  int *adj_col[3] = {nullptr, nullptr, nullptr};  // adjoint of the pressure operator, per axis
-  float *adj_val[3] = {nullptr, nullptr, nullptr};
   long long last_plain_iters = 250;
   float last_plain_ms = 0;  // device time of the last plain solve (0: none yet)
   bool fell_back = false;
@@ -88,7 +86,8 @@ struct boussinesq {
   int nl_cand[kNlCand] = {1, 2, 4, 0};
   double nl_ms[kNlCand] = {0, 0, 0, 0};
   int nl_tries[kNlCand] = {0, 0, 0, 0};
-  int nl_last = -1;          // candidate index of the last learned solve
+  int nl_fixed = 1;          // >= 0: every learned solve takes this many learned corrections; -1: tuned
+  long long nl_used = -1;    // learned corrections of the last learned solve
   long long n_learned = 0;   // learned solves so far
   int pick_nl();
   long long max_pairs = 0, n_pairs = 0;

@@ -110,15 +110,21 @@ struct conv_out {
 };
 
 // X: [vox][CIN] BF16 on grid g; Wf: fragments [chunk][COUT/8][32] x uint2.
-// UP: X lives on the coarse grid cg and the input is its nearest up-sampling,
-// X(p) = X_coarse(floor(p / 2)) (k_up), read straight into the halo tile
-template <int CIN, int COUT, int ND, bool UP, int R>
+// UP = 1: X lives on the coarse grid cg and the input is its nearest up-sampling,
+// X(p) = X_coarse(floor(p / 2)) (k_up), read straight into the halo tile.
+// UP = 2: the same for a fine grid of even sides (padding and wrapping then agree
+// between the fine and the coarse grid): the CTA stages the coarse points its halo
+// tile covers, (T/2 + 2) per axis, and each lane's ldmatrix row points at the
+// coarse point of its fine point.
+template <int CIN, int COUT, int ND, int UP, int R>
 __global__ void __launch_bounds__(256) k_conv_tc(grid3 g, grid3 cg, const uint16_t *__restrict__ X, const uint2 *__restrict__ Wf,
                                                  conv_out o, const int *skip_flag) {
   if (skip_flag && *skip_flag) return;
   using TL = ctile<ND, R>;
   constexpr int T0 = TL::T0, T1 = TL::T1, T2 = TL::T2;
-  constexpr int H0 = T0 + 2, H1 = T1 + 2, H2 = ND == 3 ? T2 + 2 : 1;
+  constexpr bool CO = UP == 2;  // coarse staging
+  constexpr int H0 = CO ? T0 / 2 + 2 : T0 + 2, H1 = CO ? T1 / 2 + 2 : T1 + 2;
+  constexpr int H2 = ND == 3 ? (CO ? T2 / 2 + 2 : T2 + 2) : 1;
   constexpr int CB = CIN / 8, SV = sv<CIN>::v, NTAPS = ND == 3 ? 27 : 9;
   constexpr int NG = NTAPS * CB, NCH = (NG + 1) / 2, NT = COUT / 8;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -131,7 +137,10 @@ __global__ void __launch_bounds__(256) k_conv_tc(grid3 g, grid3 cg, const uint16
     const int hv = q / CB, cb = q % CB;
     const int hk = hv % H2, hj = (hv / H2) % H1, hi = hv / (H2 * H1);
     long long v;
-    if constexpr (UP) {
+    if constexpr (CO) {
+      // coarse coordinates i0/2 - 1 + hi (i0 even), padded on the coarse grid
+      v = nbr(cg, i0 / 2 - 1 + hi, j0 / 2 - 1 + hj, ND == 3 ? k0 / 2 - 1 + hk : 0, 0, 0, 0);
+    } else if constexpr (UP == 1) {
       const int x = padx(i0 - 1 + hi, g.n[0], g.wrap[0]), y = padx(j0 - 1 + hj, g.n[1], g.wrap[1]);
       const int z = ND == 3 ? padx(k0 - 1 + hk, g.n[2], g.wrap[2]) : 0;
       v = (x < 0 || y < 0 || z < 0) ? -1
@@ -180,8 +189,13 @@ __global__ void __launch_bounds__(256) k_conv_tc(grid3 g, grid3 cg, const uint16
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
       int hv;
-      if (ND == 3) hv = ((ti[rr] + 1 + a) * H1 + (tj[rr] + 1 + b)) * H2 + (lm + 1 + c);
-      else hv = (ti[rr] + 1 + a) * H1 + (lm + 1 + b);
+      if constexpr (CO) {  // fine tile coordinate f in [-1, T] -> staged coarse row (f + 2) / 2
+        if (ND == 3) hv = (((ti[rr] + a + 2) >> 1) * H1 + ((tj[rr] + b + 2) >> 1)) * H2 + ((lm + c + 2) >> 1);
+        else hv = ((ti[rr] + a + 2) >> 1) * H1 + ((lm + b + 2) >> 1);
+      } else {
+        if (ND == 3) hv = ((ti[rr] + 1 + a) * H1 + (tj[rr] + 1 + b)) * H2 + (lm + 1 + c);
+        else hv = (ti[rr] + 1 + a) * H1 + (lm + 1 + b);
+      }
       unsigned af[4];
       asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                    : "=r"(af[0]), "=r"(af[1]), "=r"(af[2]), "=r"(af[3])
@@ -897,12 +911,14 @@ long long ctile_count(const grid3 &g) {
   using TL = ctile<ND, R>;
   return (long long)((g.n[0] + TL::T0 - 1) / TL::T0) * ((g.n[1] + TL::T1 - 1) / TL::T1) * ((g.n[2] + TL::T2 - 1) / TL::T2);
 }
-template <int CIN, int COUT, int ND, bool UP, int R>
+template <int CIN, int COUT, int ND, int UP, int R>
 void conv_tc_launch_r(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
                       cudaStream_t s) {
   using TL = ctile<ND, R>;
-  constexpr int H2 = ND == 3 ? TL::T2 + 2 : 1;
-  const size_t smem = size_t(TL::T0 + 2) * (TL::T1 + 2) * H2 * sv<CIN>::v;
+  constexpr bool CO = UP == 2;
+  constexpr int H0 = CO ? TL::T0 / 2 + 2 : TL::T0 + 2, H1 = CO ? TL::T1 / 2 + 2 : TL::T1 + 2;
+  constexpr int H2 = ND == 3 ? (CO ? TL::T2 / 2 + 2 : TL::T2 + 2) : 1;
+  const size_t smem = size_t(H0) * H1 * H2 * sv<CIN>::v;
   auto kern = k_conv_tc<CIN, COUT, ND, UP, R>;
   static bool attr = false;
   if (!attr) { MPDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); attr = true; }
@@ -911,13 +927,27 @@ void conv_tc_launch_r(const grid3 &g, const grid3 &cg, const uint16_t *X, const 
 }
 // four rows per warp where the grid still gives every SM four or more tiles (and
 // the tile fits shared memory comfortably), one row per warp otherwise
-template <int CIN, int COUT, int ND, bool UP>
-void conv_tc_launch2(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
+template <int CIN, int COUT, int ND, int UP>
+void conv_tc_launch3(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
                      cudaStream_t s) {
   if constexpr (ND == 3 && CIN <= 32) {
     if (ctile_count<3, 4>(g) >= 4 * 148) return conv_tc_launch_r<CIN, COUT, ND, UP, 4>(g, cg, X, Wf, o, skip, s);
   }
   conv_tc_launch_r<CIN, COUT, ND, UP, 1>(g, cg, X, Wf, o, skip, s);
+}
+// the coarse staging of the up-sampled input where every axis of the fine grid
+// has an even number of points (or one point)
+template <int CIN, int COUT, int ND, bool UP>
+void conv_tc_launch2(const grid3 &g, const grid3 &cg, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip,
+                     cudaStream_t s) {
+  if constexpr (!UP) {
+    conv_tc_launch3<CIN, COUT, ND, 0>(g, cg, X, Wf, o, skip, s);
+  } else {
+    bool even = true;
+    for (int d = 0; d < ND; ++d) even = even && (g.n[d] % 2 == 0) && cg.n[d] * 2 == g.n[d];
+    if (even) conv_tc_launch3<CIN, COUT, ND, 2>(g, cg, X, Wf, o, skip, s);
+    else conv_tc_launch3<CIN, COUT, ND, 1>(g, cg, X, Wf, o, skip, s);
+  }
 }
 template <int CIN, int COUT, int ND>
 void conv_tc_launch(const grid3 &g, const uint16_t *X, const uint16_t *Wf, conv_out o, const int *skip, cudaStream_t s) {

@@ -128,6 +128,7 @@ struct solver_base {
   virtual void precond_enable(bool) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual long long precond_pairs() { return 0; }
   virtual long long precond_directions() { return -1; }
+  virtual void precond_set_directions(long long) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual long long precond_num_params() { return 0; }
   virtual void precond_params(float *, const float *) { throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver"); }
   virtual double precond_loss_grad(const double *, const double *, double, float *) {
@@ -341,7 +342,11 @@ struct boussinesq_solver : solver_base {
   void precond_record(long long n) override { b->precond_record(n); }
   double precond_train(long long steps, double lr, unsigned long long seed) override { return b->precond_train(steps, lr, seed); }
   void precond_enable(bool on) override { b->precond_enable(on); }
-  long long precond_directions() override { return b->nl_last < 0 ? -1 : b->nl_cand[b->nl_last]; }
+  long long precond_directions() override { return b->nl_used; }
+  void precond_set_directions(long long nl) override {
+    if (nl < -1 || nl > 64) throw error(MPDX_E_ARG, "learned corrections per solve must be -1 (tuned) or 0..64");
+    b->nl_fixed = int(nl);
+  }
   long long precond_pairs() override { return b->n_pairs; }
   long long precond_num_params() override {
     b->ensure_net();
@@ -879,6 +884,10 @@ mpdx_status mpdx_precond_train(mpdx_handle h, int64_t steps, double lr, uint64_t
     const double l = h->impl->precond_train(steps, lr, seed);
     if (final_loss) *final_loss = l;
   });
+}
+
+mpdx_status mpdx_precond_set_directions(mpdx_handle h, int64_t nl) {
+  return guarded(h, [&] { h->impl->precond_set_directions(nl); });
 }
 
 int64_t mpdx_precond_directions(mpdx_handle h) {

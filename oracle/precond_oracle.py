@@ -251,15 +251,43 @@ def pressure_lap_adj(x, bcs, dx):
     return _apply_axes(x, [lap1d_matrix(n, lo, hi, h).T for n, (lo, hi), h in zip(x.shape, bcs, dx)])
 
 
+def grad1d_matrix(n, rigid_lo, rigid_hi, dx):
+    """Matrix of the centred gradient of the pressure solve along a line of n points
+    (lap_tmp of mpdata_rhs_vip_prs_common.hpp:49-84 before the divergence: pressure
+    halo rule for the neighbours, zero on a rigid wall point)."""
+    M = np.zeros((n, n))
+
+    def aval(x, q):
+        a, b = _pres_src(q, n, rigid_lo, rigid_hi)
+        return x[a] if b < 0 else 2 * x[a] - x[b]
+
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        for i in range(n):
+            if (i == 0 and rigid_lo) or (i == n - 1 and rigid_hi):
+                continue
+            M[i, j] = (aval(e, i + 1) - aval(e, i - 1)) / dx / 2
+    return M
+
+
+def _along(M, x, ax):
+    return np.moveaxis(np.tensordot(M, np.moveaxis(x, ax, 0), axes=(1, 0)), 0, ax)
+
+
 def energy_loss(P, r, t, c, grid, wrap, bcs, dx, ch=(8, 16, 32, 64)):
     """Training loss of the preconditioner for a pair (residual r, correction t,
-    A t = -r): the energy of the error e = c net(r) - t in the operator's norm
-    relative to that of t, E = e^T (-A) e / (t^T (-A) t); 1 for a zero output.
-    Returns (E, gradient dict of the parameters)."""
+    A t = -r): the energy of the error e = c net(r) - t relative to that of t,
+    measured as the squared centred gradient summed over the axes,
+    E = sum_d |G_d e|^2 / sum_d |G_d t|^2 (1 for a zero output).  With cyclic
+    axes this is e^T (-A) e / t^T (-A) t; with rigid walls -A is not symmetric and
+    its quadratic form can be negative, while this one never is.  Returns
+    (E, gradient dict of the parameters)."""
     q, cache = forward(r, P, grid, wrap, ch)
     e = c * q - t
-    Ae = pressure_lap(e, bcs, dx)
-    den = -float((t * pressure_lap(t, bcs, dx)).sum())
-    E = -float((e * Ae).sum()) / den
-    dq = -c * (Ae + pressure_lap_adj(e, bcs, dx)) / den
+    Gs = [grad1d_matrix(n, lo, hi, h) for n, (lo, hi), h in zip(e.shape, bcs, dx)]
+    ge = [_along(G, e, ax) for ax, G in enumerate(Gs)]
+    den = float(sum((_along(G, t, ax) ** 2).sum() for ax, G in enumerate(Gs)))
+    E = float(sum((g ** 2).sum() for g in ge)) / den
+    dq = 2 * c * sum(_along(G.T, g, ax) for ax, (G, g) in enumerate(zip(Gs, ge))) / den
     return E, backward(dq, cache, P, grid, wrap)

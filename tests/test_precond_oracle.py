@@ -55,9 +55,9 @@ def test_network_is_linear_and_shapes():
 
 @pytest.mark.parametrize("grid,rigid", [((9, 7, 8), ((0, 0), (0, 0), (1, 1))), ((10, 9), ((0, 0), (1, 1)))])
 def test_training_loss_gradient_matches_finite_differences(grid, rigid):
-    """The whole training loss, the pressure operator with its rigid-wall rows
-    included: the energy-norm loss and its gradient (through the exact adjoint of
-    the operator) against central differences."""
+    """The whole training loss, the pressure solve's gradient with its rigid-wall
+    rows included: the gradient-norm energy loss and its parameter gradient
+    (through the transpose of the gradient operator) against central differences."""
     nd = len(grid)
     ch = (2, 3, 4, 5)
     dx = (10.0, 10.0, 10.0)[:nd]
@@ -83,9 +83,26 @@ def test_training_loss_gradient_matches_finite_differences(grid, rigid):
 
 def test_pressure_operator_rigid_rows_are_not_symmetric():
     """With a rigid wall the one-dimensional operator differs from its transpose
-    in the rows next to the wall (the reason the training gradient needs the adjoint)."""
+    in the rows next to the wall (the reason the training loss measures the error
+    through the gradient, whose squared norm cannot be negative)."""
     M = po.lap1d_matrix(12, True, True, 1.0)
     assert not np.allclose(M, M.T)
     assert np.allclose(M[4:-4, 4:-4], M.T[4:-4, 4:-4])
     C = po.lap1d_matrix(12, False, False, 1.0)
     assert np.allclose((C @ np.ones(12)), 0.0)  # constants are in the kernel on a cyclic line
+
+
+@pytest.mark.parametrize("n,rigid", [(9, False), (12, False), (8, True), (7, True)])
+def test_gradient_energy_is_the_operator_energy_where_symmetric(n, rigid):
+    """The loss's gradient-norm energy |G x|^2 equals x^T (-A) x of the pressure
+    operator on a cyclic line, summed over the distinct points (the last point
+    duplicates the first), and is never negative."""
+    G = po.grad1d_matrix(n, rigid, rigid, 2.0)
+    A = po.lap1d_matrix(n, rigid, rigid, 2.0)
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=n)
+    if not rigid:
+        x[-1] = x[0]  # the cyclic duplicate point
+        g, a = G @ x, A @ x
+        assert np.isclose(float(g[:-1] @ g[:-1]), -float(x[:-1] @ a[:-1]))
+    assert float((G @ x) @ (G @ x)) >= 0.0
