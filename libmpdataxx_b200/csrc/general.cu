@@ -178,6 +178,26 @@ template <class T> __device__ __forceinline__ T cxx(T C, T gb) { return (T(3) * 
 template <class T> __device__ __forceinline__ T cxy(T C, T g, T gb) { return (fabs(C) - T(2) * (C * C) / gb) * g / (T(2) * gb); }
 template <class T> __device__ __forceinline__ T cyz(T C, T g1, T g2, T gb) { return T(-2) * C * g1 * g2 / T(3) / (gb * gb); }
 
+// fourth-order terms of the 2D antidiffusive velocity, iga only
+// (formulae_mpdata_hot_2d.hpp:82-157): the third derivatives ndxxx, ndxxy, ndxyy
+// (formulae_mpdata_psi_2d.hpp:360-412) times their Courant-number coefficients;
+// cy = GC1_bar_xy, gb = G_bar_x; pow2 and pow3 as products, pow4(x) as (x x)(x x)
+template <int D, class T>
+__device__ __forceinline__ T fot2(const dfield<T> &p, int a, int b, T C, T cy, T gb) {
+  auto ps = [&](int x, int y) { return P<2, D>(p, x, y, 0); };
+  const T nxxx = (ps(a + 2, b) - T(3) * ps(a + 1, b) + T(3) * ps(a, b) - ps(a - 1, b)) / T(4);
+  const T nxxy = (ps(a + 2, b + 1) - ps(a + 1, b + 1) - ps(a, b + 1) + ps(a - 1, b + 1) - ps(a + 2, b - 1)
+                  + ps(a + 1, b - 1) + ps(a, b - 1) - ps(a - 1, b - 1)) / T(8);
+  const T nxyy = (ps(a + 1, b + 1) - T(2) * ps(a + 1, b) + ps(a + 1, b - 1) - ps(a, b + 1) + T(2) * ps(a, b)
+                  - ps(a, b - 1)) / T(6);
+  const T aC = fabs(C), C2 = C * C, C4 = (C * C) * (C * C), gb2 = gb * gb, gb3 = gb * gb * gb;
+  const T acy = fabs(cy), cy2 = cy * cy;
+  const T cxxx = (T(6) * aC * C2 / gb2 - T(3) * C2 / gb - T(3) * C4 / gb3) / T(2);
+  const T cxxy = T(3) * (aC - C2 / gb) * C * cy / gb2;
+  const T cxyy = T(3) * (T(3) * acy * C2 / gb + T(3) * cy2 * aC / gb - T(2) * acy * aC - T(9) * cy2 * C2 / gb2) / gb / T(4);
+  return nxxx * cxxx + nxxy * cxxy + nxyy * cxyy;
+}
+
 // antidiffusive velocity (formulae_mpdata_{1,2,3}d.hpp antidiff, standard form).
 // TOT and DFL are added only when their options are set (the reference adds an
 // integer zero otherwise, which changes at most the sign of a zero result).
@@ -203,6 +223,8 @@ struct op_antidiff {
         const T xy = nd2(o, P<ND, D>(psi, a + 1, b + 1, c), P<ND, D>(psi, a, b + 1, c), P<ND, D>(psi, a + 1, b - 1, c), P<ND, D>(psi, a, b - 1, c));
         r = r + (xx * cxx(C, gb) + xy * cxy(C, gc1, gb));
       }
+      if constexpr (ND == 2)
+        if (o & o_fot) r = r + fot2<D>(psi, a, b, C, gc1, gb);
     } else {
       // GC1_bar_xy, GC2_bar_xz (formulae_mpdata_gc_3d.hpp:100-170)
       const T gc1 = (P<ND, D>(G1, a + 1, b, c) + P<ND, D>(G1, a, b, c) + P<ND, D>(G1, a + 1, b - 1, c) + P<ND, D>(G1, a, b - 1, c)) / T(4);
@@ -369,6 +391,9 @@ struct op_antidiff_div {
       else nfdiv_dt = m4 * frac(o, nt, gbx(a, b, c) * s_nf(pn, a, b, c, s_nf(psi, a, b, c, T(0), true), false));
       r = d2 + (up + spatial - T(0.5) * fabs(C) * ndtx + T(1.0 / 24) * (8 * C * nfdiv_dt));
     }
+    // the fourth-order terms after div_3rd (formulae_mpdata_2d.hpp:300-305; 2D only)
+    if constexpr (ND == 2)
+      if ((o & o_fot) && (o & (o_div_3rd | o_div_3rd_dt))) r = r + fot2<D>(psi, a, b, G(G0, a, b, c), g1bxy(a, b, c), gbx(a, b, c));
     P<ND, D>(res, a, b, c) = r;
   }
 };

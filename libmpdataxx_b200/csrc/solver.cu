@@ -589,9 +589,13 @@ void validate(const mpdx_config &c) {
   if (c.n_eqns < 1) throw error(MPDX_E_ARG, "n_eqns must be positive");
   if (c.n_iters < 1) throw error(MPDX_E_ARG, "n_iters must be positive");
   const unsigned o = unsigned(c.opts);
-  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl | o_nug | o_khn | o_div_2nd | o_div_3rd | o_div_3rd_dt;
+  const unsigned built = o_fct | o_abs | o_tot | o_pfc | o_npa | o_iga | o_dfl | o_nug | o_khn | o_div_2nd | o_div_3rd | o_div_3rd_dt | o_fot;
   if (o & ~built)
-    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl nug khn div_2nd div_3rd div_3rd_dt)");
+    throw error(MPDX_E_UNSUPPORTED, "MPDATA option not built on this backend (supported: fct abs tot pfc npa iga dfl nug khn div_2nd div_3rd div_3rd_dt fot)");
+  // fot: the 2D FOT's static_asserts (formulae_mpdata_hot_2d.hpp:147-149); the 1D and 3D
+  // antidiffusive velocities never add fourth-order terms, so there the option changes nothing
+  if ((o & o_fot) && c.n_dims == 2 && (!(o & o_iga) || !(o & (o_tot | o_div_3rd))))
+    throw error(MPDX_E_ARG, "fot option only available with iga, and only with tot or div_3rd");
   // the divergence form (formulae_mpdata_{1,2,3}d.hpp): div_3rd / div_3rd_dt extend div_2nd,
   // exclude each other and tot / dfl (static_asserts and enable_ifs there)
   if (o & (o_div_2nd | o_div_3rd | o_div_3rd_dt)) {

@@ -73,8 +73,11 @@ class cuda : public any<typename solver_t::real_t, solver_t::n_dims> {
   static_assert(bcxl != bcond::null && bcxr != bcond::null, "x boundary conditions are required");
   static_assert(n_dims < 2 || (bcyl != bcond::null && bcyr != bcond::null), "y boundary conditions are required");
   static_assert(n_dims < 3 || (bczl != bcond::null && bczr != bcond::null), "z boundary conditions are required");
-  static_assert(!opts::isset(ct_params_t::opts, opts::fot),
-                "MPDATA option not built on this backend (built: fct abs tot pfc npa iga dfl nug khn div_2nd div_3rd div_3rd_dt)");
+  // formulae_mpdata_hot_2d.hpp:147-149 (the 1D and 3D formulae never add fourth-order terms)
+  static_assert(n_dims != 2 || !opts::isset(ct_params_t::opts, opts::fot) ||
+                    (opts::isset(ct_params_t::opts, opts::iga) &&
+                     (opts::isset(ct_params_t::opts, opts::tot) || opts::isset(ct_params_t::opts, opts::div_3rd))),
+                "fot option only available with iga, and only with tot or div_3rd");
 
   explicit cuda(const rt_params_t &p) : p_(p) {
     mpdx_config c;

@@ -33,7 +33,7 @@ namespace mpdx_oracle {
 enum : unsigned {
   o_fct = 1u << 0, o_abs = 1u << 1, o_tot = 1u << 2, o_pfc = 1u << 3,
   o_npa = 1u << 4, o_iga = 1u << 5, o_nug = 1u << 6, o_dfl = 1u << 7,
-  o_khn = 1u << 8, o_div_2nd = 1u << 9, o_div_3rd = 1u << 10, o_div_3rd_dt = 1u << 11
+  o_khn = 1u << 8, o_div_2nd = 1u << 9, o_div_3rd = 1u << 10, o_div_3rd_dt = 1u << 11, o_fot = 1u << 12
 };
 enum { bc_cyclic = 0, bc_open = 1, bc_rigid = 2 };
 
@@ -160,6 +160,9 @@ struct mpdata {
     // that no exchange fills (mpdata_osc_2d.hpp:112-121), so the reference's result is not defined
     if ((opts & (o_div_2nd | o_div_3rd | o_div_3rd_dt)) && n_iters > 2)
       throw std::runtime_error("oracle: divergence-form options need n_iters <= 2");
+    // formulae_mpdata_hot_2d.hpp:147-149 (static_asserts of the 2D FOT; 1D and 3D never add it)
+    if (nd == 2 && (opts & o_fot) && (!(opts & o_iga) || !(opts & (o_tot | o_div_3rd))))
+      throw std::runtime_error("oracle: fot needs iga and tot or div_3rd");
     for (int d = 0; d < 3; ++d) n[d] = d < nd ? n_[d] : 1;
     for (int d = 0; d < nd; ++d) if (n[d] < 1) throw std::runtime_error("libmpdata++: bogus grid size");
     for (int d = 0; d < nd; ++d) for (int s = 0; s < 2; ++s) bcs[d][s] = bcs_[2 * d + s];
@@ -517,6 +520,25 @@ struct mpdata {
   static T cxx(T C, T gb) { return (T(3) * C * std::abs(C) / gb - T(2) * (C * C * C) / (gb * gb) - C) / T(6); }
   static T cxy(T C, T g, T gb) { return (std::abs(C) - T(2) * (C * C) / gb) * g / (T(2) * gb); }
   static T cyz(T C, T g1, T g2, T gb) { return T(-2) * C * g1 * g2 / T(3) / (gb * gb); }
+  // fourth-order terms of the 2D antidiffusive velocity, iga only
+  // (formulae_mpdata_hot_2d.hpp:82-157): the third derivatives ndxxx, ndxxy, ndxyy
+  // (formulae_mpdata_psi_2d.hpp:360-412) times their Courant-number coefficients;
+  // cy = GC1_bar_xy, gb = G_bar_x; pow2 and pow3 as products, pow4(x) as (x x)(x x)
+  // (Blitz++'s own evaluation order of pow4 cannot be checked here)
+  template <int D> T fot2(const arr<T> &p, int a, int b, T C, T cy, T gb) const {
+    auto ps = [&](int x, int y) { return P<2, D>(p, x, y, 0); };
+    const T nxxx = (ps(a + 2, b) - T(3) * ps(a + 1, b) + T(3) * ps(a, b) - ps(a - 1, b)) / T(4);
+    const T nxxy = (ps(a + 2, b + 1) - ps(a + 1, b + 1) - ps(a, b + 1) + ps(a - 1, b + 1) - ps(a + 2, b - 1)
+                    + ps(a + 1, b - 1) + ps(a, b - 1) - ps(a - 1, b - 1)) / T(8);
+    const T nxyy = (ps(a + 1, b + 1) - T(2) * ps(a + 1, b) + ps(a + 1, b - 1) - ps(a, b + 1) + T(2) * ps(a, b)
+                    - ps(a, b - 1)) / T(6);
+    const T aC = std::abs(C), C2 = C * C, C4 = (C * C) * (C * C), gb2 = gb * gb, gb3 = gb * gb * gb;
+    const T acy = std::abs(cy), cy2 = cy * cy;
+    const T cxxx = (T(6) * aC * C2 / gb2 - T(3) * C2 / gb - T(3) * C4 / gb3) / T(2);
+    const T cxxy = T(3) * (aC - C2 / gb) * C * cy / gb2;
+    const T cxyy = T(3) * (T(3) * acy * C2 / gb + T(3) * cy2 * aC / gb - T(2) * acy * aC - T(9) * cy2 * C2 / gb2) / gb / T(4);
+    return nxxx * cxxx + nxxy * cxxy + nxyy * cxyy;
+  }
 
   // ---- divergent-flow correction (formulae_mpdata_dfl_{1,2,3}d.hpp), G = 1 ----
   // -C/4/G_bar_x (div of the advector around the face) [x psi_bar_x with iga];
@@ -562,6 +584,7 @@ struct mpdata {
         T r = std::abs(C) / T(2) * (T(1) - std::abs(C) / gb) * ndx<2, D>(p, a, b, 0)
             - C * gc1 / (T(2) * gb) * ndy<2, D>(p, a, b, 0);
         if (opts & o_tot) r = r + (ndxx<2, D>(p, a, b, 0) * cxx(C, gb) + ndxy<2, D>(p, a, b, 0) * cxy(C, gc1, gb));
+        if (opts & o_fot) r = r + fot2<D>(p, a, b, C, gc1, gb);
         if (opts & o_dfl) r = r + dfl<2, D>(p, Gd, Gt, Gt, a, b, 0);
         P<2, D>(res, a, b) = r;
       }
@@ -698,7 +721,10 @@ struct mpdata {
       const T dfc = fc(a + 1, b, c) - fc(a, b, c);
       const T ndx_fdiv = iga ? dfc : m2 * frac(opts, dfc, s_ndx_fdiv());
       const T nfdiv_fdiv = iga ? nfdiv_fdiv_num() / gbx(a, b, c) : m2 * frac(opts, nfdiv_fdiv_num(), gbx(a, b, c) * s_nfdiv_fdiv());
-      return d2 + (up + spatial + T(0.5) * std::abs(C) * ndx_fdiv + T(1.0 / 24) * (-8 * C * nfdiv_fdiv));
+      const T r3 = d2 + (up + spatial + T(0.5) * std::abs(C) * ndx_fdiv + T(1.0 / 24) * (-8 * C * nfdiv_fdiv));
+      if constexpr (ND == 2)
+        if (opts & o_fot) return r3 + fot_div<D>(p, G0, G1, a, b);
+      return r3;
     }
     // div_3rd_dt (2D, 3D)
     auto dq = [&](int x, int y, int z) { return q(p, x, y, z) - q(pn, x, y, z); };
@@ -726,7 +752,16 @@ struct mpdata {
              + q(pn, a + 1, b - 1, c) + q(pn, a + 1, b, c + 1) + q(pn, a + 1, b, c - 1) + q(pn, a, b, c - 1) + q(pn, a, b, c + 1);
     }
     const T nfdiv_dt = iga ? ndt_num / gbx(a, b, c) : m4 * frac(opts, ndt_num, gbx(a, b, c) * s_dt);
-    return d2 + (up + spatial - T(0.5) * std::abs(C) * ndtx + T(1.0 / 24) * (8 * C * nfdiv_dt));
+    const T r3 = d2 + (up + spatial - T(0.5) * std::abs(C) * ndtx + T(1.0 / 24) * (8 * C * nfdiv_dt));
+    if constexpr (ND == 2)
+      if (opts & o_fot) return r3 + fot_div<D>(p, G0, G1, a, b);
+    return r3;
+  }
+  // the fourth-order terms added to the 2D divergence form (formulae_mpdata_2d.hpp:300-305)
+  template <int D> T fot_div(const arr<T> &p, const arr<T> &G0, const arr<T> &G1, int a, int b) const {
+    const T C = P<2, D>(G0, a, b, 0), gb = Gbar<2, D>(a, b, 0);
+    const T cy = (P<2, D>(G1, a + 1, b, 0) + P<2, D>(G1, a, b, 0) + P<2, D>(G1, a + 1, b - 1, 0) + P<2, D>(G1, a, b - 1, 0)) / T(4);
+    return fot2<D>(p, a, b, C, cy, gb);
   }
   // res over faces im along D x interior across (formulae_mpdata_{1,2,3}d.hpp antidiff, divergence form)
   template <int ND, int D> void antidiff_div(arr<T> &res, const arr<T> &p, const arr<T> &pn, const vctr<T> &G) {

@@ -90,8 +90,12 @@ def test_bogus_grid_size():
 
 def test_unsupported_option_rejected():
     from libmpdataxx_b200 import opts as o
-    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=o.fot))
+    rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=1 << 13))  # no such option
     assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    # fot: the 2D FOT's static_asserts (formulae_mpdata_hot_2d.hpp:147-149)
+    for bad in (o.fot, o.fot | o.tot, o.fot | o.iga, o.fot | o.iga | o.div_2nd):
+        rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=bad))
+        assert rc == _lib.MPDX_E_ARG and "fot" in msg, bad
     # the divergence form's own rules (formulae_mpdata_{1,2,3}d.hpp enable_ifs / static_asserts)
     for bad in (o.div_3rd, o.div_2nd | o.div_3rd | o.div_3rd_dt, o.div_2nd | o.tot, o.div_2nd | o.dfl):
         rc, _ = _create(_cfg(n_dims=2, grid=(8, 8, 1), opts=bad))
@@ -115,9 +119,12 @@ def test_option_and_parameter_validation():
     assert rc == _lib.MPDX_E_UNSUPPORTED and "nug" in msg
     rc, msg = _create(_cfg(n_dims=2, grid=(8, 8, 1), upwind_filter_freq=-1))
     assert rc == _lib.MPDX_E_ARG and "upwind_filter_freq" in msg
-    # the unbuilt MPDATA variant (fot) is refused whatever else is set
-    rc, msg = _create(_cfg(n_dims=3, grid=(8, 8, 8, ), opts=o.iga | o.fot))
-    assert rc == _lib.MPDX_E_UNSUPPORTED and "not built" in msg
+    # fot with iga and tot (or div_3rd) in 2D; in 1D and 3D the reference's formulae never
+    # add fourth-order terms, so there the option is accepted and changes nothing
+    for nd, grid, opts in ((2, (8, 8, 1), o.iga | o.tot | o.fot), (2, (8, 8, 1), o.iga | o.div_2nd | o.div_3rd | o.fot),
+                           (3, (8, 8, 8), o.iga | o.fot), (1, (8, 1, 1), o.fot)):
+        rc, msg = _create(_cfg(n_dims=nd, grid=grid, opts=opts))
+        assert rc in (_lib.MPDX_OK, _lib.MPDX_E_CUDA), (nd, opts, msg)  # validation passed (no GPU: CUDA error)
     # the divergence form is built for solvers::mpdata (its advector is constant in time)
     rc, msg = _create(_cfg(solver=_lib.SOLVER_BOUSSINESQ, n_dims=2, n_eqns=3, grid=(8, 8, 1), opts=o.div_2nd,
                            dt=0.1, tht_ref=300.0))

@@ -279,3 +279,35 @@ def test_block1d_equals_general_path(opts, iters, uff, dtype):
         load(orc, s)
         orc.advance(20)
         assert rel_err(runs["auto"].advectee(), orc.advectee()) <= RTOL64
+
+
+FOT_CASES = [(bc, opts, iters) for bc in ("cyclic", "open", "rigid")
+             for opts, iters in ((o.iga | o.tot | o.fot, 2), (o.iga | o.tot | o.fot, 3), (o.iga | o.tot | o.fot | o.fct, 2),
+                                 (o.iga | o.div_2nd | o.div_3rd | o.fot, 2))]
+
+
+@pytest.mark.parametrize("bc,opts,iters", FOT_CASES)
+def test_fot_fp64_matches_oracle(bc, opts, iters):
+    """Fourth-order terms (2D, iga with tot or div_3rd): the general path against the oracle."""
+    grid = (23, 19)
+    bcs = [bc] * 4
+    s = random_setup(grid, bcs, seed=iters + 7, signed=True)
+    _check_parity(s, grid, bcs, opts, iters, eps=1e30 if bc == "rigid" else 1e-10)
+
+
+def test_fot_convergence_order_on_gpu():
+    """The reference's convergence check of fot (tests/sandbox/convergence_2d_3d/convergence_2d.cpp)
+    through the GPU path: order 4 for iga|tot|fot, 3 for iga|tot."""
+    def err(opts, np_):
+        dx = 1.0 / (np_ - 1)
+        dt = 0.2 * dx
+        i, j = np.meshgrid(np.arange(np_), np.arange(np_), indexing="ij")
+        psi = 2 + np.sin(2 * np.pi * i * dx) * np.sin(2 * np.pi * j * dx)
+        run = make_run((np_, np_), opts, n_iters=2, bcs=["cyclic"] * 4)
+        run.set_advectee(psi)
+        run.set_advector(np.full(run._shape(1, 0), 1.0 * dt / dx), 0)
+        run.set_advector(np.full(run._shape(1, 1), 2.0 * dt / dx), 1)
+        run.advance(int(1.0 / dt))
+        return float(np.sqrt(((run.advectee() - psi) ** 2).sum() / (np_ * np_)))
+    for opts, order in ((o.iga | o.tot, 3), (o.iga | o.tot | o.fot, 4)):
+        assert round(np.log2(err(opts, 33) / err(opts, 65))) == order

@@ -233,3 +233,49 @@ def test_div_third_pass_refused():
     for opts in (D2, D2 | D3, o.fct | D2 | DT):
         with pytest.raises(RuntimeError, match="n_iters"):
             Oracle((9, 9), opts, n_iters=3, bcs=["cyclic"] * 4)
+
+
+def _convergence_2d(opts, iters, np_):
+    """The reference's 2D convergence set-up (tests/sandbox/convergence_2d_3d/convergence_2d.cpp:18-64):
+    np x np cyclic points, dx = dy = 1 / (np - 1), dt = 0.2 dx, psi = 2 + sin(2 pi i dx) sin(2 pi j dy),
+    velocity (1, 2) (Courant numbers 0.2, 0.4), int(1 / dt) steps; the L2 error against the start
+    divided by the time (1)."""
+    dx = 1.0 / (np_ - 1)
+    dt = 0.2 * dx
+    nt = int(1.0 / dt)
+    i, j = np.meshgrid(np.arange(np_), np.arange(np_), indexing="ij")
+    psi = 2 + np.sin(2 * np.pi * i * dx) * np.sin(2 * np.pi * j * dx)
+    orc = Oracle((np_, np_), opts, n_iters=iters, bcs=["cyclic"] * 4)
+    orc.set_advectee(psi)
+    orc.set_advector(np.full(orc.advector_shape(0), 1.0 * dt / dx), 0)
+    orc.set_advector(np.full(orc.advector_shape(1), 2.0 * dt / dx), 1)
+    orc.advance(nt)
+    return float(np.sqrt(((orc.advectee() - psi) ** 2).sum() / (np_ * np_)))
+
+
+@pytest.mark.parametrize("opts,iters,order", [(0, 2, 2), (o.iga | o.fct, 2, 2), (o.tot, 3, 3), (o.abs | o.tot, 3, 3),
+                                              (o.iga | o.tot, 2, 3), (o.iga | o.tot | o.fot, 2, 4)])
+def test_convergence_order_2d(opts, iters, order):
+    """The reference's own check of the fourth-order terms (fot) and of the lower
+    orders (tests/sandbox/convergence_2d_3d/convergence_2d.cpp:66-124): the order
+    round(log2(err(33) / err(65))) of each option set."""
+    assert round(np.log2(_convergence_2d(opts, iters, 33) / _convergence_2d(opts, iters, 65))) == order
+
+
+def test_fot_rules():
+    """fot needs iga and tot or div_3rd in 2D (formulae_mpdata_hot_2d.hpp:147-149);
+    the 1D and 3D formulae never add fourth-order terms."""
+    for bad in (o.fot, o.fot | o.tot, o.fot | o.iga):
+        with pytest.raises(RuntimeError, match="fot"):
+            Oracle((9, 9), bad, n_iters=2, bcs=["cyclic"] * 4)
+    rng = np.random.default_rng(3)
+    psi = rng.uniform(0.5, 2.0, 20)
+    psi[-1] = psi[0]
+    runs = []
+    for opts in (o.iga | o.tot, o.iga | o.tot | o.fot):
+        orc = Oracle((20,), opts, n_iters=2, bcs=["cyclic"] * 2)
+        orc.set_advectee(psi)
+        orc.set_advector(np.full(orc.advector_shape(0), 0.3), 0)
+        orc.advance(5)
+        runs.append(orc.advectee())
+    np.testing.assert_array_equal(runs[0], runs[1])
