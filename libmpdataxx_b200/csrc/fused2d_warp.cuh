@@ -66,13 +66,25 @@ __device__ __forceinline__ T el(const q4<T> &v, int e) {
   else return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w;
 }
 
+// the quotients of the antidiffusive velocities: in FP32 the approximate-reciprocal
+// quotient (__fdividef: within 2 ulp for the denominators here, sums of psi plus
+// FLT_MIN, below 2^126); in FP64 the IEEE quotient.  The FCT betas keep the
+// correctly rounded quotient (the exact bound properties rest on them).
+__device__ __forceinline__ q4<float> adq(const q4<float> &a, const q4<float> &b) {
+  return qd::mk(__fdividef(a.a.x, b.a.x), __fdividef(a.a.y, b.a.y), __fdividef(a.b.x, b.b.x), __fdividef(a.b.y, b.b.y));
+}
+__device__ __forceinline__ q4<double> adq(const q4<double> &a, const q4<double> &b) { return a / b; }
 // ndx_psi 2D (formulae_mpdata_psi_2d.hpp:127-185): iga 2 (p1 - p0) / 2 = p1 - p0
 template <class T, bool IGA>
-__device__ __forceinline__ q4<T> ndx(const q4<T> &p1, const q4<T> &p0) { return f3::qndx<T, IGA>(p1, p0); }
+__device__ __forceinline__ q4<T> ndx(const q4<T> &p1, const q4<T> &p0) {
+  if (IGA) return p1 - p0;
+  return qd::bc<T>(T(2)) * adq(p1 - p0, (p1 + p0) + qd::bc<T>(lims<T>::tiny()));
+}
 // ndy_psi 2D (formulae_mpdata_psi_2d.hpp:188-240)
 template <class T, bool IGA>
 __device__ __forceinline__ q4<T> ndy(const q4<T> &a, const q4<T> &b, const q4<T> &c, const q4<T> &d) {
-  return f3::qnd4<T, IGA>(a, b, c, d);
+  if (IGA) return (((a + b) - c) - d) * qd::bc<T>(T(0.25));
+  return adq(((a + b) - c) - d, (((a + b) + c) + d) + qd::bc<T>(lims<T>::tiny()));
 }
 // antidiff 2D (formulae_mpdata_2d.hpp:256-277) with G = 1:
 // |C|/2 (1 - |C|) ndx - (C gc1)/2 ndy
@@ -143,6 +155,7 @@ __device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int 
   Q eu4 = zero, ed4 = zero;            // betas2 row t-4
   Q gx5 = zero;                        // limited x flux of iteration 2, face t-5
 
+  Q fx_up = qflux(pn1, pn0, gx1);     // upwind x flux through face ts-1/2
   // rows loaded one step ahead (psi^n t+2, Courant components t+1), reduced modulo
   // the period by a compare per step
   int xin = pmod(ts + 2, A.P0), xg = pmod(ts + 1, A.P0);
@@ -157,8 +170,12 @@ __device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int 
     if (++xg == A.P0) xg = 0;
 
     // ---- psi1(t) (donor-cell, donorcell_formulae.hpp:104-130) ----
-    const Q fxp = qflux(pn0, pnp, gx0), fxm = qflux(pn1, pn0, gx1);
-    const Q fyp = qflux(pn0, qd::kp1(pn0), gy0), fym = qflux(qd::km1(pn0), pn0, qd::km1(gy0));
+    // every face flux is evaluated once: the flux through face t-1/2 is the one
+    // computed for face t+1/2 of the previous row, the flux through j-1/2 of a
+    // column the j+1/2 flux of its left neighbour (the same operands, the same value)
+    const Q fxp = qflux(pn0, pnp, gx0), fxm = fx_up;
+    const Q fyp = qflux(pn0, qd::kp1(pn0), gy0), fym = qd::km1(fyp);
+    fx_up = fxp;
     const Q p1_0 = pn0 + (((-fxp) + fxm) + ((-fyp) + fym));
 
     // ---- C~x face t-1 (between rows t-1 and t), C~y row t-1 ----
