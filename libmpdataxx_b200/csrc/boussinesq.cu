@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_gcr_update(geom g, T err_tol
 constexpr int kTJ = 8, kTK = 32, kPJ = kTJ + 4, kPK = kTK + 4, kGcrChunk = 32, kSteps = 2;
 static_assert(kTJ * kTK == kRedThreads, "one tile column per thread");
 template <class T, int NV>
-__global__ void __launch_bounds__(kRedThreads, NV == 1 ? 3 : 2) k_gcr_update3(geom g, T err_tol, dfield<T> err0,
+__global__ void __launch_bounds__(kRedThreads, NV == 1 ? 4 : 2) k_gcr_update3(geom g, T err_tol, dfield<T> err0,
                                                                 dfield<T> err1, dfield<T> lap_err, dirs<T> D,
                                                                 gcr_dev<T> *dv, double *part, int chunk) {
   constexpr int v = NV - 1;
