@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SO_PATH = os.path.join(HERE, "libmpdx.so")
+# MPDX_LIBRARY=debug loads the bounds-checked, NaN-poisoned build (libmpdx_debug.so)
+SO_PATH = os.path.join(HERE, "libmpdx_debug.so" if os.environ.get("MPDX_LIBRARY") == "debug" else "libmpdx.so")
 
 MPDX_OK, MPDX_E_GRID, MPDX_E_DIVERGENT, MPDX_E_PRS_STUCK, MPDX_E_UNSUPPORTED, MPDX_E_CUDA, MPDX_E_TIMEOUT, MPDX_E_ARG = range(8)
 BC = {"cyclic": 0, "open": 1, "rigid": 2, "gndsky": 3}

@@ -1184,6 +1184,9 @@ boussinesq<T, P>::boussinesq(const mpdx_config &c, cudaStream_t s) {
   if (vab != MPDX_VAB_NONE && vab != MPDX_VAB_EXPL && vab != MPDX_VAB_IMPL) throw error(MPDX_E_ARG, "unknown velocity absorber");
   for (int d = 0; d < st.nd; ++d) { st.alloc_sclr(stash[d]); st.alloc_sclr(vip_rhs[d]); st.alloc_sclr(vab_relax[d]); }
   st.alloc_sclr(tht_abs); st.alloc_sclr(hflux_frc); st.alloc_sclr(vab_coeff); st.alloc_sclr(dtht_e);
+  // hflux_frc = 0, tht_abs = 0 (boussinesq_common.hpp:51-52), whatever the allocation holds
+  MPDX_CUDA(cudaMemsetAsync(tht_abs.base, 0, tht_abs.bytes, s));
+  MPDX_CUDA(cudaMemsetAsync(hflux_frc.base, 0, hflux_frc.bytes, s));
   if (normalizes())
     for (int d = 0; d < st.nd; ++d) st.alloc_sclr(den[d]);
   for (int e = 0; e < st.n_eqns; ++e) st.alloc_sclr(rhs[e]);
@@ -1554,6 +1557,7 @@ void boussinesq<T, P>::ante_loop() {
   for (int d = 0; d < st.nd; ++d) {
     MPDX_CUDA(cudaMemsetAsync(st.GC[d].base, 0, st.GC[d].bytes, s));
     MPDX_CUDA(cudaMemsetAsync(stash[d].base, 0, stash[d].bytes, s));
+    MPDX_CUDA(cudaMemsetAsync(vip_rhs[d].base, 0, vip_rhs[d].bytes, s));
   }
   gen.ante_loop(scratch);
   bq::eqns<T> E;

@@ -55,11 +55,45 @@ inline rng exh(rng r) { return {r.f - 1, r.l}; }             // r^h
 
 // Device view of a field stored with its halo: element (i, j, k) lives at
 // o[i*s0 + j*s1 + k*s2]; unused dimensions are pinned to index 0.
+#ifdef MPDX_BOUNDS_CHECK
+// where the bounds-checked build records the first out-of-range field access
+struct oob_info {
+  unsigned hit;
+  int i, j, k;
+};
+// one record per device, allocated on first use (the current device's)
+inline oob_info *oob_record() {
+  static oob_info *rec[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!rec[dev]) {
+    if (cudaMalloc(&rec[dev], sizeof(oob_info)) != cudaSuccess) { rec[dev] = nullptr; return nullptr; }
+    cudaMemset(rec[dev], 0, sizeof(oob_info));
+  }
+  return rec[dev];
+}
+#endif
+
 template <class T>
 struct dfield {
   T *o = nullptr;
   long long s0 = 0, s1 = 0, s2 = 0;
+#ifdef MPDX_BOUNDS_CHECK
+  // the bounds-checked build (libmpdx_debug.so): the index ranges of the allocation
+  // (lo > hi: not checked, as for views built from a bare pointer) and the flag that
+  // an access outside them sets instead of touching memory outside the field
+  int lo[3] = {1, 1, 1}, hi[3] = {0, 0, 0};
+  oob_info *oob = nullptr;
+#endif
   __host__ __device__ __forceinline__ T &operator()(int i, int j, int k) const {
+#if defined(MPDX_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
+    if (oob && lo[0] <= hi[0] &&
+        (i < lo[0] || i > hi[0] || j < lo[1] || j > hi[1] || k < lo[2] || k > hi[2])) {
+      if (atomicExch(&oob->hit, 1u) == 0u) { oob->i = i; oob->j = j; oob->k = k; }
+      return o[lo[0] * s0 + lo[1] * s1 + lo[2] * s2];  // the field's first point: the call fails afterwards
+    }
+#endif
     return o[i * s0 + j * s1 + k * s2];
   }
 };
@@ -101,13 +135,26 @@ struct field {
     for (int q = f - 1; q >= 0; --q) { s[q] = acc; acc *= r[q].n(); }
     bytes = size_t(acc) * sizeof(T);
     MPDX_CUDA(cudaMalloc(&base, bytes));
+#ifdef MPDX_POISON
+    // the debug build fills new fields with NaN (all bits set), so that a value read
+    // before anything wrote it shows in the results
+    MPDX_CUDA(cudaMemsetAsync(base, 0xff, bytes, stream));
+#else
     MPDX_CUDA(cudaMemsetAsync(base, 0, bytes, stream));
+#endif
     long long off = front;
     for (int q = 0; q < f; ++q) off += (long long)(-r[q].f) * s[q];
     v.o = static_cast<T *>(base) + off;
     v.s0 = s[0]; v.s1 = s[1]; v.s2 = s[2];
     // indices of unused dimensions are always 0; give them stride 0
     for (int q = nd; q < 3; ++q) (q == 0 ? v.s0 : q == 1 ? v.s1 : v.s2) = 0;
+#ifdef MPDX_BOUNDS_CHECK
+    for (int q = 0; q < 3; ++q) {
+      v.lo[q] = q < nd ? r[q].f : -2147483647;
+      v.hi[q] = q < nd ? r[q].l : 2147483647;
+    }
+    v.oob = oob_record();
+#endif
   }
 };
 

@@ -564,11 +564,29 @@ struct mpdx_solver {
 namespace {
 thread_local std::string g_create_error;
 
+// the bounds-checked build reports an out-of-range field access of the call's
+// kernels as the call's error (after waiting for the device)
+inline void check_bounds() {
+#ifdef MPDX_BOUNDS_CHECK
+  mpdx::oob_info *r = mpdx::oob_record();
+  if (!r) return;
+  MPDX_CUDA(cudaDeviceSynchronize());
+  mpdx::oob_info h;
+  MPDX_CUDA(cudaMemcpy(&h, r, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h.hit) {
+    MPDX_CUDA(cudaMemset(r, 0, sizeof(h)));
+    throw mpdx::error(MPDX_E_CUDA, "bounds-checked build: a field was indexed at (" + std::to_string(h.i) + ", " +
+                                       std::to_string(h.j) + ", " + std::to_string(h.k) + "), outside its allocation");
+  }
+#endif
+}
+
 template <class F>
 mpdx_status guarded(mpdx_handle h, F f) {
   if (!h || !h->impl) return MPDX_E_ARG;
   try {
     f();
+    check_bounds();
     h->impl->err.clear();
     return MPDX_OK;
   } catch (const mpdx::error &e) {
@@ -847,6 +865,7 @@ static mpdx_status batch_guarded(mpdx_batch_handle b, const std::function<void()
   if (!b || !b->impl) return MPDX_E_ARG;
   try {
     f();
+    check_bounds();
     b->impl->err.clear();
     return MPDX_OK;
   } catch (const mpdx::error &e) {
