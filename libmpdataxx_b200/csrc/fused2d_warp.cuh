@@ -68,12 +68,15 @@ __device__ __forceinline__ T el(const q4<T> &v, int e) {
 
 // the quotients of the antidiffusive velocities: in FP32 the approximate-reciprocal
 // quotient (__fdividef: within 2 ulp for the denominators here, sums of psi plus
-// FLT_MIN, below 2^126); in FP64 the IEEE quotient.  The FCT betas keep the
-// correctly rounded quotient (the exact bound properties rest on them).
+// FLT_MIN, below 2^126; the FP32 FCT betas keep the correctly rounded quotient, on
+// which the exact bound properties rest); in FP64 mpdx::rdivd for these and the betas.
 __device__ __forceinline__ q4<float> adq(const q4<float> &a, const q4<float> &b) {
   return qd::mk(__fdividef(a.a.x, b.a.x), __fdividef(a.a.y, b.a.y), __fdividef(a.b.x, b.b.x), __fdividef(a.b.y, b.b.y));
 }
-__device__ __forceinline__ q4<double> adq(const q4<double> &a, const q4<double> &b) { return a / b; }
+// FP64: the quotient without the division's slow path (mpdx::rdivd, within one ulp)
+__device__ __forceinline__ q4<double> adq(const q4<double> &a, const q4<double> &b) {
+  return qd::mkd(rdivd(a.x, b.x), rdivd(a.y, b.y), rdivd(a.z, b.z), rdivd(a.w, b.w));
+}
 // ndx_psi 2D (formulae_mpdata_psi_2d.hpp:127-185): iga 2 (p1 - p0) / 2 = p1 - p0
 template <class T, bool IGA>
 __device__ __forceinline__ q4<T> ndx(const q4<T> &p1, const q4<T> &p0) {
@@ -108,8 +111,13 @@ __device__ __forceinline__ void betas(const q4<T> &c, const q4<T> &xm, const q4<
   const q4<T> du = (qd::pos(fxm) - qd::neg(fxp)) + (qd::pos(fym) - qd::neg(fyp));
   const q4<T> dd = (qd::pos(fxp) - qd::neg(fxm)) + (qd::pos(fyp) - qd::neg(fym));
   const q4<T> e = qd::bc<T>(lims<T>::eps());
-  bu = (hi - c) / (du + e);
-  bd = (c - lo) / (dd + e);
+  if constexpr (sizeof(T) == 8) {  // FP64: mpdx::rdivd, as the antidiffusive velocities
+    bu = adq(hi - c, du + e);
+    bd = adq(c - lo, dd + e);
+  } else {
+    bu = (hi - c) / (du + e);
+    bd = (c - lo) / (dd + e);
+  }
 }
 
 // psi_min / psi_max of psi^n over the 5-point stencil (mpdata_fct_2d.hpp:31-46):

@@ -189,4 +189,18 @@ __device__ __forceinline__ float rdivf(float a, float b) {
   return qdiv(a, b, y);
 }
 
+// a / b in FP64 without the division's slow path, for normal b whose reciprocal is
+// normal and quotients that neither overflow nor underflow: y0 = rcp.approx.ftz.f64(b),
+// two Newton-Raphson steps y <- y + y (1 - b y) (each squares the relative error,
+// down to the rounding of y), then Markstein's correction (qdiv).  The result is
+// within one ulp of the IEEE quotient (equal to it for all but a small fraction of
+// operands; tests/cuda/qdiv_check.cu counts both).
+__device__ __forceinline__ double rdivd(double a, double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  y = fma(fma(-b, y, 1.0), y, y);
+  y = fma(fma(-b, y, 1.0), y, y);
+  return qdiv(a, b, y);
+}
+
 }  // namespace mpdx
