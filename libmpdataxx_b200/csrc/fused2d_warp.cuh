@@ -283,11 +283,6 @@ __device__ __forceinline__ void march(const f2::prob<T> &A, int j0, int x0, int 
   }
 }
 
-template <class T, int NI, bool IGA, bool FCT>
-__device__ __noinline__ void march_call(const f2::prob<T> &A, int j0, int x0, int x1) {
-  march<T, NI, IGA, FCT>(A, j0, x0, x1);
-}
-
 // resident CTAs of 4 warps per SM that the register budget is sized for
 // (FP64 quads take twice the registers of FP32 ones)
 template <class T, int NI>
@@ -310,15 +305,8 @@ __global__ void __launch_bounds__(128, kMinBlocks2<T, NI>) k_fused2d_w(const f2:
     q = __shfl_sync(0xffffffffu, q, 0);
     if (q >= n_items) break;
     const f2::item it = items[q];
-    if constexpr (sizeof(T) == 4) {
-      const f2::prob<T> A = probs[it.prob];  // FP32: the descriptor in registers
-      march<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
-    } else {
-      // FP64: the quads fill the registers; the march runs as a called function
-      // (its own register allocation, the descriptor read from the stack)
-      const f2::prob<T> A = probs[it.prob];
-      march_call<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
-    }
+    const f2::prob<T> A = probs[it.prob];  // the descriptor in registers
+    march<T, NI, IGA, FCT>(A, it.j0, it.x0, it.x1);
   }
   if (lane == 0) {
     __threadfence();  // this warp's last take from counter[0] precedes its count
