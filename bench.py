@@ -234,7 +234,7 @@ def batched_extra(n_problems=256, steps=50):
                 r.set_advector(a, d)
             runs.append(r)
         b = concurr.batch(runs, mode=mode)
-        b.advance(10)  # first steps include the autotuner
+        b.advance(30)  # the first 24 steps are the autotuner's (8 candidates x 3 steps)
         b.sync()
         t0 = time.perf_counter()
         b.advance(k)
@@ -243,7 +243,8 @@ def batched_extra(n_problems=256, steps=50):
         out[mode] = {"ms_per_step": dt * 1e3, "cell_updates_per_s": cells / dt}
         if mode == "persistent":
             i = b.info()
-            out["tile"] = {"nt": i["tile_nt"], "lx": i["tile_lx"], "grid": i["grid"], "tune_ms": i["tune_ms"]}
+            out["tile"] = {"nt": i["tile_nt"], "lx": i["tile_lx"], "grid": i["grid"], "tune_ms": i["tune_ms"],
+                           "candidates": "rows per item 16/32/64/128 x all or half of the resident CTAs, 3 timed steps each"}
         b.close()
         for r in runs:
             r.close()

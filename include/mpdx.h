@@ -209,9 +209,10 @@ typedef struct {
   int64_t cells;        /* sum over the problems of n0 x n1 */
   int mode;             /* MPDX_BATCH_* */
   int tile_nt, tile_lx; /* tile chosen by the autotuner (0 until tuning ends) */
-  int grid;             /* resident CTAs of the persistent launch */
-  int n_candidates;     /* tile candidates timed by the autotuner */
-  double tune_ms[8];    /* measured ms of one batched step per candidate (0 = not measured yet) */
+  int grid;             /* CTAs of the persistent launch chosen by the autotuner */
+  int n_candidates;     /* candidates timed by the autotuner: rows per item 16, 32, 64, 128 with
+                           every resident CTA, then the same with half of them */
+  double tune_ms[8];    /* mean ms of a batched step per candidate, over 3 steps (0 = not measured yet) */
 } mpdx_batch_info;
 
 mpdx_status mpdx_batch_create(const mpdx_handle *handles, int n, int mode, mpdx_batch_handle *out);

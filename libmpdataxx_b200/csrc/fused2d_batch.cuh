@@ -16,12 +16,17 @@
 
 namespace mpdx {
 
-// tile candidates of the autotuner: threads per item (one warp) and rows per item
+// candidates of the autotuner: threads per item (one warp), rows per item, and the
+// share of the resident CTAs the persistent grid launches (occ_div 1: every CTA
+// the SMs can hold; 2: half of them, fewer warps contending for the issue slots);
+// each is timed over kTuneSteps steps
 struct batch_tile {
-  int nt, lx;
+  int nt, lx, occ_div;
 };
-constexpr int kNumBatchTiles = 4;
-constexpr batch_tile kBatchTiles[kNumBatchTiles] = {{32, 16}, {32, 32}, {32, 64}, {32, 128}};
+constexpr int kNumBatchTiles = 8;
+constexpr int kTuneSteps = 3;
+constexpr batch_tile kBatchTiles[kNumBatchTiles] = {{32, 16, 1}, {32, 32, 1}, {32, 64, 1}, {32, 128, 1},
+                                                    {32, 16, 2}, {32, 32, 2}, {32, 64, 2}, {32, 128, 2}};
 
 // launch (or, with occ, return the resident CTAs per SM of) tile candidate
 // `tile` of the persistent kernel; instantiated per real type in fused_f32.cu /

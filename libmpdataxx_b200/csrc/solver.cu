@@ -442,6 +442,10 @@ struct batch_impl : batch_base {
 
   void use_tile(int t) {
     if (t == items_tile) return;
+    const bool same_items = items_tile >= 0 && kBatchTiles[items_tile].lx == kBatchTiles[t].lx;
+    const int occ = fused2d_batched<T>(t, ni, iga, fct, nullptr, nullptr, 0, nullptr, 0, stream, true);
+    grid = std::max(1, std::max(1, occ) / kBatchTiles[t].occ_div) * n_sm;
+    if (same_items) { items_tile = t; return; }
     std::vector<int> P0(hs.size()), P1(hs.size());
     for (size_t p = 0; p < hs.size(); ++p) { P0[p] = hs[p]->st.n[0] - 1; P1[p] = hs[p]->st.n[1] - 1; }
     const auto items = fused2d_batch_items(t, ni, P0, P1);
@@ -454,8 +458,6 @@ struct batch_impl : batch_base {
     MPDX_CUDA(cudaMemcpyAsync(items_dev, items.data(), items.size() * sizeof(f2::item), cudaMemcpyHostToDevice, stream));
     MPDX_CUDA(cudaStreamSynchronize(stream));
     n_items = int(items.size());
-    const int occ = fused2d_batched<T>(t, ni, iga, fct, nullptr, nullptr, 0, nullptr, 0, stream, true);
-    grid = std::max(1, occ) * n_sm;
     items_tile = t;
   }
   void one_step(int parity) {
@@ -508,18 +510,22 @@ struct batch_impl : batch_base {
           h->st.tl[0] ^= 1;
         }
     } else {
-      // autotuning: one timed step per candidate tile, then the fastest one in a graph
+      // autotuning: every candidate timed over kTuneSteps consecutive steps (fewer if the
+      // call ends first; the next call times a candidate afresh), then the fastest in a graph
       while (s < nt && tile < 0) {
-        const int c = next_candidate++;
+        const int c = next_candidate;
         use_tile(c);
+        const long long k = std::min<long long>(kTuneSteps, nt - s);
         MPDX_CUDA(cudaEventRecord(ev_a, stream));
-        one_step(int(s & 1));
+        for (long long q = 0; q < k; ++q) one_step(int((s + q) & 1));
         MPDX_CUDA(cudaEventRecord(ev_b, stream));
         MPDX_CUDA(cudaEventSynchronize(ev_b));
         float ms = 0;
         MPDX_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
-        tune_ms[c] = ms;
-        ++s;
+        s += k;
+        if (k < kTuneSteps) continue;  // too few steps for a measurement
+        tune_ms[c] = ms / double(k);
+        ++next_candidate;
         if (next_candidate == kNumBatchTiles) {
           int best = 0;
           for (int q = 1; q < kNumBatchTiles; ++q)

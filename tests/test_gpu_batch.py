@@ -35,19 +35,21 @@ def test_batch_equals_individual_runs_fp32(opts, n_iters, mode):
     probs = setups.batched_problems(n=9, seed=11, lo=20, hi=300)
     alone = [make(s, opts, n_iters, np.float32) for s in probs]
     for r in alone:
-        r.advance(13)
+        r.advance(33)
     runs = [make(s, opts, n_iters, np.float32) for s in probs]
     b = concurr.batch(runs, mode=mode)
     b.advance(5)
-    b.advance(8)   # tuning spans calls; odd step counts exercise both parities
+    b.advance(8)   # tuning (8 candidates x 3 steps) spans calls; odd step counts exercise both parities
+    b.advance(20)
     for r, a in zip(runs, alone):
-        assert r.stats()["timestep"] == 13
+        assert r.stats()["timestep"] == 33
         np.testing.assert_array_equal(r.advectee(), a.advectee())
     info = b.info()
     assert info["n_problems"] == 9 and info["cells"] == sum(s["grid"][0] * s["grid"][1] for s in probs)
     if mode == "persistent":
-        assert info["tile_nt"] == 32 and info["tile_lx"] in (16, 32, 64, 128)
+        assert info["n_candidates"] == 8 and info["tile_nt"] == 32 and info["tile_lx"] in (16, 32, 64, 128)
         assert all(t > 0 for t in info["tune_ms"][:info["n_candidates"]])
+        assert info["grid"] > 0
     b.close()
 
 
