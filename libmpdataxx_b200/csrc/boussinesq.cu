@@ -634,6 +634,52 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
   for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < g.nrows; row += gridDim.x * blockDim.y) {
     int i = row, j = 0;
     if (g.nd == 3) { i = row / g.n[1]; j = row - i * g.n[1]; }
+    if constexpr (std::is_same<T, double>::value && NV == 1) {
+      // one search direction in FP64 (cr, and the first inner step of gcrk): pairs of
+      // points with 16-byte loads and stores (a row starts on a 128-byte boundary);
+      // both branches of the reference compute p = err + alpha p, lap_p = lap_err + alpha lap_p
+      const long long ob = g.nd == 3 ? off3(e, i, j, 0) : off3(e, i, 0, 0);
+      const T a0 = a[0];
+      for (int f0 = 2 * threadIdx.x; f0 < g.nf; f0 += 4 * blockDim.x) {
+        double2 E[2], L[2], H[2], PV[2], LV[2];
+        int nv[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int f = f0 + 2 * u * blockDim.x;
+          nv[u] = f + 1 < g.nf ? 2 : (f < g.nf ? 1 : 0);
+          const long long q = ob + f;
+          if (nv[u] == 2) {
+            E[u] = *reinterpret_cast<const double2 *>(eo + q);
+            L[u] = *reinterpret_cast<const double2 *>(leo + q);
+            H[u] = *reinterpret_cast<const double2 *>(phio + q);
+            PV[u] = *reinterpret_cast<const double2 *>(po[0] + q);
+            LV[u] = *reinterpret_cast<const double2 *>(lpo[0] + q);
+          } else if (nv[u] == 1) {
+            E[u] = make_double2(eo[q], 0.0); L[u] = make_double2(leo[q], 0.0); H[u] = make_double2(phio[q], 0.0);
+            PV[u] = make_double2(po[0][q], 0.0); LV[u] = make_double2(lpo[0][q], 0.0);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (nv[u] == 0) continue;
+          const long long q = ob + f0 + 2 * u * blockDim.x;
+          const double ph0 = H[u].x + b * PV[u].x, ph1 = H[u].y + b * PV[u].y;  // Phi += beta p_v
+          const double pn0 = E[u].x + a0 * PV[u].x, pn1 = E[u].y + a0 * PV[u].y;
+          const double ln0 = L[u].x + a0 * LV[u].x, ln1 = L[u].y + a0 * LV[u].y;
+          acc[0] = dd_add(acc[0], dd{ln0 * ln0, 0.0});
+          acc[1] = dd_add(acc[1], dd{E[u].x * ln0, 0.0});
+          if (nv[u] == 2) {
+            *reinterpret_cast<double2 *>(phio + q) = make_double2(ph0, ph1);
+            *reinterpret_cast<double2 *>(pdo + q) = make_double2(pn0, pn1);
+            *reinterpret_cast<double2 *>(lpdo + q) = make_double2(ln0, ln1);
+            acc[0] = dd_add(acc[0], dd{ln1 * ln1, 0.0});
+            acc[1] = dd_add(acc[1], dd{E[u].y * ln1, 0.0});
+          } else {
+            phio[q] = ph0; pdo[q] = pn0; lpdo[q] = ln0;
+          }
+        }
+      }
+    } else {
     for (int f0 = threadIdx.x; f0 < g.nf; f0 += U * blockDim.x) {
       long long o[U];
       bool ok[U];
@@ -679,6 +725,7 @@ __global__ void __launch_bounds__(kRedThreads, 3) k_gcr_direction(geom g, int kk
         acc[0] = dd_add(acc[0], dd{double(T(ln * ln)), 0.0});
         acc[1] = dd_add(acc[1], dd{double(T(ev[u] * ln)), 0.0});
       }
+    }
     }
   }
   double mx = 0, mn = 0;
