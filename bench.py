@@ -157,6 +157,45 @@ def build_run(w, dtype, torch):
     return run
 
 
+def bulk_copy_tiles(n, rows=32, ty=26, tz=56):
+    """(tiles whose planes come in as bulk-tensor copies, tiles) of one plane chunk
+    of the fused 3D kernel on an n^3 grid: the tiles inside the periods along j and k."""
+    P = n - 1
+    nz, ny = -(-P // tz), -(-P // ty)
+    inner = 0
+    if P >= 64 and P >= rows:
+        for t in range(ny * nz):
+            j0, k0 = (t // nz) * ty, (t % nz) * tz
+            inner += k0 >= 4 and k0 + 60 <= P and j0 >= 3 and j0 + rows - 3 <= P
+    return inner, ny * nz
+
+
+def plane_copy_ab(run, stream, torch, n, steps=10):
+    """Device time per step of the headline kernel with its bulk-tensor plane copies
+    (the default) and with per-thread copies in every tile, alternated twice,
+    outside the timed region; both modes give bitwise-identical fields."""
+    from libmpdataxx_b200 import _lib
+    L = _lib.lib()
+    res = {1: [], 0: []}
+    try:
+        for _ in range(2):
+            for mode in (1, 0):
+                L.mpdx_fused3d_bulk_copies(mode)
+                run.advance(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    run.advance(steps)
+                    e1.record(stream)
+                torch.cuda.synchronize()
+                res[mode].append(e0.elapsed_time(e1) / steps)
+    finally:
+        L.mpdx_fused3d_bulk_copies(1)
+    inner, tiles = bulk_copy_tiles(n)
+    return {"bulk_tensor_ms": min(res[1]), "per_thread_ms": min(res[0]), "tiles_with_bulk_copies": inner,
+            "tiles_per_plane_chunk": tiles}
+
+
 def cpu_port_time(host, steps, warmup):
     """The oracle's -Ofast + OpenMP build (the CPU restatement of the reference's
     path) on the whole 3D workload `host` (numpy advectee and advector views):
@@ -530,6 +569,10 @@ def main():
         run.close()
         dist_done(world)
         return
+    try:
+        copies = plane_copy_ab(run, stream, torch, args.size)
+    except Exception as e:  # noqa: BLE001
+        copies = {"error": f"{type(e).__name__}: {e}"}
     hbm, src = peaks()
     avg_launch_ms = statistics.mean(per)
     achieved = BYTES_PER_CELL * n_cells / (avg_launch_ms / 1e3) / 1e9
@@ -556,6 +599,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps,
         "clocks": clocks,
+        "plane_copies": copies,
     }
     line["error"] = fp64_error(w, state, steps_done, torch)
     del state

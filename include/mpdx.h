@@ -166,6 +166,16 @@ mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out);
 /* The handle's CUDA stream (cudaStream_t), for callers that order work with it. */
 void *mpdx_stream(mpdx_handle h);
 
+/* Plane copies of the fused FP32 3D kernel (all boundaries cyclic, iga or
+ * iga|fct, n_iters 2), process-wide: mode 1 (the default) copies each plane of
+ * a CTA whose tile lies inside the periods along the two inner axes with one
+ * bulk-tensor copy (TMA) counted on an mbarrier, mode 0 copies with per-thread
+ * asynchronous copies everywhere; both give bitwise-identical results.  A
+ * negative mode only queries.  Returns the mode before the call.  A bulk copy
+ * whose completion wait gives up (after about two seconds) makes the next call
+ * on any handle fail with MPDX_E_CUDA. */
+int mpdx_fused3d_bulk_copies(int mode);
+
 /* Message of the last failing call on this handle ("" if none). */
 const char *mpdx_last_error(mpdx_handle h);
 

@@ -28,7 +28,7 @@ VAB_NONE, VAB_EXPL, VAB_IMPL = 0, 1, 2
 
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
-           "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_last_error",
+           "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_fused3d_bulk_copies", "mpdx_last_error",
            "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc", "mpdx_batch_create", "mpdx_batch_advance",
            "mpdx_batch_get_info", "mpdx_batch_sync", "mpdx_batch_last_error", "mpdx_batch_destroy",
            "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
@@ -96,6 +96,8 @@ def lib():
     L.mpdx_stats.restype = ctypes.c_int
     L.mpdx_stream.argtypes = [vp]
     L.mpdx_stream.restype = vp
+    L.mpdx_fused3d_bulk_copies.argtypes = [ctypes.c_int]
+    L.mpdx_fused3d_bulk_copies.restype = ctypes.c_int
     L.mpdx_last_error.argtypes = [vp]
     L.mpdx_last_error.restype = ctypes.c_char_p
     L.mpdx_destroy.argtypes = [vp]

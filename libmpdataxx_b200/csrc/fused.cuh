@@ -23,6 +23,18 @@ template <class T> void fused2d_launch(const mpdata_state<T> &st, const fused2d_
 template <class T> bool fused_seams_consistent(mpdata_state<T> &st, double *scratch);
 template <class T> bool fused_configurable(const mpdata_state<T> &st);
 
+// The plane copies of the fused FP32 3D kernel, process-wide: 1 (the default)
+// bulk-tensor copies in the CTAs whose tile lies inside the periods along j and
+// k, 0 per-thread copies everywhere; a negative mode only queries.  Returns the
+// mode before the call.
+int fused3d_bulk_copies(int mode);
+// The host-mapped status word of those bulk copies: a completion wait that gave
+// up sets *host (both null until the first launch that uses bulk copies).
+struct copy_wait_word {
+  unsigned *host = nullptr, *dev = nullptr;
+};
+copy_wait_word &fused_copy_wait_flag();
+
 // 2D step descriptor of equation e whose input is time level tl
 template <class T>
 f2::prob<T> fused2d_prob(const mpdata_state<T> &st, int e, int tl) {

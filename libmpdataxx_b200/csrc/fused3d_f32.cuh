@@ -36,7 +36,15 @@
 // the limiter uses the same antidiffusive velocities as the limited fluxes
 // (FCT bounds).  The FP64 instantiation of fused3d.cuh keeps the reference's
 // operation order for bitwise parity.
+//
+// Plane prefetch: a CTA whose tile lies inside the periods along j and k (most
+// of them) brings each plane of the march in with one bulk-tensor copy
+// (cp.async.bulk.tensor, issued by one thread) whose completion is counted on an
+// mbarrier in bytes, two barriers alternating by step; the other CTAs copy their
+// quads with per-thread cp.async, wrapping around the seams.
 #pragma once
+
+#include <cuda.h>
 
 #include "fused3d.cuh"
 
@@ -103,8 +111,9 @@ __device__ __forceinline__ Q adiff(const Q &C, const Q &nx, const Q &S1, const Q
 // the march unrolled by 4 every slot is a compile-time constant: plane x lives
 // in slot (x - ts) & 3 of its ring, ts being the first step of the CTA.
 //   S0: psi^n planes t-1, t, t+1, t+2; with FCT the prefetch of plane t+3
-//       into the slot of t-1 is issued once the limiter has read t-1 (each
-//       thread reads and refills only its own quad of that slot);
+//       into the slot of t-1 is issued once the limiter has read t-1 (with
+//       per-thread copies each thread reads and refills only its own quad of
+//       that slot; the bulk copy waits for the last warp);
 //   G0: GC_x planes t-1, t, t+1, prefetch t+2;  G1, G2: t, t+1, prefetch t+2;
 //   S1: psi1 planes t-1, t, t+1;  CY, BU, BD: planes t-1, t
 template <int CR>
@@ -149,8 +158,60 @@ __device__ __forceinline__ void cpq(unsigned a, const float *row, bool contig, u
   }
 }
 
+// ---- bulk-tensor (TMA) plane copies ----
+// Tensor maps of the four input fields, each a 3D tiled map over (k, j, x) with
+// extents (P2, P1, P0) and a box of 64 columns x CR rows x 1 plane: one box is one
+// canvas plane of a CTA whose tile does not cross a periodic seam, at the canvas
+// origin (k0 - 4, j0 - 3), k0 a multiple of 56 (16-byte aligned x coordinate).
+struct tma_planes {
+  CUtensorMap in, g0, g1, g2;
+  unsigned *timeout;   // host-mapped word set when a completion wait gives up
+  int on;              // 0: every CTA copies with per-thread cp.async
+};
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// one arrival that also adds `bytes` to the transaction count of the current phase
+__device__ __forceinline__ void mbar_arrive_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// waits for the phase of parity `parity` to complete, for about two seconds at
+// most; a wait that gives up sets *flag and clears `live`, after which this
+// thread's further waits return at once (the results of the launch are invalid
+// and the host reports the flag)
+__device__ __forceinline__ void mbar_wait(unsigned bar, unsigned parity, bool &live, unsigned *flag) {
+  if (!live || mbar_test(bar, parity)) return;
+  const long long t0 = clock64();
+  while (!mbar_test(bar, parity)) {
+    if (clock64() - t0 > (1LL << 32)) {
+      live = false;
+      if (flag) { *reinterpret_cast<volatile unsigned *>(flag) = 1u; __threadfence_system(); }
+      return;
+    }
+  }
+}
+// one box of a 3D map into shared memory; completion counted on `bar` in bytes
+__device__ __forceinline__ void tma_plane(unsigned dst, const CUtensorMap *map, unsigned bar, int k, int j, int x) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(bar), "r"(k), "r"(j), "r"(x)
+      : "memory");
+}
+
 template <bool FCT, int CR>
-__global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> A) {
+__global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> A, const __grid_constant__ tma_planes TM) {
   using C = canvas_s<CR>;
   constexpr int N = C::N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -168,6 +229,12 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
   const int tile = blockIdx.x;
   const int j0 = (tile / A.tiles_z) * C::TY, k0 = (tile % A.tiles_z) * C::TZ;
   const int x0 = blockIdx.y * A.LX, x1 = min(x0 + A.LX, A.P0);
+  // bulk-tensor plane copies for a tile inside the periods along j and k, into
+  // 128-byte aligned planes; the two barriers and the warp counter of phase C
+  // follow the planes
+  const unsigned bar0 = s_base + unsigned(C::total * N * 4), bar1 = bar0 + 8u, cnt = bar0 + 16u;
+  const bool tma = TM.on && k0 >= 4 && k0 + 60 <= A.P2 && j0 >= 3 && j0 + CR - 3 <= A.P1 && (s_base & 127u) == 0u;
+  bool live = true;
 
   const int jg = f3::pmod(j0 - 3 + r, A.P1);
   const int kb = k0 - 4 + 4 * q;
@@ -192,6 +259,12 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
   };
 
   for (int p = tid; p < C::total * N; p += C::NT) sm[p] = 0.f;
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar1, 1);
+    asm volatile("st.shared.u32 [%0], 0;" ::"r"(cnt) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   __syncthreads();
 
   for (int x = ts - 1; x <= ts + 2; ++x) cp(slot(C::S0, x), A.in, x);
@@ -199,6 +272,8 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
   for (int x = ts; x <= ts + 1; ++x) { cp(slot(C::G1, x), A.g1, x); cp(slot(C::G2, x), A.g2, x); }
   f3::cp_commit();
   f3::cp_wait_all();
+  // the planes written so far (zeros, per-thread copies) before any bulk copy rewrites them
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
   const Q zero = qd::bc<float>(0.f);
   // carried along the march (own quad): psi1 at t-1, t; the upwind x-flux
@@ -227,14 +302,33 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
     constexpr int S1m = (C::S1 + M) * N * 4, S1c = (C::S1 + T0) * N * 4, S1p = (C::S1 + T1) * N * 4;
     constexpr int CYc = (C::CY + C2) * N * 4, BUc = (C::BU + C2) * N * 4, BDc = (C::BD + C2) * N * 4;
     constexpr int CYm = (C::CY + M2) * N * 4, BUm = (C::BU + M2) * N * 4, BDm = (C::BD + M2) * N * 4;
-    f3::cp_wait_all();
+    // the copies of the previous step (barrier (PH - 1) & 1, its use (PH - 1) >> 1
+    // in the group of four steps); the first step's planes came in above
+    constexpr int PB = (PH + 3) & 3;
+    const unsigned bar = (PH & 1) ? bar1 : bar0;
+    if (tma) {
+      if (t != ts) mbar_wait((PB & 1) ? bar1 : bar0, unsigned(PB >> 1), live, TM.timeout);
+    } else {
+      f3::cp_wait_all();
+    }
     __syncthreads();
-    // prefetch: the advector planes t+2 and (without FCT) psi^n plane t+3
-    if (!FCT) cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
-    cpq<G0n>(a_me, A.g0.o + ((long long)xg * A.g0.s0 + o_g0), contig, wk, A.P2);
-    cpq<G1n>(a_me, A.g1.o + ((long long)xg * A.g1.s0 + o_g1), contig, wk, A.P2);
-    cpq<G2n>(a_me, A.g2.o + ((long long)xg * A.g2.s0 + o_g2), contig, wk, A.P2);
-    f3::cp_commit();
+    // prefetch: the advector planes t+2 and psi^n plane t+3 (with FCT issued below,
+    // once the limiter has read the slot of t-1; its bytes are counted here)
+    if (tma) {
+      if (tid == 0) {
+        mbar_arrive_tx(bar, 4u * N * 4u);
+        if (!FCT) tma_plane(s_base + S0n, &TM.in, bar, k0 - 4, j0 - 3, xi);
+        tma_plane(s_base + G0n, &TM.g0, bar, k0 - 4, j0 - 3, xg);
+        tma_plane(s_base + G1n, &TM.g1, bar, k0 - 4, j0 - 3, xg);
+        tma_plane(s_base + G2n, &TM.g2, bar, k0 - 4, j0 - 3, xg);
+      }
+    } else {
+      if (!FCT) cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
+      cpq<G0n>(a_me, A.g0.o + ((long long)xg * A.g0.s0 + o_g0), contig, wk, A.P2);
+      cpq<G1n>(a_me, A.g1.o + ((long long)xg * A.g1.s0 + o_g1), contig, wk, A.P2);
+      cpq<G2n>(a_me, A.g2.o + ((long long)xg * A.g2.s0 + o_g2), contig, wk, A.P2);
+      f3::cp_commit();
+    }
     xg = xg + 1 == A.P0 ? 0 : xg + 1;
 
     // ---- A: psi1 at plane t+1 (mpdata_osc_3d.hpp:181-197) ----
@@ -313,9 +407,20 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
         stq<BUc>(a_me, bu_c);
         stq<BDc>(a_me, bd_c);
       }
-      // psi^n plane t+3 into the slot of t-1, now read
-      cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
-      f3::cp_commit();
+      // psi^n plane t+3 into the slot of t-1, now read: per thread its own quad;
+      // in bulk by the last warp through here (the counter's acquire-release
+      // orders every warp's reads of the slot before the copy)
+      if (tma) {
+        __syncwarp();
+        if (lane == 0) {
+          unsigned old;
+          asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;" : "=r"(old) : "r"(cnt) : "memory");
+          if (old % unsigned(C::NT / 32) == unsigned(C::NT / 32 - 1)) tma_plane(s_base + S0n, &TM.in, bar, k0 - 4, j0 - 3, xi);
+        }
+      } else {
+        cpq<S0n>(a_me, A.in.o + ((long long)xi * A.in.s0 + o_in), contig, wk, A.P2);
+        f3::cp_commit();
+      }
     }
     xi = xi + 1 == A.P0 ? 0 : xi + 1;
 
@@ -380,7 +485,14 @@ __global__ void __launch_bounds__(CR * 16, 1) k_fused3d_s(const f3::args<float> 
     step(ts + u + 2, phase<2>{});
     step(ts + u + 3, phase<3>{});
   }
-  f3::cp_wait_all();
+  // no copy may land after the CTA has left: the last step (phase 3) counted its
+  // copies on barrier 1, second use of the group (parity 1)
+  if (tma) {
+    bool fin = true;
+    mbar_wait(bar1, 1u, fin, TM.timeout);
+  } else {
+    f3::cp_wait_all();
+  }
 }
 
 }  // namespace f3s

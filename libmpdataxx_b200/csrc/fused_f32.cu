@@ -1,7 +1,18 @@
 // FP32 instantiation of the fused kernels (FMA contraction allowed).
 #include "fused_impl.cuh"
 
+#include <atomic>
+
 namespace mpdx {
+int fused3d_bulk_copies(int mode) {
+  static std::atomic<int> m{1};
+  return mode < 0 ? m.load() : m.exchange(mode != 0 ? 1 : 0);
+}
+copy_wait_word &fused_copy_wait_flag() {
+  static copy_wait_word w;
+  return w;
+}
+
 template bool fused_configurable<float>(const mpdata_state<float> &);
 template void fused3d_launch<float>(mpdata_state<float> &, int, cudaStream_t);
 template void fused2d_plan_init<float>(const mpdata_state<float> &, fused2d_plan<float> &);

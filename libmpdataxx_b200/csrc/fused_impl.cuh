@@ -3,6 +3,10 @@
 // gets its own compiler flags.
 #pragma once
 
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "fused.cuh"
@@ -54,16 +58,79 @@ static void launch3(const f3::args<T> &a, cudaStream_t s, dim3 grid) {
   MPDX_LAUNCH_CHECK();
 }
 
+// the driver's tensor-map encoder, found through the runtime's entry-point query
+// (so that the library links no driver library); null where the query fails
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// the tiled map of one FP32 field over (k, j, x) with extents (P2, P1, P0) and a
+// box of one canvas plane (64 columns x `rows` rows); false where the field's
+// layout does not meet the copy's rules (16-byte aligned origin and strides)
+inline bool plane_map(CUtensorMap &m, const dfield<float> &f, const f3::args<float> &a, int rows) {
+  const auto enc = tensor_map_encoder();
+  if (!enc || f.s2 != 1 || (reinterpret_cast<std::uintptr_t>(f.o) & 15u) || f.s1 <= 0 || f.s0 <= 0 || (f.s1 % 4) ||
+      (f.s0 % 4))
+    return false;
+  const cuuint64_t dims[3] = {cuuint64_t(a.P2), cuuint64_t(a.P1), cuuint64_t(a.P0)};
+  const cuuint64_t strides[2] = {cuuint64_t(f.s1) * 4u, cuuint64_t(f.s0) * 4u};
+  const cuuint32_t box[3] = {64u, cuuint32_t(rows), 1u}, elem[3] = {1u, 1u, 1u};
+  return enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(f.o), dims, strides, box, elem,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the host-mapped word that a bulk-copy wait which gives up sets (allocated at the
+// first launch that uses bulk copies; null where that allocation fails)
+inline unsigned *copy_wait_flag_device() {
+  auto &f = fused_copy_wait_flag();
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    unsigned *h = nullptr, *d = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&h), sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return;
+    }
+    *h = 0u;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&d), h, 0) != cudaSuccess) {
+      (void)cudaGetLastError();
+      cudaFreeHost(h);
+      return;
+    }
+    f.dev = d;
+    f.host = h;
+  });
+  return f.dev;
+}
+
 // the FP32 kernel with the regrouped single-precision arithmetic (iga variants)
 template <bool FCT>
 static void launch3s(const f3::args<float> &a, cudaStream_t s, dim3 grid) {
   constexpr int CR = tiles<float>::CR;
   using C = f3s::canvas_s<CR>;
   auto kern = f3s::k_fused3d_s<FCT, CR>;
-  const size_t bytes = size_t(C::total) * C::N * sizeof(float);
+  // the planes, then two mbarriers and the warp counter
+  const size_t bytes = size_t(C::total) * C::N * sizeof(float) + 32;
   static bool attr = false;
   if (!attr) { set_smem(kern, bytes); attr = true; }
-  kern<<<grid, C::NT, bytes, s>>>(a);
+  f3s::tma_planes m{};
+  // bulk copies only where some tile lies inside the periods along j and k
+  if (fused3d_bulk_copies(-1) == 1 && a.P2 >= 64 && a.P1 >= CR) {
+    m.timeout = copy_wait_flag_device();
+    m.on = m.timeout && plane_map(m.in, a.in, a, CR) && plane_map(m.g0, a.g0, a, CR) && plane_map(m.g1, a.g1, a, CR) &&
+           plane_map(m.g2, a.g2, a, CR);
+  }
+  kern<<<grid, C::NT, bytes, s>>>(a, m);
   MPDX_LAUNCH_CHECK();
 }
 

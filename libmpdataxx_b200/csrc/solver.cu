@@ -587,12 +587,26 @@ inline void check_bounds() {
 #endif
 }
 
+// a bulk plane copy of the fused 3D kernel whose completion wait gave up (a
+// host-mapped word that the kernel sets; read without waiting for the device)
+inline void check_copy_waits() {
+  auto &w = mpdx::fused_copy_wait_flag();
+  if (!w.host) return;
+  volatile unsigned *v = w.host;
+  if (*v) {
+    *v = 0u;
+    throw mpdx::error(MPDX_E_CUDA, "fused 3D kernel: a bulk plane copy did not complete within its wait limit; "
+                                   "the results of the steps since the previous call are invalid");
+  }
+}
+
 template <class F>
 mpdx_status guarded(mpdx_handle h, F f) {
   if (!h || !h->impl) return MPDX_E_ARG;
   try {
     f();
     check_bounds();
+    check_copy_waits();
     h->impl->err.clear();
     return MPDX_OK;
   } catch (const mpdx::error &e) {
@@ -824,6 +838,8 @@ mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
 
 void *mpdx_stream(mpdx_handle h) { return (h && h->impl) ? (void *)h->impl->stream : nullptr; }
 
+int mpdx_fused3d_bulk_copies(int mode) { return mpdx::fused3d_bulk_copies(mode); }
+
 const char *mpdx_last_error(mpdx_handle h) { return (h && h->impl) ? h->impl->err.c_str() : "invalid handle"; }
 
 }  // extern "C"
@@ -872,6 +888,7 @@ static mpdx_status batch_guarded(mpdx_batch_handle b, const std::function<void()
   try {
     f();
     check_bounds();
+    check_copy_waits();
     b->impl->err.clear();
     return MPDX_OK;
   } catch (const mpdx::error &e) {

@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "mpdx.h")
 
 def declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(mpdx_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(mpdx_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_header_declares_python_binding_exports():
@@ -138,3 +138,14 @@ def test_async_transfer_arguments():
     L = _lib.lib()
     assert L.mpdx_set_field_async(None, 0, 0, None) == _lib.MPDX_E_ARG
     assert L.mpdx_get_field_async(None, 0, 0, None) == _lib.MPDX_E_ARG
+
+
+def test_fused3d_bulk_copy_mode():
+    """The process-wide plane-copy mode of the fused FP32 3D kernel: bulk copies by
+    default, a negative mode only queries, any nonzero mode means on."""
+    L = _lib.lib()
+    assert L.mpdx_fused3d_bulk_copies(-1) == 1
+    assert L.mpdx_fused3d_bulk_copies(0) == 1
+    assert L.mpdx_fused3d_bulk_copies(-1) == 0
+    assert L.mpdx_fused3d_bulk_copies(5) == 0
+    assert L.mpdx_fused3d_bulk_copies(-1) == 1
