@@ -176,6 +176,30 @@ void *mpdx_stream(mpdx_handle h);
  * on any handle fail with MPDX_E_CUDA. */
 int mpdx_fused3d_bulk_copies(int mode);
 
+/* Planes per CTA of the fused 3D kernel (the length of the x-chunk one CTA
+ * marches through), process-wide: 0 (the default) lets each handle tune it on
+ * its first fused steps, a positive value fixes it (a multiple of 4 from 8 to
+ * 512); a negative value only queries.  Returns the setting before the call, or
+ * -1 for an invalid value (which changes nothing).  Every value gives
+ * bitwise-identical fields: a point is computed by the same operations whichever
+ * CTA holds it.  No reference counterpart (the reference's threads split the
+ * domain along x by its own rule, concurr/detail/concurr_common.hpp). */
+int mpdx_fused3d_planes_per_cta(int lx);
+
+/* The tuner of a handle that takes the fused 3D path: its first fused step runs
+ * untimed with 64 planes per CTA, then each candidate in lx[] runs two timed
+ * steps (each waiting for its own end on the host), then the fastest is kept
+ * for the handle's life.  chosen is 0 while tuning (or on a handle that has not
+ * taken the fused 3D path); ms[] holds each candidate's time per step once the
+ * choice is made. */
+typedef struct {
+  int chosen;
+  int n_candidates;
+  int lx[8];
+  float ms[8];
+} mpdx_tuning3d;
+mpdx_status mpdx_fused3d_tuning(mpdx_handle h, mpdx_tuning3d *out);
+
 /* Message of the last failing call on this handle ("" if none). */
 const char *mpdx_last_error(mpdx_handle h);
 

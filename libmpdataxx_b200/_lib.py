@@ -28,7 +28,8 @@ VAB_NONE, VAB_EXPL, VAB_IMPL = 0, 1, 2
 
 # every entry point declared in include/mpdx.h
 EXPORTS = ["mpdx_config_default", "mpdx_create", "mpdx_set_field", "mpdx_get_field", "mpdx_set_field_device",
-           "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_fused3d_bulk_copies", "mpdx_last_error",
+           "mpdx_get_field_device", "mpdx_set_field_async", "mpdx_get_field_async", "mpdx_advance", "mpdx_sync", "mpdx_stats", "mpdx_stream", "mpdx_fused3d_bulk_copies", "mpdx_fused3d_planes_per_cta",
+           "mpdx_fused3d_tuning", "mpdx_last_error",
            "mpdx_create_error", "mpdx_destroy", "mpdx_field_stats_noalloc", "mpdx_batch_create", "mpdx_batch_advance",
            "mpdx_batch_get_info", "mpdx_batch_sync", "mpdx_batch_last_error", "mpdx_batch_destroy",
            "mpdx_pcnet_create", "mpdx_pcnet_create_error", "mpdx_pcnet_num_params", "mpdx_pcnet_set_params",
@@ -57,6 +58,12 @@ class StepStats(ctypes.Structure):
                 ("min", ctypes.c_double), ("max", ctypes.c_double), ("gcr_iters", ctypes.c_int64),
                 ("gcr_iters_total", ctypes.c_int64), ("gcr_residual", ctypes.c_double), ("path", ctypes.c_int),
                 ("gcr_ms", ctypes.c_double), ("gcr_fallback", ctypes.c_int)]
+
+
+class Tuning3D(ctypes.Structure):
+    """mpdx_tuning3d: the fused 3D kernel's chunk-length tuner of one handle."""
+    _fields_ = [("chosen", ctypes.c_int), ("n_candidates", ctypes.c_int), ("lx", ctypes.c_int * 8),
+                ("ms", ctypes.c_float * 8)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -98,6 +105,10 @@ def lib():
     L.mpdx_stream.restype = vp
     L.mpdx_fused3d_bulk_copies.argtypes = [ctypes.c_int]
     L.mpdx_fused3d_bulk_copies.restype = ctypes.c_int
+    L.mpdx_fused3d_planes_per_cta.argtypes = [ctypes.c_int]
+    L.mpdx_fused3d_planes_per_cta.restype = ctypes.c_int
+    L.mpdx_fused3d_tuning.argtypes = [vp, ctypes.POINTER(Tuning3D)]
+    L.mpdx_fused3d_tuning.restype = ctypes.c_int
     L.mpdx_last_error.argtypes = [vp]
     L.mpdx_last_error.restype = ctypes.c_char_p
     L.mpdx_destroy.argtypes = [vp]

@@ -198,6 +198,13 @@ class cuda:
         _check(self.L, self.h, self.L.mpdx_stats(self.h, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in _lib.StepStats._fields_}
 
+    def tuning3d(self):
+        """The fused 3D kernel's planes-per-CTA tuner on this handle (no counterpart in the
+        reference): {"chosen": planes per CTA (0 while tuning), "candidates": [(planes, ms per step)]}."""
+        t = _lib.Tuning3D()
+        _check(self.L, self.h, self.L.mpdx_fused3d_tuning(self.h, ctypes.byref(t)))
+        return {"chosen": t.chosen, "candidates": [(t.lx[q], t.ms[q]) for q in range(t.n_candidates)]}
+
     # -- learned GCR preconditioner (Boussinesq solvers; no counterpart in the reference) --
     def precond_record(self, max_pairs):
         """Keep the (initial residual, correction) pair of each of the next max_pairs pressure solves."""

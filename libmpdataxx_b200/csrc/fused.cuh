@@ -16,7 +16,8 @@
 namespace mpdx {
 
 // launchers (one translation unit per real type)
-template <class T> void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s);
+// one step of equation e with `lx` planes per CTA (0: the default of the type)
+template <class T> void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s, int lx);
 template <class T> struct fused2d_plan;
 template <class T> void fused2d_plan_init(const mpdata_state<T> &st, fused2d_plan<T> &p);
 template <class T> void fused2d_launch(const mpdata_state<T> &st, const fused2d_plan<T> &p, int e, cudaStream_t s);
@@ -34,6 +35,11 @@ struct copy_wait_word {
   unsigned *host = nullptr, *dev = nullptr;
 };
 copy_wait_word &fused_copy_wait_flag();
+// Planes per CTA of the fused 3D kernel, process-wide: 0 (the default) lets each
+// handle tune it on its first fused steps, a positive value (a multiple of 4 from
+// 8 to 512) fixes it; a negative value only queries.  Returns the setting before
+// the call; an invalid value changes nothing and returns -1.
+int fused3d_planes_setting(int lx);
 
 // 2D step descriptor of equation e whose input is time level tl
 template <class T>
@@ -70,6 +76,24 @@ template <class T>
 struct fused_engine {
   int known = -1;  // cached seam check: -1 unknown, 0 inconsistent, 1 consistent
   fused2d_plan<T> plan2;
+  // chunk-length tuner of the 3D kernel: its first fused step runs untimed with the
+  // default, then every candidate runs kTune3 timed steps (each step synchronises
+  // on its end), then the fastest is kept.  The planes per CTA change only which
+  // CTA computes a point, not how, so every candidate gives the same fields.
+  static constexpr int kNumCand3 = 4, kTune3 = 2;
+  static constexpr int kCand3[kNumCand3] = {32, 64, 96, 128};
+  int lx3 = 0;        // chosen planes per CTA (0 while tuning)
+  int tune_pos = -1;  // -1 before the untimed step, then timed steps so far
+  float tune_ms[kNumCand3] = {};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+
+  fused_engine() = default;
+  fused_engine(const fused_engine &) = delete;
+  fused_engine &operator=(const fused_engine &) = delete;
+  ~fused_engine() {
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
 
   void init(const mpdata_state<T> &st) {
     if (st.nd == 2) fused2d_plan_init(st, plan2);
@@ -84,9 +108,43 @@ struct fused_engine {
   void invalidate() { known = -1; }
 
   void step(mpdata_state<T> &st) {
+    if (st.nd != 3) {
+      for (int e = 0; e < st.n_eqns; ++e) {
+        fused2d_launch(st, plan2, e, st.stream);
+        st.tl[e] ^= 1;
+      }
+      return;
+    }
+    const int fixed = fused3d_planes_setting(-1);
+    if (fixed > 0 || lx3 > 0 || tune_pos < 0) {
+      launch3d(st, fixed > 0 ? fixed : lx3);
+      if (fixed <= 0 && tune_pos < 0) tune_pos = 0;
+      return;
+    }
+    const int c = tune_pos / kTune3;
+    if (!ev[0]) {
+      MPDX_CUDA(cudaEventCreate(&ev[0]));
+      MPDX_CUDA(cudaEventCreate(&ev[1]));
+    }
+    MPDX_CUDA(cudaEventRecord(ev[0], st.stream));
+    launch3d(st, kCand3[c]);
+    MPDX_CUDA(cudaEventRecord(ev[1], st.stream));
+    MPDX_CUDA(cudaEventSynchronize(ev[1]));
+    float ms = 0.f;
+    MPDX_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    tune_ms[c] += ms / float(kTune3);
+    if (++tune_pos == kNumCand3 * kTune3) {
+      int best = 0;
+      for (int q = 1; q < kNumCand3; ++q)
+        if (tune_ms[q] < tune_ms[best]) best = q;
+      lx3 = kCand3[best];
+    }
+  }
+
+ private:
+  void launch3d(mpdata_state<T> &st, int lx) {
     for (int e = 0; e < st.n_eqns; ++e) {
-      if (st.nd == 3) fused3d_launch(st, e, st.stream);
-      else fused2d_launch(st, plan2, e, st.stream);
+      fused3d_launch(st, e, st.stream, lx);
       st.tl[e] ^= 1;
     }
   }

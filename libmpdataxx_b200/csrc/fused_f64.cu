@@ -4,7 +4,7 @@
 
 namespace mpdx {
 template bool fused_configurable<double>(const mpdata_state<double> &);
-template void fused3d_launch<double>(mpdata_state<double> &, int, cudaStream_t);
+template void fused3d_launch<double>(mpdata_state<double> &, int, cudaStream_t, int);
 template void fused2d_plan_init<double>(const mpdata_state<double> &, fused2d_plan<double> &);
 template void fused2d_launch<double>(const mpdata_state<double> &, const fused2d_plan<double> &, int, cudaStream_t);
 template bool fused_seams_consistent<double>(mpdata_state<double> &, double *);

@@ -135,9 +135,9 @@ static void launch3s(const f3::args<float> &a, cudaStream_t s, dim3 grid) {
 }
 
 template <class T>
-void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s) {
+void fused3d_launch(mpdata_state<T> &st, int e, cudaStream_t s, int lx) {
   using C = f3::canvas<tiles<T>::CR>;
-  constexpr int LX = tiles<T>::LX3;
+  const int LX = lx > 0 ? lx : tiles<T>::LX3;
   f3::args<T> a;
   a.in = st.psi[e][st.tl[e]].v;
   a.out = st.psi[e][st.tl[e] ^ 1].v;

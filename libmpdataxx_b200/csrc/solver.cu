@@ -134,6 +134,8 @@ struct solver_base {
   virtual double precond_loss_grad(const double *, const double *, double, float *) {
     throw error(MPDX_E_UNSUPPORTED, "no pressure solve in this solver");
   }
+  // the fused 3D kernel's chunk-length tuner (MPDATA solvers only)
+  virtual void tuning3d(mpdx_tuning3d *out) { std::memset(out, 0, sizeof(*out)); }
 };
 
 // common transfer machinery for solvers built on mpdata_state<T>
@@ -275,6 +277,16 @@ struct mpdata_solver : solver_base {
     out->timestep = st.timestep;
     stat.reduce(st, st.psi[0][st.tl[0]], out);
     out->path = last_path;
+  }
+  void tuning3d(mpdx_tuning3d *out) override {
+    std::memset(out, 0, sizeof(*out));
+    const int fixed = fused3d_planes_setting(-1);
+    out->chosen = fixed > 0 ? fixed : fus.lx3;
+    out->n_candidates = fused_engine<T>::kNumCand3;
+    for (int q = 0; q < fused_engine<T>::kNumCand3; ++q) {
+      out->lx[q] = fused_engine<T>::kCand3[q];
+      out->ms[q] = fus.lx3 > 0 ? fus.tune_ms[q] : 0.f;
+    }
   }
 };
 
@@ -839,6 +851,13 @@ mpdx_status mpdx_stats(mpdx_handle h, mpdx_step_stats *out) {
 void *mpdx_stream(mpdx_handle h) { return (h && h->impl) ? (void *)h->impl->stream : nullptr; }
 
 int mpdx_fused3d_bulk_copies(int mode) { return mpdx::fused3d_bulk_copies(mode); }
+
+int mpdx_fused3d_planes_per_cta(int lx) { return mpdx::fused3d_planes_setting(lx); }
+
+mpdx_status mpdx_fused3d_tuning(mpdx_handle h, mpdx_tuning3d *out) {
+  if (!out) return MPDX_E_ARG;
+  return guarded(h, [&] { h->impl->tuning3d(out); });
+}
 
 const char *mpdx_last_error(mpdx_handle h) { return (h && h->impl) ? h->impl->err.c_str() : "invalid handle"; }
 

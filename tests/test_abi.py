@@ -40,8 +40,9 @@ def test_struct_layout_matches_header():
     #include <stddef.h>
     #include "{HEADER}"
     int main() {{
-      printf("%zu %zu %zu %zu\\n", sizeof(mpdx_config), offsetof(mpdx_config, prs_fp64),
-             sizeof(mpdx_step_stats), offsetof(mpdx_step_stats, path));
+      printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(mpdx_config), offsetof(mpdx_config, prs_fp64),
+             sizeof(mpdx_step_stats), offsetof(mpdx_step_stats, path), sizeof(mpdx_tuning3d),
+             offsetof(mpdx_tuning3d, ms));
       return 0;
     }}"""
     with tempfile.TemporaryDirectory() as d:
@@ -51,7 +52,8 @@ def test_struct_layout_matches_header():
         subprocess.run(["gcc", "-std=c99", "-o", exe, c], check=True)
         vals = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     assert vals == [ctypes.sizeof(_lib.Config), _lib.Config.prs_fp64.offset,
-                    ctypes.sizeof(_lib.StepStats), _lib.StepStats.path.offset]
+                    ctypes.sizeof(_lib.StepStats), _lib.StepStats.path.offset,
+                    ctypes.sizeof(_lib.Tuning3D), _lib.Tuning3D.ms.offset]
 
 
 def _cfg(**kw):
@@ -149,3 +151,19 @@ def test_fused3d_bulk_copy_mode():
     assert L.mpdx_fused3d_bulk_copies(-1) == 0
     assert L.mpdx_fused3d_bulk_copies(5) == 0
     assert L.mpdx_fused3d_bulk_copies(-1) == 1
+
+
+def test_fused3d_planes_per_cta_setting():
+    """The process-wide planes per CTA of the fused 3D kernel: tuned (0) by default,
+    a negative value only queries, invalid values change nothing and return -1."""
+    L = _lib.lib()
+    assert L.mpdx_fused3d_planes_per_cta(-1) == 0
+    for bad in (4, 6, 514, 1000, 33):
+        assert L.mpdx_fused3d_planes_per_cta(bad) == -1
+    assert L.mpdx_fused3d_planes_per_cta(-1) == 0
+    assert L.mpdx_fused3d_planes_per_cta(96) == 0
+    assert L.mpdx_fused3d_planes_per_cta(-1) == 96
+    assert L.mpdx_fused3d_planes_per_cta(0) == 96
+    assert L.mpdx_fused3d_planes_per_cta(-1) == 0
+    out = _lib.Tuning3D()
+    assert L.mpdx_fused3d_tuning(None, ctypes.byref(out)) == _lib.MPDX_E_ARG

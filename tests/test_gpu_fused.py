@@ -129,3 +129,58 @@ def test_fused3d_fp32_bulk_copies_bitwise(grid, opts):
     orc.advance(6)
     b = orc.advectee()
     assert np.abs(res[1].astype(np.float64) - b).max() / np.abs(b).max() <= 1e-5
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_fused3d_planes_per_cta_bitwise(dtype):
+    """The planes per CTA of the fused 3D kernel (the x-chunk one CTA marches
+    through, after its warm-up planes) change only which CTA computes a point:
+    chunks of 8 to 512 planes give bitwise-identical fields (130 x 64 x 130,
+    iga|fct, 5 steps; 17 chunks of 8 down to one chunk of 512), so tuning the chunk
+    length never changes a result."""
+    from libmpdataxx_b200 import _lib
+    L = _lib.lib()
+    s = periodic_setup((130, 64, 130), seed=23)
+    res = {}
+    try:
+        for lx in (64, 8, 32, 96, 128, 512):
+            assert L.mpdx_fused3d_planes_per_cta(lx) >= 0
+            run, _ = run_both(s, o.iga | o.fct, 2, dtype, 5)
+            run.advance(5)
+            assert run.stats()["path"] == FUSED
+            assert run.tuning3d()["chosen"] == lx
+            res[lx] = run.advectee()
+    finally:
+        L.mpdx_fused3d_planes_per_cta(0)
+    for lx, a in res.items():
+        assert np.array_equal(a, res[64]), lx
+
+
+def test_fused3d_tuner_keeps_fastest():
+    """With the process-wide setting at 0 a handle tunes its planes per CTA on its
+    first fused steps (one untimed step, two timed steps per candidate), keeps the
+    fastest candidate, reports every candidate's time, and its fields equal those
+    of a run with the chosen chunk length fixed."""
+    from libmpdataxx_b200 import _lib
+    L = _lib.lib()
+    assert L.mpdx_fused3d_planes_per_cta(-1) == 0
+    s = periodic_setup((130, 64, 130), seed=29)
+    run, _ = run_both(s, o.iga | o.fct, 2, np.float32, 12)
+    run.advance(3)
+    assert run.tuning3d()["chosen"] == 0
+    run.advance(9)
+    t = run.tuning3d()
+    lxs = [c[0] for c in t["candidates"]]
+    ms = [c[1] for c in t["candidates"]]
+    assert lxs == [32, 64, 96, 128]
+    assert all(m > 0 for m in ms)
+    assert t["chosen"] == lxs[int(np.argmin(ms))]
+    run.advance(2)
+    tuned = run.advectee()
+    try:
+        L.mpdx_fused3d_planes_per_cta(t["chosen"])
+        ref, _ = run_both(s, o.iga | o.fct, 2, np.float32, 14)
+        ref.advance(14)
+    finally:
+        L.mpdx_fused3d_planes_per_cta(0)
+    assert np.array_equal(tuned, ref.advectee())
