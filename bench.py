@@ -35,7 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CELL = 20  # FP32: psi^n 4 + GC 3 x 4 + psi^{n+1} 4
-TUNE_STEPS_3D = 9  # the fused 3D chunk-length tuner: 1 untimed step + 4 candidates x 2 timed steps
+TUNE_STEPS_3D = 15  # the fused 3D chunk-length tuner: 1 untimed step + 7 candidates x 2 timed steps
 
 
 def peaks():
@@ -403,7 +403,8 @@ def rotation_extra(n=1024, steps=200, revolution=6283):
 
 
 def gcr_extra(grid=(256, 256, 128), record=200, train=400, compare=1000):
-    """C5: 3D Boussinesq, FP32 advection with FP64 GCR (cr) to max|err| <= 1e-7/dt.
+    """C5: 3D Boussinesq, FP32 advection with FP64 GCR (cr; a third run with gcrk,
+    k = 4, alongside) to max|err| <= 1e-7/dt.
     Two identical runs advance `record` steps; one records the (residual,
     correction) pairs of its solves (their start and iterations 16/32/64), which
     train the learned preconditioner.  Then both advance `compare` more steps, one
@@ -416,8 +417,9 @@ def gcr_extra(grid=(256, 256, 128), record=200, train=400, compare=1000):
     s = setups.boussinesq_bubble_3d(*grid)
     plain = setups.boussinesq_run(s, dtype=np.float32, prs_fp64=True)
     learn = setups.boussinesq_run(s, dtype=np.float32, prs_fp64=True)
+    gcrk4 = setups.boussinesq_run(dict(s, prs_k=4), dtype=np.float32, prs_fp64=True)
     learn.precond_record(4 * record)
-    for r in (plain, learn):
+    for r in (plain, learn, gcrk4):
         r.advance(record)
         r.sync()
     n_pairs = learn.precond_pairs()
@@ -425,21 +427,26 @@ def gcr_extra(grid=(256, 256, 128), record=200, train=400, compare=1000):
     loss = learn.precond_train(train, lr=1e-3)
     t_train = time.perf_counter() - t0
     learn.precond_enable(True)
-    it_p, ms_p, it_l, ms_l, fb, nls = [], [], [], [], 0, {}
+    it_p, ms_p, it_l, ms_l, it_k, ms_k, fb, nls = [], [], [], [], [], [], 0, {}
     for _ in range(compare):
         plain.advance(1)
         learn.advance(1)
-        sp, sl = plain.stats(), learn.stats()
+        gcrk4.advance(1)
+        sp, sl, sk = plain.stats(), learn.stats(), gcrk4.stats()
         it_p.append(sp["gcr_iters"]); ms_p.append(sp["gcr_ms"])
         it_l.append(sl["gcr_iters"]); ms_l.append(sl["gcr_ms"])
+        it_k.append(sk["gcr_iters"]); ms_k.append(sk["gcr_ms"])
         fb += int(sl["gcr_fallback"] == 2)
         nl = learn.precond_directions()
         nls[nl] = nls.get(nl, 0) + 1
     plain.close()
     learn.close()
+    gcrk4.close()
     return {"workload": f"3D Boussinesq {grid[0]}x{grid[1]}x{grid[2]}, x/y cyclic, z rigid, FP32 advection, FP64 GCR (cr), "
                         f"prs_tol 1e-7; {record} recorded plain solves, then {compare} solves each, plain and learned",
             "plain": {"iters_per_solve": statistics.mean(it_p), "ms_per_solve": statistics.mean(ms_p)},
+            "plain_gcrk4": {"iters_per_solve": statistics.mean(it_k), "ms_per_solve": statistics.mean(ms_k),
+                            "scheme": "gcrk, k = 4 (restarted every 4 directions), same flow, same solves"},
             "learned": {"iters_per_solve": statistics.mean(it_l), "ms_per_solve": statistics.mean(ms_l),
                         "solves_redone_with_plain_gcr": fb,
                         "learned_directions_per_solve": {str(k): v for k, v in sorted(nls.items())},
@@ -516,7 +523,7 @@ def main():
             dist.barrier()
 
     # untimed set-up steps: the handle's chunk-length tuner (one untimed step, then two
-    # timed steps for each of four planes-per-CTA candidates), then the warm-up
+    # timed steps for each of seven planes-per-CTA candidates), then the warm-up
     run.advance(TUNE_STEPS_3D)
     for _ in range(max(args.warmup, 3)):
         run.advance(1)
