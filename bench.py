@@ -35,7 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CELL = 20  # FP32: psi^n 4 + GC 3 x 4 + psi^{n+1} 4
-TUNE_STEPS_3D = 15  # the fused 3D chunk-length tuner: 1 untimed step + 7 candidates x 2 timed steps
+TUNE_STEPS_3D = 17  # the fused 3D chunk-length tuner: 1 untimed step + 8 candidates x 2 timed steps
 
 
 def peaks():
@@ -523,7 +523,7 @@ def main():
             dist.barrier()
 
     # untimed set-up steps: the handle's chunk-length tuner (one untimed step, then two
-    # timed steps for each of seven planes-per-CTA candidates), then the warm-up
+    # timed steps for each of eight planes-per-CTA candidates), then the warm-up
     run.advance(TUNE_STEPS_3D)
     for _ in range(max(args.warmup, 3)):
         run.advance(1)

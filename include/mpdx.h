@@ -187,10 +187,10 @@ int mpdx_fused3d_bulk_copies(int mode);
 int mpdx_fused3d_planes_per_cta(int lx);
 
 /* The tuner of a handle that takes the fused 3D path: its first fused step runs
- * untimed with 64 planes per CTA, then each candidate in lx[] (32 to 128 planes
- * in steps of 16) runs two timed steps (each waiting for its own end on the
- * host, so a caller that captures mpdx_advance into a CUDA graph does so after
- * these 15 steps, or fixes the value with mpdx_fused3d_planes_per_cta), then the
+ * untimed with 64 planes per CTA, then each candidate in lx[] (24, 32, 40, 48,
+ * 64, 80, 96 and 128 planes) runs two timed steps (each waiting for its own end
+ * on the host, so a caller that captures mpdx_advance into a CUDA graph does so
+ * after these 17 steps, or fixes the value with mpdx_fused3d_planes_per_cta), then the
  * fastest is kept for the handle's life.  chosen is 0 while tuning (or on a
  * handle that has not taken the fused 3D path); ms[] holds each candidate's time
  * per step once the choice is made. */

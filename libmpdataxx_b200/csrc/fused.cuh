@@ -80,8 +80,8 @@ struct fused_engine {
   // default, then every candidate runs kTune3 timed steps (each step synchronises
   // on its end), then the fastest is kept.  The planes per CTA change only which
   // CTA computes a point, not how, so every candidate gives the same fields.
-  static constexpr int kNumCand3 = 7, kTune3 = 2;
-  static constexpr int kCand3[kNumCand3] = {32, 48, 64, 80, 96, 112, 128};
+  static constexpr int kNumCand3 = 8, kTune3 = 2;
+  static constexpr int kCand3[kNumCand3] = {24, 32, 40, 48, 64, 80, 96, 128};
   int lx3 = 0;        // chosen planes per CTA (0 while tuning)
   int tune_pos = -1;  // -1 before the untimed step, then timed steps so far
   float tune_ms[kNumCand3] = {};

@@ -165,22 +165,22 @@ def test_fused3d_tuner_keeps_fastest():
     L = _lib.lib()
     assert L.mpdx_fused3d_planes_per_cta(-1) == 0
     s = periodic_setup((130, 64, 130), seed=29)
-    run, _ = run_both(s, o.iga | o.fct, 2, np.float32, 17)
+    run, _ = run_both(s, o.iga | o.fct, 2, np.float32, 19)
     run.advance(3)
     assert run.tuning3d()["chosen"] == 0
-    run.advance(12)
+    run.advance(14)
     t = run.tuning3d()
     lxs = [c[0] for c in t["candidates"]]
     ms = [c[1] for c in t["candidates"]]
-    assert lxs == [32, 48, 64, 80, 96, 112, 128]
+    assert lxs == [24, 32, 40, 48, 64, 80, 96, 128]
     assert all(m > 0 for m in ms)
     assert t["chosen"] == lxs[int(np.argmin(ms))]
     run.advance(2)
     tuned = run.advectee()
     try:
         L.mpdx_fused3d_planes_per_cta(t["chosen"])
-        ref, _ = run_both(s, o.iga | o.fct, 2, np.float32, 17)
-        ref.advance(17)
+        ref, _ = run_both(s, o.iga | o.fct, 2, np.float32, 19)
+        ref.advance(19)
     finally:
         L.mpdx_fused3d_planes_per_cta(0)
     assert np.array_equal(tuned, ref.advectee())
